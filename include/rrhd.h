@@ -1,0 +1,225 @@
+/* rrhd.h - C ABI of the B200 implementation of the RadRHD_solver coupled step.
+ *
+ * Drop-in boundary for the reference's hot path (Lartsev-Artem/RadRHD_solver):
+ * the relativistic HLLC hydro step with con2prim, the radiation scattering
+ * integral and its energy/stream/impulse moments, and the radiation 4-force
+ * source.  Every entry point below names the reference interface it stands
+ * behind (paths are inside the reference project).
+ *
+ * Conventions
+ *  - Plain pointers and sizes only.  States are 5 doubles per cell, the flux_t
+ *    layout of lib/grids/include/solvers_struct.h:51-70: primitive
+ *    W = {rho, vx, vy, vz, p}; conservative U = {D, Sx, Sy, Sz, E}.
+ *  - Every function returns rrhd_status (0 = success) and never aborts the
+ *    process; rrhd_last_error() gives a message for the calling thread.
+ *  - Pointers marked "device" must be device memory of the context's GPU;
+ *    "host" pointers may be pageable or pinned.  Functions taking a `where`
+ *    argument accept either (RRHD_HOST / RRHD_DEVICE).
+ *  - Work is ordered on the context's CUDA stream (or the stream argument);
+ *    functions that return data to host pointers synchronise that stream.
+ *  - One context per host thread at a time.
+ */
+#ifndef RRHD_H
+#define RRHD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t rrhd_status;
+#define RRHD_OK 0
+#define RRHD_ERR_INVALID 1 /* bad argument */
+#define RRHD_ERR_CUDA 2    /* a CUDA call failed */
+#define RRHD_ERR_OOM 3     /* device allocation failed */
+#define RRHD_ERR_C2P 4     /* con2prim failed in some cells even after the fallback */
+#define RRHD_ERR_STATE 5   /* call made in the wrong order / missing data */
+#define RRHD_ERR_LIMIT 6   /* size beyond a fixed limit of the entry point */
+
+#define RRHD_HOST 0
+#define RRHD_DEVICE 1
+
+#define RRHD_EOS_IDEAL 1 /* h = 1 + Gamma/(Gamma-1) p/rho   (include/hd_config.h:17) */
+#define RRHD_EOS_TAUB 2  /* Taub-Matthews h                  (include/hd_config.h:18) */
+
+/* Boundary kinds for negative face neighbour codes (lib/global_types.h:25-31). */
+#define RRHD_BC_TRANSMISSIVE 0 /* copy of the inner cell (e_bound_free)            */
+#define RRHD_BC_FIXED 1        /* fixed primitive state, e.g. an inflow nozzle      */
+#define RRHD_BC_REFLECT 2      /* wall: normal velocity reversed (e_bound_lock)     */
+
+/* Per-cell status byte written by the hydro step and the batch con2prim:
+ * bits 0-2: code of rhllc::GetPhysValueStab (0 ok, 1 no solution, 2 p<0,
+ *           3 inaccurate, 4 NaN, 5 Lorentz factor < 1 where the reference aborts);
+ * bit 4: the PhysPressureFix fallback ran; bit 5: the fallback failed too. */
+#define RRHD_STATUS_FALLBACK 0x10
+#define RRHD_STATUS_FAILED 0x20
+
+typedef struct rrhd_ctx rrhd_ctx;
+
+/* Mesh in the reference's face/cell form: geo_face_t / geo_cell_t,
+ * lib/grids/include/solvers_struct.h:87-162, as assembled by ConvertBinToGeo
+ * (lib/geometry/src/convert_bin_to_geo.cpp:3-48).  Host pointers. */
+typedef struct {
+  int64_t n_cells;
+  int64_t n_faces;
+  const int32_t *face_id_l;  /* [F] cell on the normal's tail side            */
+  const int32_t *face_id_r;  /* [F] neighbour cell, or negative boundary code  */
+  const double *face_n;      /* [F][3] unit normal, outward from id_l         */
+  const double *face_area;   /* [F]                                            */
+  const int32_t *cell_faces; /* [N][4] face ids (id_faces)                     */
+  const uint8_t *cell_sign;  /* [N] bit j set: face j's normal points outward  */
+  const double *cell_volume; /* [N]                                            */
+  const double *cell_center; /* [N][3]                                         */
+} rrhd_mesh_desc;
+
+typedef struct {
+  int32_t eos;             /* RRHD_EOS_IDEAL (default when 0) or RRHD_EOS_TAUB        */
+  double gamma;            /* adiabatic index, ideal gas (default 5/3 when 0)        */
+  int32_t device;          /* CUDA device ordinal                                    */
+  int32_t cells_per_block; /* cells per CTA in the fused step; 0 = default (256)     */
+  int32_t renumber;        /* 0 = default Morton renumbering, -1 = keep input order  */
+} rrhd_opts;
+
+typedef struct {
+  double max_speed;     /* max signal speed of the step (rhllc::max_signal_speed) */
+  int64_t n_fallback;   /* cells where PhysPressureFix ran                        */
+  int64_t n_failed;     /* cells where the fallback failed too                    */
+} rrhd_step_stats;
+
+/* ------------------------------------------------------------------ context */
+
+/* Device-resident copy of the mesh and state.  Stands behind
+ * cuda::interface::separate_device::InitDevice
+ * (cuda/include/short_characteristics/separate_gpu/cuda_multi_interface.h:44)
+ * and grid_t::InitMemory (lib/grids/src/solvers_struct.cpp:146-180). */
+rrhd_status rrhd_create(const rrhd_mesh_desc *mesh, const rrhd_opts *opts, rrhd_ctx **out);
+
+/* Frees everything.  Stands behind separate_device::ClearDevice / ClearHost
+ * (cuda_multi_interface.h:50, :57). */
+rrhd_status rrhd_destroy(rrhd_ctx *ctx);
+
+/* The context's CUDA stream (a cudaStream_t). */
+void *rrhd_stream(rrhd_ctx *ctx);
+rrhd_status rrhd_sync(rrhd_ctx *ctx);
+
+/* Boundary state for a negative face code (-1..-8).  W is the primitive state
+ * for RRHD_BC_FIXED (its conservative state is made by rhllc::GetConvValue,
+ * solvers/rhllc/src/rhllc_flux.cpp:7-16); ignored otherwise.  Stands behind the
+ * compile-time per-geometry states of rhllc::BoundConditions
+ * (solvers/rhllc/src/rhllc_utils.cpp:45-133). */
+rrhd_status rrhd_set_boundary(rrhd_ctx *ctx, int32_t code, int32_t kind, const double *W);
+
+/* Cell state in the caller's numbering, [N] records of `stride` doubles whose
+ * first 5 are the state (stride 5 for packed arrays).  Either pointer may be
+ * NULL to skip it.  Mirrors grid.cells[i].phys_val / conv_val. */
+rrhd_status rrhd_set_state(rrhd_ctx *ctx, const double *W, const double *U, int64_t stride,
+                           int32_t where);
+rrhd_status rrhd_get_state(rrhd_ctx *ctx, double *W, double *U, int64_t stride, int32_t where);
+
+/* Sets W (rescaling |v| >= 1 as the reference does) and derives U on the
+ * device: rhllc::HllcPhysToConv / GetConvValueStab
+ * (solvers/rhllc/src/rhllc_utils.cpp:25-33, rhllc_flux_stab.cpp:10-38). */
+rrhd_status rrhd_set_state_prim(rrhd_ctx *ctx, const double *W, int64_t stride, int32_t where);
+
+/* One hydro step: RHLLC face fluxes, conservative update and con2prim with the
+ * PhysPressureFix fallback, fused in one kernel.  Stands behind
+ * void rhllc::Hllc3dStab(const Type tau, grid_t &grid)
+ * (solvers/rhllc/include/rhllc_calc.h:32, solvers/rhllc/src/rhllc_3d_stab.cpp:10-63).
+ * tau > 0: that time step.  tau <= 0: tau = CFL*h_min/max_speed of the previous
+ * step, computed on the device (rhllc::GetTimeStep, rhllc_utils.cpp:15-23;
+ * set CFL/h_min with rrhd_set_time_step).  stats may be NULL (no host sync);
+ * otherwise the call synchronises and fills it.  Returns RRHD_ERR_C2P when some
+ * cell failed even after the fallback (the reference aborts there). */
+rrhd_status rrhd_hydro_step(rrhd_ctx *ctx, double tau, rrhd_step_stats *stats);
+rrhd_status rrhd_set_time_step(rrhd_ctx *ctx, double cfl, double h_min, double initial_max_speed);
+/* Last time step used and the max signal speed it produced (synchronises). */
+rrhd_status rrhd_get_step_info(rrhd_ctx *ctx, double *tau_used, double *max_speed);
+
+/* Drop-in with host buffers: uploads W and U, runs one step, downloads W and U
+ * (the whole body of rhllc::Hllc3dStab on a host grid_t).  stride as above. */
+rrhd_status rrhd_hydro_step_host(rrhd_ctx *ctx, double tau, double *W, double *U, int64_t stride,
+                                 rrhd_step_stats *stats);
+
+/* Keep the face fluxes of the following steps in a [F][5] device array
+ * (off by default: it costs F*40 bytes of writes per step). */
+rrhd_status rrhd_keep_face_flux(rrhd_ctx *ctx, int32_t on);
+/* Face fluxes of the last step, [F][5] in the caller's face numbering (the
+ * grid.faces[].f the reference leaves behind).  Host pointer. */
+rrhd_status rrhd_get_face_flux(rrhd_ctx *ctx, double *F);
+/* Per-cell status bytes of the last step (bits above), caller's numbering. */
+rrhd_status rrhd_get_cell_status(rrhd_ctx *ctx, uint8_t *status);
+
+/* ------------------------------------------------------------ batch kernels */
+
+/* con2prim for n states, device pointers, on `stream` (a cudaStream_t, may be
+ * NULL).  rhllc::GetPhysValueStab (rhllc_flux_stab.cpp:123-220), and when
+ * fallback != 0 rhllc::PhysPressureFix (:40-121) where it fails, which also
+ * rewrites U.E as the reference does.  status [n] may be NULL. */
+rrhd_status rrhd_con2prim_batch(int32_t eos, double gamma, double *U, double *W, uint8_t *status,
+                                int64_t n, int32_t fallback, void *stream);
+/* prim->cons for n states, device pointers: rhllc::GetConvValueStab. */
+rrhd_status rrhd_prim2con_batch(int32_t eos, double gamma, double *W, double *U, int64_t n,
+                                void *stream);
+
+/* ------------------------------------------------------------ radiation */
+
+typedef struct rrhd_dirs rrhd_dirs;
+
+/* Direction set on the device: unit vectors [M][3], quadrature weights [M] and
+ * their normaliser full_area (grid_directions_t, lib/geometry/include/geo_types.h:110-127,
+ * read by files_sys::txt::ReadSphereDirectionCartesian, lib/files_sys/src/reader_txt.cpp:6-37). */
+rrhd_status rrhd_dirs_create(int32_t M, const double *dirs, const double *areas, double full_area,
+                             int32_t device, rrhd_dirs **out);
+rrhd_status rrhd_dirs_destroy(rrhd_dirs *d);
+
+/* Scattering integral S[r][k] = sum_d Gamma(w_d.w_k) I[r][d] a_d / full_area with
+ * the Thomson Gamma = 3(1+mu^2)/4, FP64, same operation order as
+ * cuda::kernel::GetS_MPI_multi_device (cuda/src/short_characteristics/cuda_scattering.cu:82-105).
+ * I, S device [rows][M], rows = cells x groups.  Stands behind
+ * separate_device::CalculateIntScatteringAsync (cuda_multi_interface.h:81). */
+rrhd_status rrhd_scatter_fp64(const rrhd_dirs *d, const double *I, double *S, int64_t rows,
+                              void *stream);
+
+/* The same contraction with one FMA per term on the precomputed matrix
+ * K[d][k] = Gamma(d,k) a_d / full_area (differs from the reference's three
+ * roundings per term by a few ulp). */
+rrhd_status rrhd_scatter_fp64_fma(const rrhd_dirs *d, const double *I, double *S, int64_t rows,
+                                  void *stream);
+int32_t rrhd_dirs_count(const rrhd_dirs *d);
+/* Device pointer to K [M][M] (row d), for callers that build their own kernels. */
+const double *rrhd_dirs_device_kernel(const rrhd_dirs *d);
+
+/* Energy E[r], stream F[r][3], impulse T[r][3][3] (row-major) moments, FP64,
+ * same order as cuda_sep::kernel::MakeIllumParam
+ * (cuda/src/short_characteristics/separate_gpu/cuda_illum_sep_param.cu:9-83).
+ * Stands behind separate_device::CalculateAllParamAsync (cuda_multi_interface.h:69).
+ * Device pointers. */
+rrhd_status rrhd_moments_fp64(const rrhd_dirs *d, const double *I, double *E, double *F,
+                              double *T, int64_t rows, void *stream);
+
+/* Emission constants of rad_rhd::GetRadSource: T = temp_coef*p/rho,
+ * B = T^4*sigma_sb/pi, q = -alpha*rho*B/rad_unit (lib/physics/src/plunk.cpp:87-90,
+ * lib/physics/include/gas_state.h:22-27).  rrhd_emission_reference() gives the
+ * reference's compiled-in CGS values. */
+typedef struct {
+  double temp_coef, sigma_sb, pi, rad_unit;
+} rrhd_emission;
+rrhd_emission rrhd_emission_reference(void);
+
+/* Radiation 4-force G [n][4] per cell, rad_rhd::GetRadSource
+ * (solvers/RadRHD/src/radRHD_utils.cpp:44-101), device pointers: W [n][5],
+ * alpha/sigma [n], E [n], F [n][3], T [n][9]. */
+rrhd_status rrhd_rad_source(const rrhd_emission *em, const double *W, const double *alpha,
+                            const double *sigma, const double *E, const double *F, const double *T,
+                            double *G, int64_t n, void *stream);
+
+/* ------------------------------------------------------------ misc */
+const char *rrhd_last_error(void);
+const char *rrhd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RRHD_H */

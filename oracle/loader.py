@@ -1,0 +1,337 @@
+"""ctypes wrappers of the oracle libraries (test infrastructure)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "_build", "librrhd_oracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+P, I32, I64, D = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+
+_port = None
+_refs: dict[str, C.CDLL] = {}
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def build_port() -> str:
+    if not os.path.exists(PORT_SO) or os.path.getmtime(PORT_SO) < os.path.getmtime(os.path.join(HERE, "rrhd_oracle.c")):
+        subprocess.run(["make", "-C", HERE, "port"], check=True, capture_output=True)
+    return PORT_SO
+
+
+class OrcEos(C.Structure):
+    _fields_ = [("eos", I32), ("gamma1", D)]
+
+
+class OrcMesh(C.Structure):
+    _fields_ = [("n_cells", I64), ("n_faces", I64), ("face_id_l", P), ("face_id_r", P), ("face_n", P),
+                ("face_area", P), ("cell_faces", P), ("cell_sign", P), ("cell_volume", P), ("cell_center", P)]
+
+
+class OrcBc(C.Structure):
+    _fields_ = [("kind", I32 * 8), ("W", (D * 5) * 8), ("U", (D * 5) * 8)]
+
+
+class OrcEmission(C.Structure):
+    _fields_ = [("temp_coef", D), ("sigma_sb", D), ("pi", D), ("rad_unit", D)]
+
+
+def port() -> C.CDLL:
+    global _port
+    if _port is None:
+        lib = C.CDLL(build_port())
+        sig = {
+            "orc_p2c": (None, [P, P, P]), "orc_p2c_plain": (None, [P, P, P]), "orc_c2p": (I32, [P, P, P]),
+            "orc_pressure_fix": (I32, [P, P, P]), "orc_rotation": (None, [P, P]),
+            "orc_flux": (D, [P, P, P, P, P, P, D, P]),
+            "orc_hydro_step": (D, [P, P, P, D, P, P, P, P, C.c_int]),
+            "orc_time_step": (D, [D, D, D]),
+            "orc_scatter": (None, [I64, I32, P, P, P, D, P, C.c_int]),
+            "orc_moments": (None, [I64, I32, P, P, P, D, P, P, P, C.c_int]),
+            "orc_rad_source": (None, [I64, P, P, P, P, P, P, P, P]),
+        }
+        for n, (r, a) in sig.items():
+            f = getattr(lib, n)
+            f.restype = r
+            f.argtypes = a
+        _port = lib
+    return _port
+
+
+def have_ref(variant: str) -> bool:
+    return os.path.exists(os.path.join(REF_DIR, f"librrhd_ref_{variant}.so"))
+
+
+def ref(variant: str) -> C.CDLL | None:
+    if variant in _refs:
+        return _refs[variant]
+    path = os.path.join(REF_DIR, f"librrhd_ref_{variant}.so")
+    if not os.path.exists(path):
+        return None
+    lib = C.CDLL(path)
+    sig = {
+        "ref_kgamma1": (D, []), "ref_c2p": (None, [P, P, P, I64]), "ref_pressure_fix": (None, [P, P, P, I64]),
+        "ref_p2c": (None, [P, P, I64]), "ref_p2c_plain": (None, [P, P, I64]),
+        "ref_flux": (None, [P, P, P, P, P, P, P, P, I64]),
+        "ref_hydro_create": (P, [I64, I64, P, P, P, P, P, P, P, P]), "ref_hydro_destroy": (None, [P]),
+        "ref_hydro_set_bc": (None, [P, I32, I32, P, P]), "ref_hydro_set_state": (None, [P, P, P]),
+        "ref_hydro_get_state": (None, [P, P, P]), "ref_hydro_get_face_flux": (None, [P, P]),
+        "ref_hydro_step": (D, [P, D, C.c_int]), "ref_hydro_step_bc": (D, [P, D, C.c_int, P]),
+        "ref_time_step": (D, [D, D, D]),
+        "ref_scatter": (None, [I64, I32, P, P, P, D, P, C.c_int]),
+        "ref_moments": (None, [I64, I32, P, P, P, D, P, P, P, C.c_int]),
+        "ref_rad_source": (None, [I64, P, P, P, P, P, P, P]), "ref_rad_constants": (None, [P]),
+        "ref_eos": (C.c_int, []),
+    }
+    for n, (r, a) in sig.items():
+        f = getattr(lib, n, None)
+        if f is not None:
+            f.restype = r
+            f.argtypes = a
+    _refs[variant] = lib
+    return lib
+
+
+def ref_variant_for(eos: int, gamma: float, fast: bool = False) -> str:
+    if eos == 2:
+        return "hydro_taub"
+    if abs(gamma - 5.0 / 3.0) < 1e-15:
+        v = "hydro_ideal_5_3"
+    elif abs(gamma - 4.0 / 3.0) < 1e-15:
+        v = "hydro_ideal_4_3"
+    else:
+        raise ValueError("the reference is compiled for Gamma = 5/3 and 4/3 only")
+    return v + ("_fast" if fast else "")
+
+
+def _eos(eos, gamma):
+    return OrcEos(eos, gamma)
+
+
+def _mesh(m) -> OrcMesh:
+    return OrcMesh(m.n_cells, m.n_faces, _p(m.face_id_l), _p(m.face_id_r), _p(m.face_n), _p(m.face_area),
+                   _p(m.cell_faces), _p(m.cell_sign), _p(m.cell_volume), _p(m.cell_center))
+
+
+def _bc(table) -> OrcBc:
+    """table: {code: (kind, W5, U5)}"""
+    b = OrcBc()
+    for k in range(8):
+        b.kind[k] = 0
+    for code, (kind, W, U) in (table or {}).items():
+        k = -code - 1
+        b.kind[k] = kind
+        for i in range(5):
+            b.W[k][i] = W[i] if W is not None else 0.0
+            b.U[k][i] = U[i] if U is not None else 0.0
+    return b
+
+
+# ------------------------------------------------------------------ port
+def port_c2p(U, eos=1, gamma=5.0 / 3.0, W=None):
+    U = np.ascontiguousarray(U, np.float64)
+    W = np.zeros_like(U) if W is None else np.array(W, np.float64)
+    codes = np.zeros(len(U), np.int32)
+    e = _eos(eos, gamma)
+    lib = port()
+    for i in range(len(U)):
+        codes[i] = lib.orc_c2p(C.byref(e), U[i].ctypes.data, W[i].ctypes.data)
+    return W, codes
+
+
+def port_pressure_fix(U, W, eos=1, gamma=5.0 / 3.0):
+    U = np.array(U, np.float64)
+    W = np.array(W, np.float64)
+    codes = np.zeros(len(U), np.int32)
+    e = _eos(eos, gamma)
+    lib = port()
+    for i in range(len(U)):
+        codes[i] = lib.orc_pressure_fix(C.byref(e), U[i].ctypes.data, W[i].ctypes.data)
+    return U, W, codes
+
+
+def port_p2c(W, eos=1, gamma=5.0 / 3.0):
+    W = np.array(W, np.float64)
+    U = np.zeros_like(W)
+    e = _eos(eos, gamma)
+    lib = port()
+    for i in range(len(W)):
+        lib.orc_p2c(C.byref(e), W[i].ctypes.data, U[i].ctypes.data)
+    return W, U
+
+
+def port_flux(UL, UR, WL, WR, n, S, eos=1, gamma=5.0 / 3.0):
+    k = len(UL)
+    F = np.zeros((k, 5))
+    sp = np.zeros(k)
+    e = _eos(eos, gamma)
+    lib = port()
+    arrs = [np.ascontiguousarray(a, np.float64) for a in (UL, UR, WL, WR, n)]
+    for i in range(k):
+        sp[i] = lib.orc_flux(C.byref(e), *(a[i].ctypes.data for a in arrs), float(S[i]), F[i].ctypes.data)
+    return F, sp
+
+
+def port_hydro_step(mesh, U, W, tau, eos=1, gamma=5.0 / 3.0, bc=None, nthreads=1):
+    """One step of the restated Hllc3dStab; returns (U, W, face_flux, status, max_speed)."""
+    U = np.array(U, np.float64)
+    W = np.array(W, np.float64)
+    Ff = np.zeros((mesh.n_faces, 5))
+    st = np.zeros(mesh.n_cells, np.int32)
+    m = _mesh(mesh)
+    b = _bc(bc)
+    e = _eos(eos, gamma)
+    v = port().orc_hydro_step(C.byref(e), C.byref(m), C.byref(b), tau, _p(U), _p(W), _p(Ff), _p(st), nthreads)
+    return U, W, Ff, st, v
+
+
+def port_scatter(I, dirs, areas, full_area, nthreads=1):
+    I = np.ascontiguousarray(I, np.float64)
+    S = np.zeros_like(I)
+    port().orc_scatter(I.shape[0], I.shape[1], _p(I), _p(np.ascontiguousarray(dirs)), _p(np.ascontiguousarray(areas)),
+                       full_area, _p(S), nthreads)
+    return S
+
+
+def port_moments(I, dirs, areas, full_area, nthreads=1):
+    I = np.ascontiguousarray(I, np.float64)
+    N = I.shape[0]
+    E, F, T = np.zeros(N), np.zeros((N, 3)), np.zeros((N, 3, 3))
+    port().orc_moments(N, I.shape[1], _p(I), _p(np.ascontiguousarray(dirs)), _p(np.ascontiguousarray(areas)),
+                       full_area, _p(E), _p(F), _p(T), nthreads)
+    return E, F, T
+
+
+def port_rad_source(W, alpha, sigma, E, F, T, emission):
+    N = len(W)
+    G = np.zeros((N, 4))
+    em = OrcEmission(*emission)
+    arrs = [np.ascontiguousarray(a, np.float64) for a in (W, alpha, sigma, E, F, T)]
+    port().orc_rad_source(N, C.byref(em), *(_p(a) for a in arrs), _p(G))
+    return G
+
+
+# ------------------------------------------------------------------ reference
+def ref_c2p(U, variant, W=None):
+    lib = ref(variant)
+    U = np.ascontiguousarray(U, np.float64)
+    W = np.zeros_like(U) if W is None else np.array(W, np.float64)
+    codes = np.zeros(len(U), np.int32)
+    lib.ref_c2p(_p(U), _p(W), _p(codes), len(U))
+    return W, codes
+
+
+def ref_pressure_fix(U, W, variant):
+    lib = ref(variant)
+    U = np.array(U, np.float64)
+    W = np.array(W, np.float64)
+    codes = np.zeros(len(U), np.int32)
+    lib.ref_pressure_fix(_p(U), _p(W), _p(codes), len(U))
+    return U, W, codes
+
+
+def ref_p2c(W, variant):
+    lib = ref(variant)
+    W = np.array(W, np.float64)
+    U = np.zeros_like(W)
+    lib.ref_p2c(_p(W), _p(U), len(W))
+    return W, U
+
+
+def ref_flux(UL, UR, WL, WR, n, S, variant):
+    lib = ref(variant)
+    k = len(UL)
+    F = np.zeros((k, 5))
+    sp = np.zeros(k)
+    arrs = [np.ascontiguousarray(a, np.float64) for a in (UL, UR, WL, WR, n, S)]
+    lib.ref_flux(*(_p(a) for a in arrs), _p(F), _p(sp), k)
+    return F, sp
+
+
+class HydroRef:
+    """The reference grid_t driven through rhllc::Hllc3dStab (or the same loops
+    with a fixed-state inflow boundary)."""
+
+    def __init__(self, mesh, variant):
+        self.lib = ref(variant)
+        if self.lib is None:
+            raise FileNotFoundError(f"reference variant {variant} not built")
+        self.mesh = mesh
+        self.h = self.lib.ref_hydro_create(mesh.n_cells, mesh.n_faces, _p(mesh.face_id_l), _p(mesh.face_id_r),
+                                           _p(mesh.face_n), _p(mesh.face_area), _p(mesh.cell_faces),
+                                           _p(mesh.cell_sign), _p(mesh.cell_volume), _p(mesh.cell_center))
+        self.custom_bc = False
+
+    def set_bc(self, code, kind, W=None, U=None):
+        w = None if W is None else np.ascontiguousarray(W, np.float64)
+        u = None if U is None else np.ascontiguousarray(U, np.float64)
+        self.lib.ref_hydro_set_bc(self.h, code, kind, _p(w), _p(u))
+        self.custom_bc = True
+
+    def set_state(self, W, U):
+        W = np.ascontiguousarray(W, np.float64)
+        U = np.ascontiguousarray(U, np.float64)
+        self.lib.ref_hydro_set_state(self.h, _p(W), _p(U))
+
+    def get_state(self):
+        W = np.zeros((self.mesh.n_cells, 5))
+        U = np.zeros((self.mesh.n_cells, 5))
+        self.lib.ref_hydro_get_state(self.h, _p(W), _p(U))
+        return W, U
+
+    def face_flux(self):
+        F = np.zeros((self.mesh.n_faces, 5))
+        self.lib.ref_hydro_get_face_flux(self.h, _p(F))
+        return F
+
+    def step(self, tau, nthreads=0, codes=None):
+        if self.custom_bc or codes is not None:
+            return self.lib.ref_hydro_step_bc(self.h, tau, nthreads, _p(codes))
+        return self.lib.ref_hydro_step(self.h, tau, nthreads)
+
+    def close(self):
+        if self.h:
+            self.lib.ref_hydro_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ref_scatter(I, dirs, areas, full_area, nthreads=0):
+    lib = ref("illum")
+    I = np.ascontiguousarray(I, np.float64)
+    S = np.zeros_like(I)
+    lib.ref_scatter(I.shape[0], I.shape[1], _p(I), _p(np.ascontiguousarray(dirs)), _p(np.ascontiguousarray(areas)),
+                    full_area, _p(S), nthreads)
+    return S
+
+
+def ref_moments(I, dirs, areas, full_area, nthreads=0):
+    lib = ref("illum")
+    I = np.ascontiguousarray(I, np.float64)
+    N = I.shape[0]
+    E, F, T = np.zeros(N), np.zeros((N, 3)), np.zeros((N, 3, 3))
+    lib.ref_moments(N, I.shape[1], _p(I), _p(np.ascontiguousarray(dirs)), _p(np.ascontiguousarray(areas)), full_area,
+                    _p(E), _p(F), _p(T), nthreads)
+    return E, F, T
+
+
+def ref_rad_source(W, alpha, sigma, E, F, T, variant="rad_ideal_4_3"):
+    lib = ref(variant)
+    N = len(W)
+    G = np.zeros((N, 4))
+    arrs = [np.ascontiguousarray(a, np.float64) for a in (W, alpha, sigma, E, F, T)]
+    lib.ref_rad_source(N, *(_p(a) for a in arrs), _p(G))
+    return G

@@ -1,0 +1,522 @@
+/* Test infrastructure, not product code: the checker, never the thing measured.
+ *
+ * Plain-C restatement of the RadRHD_solver hot path.  Each function restates one
+ * reference function in the same operation order (citations below are paths
+ * inside the reference project).  Eigen's evaluation order, which the reference
+ * inherits for its 3-vector arithmetic, is spelled out explicitly: with gcc -O2
+ * on x86-64 a Vector3 dot product is (x0 + x1) + x2, a Matrix3 * Vector3 product
+ * gives rows 0 and 1 as (x0 + x1) + x2 and row 2 as x0 + (x1 + x2), and
+ * Matrix3.transpose() * Vector3 gives every row as (x0 + x1) + x2.
+ */
+#include "rrhd_oracle.h"
+
+#include <math.h>
+#include <stddef.h>
+#include <string.h>
+
+#define MAX_ITER 40 /* solvers/rhllc/src/rhllc_flux_stab.cpp:8 */
+static const double kMinPressure = 1e-12; /* lib/global_consts.h:16 */
+
+/* std::min / std::max semantics (NaN handling included). */
+static inline double smin(double a, double b) { return (b < a) ? b : a; }
+static inline double smax(double a, double b) { return (a < b) ? b : a; }
+
+static inline double dot3(const double *a, const double *b) {
+  return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2];
+}
+/* Matrix3 * Vector3 (row-major T) */
+static inline void matvec(const double *T, const double *v, double *r) {
+  r[0] = (T[0] * v[0] + T[1] * v[1]) + T[2] * v[2];
+  r[1] = (T[3] * v[0] + T[4] * v[1]) + T[5] * v[2];
+  r[2] = T[6] * v[0] + (T[7] * v[1] + T[8] * v[2]);
+}
+/* Matrix3.transpose() * Vector3 (row-major T) */
+static inline void matTvec(const double *T, const double *v, double *r) {
+  r[0] = (T[0] * v[0] + T[3] * v[1]) + T[6] * v[2];
+  r[1] = (T[1] * v[0] + T[4] * v[1]) + T[7] * v[2];
+  r[2] = (T[2] * v[0] + T[5] * v[1]) + T[8] * v[2];
+}
+
+static inline double gamma_g(const orc_eos *e) { return e->gamma1 / (e->gamma1 - 1.0); }
+
+/* rhllc::GetConvValueStab, solvers/rhllc/src/rhllc_flux_stab.cpp:10-38 */
+void orc_p2c(const orc_eos *eos, double *W, double *U) {
+  double h;
+  if (eos->eos == ORC_EOS_IDEAL) {
+    h = 1 + gamma_g(eos) * W[4] / W[0];
+  } else {
+    double theta = W[4] / W[0];
+    h = 2.5 * theta + sqrt(2.25 * theta * theta + 1.0);
+  }
+  double g = dot3(W + 1, W + 1);
+  if (g >= 1.0) {
+    const double beta_fix = 0.9999;
+    g = beta_fix / sqrt(g);
+    W[1] *= g;
+    W[2] *= g;
+    W[3] *= g;
+    g = beta_fix * beta_fix;
+  }
+  g = 1.0 / (1.0 - g);
+  double scrh = W[0] * h * g;
+  g = sqrt(g);
+  U[0] = W[0] * g;
+  U[1] = scrh * W[1];
+  U[2] = scrh * W[2];
+  U[3] = scrh * W[3];
+  U[4] = scrh - W[4];
+}
+
+/* rhllc::GetConvValue, solvers/rhllc/src/rhllc_flux.cpp:7-16 (fixed inflow states) */
+void orc_p2c_plain(const orc_eos *eos, const double *W, double *U) {
+  const double d = W[0];
+  const double Gamma = 1. / sqrt(1 - dot3(W + 1, W + 1));
+  const double h = 1 + gamma_g(eos) * W[4] / d;
+  const double dhGG = d * h * Gamma * Gamma;
+  U[0] = Gamma * W[0];
+  U[1] = dhGG * W[1];
+  U[2] = dhGG * W[2];
+  U[3] = dhGG * W[3];
+  U[4] = dhGG - W[4];
+}
+
+static inline double enthalpy_fix(const orc_eos *eos, double D, double plor, double alpha) {
+  if (eos->eos == ORC_EOS_IDEAL) return D + plor * alpha;
+  return 2.5 * plor + sqrt(2.25 * plor * plor + D * D);
+}
+
+/* rhllc::PhysPressureFix, rhllc_flux_stab.cpp:40-121 */
+int orc_pressure_fix(const orc_eos *eos, double *U, double *W) {
+  double p = kMinPressure;
+  double D = U[0];
+  double m2 = dot3(U + 1, U + 1);
+  double m = sqrt(m2);
+  double umax = m / D;
+  double u0 = umax;
+  double lor = sqrt(1.0 + u0 * u0);
+  double plor = p * lor;
+  const double alpha = (eos->eos == ORC_EOS_IDEAL) ? eos->gamma1 / (eos->gamma1 - 1.0) : 2.5;
+  double Dh = enthalpy_fix(eos, D, plor, alpha);
+  double f0 = m / Dh - u0;
+  double u1 = (-D + sqrt(D * D + 4.0 * m * alpha * p)) / (2.0 * alpha * p);
+  int done = 0;
+  double f1, du;
+  for (int k = 1; k < MAX_ITER; k++) {
+    lor = sqrt(1.0 + u1 * u1);
+    plor = p * lor;
+    Dh = enthalpy_fix(eos, D, plor, alpha);
+    f1 = m / Dh - u1;
+    if (done == 1) break;
+    du = (u1 - u0) / (f1 - f0) * f1;
+    u0 = u1;
+    f0 = f1;
+    u1 -= du;
+    u1 = smin(u1, umax);
+    u1 = smax(u1, 0.0);
+    if (fabs(f1) < 1.e-9) done = 1;
+  }
+  if (done != 1) return 2;
+  lor = sqrt(1.0 + u1 * u1);
+  plor = p * lor;
+  Dh = enthalpy_fix(eos, D, plor, alpha);
+  W[0] = U[0] / lor;
+  W[4] = p;
+  U[4] = Dh * lor - p;
+  f0 = 1.0 / (Dh * lor);
+  W[1] = U[1] * f0;
+  W[2] = U[2] * f0;
+  W[3] = U[3] * f0;
+  return 0;
+}
+
+/* rhllc::GetPhysValueStab, rhllc_flux_stab.cpp:123-220.  Returns 5 where the
+ * reference would abort the process (DIE_IF(lor2 < 1.0), :149). */
+int orc_c2p(const orc_eos *eos, const double *U, double *W) {
+  const double tol = 1.e-11;
+  const double eps2 = 1.e-12;
+  const double kg = gamma_g(eos);
+  double D = U[0];
+  double E = U[4];
+  double m2 = dot3(U + 1, U + 1);
+  double Q = E - sqrt(m2 + D * D);
+  if (Q < 0.0) return 1;
+  double m = sqrt(m2);
+  double p = smax(m - E, 0.0);
+  double D_1 = 1.0 / D;
+  double pmin = sqrt(m2 / (1.0 - eps2)) - E;
+  double alpha, alpha2, lor2, lor, tau, theta;
+  double h, dh_dp, dh_dtau, yp = 0, dp, dyp, scrh;
+  p = smax(p, pmin);
+  int iter;
+  for (iter = 0; iter < MAX_ITER; iter++) {
+    alpha = E + p;
+    alpha2 = alpha * alpha;
+    lor2 = 1.0 - m2 / alpha2;
+    lor2 = 1.0 / lor2;
+    if (lor2 < 1.0) return 5;
+    lor = sqrt(lor2);
+    tau = lor * D_1;
+    theta = p * tau;
+    if (eos->eos == ORC_EOS_IDEAL) {
+      h = 1.0 + kg * theta;
+      dh_dp = kg * tau;
+      dh_dtau = kg * p;
+    } else {
+      h = 2.5 * theta + sqrt(2.25 * theta * theta + 1.0);
+      scrh = (5.0 * h - 8.0 * theta) / (2.0 * h - 5.0 * theta);
+      dh_dp = tau * scrh;
+      dh_dtau = p * scrh;
+    }
+    yp = D * h * lor - E - p;
+    dyp = D * lor * dh_dp - m2 * lor2 * lor / (alpha2 * alpha) * (lor * dh_dtau + D * h) - 1.0;
+    dp = yp / dyp;
+    p -= dp;
+    if (p < pmin) p = pmin;
+    if (fabs(dp) < tol * E) break;
+  }
+  if (p < 0.0) return 2;
+  if (isnan(p)) return 4;
+  if (iter >= MAX_ITER || fabs(yp / (E + p)) > 1.e-4 || p < (m - E)) return 3;
+  alpha = E + p;
+  alpha2 = alpha * alpha;
+  lor2 = alpha2 / (alpha2 - m2);
+  lor = sqrt(lor2);
+  tau = lor * D_1;
+  W[0] = 1.0 / tau;
+  W[4] = p;
+  const double den = U[4] + p;
+  W[1] = U[1] / den;
+  W[2] = U[2] / den;
+  W[3] = U[3] / den;
+  return 0;
+}
+
+/* GetRotationMatrix, lib/geometry/src/linear_alg.cpp:3-42 (row-major T) */
+void orc_rotation(const double *n, double *T) {
+  for (int i = 0; i < 9; i++) T[i] = 0.0;
+  const double eps = 1e-12;
+  if (fabs(n[2] * n[2] - 1) > eps) {
+    T[0] = n[0];
+    T[1] = n[1];
+    T[2] = n[2];
+    double sqr = sqrt(1 - n[2] * n[2]);
+    double sqr_inv = 1. / sqr;
+    T[3] = -n[1] * sqr_inv;
+    T[4] = n[0] * sqr_inv;
+    T[6] = -n[0] * n[2] * sqr_inv;
+    T[7] = -n[1] * n[2] * sqr_inv;
+    T[8] = sqr;
+  } else if (n[2] > 0) {
+    T[2] = 1;
+    T[4] = 1;
+    T[6] = -1;
+  } else {
+    T[2] = -1;
+    T[4] = -1;
+    T[6] = 1;
+  }
+}
+
+/* GetSignalSpeed, rhllc_flux_stab.cpp:231-238 */
+static void signal_speed(double cs2, double Vn, double V2_norm, double *cmin, double *cmax) {
+  const double Vn2 = Vn * Vn;
+  const double Vt2 = V2_norm - Vn2;
+  const double sroot_L = sqrt(cs2 * (1 - Vn2 - Vt2 * cs2) * (1 - V2_norm));
+  *cmax = (Vn * (1.0 - cs2) + sroot_L) / (1.0 - V2_norm * cs2);
+  *cmin = (Vn * (1.0 - cs2) - sroot_L) / (1.0 - V2_norm * cs2);
+}
+
+static void sound_speed(const orc_eos *eos, double d, double p, double *cs2) {
+  if (eos->eos == ORC_EOS_IDEAL) {
+    const double h = 1 + gamma_g(eos) * p / d;
+    *cs2 = ((eos->gamma1 * p) / (d * h));
+  } else {
+    double theta = p / d;
+    const double h = 2.5 * theta + sqrt(2.25 * theta * theta + 1.0);
+    *cs2 = theta / (3.0 * h) * (5.0 * h - 8.0 * theta) / (h - theta);
+  }
+}
+
+/* rhllc::GetFluxStab, rhllc_flux_stab.cpp:240-431.  F gets the flux times area. */
+double orc_flux(const orc_eos *eos, const double *UL0, const double *UR0, const double *WL0,
+                const double *WR0, const double *n, double area, double *Fout) {
+  double T[9];
+  orc_rotation(n, T);
+  double UL[5], UR[5], WL[5], WR[5];
+  UL[0] = UL0[0];
+  UL[4] = UL0[4];
+  matvec(T, UL0 + 1, UL + 1);
+  UR[0] = UR0[0];
+  UR[4] = UR0[4];
+  matvec(T, UR0 + 1, UR + 1);
+  WL[0] = WL0[0];
+  WL[4] = WL0[4];
+  matvec(T, WL0 + 1, WL + 1);
+  WR[0] = WR0[0];
+  WR[4] = WR0[4];
+  matvec(T, WR0 + 1, WR + 1);
+
+  const double *Vel_L = WL + 1, *Vel_R = WR + 1;
+  const double d_L = WL[0], d_R = WR[0];
+  const double p_L = WL[4], p_R = WR[4];
+  const double VV_L = dot3(Vel_L, Vel_L);
+  const double VV_R = dot3(Vel_R, Vel_R);
+  double cs_L2, cs_R2;
+  sound_speed(eos, d_L, p_L, &cs_L2);
+  sound_speed(eos, d_R, p_R, &cs_R2);
+
+  double cmax_L, cmax_R, cmin_L, cmin_R;
+  signal_speed(cs_L2, Vel_L[0], VV_L, &cmin_L, &cmax_L);
+  signal_speed(cs_R2, Vel_R[0], VV_R, &cmin_R, &cmax_R);
+  const double lambda_L = smin(cmin_L, cmin_R);
+  const double lambda_R = smax(cmax_L, cmax_R);
+
+  double F[5];
+  if (lambda_L >= 0.0) {
+    F[0] = UL[0] * Vel_L[0];
+    F[1] = UL[1] * Vel_L[0];
+    F[2] = UL[2] * Vel_L[0];
+    F[3] = UL[3] * Vel_L[0];
+    F[4] = UL[1];
+    F[1] += p_L;
+  } else if (lambda_R <= 0.0) {
+    F[0] = UR[0] * Vel_R[0];
+    F[1] = UR[1] * Vel_R[0];
+    F[2] = UR[2] * Vel_R[0];
+    F[3] = UR[3] * Vel_R[0];
+    F[4] = UR[1];
+    F[1] += p_R;
+  } else {
+    double F_L[5] = {UL[0] * Vel_L[0], UL[1] * Vel_L[0], UL[2] * Vel_L[0], UL[3] * Vel_L[0], UL[1]};
+    double F_R[5] = {UR[0] * Vel_R[0], UR[1] * Vel_R[0], UR[2] * Vel_R[0], UR[3] * Vel_R[0], UR[1]};
+    double AL = lambda_L * UL[4] - F_L[4];
+    double AR = lambda_R * UR[4] - F_R[4];
+    double BL = lambda_L * UL[1] - F_L[1] - p_L;
+    double BR = lambda_R * UR[1] - F_R[1] - p_R;
+    double a = AR * lambda_L - AL * lambda_R;
+    double b = AL + BL * lambda_R - AR - BR * lambda_L;
+    double c = BR - BL;
+    double scrh = -0.5 * (b + (b < 0.0 ? -1.0 : 1.0) * sqrt(b * b - 4.0 * a * c));
+    double us = c / scrh;
+    double ps = (AL * us - BL) / (1.0 - us * lambda_L);
+    if (us >= 0.0) {
+      double usl[5];
+      double dif = 1.0 / (lambda_L - us);
+      usl[0] = UL[0] * (lambda_L - Vel_L[0]) * dif;
+      usl[1] = (lambda_L * (UL[4] + ps) - UL[1]) * us * dif;
+      usl[2] = UL[2] * (lambda_L - Vel_L[0]) * dif;
+      usl[3] = UL[3] * (lambda_L - Vel_L[0]) * dif;
+      usl[4] = UL[4] + (usl[1] - UL[1]) / lambda_L;
+      for (int i = 0; i < 5; i++) usl[i] -= UL[i];
+      for (int i = 0; i < 5; i++) usl[i] *= lambda_L;
+      for (int i = 0; i < 5; i++) F[i] = F_L[i] + usl[i];
+      F[1] += p_L;
+    } else {
+      double usr[5];
+      double dif = 1.0 / (lambda_R - us);
+      usr[0] = UR[0] * (lambda_R - Vel_R[0]) * dif;
+      usr[1] = (lambda_R * (UR[4] + ps) - UR[1]) * us * dif;
+      usr[2] = UR[2] * (lambda_R - Vel_R[0]) * dif;
+      usr[3] = UR[3] * (lambda_R - Vel_R[0]) * dif;
+      usr[4] = UR[4] + (usr[1] - UR[1]) / lambda_R;
+      for (int i = 0; i < 5; i++) usr[i] -= UR[i];
+      for (int i = 0; i < 5; i++) usr[i] *= lambda_R;
+      for (int i = 0; i < 5; i++) F[i] = F_R[i] + usr[i];
+      F[1] += p_R;
+    }
+  }
+  Fout[0] = F[0];
+  Fout[4] = F[4];
+  matTvec(T, F + 1, Fout + 1);
+  for (int i = 0; i < 5; i++) Fout[i] *= area;
+  return smax(lambda_L, lambda_R);
+}
+
+/* rhllc::BoundConditions, solvers/rhllc/src/rhllc_utils.cpp:45-133, with the
+ * boundary states taken from a runtime table instead of compile-time geometry. */
+static void boundary_state(const orc_mesh *m, const orc_bc *bc, int64_t f, const double *U,
+                           const double *W, double *Ub, double *Wb) {
+  const int32_t id_l = m->face_id_l[f];
+  const int32_t id_r = m->face_id_r[f];
+  if (id_r >= 0) {
+    memcpy(Ub, U + 5 * (int64_t)id_r, 5 * sizeof(double));
+    memcpy(Wb, W + 5 * (int64_t)id_r, 5 * sizeof(double));
+    return;
+  }
+  const int k = -id_r - 1;
+  const int kind = (k < 8 && bc) ? bc->kind[k] : 0;
+  if (kind == 1) {
+    memcpy(Ub, bc->U[k], 5 * sizeof(double));
+    memcpy(Wb, bc->W[k], 5 * sizeof(double));
+    return;
+  }
+  memcpy(Ub, U + 5 * (int64_t)id_l, 5 * sizeof(double));
+  memcpy(Wb, W + 5 * (int64_t)id_l, 5 * sizeof(double));
+  if (kind == 2) {
+    /* reflecting wall: rotate into the face frame, negate the normal
+     * component, rotate back with the transposed matrix (rhllc_utils.cpp:96-114) */
+    double T[9], Tt[9], r[3];
+    orc_rotation(m->face_n + 3 * f, T);
+    matvec(T, Ub + 1, r);
+    memcpy(Ub + 1, r, sizeof r);
+    matvec(T, Wb + 1, r);
+    memcpy(Wb + 1, r, sizeof r);
+    Ub[1] = -Ub[1];
+    Wb[1] = -Wb[1];
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) Tt[3 * i + j] = T[3 * j + i];
+    matvec(Tt, Ub + 1, r);
+    memcpy(Ub + 1, r, sizeof r);
+    matvec(Tt, Wb + 1, r);
+    memcpy(Wb + 1, r, sizeof r);
+  }
+}
+
+/* rhllc::Hllc3dStab, solvers/rhllc/src/rhllc_3d_stab.cpp:10-63 */
+double orc_hydro_step(const orc_eos *eos, const orc_mesh *m, const orc_bc *bc, double tau,
+                      double *U, double *W, double *face_flux, int32_t *status, int nthreads) {
+  double max_speed_all = 0;
+  const int64_t F = m->n_faces, N = m->n_cells;
+  (void)nthreads;
+#pragma omp parallel num_threads(nthreads > 0 ? nthreads : 1)
+  {
+    double max_speed = 0;
+#pragma omp for schedule(static)
+    for (int64_t f = 0; f < F; f++) {
+      double Ub[5], Wb[5];
+      boundary_state(m, bc, f, U, W, Ub, Wb);
+      const int64_t l = m->face_id_l[f];
+      const double s = orc_flux(eos, U + 5 * l, Ub, W + 5 * l, Wb, m->face_n + 3 * f,
+                                m->face_area[f], face_flux + 5 * f);
+      max_speed = smax(max_speed, s);
+    }
+#pragma omp for schedule(static)
+    for (int64_t c = 0; c < N; c++) {
+      double sumF[5] = {0, 0, 0, 0, 0};
+      for (int j = 0; j < 4; j++) {
+        const double *fl = face_flux + 5 * (int64_t)m->cell_faces[4 * c + j];
+        if ((m->cell_sign[c] >> j) & 1)
+          for (int i = 0; i < 5; i++) sumF[i] += fl[i];
+        else
+          for (int i = 0; i < 5; i++) sumF[i] -= fl[i];
+      }
+      const double s = (tau / m->cell_volume[c]);
+      for (int i = 0; i < 5; i++) sumF[i] *= s;
+      for (int i = 0; i < 5; i++) U[5 * c + i] -= sumF[i];
+      int code = orc_c2p(eos, U + 5 * c, W + 5 * c);
+      if (code) {
+        const int fix = orc_pressure_fix(eos, U + 5 * c, W + 5 * c);
+        code = code | 0x10 | (fix ? 0x20 : 0);
+      }
+      if (status) status[c] = code;
+    }
+#pragma omp critical
+    { max_speed_all = smax(max_speed_all, max_speed); }
+  }
+  return max_speed_all;
+}
+
+/* rhllc::GetTimeStep, solvers/rhllc/src/rhllc_utils.cpp:15-23 */
+double orc_time_step(double cfl, double h_min, double max_speed) {
+  return cfl * h_min / max_speed;
+}
+
+/* Thomson phase function Gamma, cuda/src/short_characteristics/cuda_integrator.cu:10-13
+ * (same arithmetic as solvers/illum/include/scattering.h:32-35). */
+static inline double thomson(const double *a, const double *b) {
+  const double sum = dot3(a, b);
+  return (3. * (1. + sum * sum)) / 4.;
+}
+
+/* Scattering integral, cell-major: cuda::kernel::GetS_MPI_multi_device,
+ * cuda/src/short_characteristics/cuda_scattering.cu:82-105 (the CPU
+ * GetIntScatteringByDirection, solvers/illum/src/scattering.cpp:6-18, has the
+ * same sum in the same direction order). */
+void orc_scatter(int64_t N, int32_t M, const double *I, const double *dirs, const double *areas,
+                 double full_area, double *S, int nthreads) {
+#pragma omp parallel for schedule(static) num_threads(nthreads > 0 ? nthreads : 1)
+  for (int64_t c = 0; c < N; c++) {
+    const double *Ic = I + (size_t)c * M;
+    for (int32_t k = 0; k < M; k++) {
+      double scatter = 0;
+      for (int32_t d = 0; d < M; d++)
+        scatter += thomson(dirs + 3 * d, dirs + 3 * k) * Ic[d] * areas[d];
+      S[(size_t)c * M + k] = scatter / full_area;
+    }
+  }
+}
+
+/* Moments, cuda_sep::device::MakeEnergy / MakeStream / MakeImpuls,
+ * cuda/src/short_characteristics/separate_gpu/cuda_illum_sep_param.cu:9-69. */
+void orc_moments(int64_t N, int32_t M, const double *I, const double *dirs, const double *areas,
+                 double full_area, double *E, double *F, double *T, int nthreads) {
+#pragma omp parallel for schedule(static) num_threads(nthreads > 0 ? nthreads : 1)
+  for (int64_t c = 0; c < N; c++) {
+    const double *Ic = I + (size_t)c * M;
+    double e = 0, s[3] = {0, 0, 0}, t[9] = {0};
+    for (int32_t k = 0; k < M; k++) e += Ic[k] * areas[k];
+    for (int32_t k = 0; k < M; k++) {
+      const double Ia = Ic[k] * areas[k];
+      for (int i = 0; i < 3; i++) s[i] += dirs[3 * k + i] * Ia;
+    }
+    for (int32_t d = 0; d < M; d++) {
+      const double Ia = Ic[d] * areas[d];
+      for (int i = 0; i < 3; i++)
+        for (int k = 0; k < 3; k++) t[3 * i + k] += dirs[3 * d + i] * dirs[3 * d + k] * Ia;
+    }
+    E[c] = e / full_area;
+    for (int i = 0; i < 3; i++) F[3 * c + i] = s[i] / full_area;
+    for (int i = 0; i < 9; i++) T[9 * c + i] = t[i] / full_area;
+  }
+}
+
+/* rad_rhd::GetRadSource, solvers/RadRHD/src/radRHD_utils.cpp:44-101
+ * (ISOTROPIC_INTENSITY 0: the impulse moment is used directly), with the
+ * emission B_Plank(GetTemperature(rho, p)) / kRadiation of
+ * lib/physics/src/plunk.cpp:87-90 and lib/physics/include/gas_state.h:22-27. */
+void orc_rad_source(int64_t N, const orc_emission *em, const double *W, const double *alpha,
+                    const double *sigma, const double *E, const double *F, const double *T,
+                    double *G) {
+  for (int64_t c = 0; c < N; c++) {
+    const double abs_op = alpha[c];
+    const double scat_op = sigma[c];
+    const double tot_op = abs_op + scat_op;
+    const double rho = W[5 * c + 0];
+    const double prs = W[5 * c + 4];
+    const double *v = W + 5 * c + 1;
+    const double Ur = E[c];
+    const double *Fr = F + 3 * c;
+    const double *Tr = T + 9 * c; /* Tr(j,i) = Tr[3*j+i] */
+
+    double gamma = dot3(v, v);
+    double u2 = gamma;
+    double gamma2 = 1.0 / (1.0 - gamma);
+    u2 *= gamma2;
+    gamma = sqrt(gamma2);
+    double u[3] = {gamma * v[0], gamma * v[1], gamma * v[2]};
+
+    double uuD = 0.;
+    double uF = dot3(u, Fr);
+    double uD[3];
+    double D;
+    for (int i = 0; i < 3; i++) {
+      uD[i] = 0.;
+      for (int j = 0; j < 3; j++) {
+        D = Tr[3 * j + i];
+        uD[i] += u[j] * D;
+        uuD += u[i] * u[j] * D;
+      }
+    }
+    double rhogamma = rho * gamma;
+    const double Tgas = em->temp_coef * prs / rho;
+    const double T2 = Tgas * Tgas;
+    const double B = (T2 * T2) * em->sigma_sb / em->pi;
+    double q = -abs_op * rho * B / em->rad_unit;
+
+    G[4 * c + 0] = q * gamma + rhogamma * (abs_op - scat_op * (u2 + uuD)) * Ur -
+                   rho * (abs_op - scat_op * (u2 + gamma2)) * uF;
+    for (int i = 0; i < 3; i++)
+      G[4 * c + i + 1] = q * u[i] - rho * (tot_op * uD[i] + scat_op * u[i] * (gamma2 + uuD)) * Ur +
+                         rhogamma * (tot_op * Fr[i] + scat_op * 2.0 * uF * u[i]);
+  }
+}

@@ -1,0 +1,140 @@
+"""ctypes binding of librrhd.so (the C ABI declared in include/rrhd.h).
+
+There is no fallback: if the CUDA library is missing the import fails with
+an error that names the build command.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librrhd.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"{LIB_PATH} is missing: build it with `python -m radrhd_solver_b200.build` "
+                      "(or __graft_entry__.build())")
+
+lib = C.CDLL(LIB_PATH)
+
+P = C.c_void_p
+I32 = C.c_int32
+I64 = C.c_int64
+U64 = C.c_uint64
+D = C.c_double
+
+RRHD_OK = 0
+RRHD_ERR_INVALID = 1
+RRHD_ERR_CUDA = 2
+RRHD_ERR_OOM = 3
+RRHD_ERR_C2P = 4
+RRHD_ERR_STATE = 5
+RRHD_ERR_LIMIT = 6
+RRHD_HOST = 0
+RRHD_DEVICE = 1
+RRHD_EOS_IDEAL = 1
+RRHD_EOS_TAUB = 2
+RRHD_BC_TRANSMISSIVE = 0
+RRHD_BC_FIXED = 1
+RRHD_BC_REFLECT = 2
+STATUS_FALLBACK = 0x10
+STATUS_FAILED = 0x20
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("n_cells", I64), ("n_faces", I64), ("face_id_l", P), ("face_id_r", P), ("face_n", P),
+                ("face_area", P), ("cell_faces", P), ("cell_sign", P), ("cell_volume", P),
+                ("cell_center", P)]
+
+
+class Opts(C.Structure):
+    _fields_ = [("eos", I32), ("gamma", D), ("device", I32), ("cells_per_block", I32), ("renumber", I32)]
+
+
+class StepStats(C.Structure):
+    _fields_ = [("max_speed", D), ("n_fallback", I64), ("n_failed", I64)]
+
+
+class KuhnParams(C.Structure):
+    _fields_ = [("nx", I32), ("ny", I32), ("nz", I32), ("lo", D * 3), ("hi", D * 3), ("jitter", D),
+                ("seed", U64), ("bc_code", I32 * 6), ("inflow_radius", D), ("inflow_code", I32)]
+
+
+class Emission(C.Structure):
+    _fields_ = [("temp_coef", D), ("sigma_sb", D), ("pi", D), ("rad_unit", D)]
+
+
+_SIGS = {
+    "rrhd_create": (I32, [P, P, P]),
+    "rrhd_destroy": (I32, [P]),
+    "rrhd_stream": (P, [P]),
+    "rrhd_sync": (I32, [P]),
+    "rrhd_set_boundary": (I32, [P, I32, I32, P]),
+    "rrhd_set_state": (I32, [P, P, P, I64, I32]),
+    "rrhd_get_state": (I32, [P, P, P, I64, I32]),
+    "rrhd_set_state_prim": (I32, [P, P, I64, I32]),
+    "rrhd_hydro_step": (I32, [P, D, P]),
+    "rrhd_set_time_step": (I32, [P, D, D, D]),
+    "rrhd_get_step_info": (I32, [P, P, P]),
+    "rrhd_hydro_step_host": (I32, [P, D, P, P, I64, P]),
+    "rrhd_keep_face_flux": (I32, [P, I32]),
+    "rrhd_get_face_flux": (I32, [P, P]),
+    "rrhd_get_cell_status": (I32, [P, P]),
+    "rrhd_con2prim_batch": (I32, [I32, D, P, P, P, I64, I32, P]),
+    "rrhd_prim2con_batch": (I32, [I32, D, P, P, I64, P]),
+    "rrhd_dirs_create": (I32, [I32, P, P, D, I32, P]),
+    "rrhd_dirs_destroy": (I32, [P]),
+    "rrhd_dirs_count": (I32, [P]),
+    "rrhd_dirs_device_kernel": (P, [P]),
+    "rrhd_scatter_fp64": (I32, [P, P, P, I64, P]),
+    "rrhd_scatter_fp64_fma": (I32, [P, P, P, I64, P]),
+    "rrhd_moments_fp64": (I32, [P, P, P, P, P, I64, P]),
+    "rrhd_emission_reference": (Emission, []),
+    "rrhd_rad_source": (I32, [P, P, P, P, P, P, P, P, I64, P]),
+    "rrhd_last_error": (C.c_char_p, []),
+    "rrhd_version": (C.c_char_p, []),
+    "rrhd_mesh_kuhn_sizes": (I32, [P, P, P, P]),
+    "rrhd_mesh_kuhn_build": (I32, [P, P, P, P, P, P, P, P, P, P, P, P]),
+    "rrhd_directions_fibonacci": (I32, [I32, P, P, P]),
+    "rrhd_rng_u01": (D, [U64, U64, U64]),
+}
+
+for _name, (_res, _args) in _SIGS.items():
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+
+def optional(name: str, restype, argtypes):
+    """Binds an entry point that only some builds export (None if absent)."""
+    f = getattr(lib, name, None)
+    if f is not None:
+        f.restype = restype
+        f.argtypes = argtypes
+    return f
+
+
+class RrhdError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = lib.rrhd_last_error().decode(errors="replace")
+        super().__init__(f"{where}: status {status}: {msg}")
+        self.status = status
+
+
+def check(status: int, where: str = "rrhd") -> int:
+    if status != RRHD_OK:
+        raise RrhdError(status, where)
+    return status
+
+
+def ptr(a) -> int | None:
+    """Address of a numpy array or torch tensor (None passes through)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+def exported_symbols() -> list[str]:
+    return sorted(_SIGS)

@@ -1,0 +1,682 @@
+// Context, device-resident mesh/state and the fused RHLLC step.
+//
+// Layout in HBM (all in a renumbered cell order: Morton order of cell centres,
+// so that a CTA's cells and their neighbours are close in memory):
+//   state  [N][10] doubles = U(5) | W(5) per cell, 80 B, loaded as 5 x double2;
+//          two buffers (read one, write the other) so that no CTA overwrites a
+//          neighbour state another CTA still reads.
+//   per CTA (cells_per_block consecutive cells) a list of every face touching
+//   one of its cells: (l, r) int2, (n, area) double4, owner flag.  A face between
+//   two CTAs sits in both lists and is computed by both, bit-identically.
+//   per cell: 4 local face slots (ushort4), sign bits, volume.
+// One kernel does the whole step: face fluxes into shared memory, then each
+// cell sums its 4 faces in the reference's order (id_faces j = 0..3 with
+// sign_n), updates U, runs con2prim with the PhysPressureFix fallback and
+// writes U, W and a status byte.  No atomics touch the state; the max signal
+// speed and the fallback counts are reduced per CTA and combined with one
+// atomic per CTA.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "ctx.h"
+#include "hydro_phys.cuh"
+#include "rrhd_internal.h"
+
+using namespace rrhd;
+
+namespace {
+
+struct StepParams {
+  Eos eos;
+  int N;
+  int cpb;
+  const int32_t *__restrict__ off;
+  const int2 *__restrict__ lr;
+  const double4 *__restrict__ nS;
+  const int32_t *__restrict__ gid;
+  const ushort4 *__restrict__ slot;
+  const uint8_t *__restrict__ sign;
+  const double *__restrict__ V;
+  const double *__restrict__ sin;
+  double *__restrict__ sout;
+  uint8_t *__restrict__ status;
+  double *__restrict__ face_flux;
+  const StepScalars *prev;
+  StepScalars *out;
+  double tau;
+  int device_tau;
+  double cfl_hmin;
+  BcTable bc;
+};
+
+__device__ __forceinline__ void load_state(const double *s, int c, double *U, double *W) {
+  const double2 *p = reinterpret_cast<const double2 *>(s + 10 * (size_t)c);
+  const double2 a = __ldg(p), b = __ldg(p + 1), d = __ldg(p + 2), e = __ldg(p + 3), f = __ldg(p + 4);
+  U[0] = a.x;
+  U[1] = a.y;
+  U[2] = b.x;
+  U[3] = b.y;
+  U[4] = d.x;
+  W[0] = d.y;
+  W[1] = e.x;
+  W[2] = e.y;
+  W[3] = f.x;
+  W[4] = f.y;
+}
+
+__device__ __forceinline__ void store_state(double *s, int c, const double *U, const double *W) {
+  double2 *p = reinterpret_cast<double2 *>(s + 10 * (size_t)c);
+  p[0] = make_double2(U[0], U[1]);
+  p[1] = make_double2(U[2], U[3]);
+  p[2] = make_double2(U[4], W[0]);
+  p[3] = make_double2(W[1], W[2]);
+  p[4] = make_double2(W[3], W[4]);
+}
+
+// rhllc::BoundConditions (solvers/rhllc/src/rhllc_utils.cpp:45-133) from the table.
+__device__ __forceinline__ void boundary(const BcTable &bc, int code, const double4 &g,
+                                         const double *UL, const double *WL, double *UR,
+                                         double *WR) {
+  const int k = -code - 1;
+  const int kind = (k < 8) ? bc.kind[k] : 0;
+  if (kind == RRHD_BC_FIXED) {
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+      UR[i] = bc.U[k][i];
+      WR[i] = bc.W[k][i];
+    }
+    return;
+  }
+#pragma unroll
+  for (int i = 0; i < 5; i++) {
+    UR[i] = UL[i];
+    WR[i] = WL[i];
+  }
+  if (kind == RRHD_BC_REFLECT) {
+    Rot R, Rt;
+    rotation(g.x, g.y, g.z, R);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) Rt.t[3 * i + j] = R.t[3 * j + i];
+    double r[3];
+    matvec(R, UR + 1, r);
+    UR[1] = -r[0];
+    UR[2] = r[1];
+    UR[3] = r[2];
+    matvec(R, WR + 1, r);
+    WR[1] = -r[0];
+    WR[2] = r[1];
+    WR[3] = r[2];
+    matvec(Rt, UR + 1, r);
+    UR[1] = r[0];
+    UR[2] = r[1];
+    UR[3] = r[2];
+    matvec(Rt, WR + 1, r);
+    WR[1] = r[0];
+    WR[2] = r[1];
+    WR[3] = r[2];
+  }
+}
+
+constexpr int kStepThreads = 256;
+
+__global__ void __launch_bounds__(kStepThreads) k_hydro_step(const StepParams P) {
+  extern __shared__ double sflux[];
+  __shared__ double s_red[kStepThreads / 32];
+  __shared__ unsigned long long s_cnt[2];
+  const int b = blockIdx.x;
+  const int e0 = P.off[b], e1 = P.off[b + 1];
+  double tau = P.tau;
+  if (P.device_tau) tau = P.cfl_hmin / P.prev->max_speed;
+  if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0;
+
+  // phase 1: every face touching this CTA's cells
+  double vmax = 0.0;
+  for (int e = e0 + threadIdx.x; e < e1; e += kStepThreads) {
+    const int2 lr = P.lr[e];
+    const double4 g = P.nS[e];
+    double UL[5], WL[5], UR[5], WR[5], Fl[5];
+    load_state(P.sin, lr.x, UL, WL);
+    if (lr.y >= 0)
+      load_state(P.sin, lr.y, UR, WR);
+    else
+      boundary(P.bc, lr.y, g, UL, WL, UR, WR);
+    const double s = hllc_flux(P.eos, UL, UR, WL, WR, g.x, g.y, g.z, g.w, Fl);
+    vmax = smax(vmax, s);
+    double *dst = sflux + 5 * (e - e0);
+#pragma unroll
+    for (int i = 0; i < 5; i++) dst[i] = Fl[i];
+    if (P.face_flux) {
+      const int gf = P.gid[e];
+      if (gf >= 0) {
+#pragma unroll
+        for (int i = 0; i < 5; i++) P.face_flux[5 * (size_t)gf + i] = Fl[i];
+      }
+    }
+  }
+  __syncthreads();
+
+  // phase 2: gather, update, con2prim
+  unsigned n_fb = 0, n_fail = 0;
+  for (int cl = threadIdx.x; cl < P.cpb; cl += kStepThreads) {
+    const int c = b * P.cpb + cl;
+    if (c >= P.N) break;
+    const ushort4 sl = P.slot[c];
+    const unsigned sg = P.sign[c];
+    const unsigned short sls[4] = {sl.x, sl.y, sl.z, sl.w};
+    double sum[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const double *f = sflux + 5 * sls[j];
+      if ((sg >> j) & 1u) {
+#pragma unroll
+        for (int i = 0; i < 5; i++) sum[i] += f[i];
+      } else {
+#pragma unroll
+        for (int i = 0; i < 5; i++) sum[i] -= f[i];
+      }
+    }
+    const double sc = (tau / P.V[c]);
+    double U[5], W[5];
+    load_state(P.sin, c, U, W);
+#pragma unroll
+    for (int i = 0; i < 5; i++) U[i] -= sum[i] * sc;
+    const uint8_t st = c2p_with_fix(P.eos, U, W);
+    store_state(P.sout, c, U, W);
+    P.status[c] = st;
+    n_fb += (st & RRHD_STATUS_FALLBACK) ? 1u : 0u;
+    n_fail += (st & RRHD_STATUS_FAILED) ? 1u : 0u;
+  }
+
+  // CTA reduction of the max speed and the counters
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) vmax = smax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = vmax;
+  if (n_fb) atomicAdd(&s_cnt[0], (unsigned long long)n_fb);
+  if (n_fail) atomicAdd(&s_cnt[1], (unsigned long long)n_fail);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int w = 0; w < kStepThreads / 32; w++) m = smax(m, s_red[w]);
+    // non-negative doubles order like their bit patterns
+    atomicMax(reinterpret_cast<unsigned long long *>(&P.out->max_speed),
+              (unsigned long long)__double_as_longlong(m));
+    if (s_cnt[0]) atomicAdd(&P.out->n_fallback, s_cnt[0]);
+    if (s_cnt[1]) atomicAdd(&P.out->n_failed, s_cnt[1]);
+    if (b == 0) P.out->tau = tau;
+  }
+}
+
+// caller order <-> context order
+__global__ void k_set_state(int64_t N, const double *W, int64_t sw, const double *U, int64_t su,
+                            const int32_t *iperm, double *state) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double *dst = state + 10 * (size_t)iperm[i];
+  if (U)
+    for (int k = 0; k < 5; k++) dst[k] = U[i * su + k];
+  if (W)
+    for (int k = 0; k < 5; k++) dst[5 + k] = W[i * sw + k];
+}
+
+__global__ void k_get_state(int64_t N, double *W, int64_t sw, double *U, int64_t su,
+                            const int32_t *iperm, const double *state) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double *src = state + 10 * (size_t)iperm[i];
+  if (U)
+    for (int k = 0; k < 5; k++) U[i * su + k] = src[k];
+  if (W)
+    for (int k = 0; k < 5; k++) W[i * sw + k] = src[5 + k];
+}
+
+__global__ void k_prim2con_state(int64_t N, Eos eos, double *state) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  double *s = state + 10 * (size_t)c;
+  double U[5], W[5];
+  for (int k = 0; k < 5; k++) W[k] = s[5 + k];
+  p2c(eos, W, U);
+  for (int k = 0; k < 5; k++) {
+    s[k] = U[k];
+    s[5 + k] = W[k];
+  }
+}
+
+__global__ void k_get_status(int64_t N, const int32_t *iperm, const uint8_t *st, uint8_t *out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < N) out[i] = st[iperm[i]];
+}
+
+__global__ void k_c2p_batch(Eos eos, double *U, double *W, uint8_t *status, int64_t n,
+                            int fallback) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double u[5], w[5];
+  for (int k = 0; k < 5; k++) {
+    u[k] = U[5 * i + k];
+    w[k] = W[5 * i + k];
+  }
+  int code = c2p(eos, u, w);
+  if (code && fallback) {
+    const int fix = pressure_fix(eos, u, w);
+    code = code | 0x10 | (fix ? 0x20 : 0);
+    for (int k = 0; k < 5; k++) U[5 * i + k] = u[k];
+  }
+  for (int k = 0; k < 5; k++) W[5 * i + k] = w[k];
+  if (status) status[i] = (uint8_t)code;
+}
+
+__global__ void k_p2c_batch(Eos eos, double *W, double *U, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double u[5], w[5];
+  for (int k = 0; k < 5; k++) w[k] = W[5 * i + k];
+  p2c(eos, w, u);
+  for (int k = 0; k < 5; k++) {
+    U[5 * i + k] = u[k];
+    W[5 * i + k] = w[k];
+  }
+}
+
+inline unsigned grid1d(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+Eos make_eos(int eos, double gamma) {
+  Eos e;
+  e.eos = eos;
+  e.g1 = gamma;
+  e.gg = gamma / (gamma - 1.0);
+  return e;
+}
+
+uint64_t spread3(uint64_t x) {
+  x &= 0x1fffff;
+  x = (x | x << 32) & 0x1f00000000ffffull;
+  x = (x | x << 16) & 0x1f0000ff0000ffull;
+  x = (x | x << 8) & 0x100f00f00f00f00full;
+  x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+  x = (x | x << 2) & 0x1249249249249249ull;
+  return x;
+}
+
+template <class T>
+rrhd_status upload(T **dst, const std::vector<T> &src) {
+  RRHD_CUDA(cudaMalloc((void **)dst, sizeof(T) * std::max<size_t>(src.size(), 1)));
+  RRHD_CUDA(cudaMemcpy(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice));
+  return RRHD_OK;
+}
+
+void free_ctx(rrhd_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  void *ptrs[] = {c->d_perm, c->d_iperm, c->d_bface_off, c->d_bface_lr, c->d_bface_nS,
+                  c->d_bface_gid, c->d_cell_slot, c->d_cell_sign, c->d_cell_V, c->d_state[0],
+                  c->d_state[1], c->d_status, c->d_scal, c->d_face_flux, c->d_scratch_io};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (c->h_pinned) cudaFreeHost(c->h_pinned);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+}  // namespace
+
+extern "C" rrhd_status rrhd_create(const rrhd_mesh_desc *m, const rrhd_opts *opts, rrhd_ctx **out) {
+  RRHD_CHECK_ARG(m && out, "null argument");
+  *out = nullptr;
+  RRHD_CHECK_ARG(m->n_cells > 0 && m->n_faces > 0 && m->n_cells < (int64_t(1) << 30) &&
+                     m->n_faces < (int64_t(1) << 31),
+                 "bad mesh sizes");
+  RRHD_CHECK_ARG(m->face_id_l && m->face_id_r && m->face_n && m->face_area && m->cell_faces &&
+                     m->cell_sign && m->cell_volume && m->cell_center,
+                 "null mesh array");
+  const int64_t N = m->n_cells, F = m->n_faces;
+  for (int64_t f = 0; f < F; f++) {
+    RRHD_CHECK_ARG(m->face_id_l[f] >= 0 && m->face_id_l[f] < N, "face %lld: bad id_l", (long long)f);
+    RRHD_CHECK_ARG(m->face_id_r[f] < N && m->face_id_r[f] >= -8, "face %lld: bad id_r", (long long)f);
+  }
+  for (int64_t c = 0; c < 4 * N; c++)
+    RRHD_CHECK_ARG(m->cell_faces[c] >= 0 && m->cell_faces[c] < F, "cell %lld: bad face id", (long long)(c / 4));
+
+  rrhd_ctx *c = new rrhd_ctx();
+  rrhd_status st = RRHD_OK;
+  auto fail = [&](rrhd_status s) {
+    free_ctx(c);
+    return s;
+  };
+  c->device = opts ? opts->device : 0;
+  c->eos = (opts && opts->eos) ? opts->eos : RRHD_EOS_IDEAL;
+  c->gamma = (opts && opts->gamma > 0) ? opts->gamma : 5.0 / 3.0;
+  c->cpb = (opts && opts->cells_per_block > 0) ? opts->cells_per_block : 256;
+  if (c->eos != RRHD_EOS_IDEAL && c->eos != RRHD_EOS_TAUB) return fail(rrhd_fail(RRHD_ERR_INVALID, "bad eos"));
+  if (c->cpb > 1024 || c->cpb < 32) return fail(rrhd_fail(RRHD_ERR_INVALID, "cells_per_block out of [32,1024]"));
+  c->N = N;
+  c->F = F;
+  if (cudaSetDevice(c->device) != cudaSuccess) return fail(rrhd_fail(RRHD_ERR_CUDA, "cudaSetDevice(%d) failed", c->device));
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(rrhd_fail(RRHD_ERR_CUDA, "stream creation failed"));
+
+  // renumbering: Morton order of cell centres
+  std::vector<int32_t> perm(N), iperm(N);
+  std::iota(perm.begin(), perm.end(), 0);
+  const bool renumber = !(opts && opts->renumber < 0);
+  if (renumber) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int64_t i = 0; i < N; i++)
+      for (int a = 0; a < 3; a++) {
+        lo[a] = std::min(lo[a], m->cell_center[3 * i + a]);
+        hi[a] = std::max(hi[a], m->cell_center[3 * i + a]);
+      }
+    std::vector<uint64_t> key(N);
+    for (int64_t i = 0; i < N; i++) {
+      uint64_t code = 0;
+      for (int a = 0; a < 3; a++) {
+        const double ext = hi[a] - lo[a];
+        const double t = ext > 0 ? (m->cell_center[3 * i + a] - lo[a]) / ext : 0.0;
+        const uint64_t q = (uint64_t)std::min(2097151.0, std::max(0.0, t * 2097151.0));
+        code |= spread3(q) << a;
+      }
+      key[i] = code;
+    }
+    std::stable_sort(perm.begin(), perm.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
+  }
+  for (int64_t i = 0; i < N; i++) iperm[perm[i]] = (int32_t)i;
+
+  // per-CTA face lists
+  const int cpb = c->cpb;
+  const int nb = (int)((N + cpb - 1) / cpb);
+  c->nblocks = nb;
+  std::vector<int32_t> off(nb + 1, 0);
+  std::vector<int2> lr;
+  std::vector<double4> nS;
+  std::vector<int32_t> gid;
+  lr.reserve((size_t)(F * 1.3));
+  nS.reserve((size_t)(F * 1.3));
+  gid.reserve((size_t)(F * 1.3));
+  std::vector<ushort4> slot(N);
+  std::vector<uint8_t> sign(N);
+  std::vector<double> vol(N);
+  std::vector<int32_t> stamp(F, -1), local(F, 0);
+  int max_e = 0;
+  for (int b = 0; b < nb; b++) {
+    int ne = 0;
+    const int64_t c0 = (int64_t)b * cpb, c1 = std::min<int64_t>(N, c0 + cpb);
+    for (int64_t cn = c0; cn < c1; cn++) {
+      const int32_t co = perm[cn];
+      unsigned short s4[4];
+      for (int j = 0; j < 4; j++) {
+        const int32_t f = m->cell_faces[4 * co + j];
+        if (stamp[f] != b) {
+          stamp[f] = b;
+          local[f] = ne++;
+          const int32_t l = iperm[m->face_id_l[f]];
+          const int32_t r = m->face_id_r[f] >= 0 ? iperm[m->face_id_r[f]] : m->face_id_r[f];
+          lr.push_back(make_int2(l, r));
+          nS.push_back(make_double4(m->face_n[3 * f], m->face_n[3 * f + 1], m->face_n[3 * f + 2],
+                                    m->face_area[f]));
+          gid.push_back((l / cpb == b) ? f : -1);
+        }
+        s4[j] = (unsigned short)local[f];
+      }
+      slot[cn] = make_ushort4(s4[0], s4[1], s4[2], s4[3]);
+      sign[cn] = m->cell_sign[co];
+      vol[cn] = m->cell_volume[co];
+    }
+    if (ne > 65535) return fail(rrhd_fail(RRHD_ERR_LIMIT, "CTA face list too long"));
+    max_e = std::max(max_e, ne);
+    off[b + 1] = off[b] + ne;
+  }
+  c->max_entries = max_e;
+  c->n_entries = off[nb];
+  c->h_perm = perm;
+  if ((st = upload(&c->d_perm, perm)) || (st = upload(&c->d_iperm, iperm)) ||
+      (st = upload(&c->d_bface_off, off)) || (st = upload(&c->d_bface_lr, lr)) ||
+      (st = upload(&c->d_bface_nS, nS)) || (st = upload(&c->d_bface_gid, gid)) ||
+      (st = upload(&c->d_cell_slot, slot)) || (st = upload(&c->d_cell_sign, sign)) ||
+      (st = upload(&c->d_cell_V, vol)))
+    return fail(st);
+  const size_t ssz = sizeof(double) * 10 * N;
+  if (cudaMalloc(&c->d_state[0], ssz) != cudaSuccess || cudaMalloc(&c->d_state[1], ssz) != cudaSuccess ||
+      cudaMalloc(&c->d_status, N) != cudaSuccess || cudaMalloc(&c->d_scal, 2 * sizeof(StepScalars)) != cudaSuccess ||
+      cudaMalloc(&c->d_scratch_io, ssz) != cudaSuccess)
+    return fail(rrhd_fail(RRHD_ERR_OOM, "device allocation of the state failed"));
+  cudaMemset(c->d_state[0], 0, ssz);
+  cudaMemset(c->d_state[1], 0, ssz);
+  cudaMemset(c->d_status, 0, N);
+  StepScalars init[2] = {{0, 0, 0, 0}, {1.0, 0, 0, 0}};  // rhllc::max_signal_speed = 1 initially
+  cudaMemcpy(c->d_scal, init, sizeof init, cudaMemcpyHostToDevice);
+  c->scal_cur = 0;
+  for (int k = 0; k < 8; k++) c->bc.kind[k] = RRHD_BC_TRANSMISSIVE;
+  const size_t smem = sizeof(double) * 5 * (size_t)max_e;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(k_hydro_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return fail(rrhd_fail(RRHD_ERR_LIMIT, "CTA face list needs %zu B of shared memory", smem));
+  if (cudaDeviceSynchronize() != cudaSuccess) return fail(rrhd_fail(RRHD_ERR_CUDA, "%s", cudaGetErrorString(cudaGetLastError())));
+  *out = c;
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_destroy(rrhd_ctx *c) {
+  if (c) {
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    free_ctx(c);
+  }
+  return RRHD_OK;
+}
+
+extern "C" void *rrhd_stream(rrhd_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+extern "C" rrhd_status rrhd_sync(rrhd_ctx *c) {
+  RRHD_CHECK_ARG(c, "null context");
+  RRHD_CUDA(cudaStreamSynchronize(c->stream));
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_set_boundary(rrhd_ctx *c, int32_t code, int32_t kind, const double *W) {
+  RRHD_CHECK_ARG(c && code <= -1 && code >= -8, "boundary code must be in [-8, -1]");
+  RRHD_CHECK_ARG(kind >= 0 && kind <= 2, "bad boundary kind");
+  const int k = -code - 1;
+  c->bc.kind[k] = kind;
+  if (kind == RRHD_BC_FIXED) {
+    RRHD_CHECK_ARG(W, "fixed boundary needs a state");
+    const double gg = c->gamma / (c->gamma - 1.0);
+    for (int i = 0; i < 5; i++) c->bc.W[k][i] = W[i];
+    p2c_plain(gg, c->bc.W[k], c->bc.U[k]);
+  }
+  return RRHD_OK;
+}
+
+static rrhd_status state_transfer(rrhd_ctx *c, double *W, double *U, int64_t stride, int32_t where, bool set) {
+  RRHD_CHECK_ARG(c, "null context");
+  RRHD_CHECK_ARG(stride >= 5, "stride must be >= 5");
+  RRHD_CHECK_ARG(where == RRHD_HOST || where == RRHD_DEVICE, "bad `where`");
+  RRHD_CUDA(cudaSetDevice(c->device));
+  const int64_t N = c->N;
+  double *state = c->d_state[c->cur];
+  if (where == RRHD_DEVICE) {
+    if (set)
+      k_set_state<<<grid1d(N, 256), 256, 0, c->stream>>>(N, W, stride, U, stride, c->d_iperm, state);
+    else
+      k_get_state<<<grid1d(N, 256), 256, 0, c->stream>>>(N, W, stride, U, stride, c->d_iperm, state);
+    RRHD_CUDA(cudaGetLastError());
+    return RRHD_OK;
+  }
+  // host: contiguous [N][5] arrays go straight to/from the device staging area
+  // (fast when the caller's memory is pinned); strided records are packed
+  // through the context's pinned buffer.
+  double *dW = c->d_scratch_io, *dU = c->d_scratch_io + 5 * N;
+  const size_t bytes = sizeof(double) * 5 * N;
+  if (stride != 5 && !c->h_pinned) RRHD_CUDA(cudaMallocHost(&c->h_pinned, 2 * bytes));
+  double *hW = c->h_pinned, *hU = c->h_pinned ? c->h_pinned + 5 * N : nullptr;
+  if (set) {
+    if (stride != 5) {
+      for (int64_t i = 0; i < N; i++) {
+        if (W) memcpy(hW + 5 * i, W + i * stride, 5 * sizeof(double));
+        if (U) memcpy(hU + 5 * i, U + i * stride, 5 * sizeof(double));
+      }
+    }
+    if (W) RRHD_CUDA(cudaMemcpyAsync(dW, stride == 5 ? W : hW, bytes, cudaMemcpyHostToDevice, c->stream));
+    if (U) RRHD_CUDA(cudaMemcpyAsync(dU, stride == 5 ? U : hU, bytes, cudaMemcpyHostToDevice, c->stream));
+    k_set_state<<<grid1d(N, 256), 256, 0, c->stream>>>(N, W ? dW : nullptr, 5, U ? dU : nullptr, 5,
+                                                        c->d_iperm, state);
+    RRHD_CUDA(cudaGetLastError());
+    if (stride != 5) RRHD_CUDA(cudaStreamSynchronize(c->stream));
+  } else {
+    k_get_state<<<grid1d(N, 256), 256, 0, c->stream>>>(N, W ? dW : nullptr, 5, U ? dU : nullptr, 5,
+                                                        c->d_iperm, state);
+    RRHD_CUDA(cudaGetLastError());
+    if (W) RRHD_CUDA(cudaMemcpyAsync(stride == 5 ? W : hW, dW, bytes, cudaMemcpyDeviceToHost, c->stream));
+    if (U) RRHD_CUDA(cudaMemcpyAsync(stride == 5 ? U : hU, dU, bytes, cudaMemcpyDeviceToHost, c->stream));
+    RRHD_CUDA(cudaStreamSynchronize(c->stream));
+    if (stride != 5) {
+      for (int64_t i = 0; i < N; i++) {
+        if (W) memcpy(W + i * stride, hW + 5 * i, 5 * sizeof(double));
+        if (U) memcpy(U + i * stride, hU + 5 * i, 5 * sizeof(double));
+      }
+    }
+  }
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_set_state(rrhd_ctx *c, const double *W, const double *U, int64_t stride,
+                                      int32_t where) {
+  return state_transfer(c, const_cast<double *>(W), const_cast<double *>(U), stride, where, true);
+}
+
+extern "C" rrhd_status rrhd_get_state(rrhd_ctx *c, double *W, double *U, int64_t stride, int32_t where) {
+  return state_transfer(c, W, U, stride, where, false);
+}
+
+extern "C" rrhd_status rrhd_set_state_prim(rrhd_ctx *c, const double *W, int64_t stride, int32_t where) {
+  rrhd_status st = state_transfer(c, const_cast<double *>(W), nullptr, stride, where, true);
+  if (st) return st;
+  k_prim2con_state<<<grid1d(c->N, 256), 256, 0, c->stream>>>(c->N, make_eos(c->eos, c->gamma),
+                                                               c->d_state[c->cur]);
+  RRHD_CUDA(cudaGetLastError());
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_set_time_step(rrhd_ctx *c, double cfl, double h_min, double initial_max_speed) {
+  RRHD_CHECK_ARG(c && cfl > 0 && h_min > 0, "bad time-step parameters");
+  c->cfl = cfl;
+  c->h_min = h_min;
+  if (initial_max_speed > 0) {
+    RRHD_CUDA(cudaStreamSynchronize(c->stream));
+    StepScalars s = {initial_max_speed, 0, 0, 0};
+    RRHD_CUDA(cudaMemcpy(&c->d_scal[c->scal_cur ^ 1], &s, sizeof s, cudaMemcpyHostToDevice));
+  }
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_hydro_step(rrhd_ctx *c, double tau, rrhd_step_stats *stats) {
+  RRHD_CHECK_ARG(c, "null context");
+  if (tau <= 0) RRHD_CHECK_ARG(c->h_min > 0, "tau <= 0 needs rrhd_set_time_step first");
+  RRHD_CUDA(cudaSetDevice(c->device));
+  if (c->keep_face_flux && !c->d_face_flux) RRHD_CUDA(cudaMalloc(&c->d_face_flux, sizeof(double) * 5 * c->F));
+  StepParams P;
+  P.eos = make_eos(c->eos, c->gamma);
+  P.N = (int)c->N;
+  P.cpb = c->cpb;
+  P.off = c->d_bface_off;
+  P.lr = c->d_bface_lr;
+  P.nS = c->d_bface_nS;
+  P.gid = c->d_bface_gid;
+  P.slot = c->d_cell_slot;
+  P.sign = c->d_cell_sign;
+  P.V = c->d_cell_V;
+  P.sin = c->d_state[c->cur];
+  P.sout = c->d_state[c->cur ^ 1];
+  P.status = c->d_status;
+  P.face_flux = c->keep_face_flux ? c->d_face_flux : nullptr;
+  P.prev = c->d_scal + (c->scal_cur ^ 1);
+  P.out = c->d_scal + c->scal_cur;
+  P.tau = tau;
+  P.device_tau = tau <= 0 ? 1 : 0;
+  P.cfl_hmin = c->cfl * c->h_min;
+  P.bc = c->bc;
+  RRHD_CUDA(cudaMemsetAsync(P.out, 0, sizeof(StepScalars), c->stream));
+  const size_t smem = sizeof(double) * 5 * (size_t)c->max_entries;
+  k_hydro_step<<<c->nblocks, kStepThreads, smem, c->stream>>>(P);
+  RRHD_CUDA(cudaGetLastError());
+  c->cur ^= 1;
+  c->scal_cur ^= 1;
+  if (stats) {
+    StepScalars s;
+    RRHD_CUDA(cudaMemcpyAsync(&s, P.out, sizeof s, cudaMemcpyDeviceToHost, c->stream));
+    RRHD_CUDA(cudaStreamSynchronize(c->stream));
+    stats->max_speed = s.max_speed;
+    stats->n_fallback = (int64_t)s.n_fallback;
+    stats->n_failed = (int64_t)s.n_failed;
+    if (s.n_failed) return rrhd_fail(RRHD_ERR_C2P, "con2prim failed in %llu cells after the fallback", s.n_failed);
+  }
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_get_step_info(rrhd_ctx *c, double *tau_used, double *max_speed) {
+  RRHD_CHECK_ARG(c, "null context");
+  StepScalars s;
+  RRHD_CUDA(cudaMemcpyAsync(&s, c->d_scal + (c->scal_cur ^ 1), sizeof s, cudaMemcpyDeviceToHost, c->stream));
+  RRHD_CUDA(cudaStreamSynchronize(c->stream));
+  if (tau_used) *tau_used = s.tau;
+  if (max_speed) *max_speed = s.max_speed;
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_hydro_step_host(rrhd_ctx *c, double tau, double *W, double *U, int64_t stride,
+                                           rrhd_step_stats *stats) {
+  rrhd_status st = rrhd_set_state(c, W, U, stride, RRHD_HOST);
+  if (st) return st;
+  rrhd_status step = rrhd_hydro_step(c, tau, stats);
+  if (step && step != RRHD_ERR_C2P) return step;
+  st = rrhd_get_state(c, W, U, stride, RRHD_HOST);
+  return st ? st : step;
+}
+
+extern "C" rrhd_status rrhd_keep_face_flux(rrhd_ctx *c, int32_t on) {
+  RRHD_CHECK_ARG(c, "null context");
+  c->keep_face_flux = on != 0;
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_get_face_flux(rrhd_ctx *c, double *F) {
+  RRHD_CHECK_ARG(c && F, "null argument");
+  RRHD_CHECK_ARG(c->keep_face_flux && c->d_face_flux, "call rrhd_keep_face_flux(ctx, 1) before the step");
+  RRHD_CUDA(cudaMemcpyAsync(F, c->d_face_flux, sizeof(double) * 5 * c->F, cudaMemcpyDeviceToHost, c->stream));
+  RRHD_CUDA(cudaStreamSynchronize(c->stream));
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_get_cell_status(rrhd_ctx *c, uint8_t *status) {
+  RRHD_CHECK_ARG(c && status, "null argument");
+  uint8_t *d = reinterpret_cast<uint8_t *>(c->d_scratch_io);
+  k_get_status<<<grid1d(c->N, 256), 256, 0, c->stream>>>(c->N, c->d_iperm, c->d_status, d);
+  RRHD_CUDA(cudaGetLastError());
+  RRHD_CUDA(cudaMemcpyAsync(status, d, c->N, cudaMemcpyDeviceToHost, c->stream));
+  RRHD_CUDA(cudaStreamSynchronize(c->stream));
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_con2prim_batch(int32_t eos, double gamma, double *U, double *W, uint8_t *status,
+                                           int64_t n, int32_t fallback, void *stream) {
+  RRHD_CHECK_ARG(U && W && n >= 0, "bad arguments");
+  RRHD_CHECK_ARG(eos == RRHD_EOS_IDEAL || eos == RRHD_EOS_TAUB, "bad eos");
+  if (n == 0) return RRHD_OK;
+  k_c2p_batch<<<grid1d(n, 128), 128, 0, (cudaStream_t)stream>>>(make_eos(eos, gamma), U, W, status, n, fallback);
+  RRHD_CUDA(cudaGetLastError());
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_prim2con_batch(int32_t eos, double gamma, double *W, double *U, int64_t n,
+                                           void *stream) {
+  RRHD_CHECK_ARG(U && W && n >= 0, "bad arguments");
+  RRHD_CHECK_ARG(eos == RRHD_EOS_IDEAL || eos == RRHD_EOS_TAUB, "bad eos");
+  if (n == 0) return RRHD_OK;
+  k_p2c_batch<<<grid1d(n, 256), 256, 0, (cudaStream_t)stream>>>(make_eos(eos, gamma), W, U, n);
+  RRHD_CUDA(cudaGetLastError());
+  return RRHD_OK;
+}

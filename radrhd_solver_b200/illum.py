@@ -1,0 +1,72 @@
+"""Radiation scattering integral and moments, mirroring the reference's
+`illum` / `cuda::interface::separate_device` calls.
+
+    dg = DirectionGrid(fibonacci_directions(256))          # InitDevice (directions)
+    S = CalculateIntScattering(dg, I)                      # GetS_MPI_multi_device
+    E, F, T = CalculateAllParam(dg, I)                     # MakeIllumParam
+
+I is a CUDA tensor [rows, M] with rows = cells x groups (cell-major, the
+layout of grid.Illum, solvers/illum/src/illum_utils.cpp:362).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+from . import _lib as L
+from .mesh import Directions
+
+
+class DirectionGrid:
+    def __init__(self, d: Directions, device: int = 0):
+        self.directions = d
+        self.size = d.size
+        self.full_area = d.full_area
+        h = C.c_void_p()
+        L.check(L.lib.rrhd_dirs_create(d.size, L.ptr(d.dirs), L.ptr(d.areas), d.full_area, device, C.byref(h)),
+                "rrhd_dirs_create")
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            L.lib.rrhd_dirs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return stream
+
+
+def CalculateIntScattering(dg: DirectionGrid, I, S=None, exact: bool = True, stream=None):
+    """FP64 scattering integral (cuda/src/short_characteristics/cuda_scattering.cu:82-105).
+    exact=True: the reference's rounding sequence; exact=False: one FMA per term."""
+    import torch
+    if S is None:
+        S = torch.empty_like(I)
+    fn = L.lib.rrhd_scatter_fp64 if exact else L.lib.rrhd_scatter_fp64_fma
+    L.check(fn(dg.handle, L.ptr(I), L.ptr(S), I.shape[0], _stream(stream)), "CalculateIntScattering")
+    return S
+
+
+def CalculateAllParam(dg: DirectionGrid, I, stream=None):
+    """Energy/stream/impulse moments (separate_gpu/cuda_illum_sep_param.cu:9-83)."""
+    import torch
+    rows = I.shape[0]
+    E = torch.empty(rows, dtype=torch.float64, device=I.device)
+    F = torch.empty(rows, 3, dtype=torch.float64, device=I.device)
+    T = torch.empty(rows, 3, 3, dtype=torch.float64, device=I.device)
+    L.check(L.lib.rrhd_moments_fp64(dg.handle, L.ptr(I), L.ptr(E), L.ptr(F), L.ptr(T), rows, _stream(stream)),
+            "CalculateAllParam")
+    return E, F, T

@@ -1,0 +1,64 @@
+"""Seeded synthetic inputs shared by the tests (shapes and value ranges of the
+benchmark configurations, at sizes the oracle finishes in seconds)."""
+from __future__ import annotations
+
+import numpy as np
+
+from radrhd_solver_b200 import mesh as M
+
+GAMMA_53 = 5.0 / 3
+GAMMA_43 = 4.0 / 3
+
+
+def shock_tube(nx=40, ny=4, nz=4, seed=7):
+    """Relativistic shock tube on [0,1] x [0,ny/nx] x [0,nz/nx] (cubic hexes;
+    200x10x10 is the [0,1]x[0,0.05]^2 benchmark box): left rho=10, p=13.33;
+    right rho=1, p=0.01; v=0 (by cell centroid)."""
+    m = M.kuhn_box(nx, ny, nz, hi=(1.0, ny / nx, nz / nx), jitter=0.15, seed=seed)
+    xc = m.cell_center[:, 0]
+    W = np.zeros((m.n_cells, 5))
+    W[:, 0] = np.where(xc < 0.5, 10.0, 1.0)
+    W[:, 4] = np.where(xc < 0.5, 13.33, 0.01)
+    return m, W
+
+
+JET_INFLOW = np.array([0.01, 0.0, 0.0, np.sqrt(1.0 - 1.0 / 49.0), 1e-3])  # rho, v (W=7 along +z), p
+
+
+def jet(n=12, seed=11):
+    """Coupled-jet mesh: cube [-1,1]^3, ambient rho=1, p=1e-3, v=0; z=-1 faces
+    with centroid radius < 0.1 carry code -3 (fixed inflow state JET_INFLOW).
+    For small n the nozzle radius is widened so that some faces are inside."""
+    r = max(0.1, 2.5 * 2.0 / n)
+    m = M.kuhn_box(n, n, n, lo=(-1, -1, -1), hi=(1, 1, 1), jitter=0.15, seed=seed, inflow_radius=r,
+                   inflow_code=-3, with_vertices=True)
+    W = np.zeros((m.n_cells, 5))
+    W[:, 0] = 1.0
+    W[:, 4] = 1e-3
+    return m, W
+
+
+def c2p_states(n, gamma=GAMMA_43, seed=5):
+    """Config-3 style primitive states: rho log-uniform [1e-4,1e2], p/rho
+    log-uniform [1e-6,1e2], Lorentz factor log-uniform [1,50], isotropic v."""
+    rng = np.random.default_rng(seed)
+    rho = 10 ** rng.uniform(-4, 2, n)
+    p = rho * 10 ** rng.uniform(-6, 2, n)
+    lor = 10 ** rng.uniform(0, np.log10(50), n)
+    v = np.sqrt(1 - 1 / lor ** 2)
+    mu = rng.uniform(-1, 1, n)
+    ph = rng.uniform(0, 2 * np.pi, n)
+    s = np.sqrt(1 - mu ** 2)
+    W = np.stack([rho, v * s * np.cos(ph), v * s * np.sin(ph), v * mu, p], axis=1)
+    return W
+
+
+def intensity(N, M_, seed=3, centers=None, groups=1):
+    """Config-1 style intensity: lognormal(0, 0.5) * exp(-|x|^2/0.2), cell-major
+    [N*groups, M]."""
+    rng = np.random.default_rng(seed)
+    I = np.exp(rng.normal(0.0, 0.5, (N * groups, M_)))
+    if centers is not None:
+        r2 = (centers ** 2).sum(1)
+        I *= np.repeat(np.exp(-r2 / 0.2), groups)[:, None]
+    return I
