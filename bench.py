@@ -1,0 +1,325 @@
+"""Benchmark of the RadRHD_solver hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): one RHLLC hydro step (face fluxes + conservative update +
+con2prim with the PhysPressureFix fallback, FP64) on the coupled-jet mesh:
+cube [-1,1]^3 as 96^3 hexes x 6 Kuhn tets = 5,308,416 cells, 10,672,128 faces
+(vertices jittered +-0.15h, seeded), ambient rho=1, p=1e-3, v=0, Gamma=4/3,
+inflow nozzle r<0.1 at z=-1 (rho=0.01, W=7 along +z, p=1e-3), transmissive
+walls, tau = 0.3 h_min / c.  Synthetic, seeded; no dataset exists for this.
+
+value = cell-updates/s with the state resident in HBM (CUDA events on the
+solver's stream, max over ranks); e2e = the same through the C ABI drop-in
+rrhd_hydro_step_host with host (pinned) buffers: H2D of W,U + step + D2H of W,U
+every step.  The state (2 x 425 MB) is larger than L2, so no flush is needed.
+
+--impl reference: the reference's own CPU implementation of the same step
+(rhllc::Hllc3dStab compiled from its sources with -Ofast -fopenmp, oracle/_ref)
+on all host cores; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s (RHLLC+con2prim); scatter cell-dir/s; chosen vs plain form"
+UNIT = "cell-updates/s"
+NHEX = 96
+GAMMA = 4.0 / 3.0
+CFL = 0.3
+INFLOW = [0.01, 0.0, 0.0, float(np.sqrt(1.0 - 1.0 / 49.0)), 1e-3]
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+def make_jet(n=None, seed=2024):
+    n = n or NHEX
+    from radrhd_solver_b200 import mesh as M
+    m = M.kuhn_box(n, n, n, lo=(-1, -1, -1), hi=(1, 1, 1), jitter=0.15, seed=seed, inflow_radius=0.1,
+                   inflow_code=-3)
+    W = np.zeros((m.n_cells, 5))
+    W[:, 0] = 1.0
+    W[:, 4] = 1e-3
+    return m, W
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        rows = []
+        for ln in (self.out or "").strip().splitlines():
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) >= 8:
+                rows.append(f)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_steps(m, W, U, steps, threads, bc_u):
+    """Times `steps` reference hydro steps on the host; returns seconds per step and kind."""
+    import oracle
+    variant = "hydro_ideal_4_3_fast"
+    if oracle.have_ref(variant):
+        h = oracle.HydroRef(m, variant)
+        h.set_bc(-3, 1, np.array(INFLOW), bc_u)
+        h.set_state(W, U)
+        tau = CFL * m.h_min
+        h.step(tau, threads)  # first touch
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            h.step(tau, threads)
+        dt = (time.perf_counter() - t0) / steps
+        h.close()
+        return dt, "reference"
+    # the C restatement when the reference could not be built
+    bc = {-3: (1, np.array(INFLOW), bc_u)}
+    tau = CFL * m.h_min
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        U, W, _, _, _ = oracle.port_hydro_step(m, U, W, tau, 1, GAMMA, bc=bc, nthreads=threads)
+    return (time.perf_counter() - t0) / steps, "port"
+
+
+def inflow_conservative():
+    """Conservative inflow state (rhllc::GetConvValue) for the CPU legs."""
+    import oracle
+    u = np.zeros(5)
+    e = oracle.loader.OrcEos(1, GAMMA)
+    oracle.port().orc_p2c_plain(ctypes.byref(e), np.array(INFLOW).ctypes.data, u.ctypes.data)
+    return u
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    m, W = make_jet()
+    W, U = oracle.port_p2c(W, 1, GAMMA) if m.n_cells < 100000 else _p2c_fast(W)
+    threads = cpu_threads()
+    bc_u = inflow_conservative()
+    dt, kind = reference_steps(m, W, U, max(1, args.steps), threads, bc_u)
+    v = m.n_cells / dt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"coupled-jet mesh {NHEX}^3x6 tets, RHLLC hydro step", "cells": m.n_cells,
+                       "faces": m.n_faces},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": f"{args.steps} full steps of the {m.n_cells}-cell mesh"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _p2c_fast(W):
+    """prim->cons for the uniform bench state through the library's batch kernel
+    would need a GPU; the ambient state is uniform, so compute it once."""
+    import oracle
+    Wu, Uu = oracle.port_p2c(W[:1], 1, GAMMA)
+    return np.repeat(Wu, len(W), 0), np.repeat(Uu, len(W), 0)
+
+
+def profile_traffic(name):
+    """dram bytes per launch recorded from an ncu capture in profiles/<name>."""
+    p = os.path.join(ROOT, "profiles", name)
+    try:
+        for ln in open(p):
+            if ln.strip().startswith("traffic_bytes_per_launch:"):
+                return float(ln.split(":", 1)[1].split()[0])
+    except Exception:
+        pass
+    return None
+
+
+def run_ours(args):
+    import torch
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = local
+    torch.cuda.set_device(dev)
+    from radrhd_solver_b200 import _lib as L
+    from radrhd_solver_b200 import rhllc
+
+    m, W = make_jet()
+    g = rhllc.Grid(m, eos=rhllc.EOS_IDEAL, gamma=GAMMA, device=dev)
+    g.set_boundary(-3, rhllc.BC_FIXED, INFLOW)
+    g.set_state_prim(W)
+    tau = CFL * m.h_min
+    stream = torch.cuda.ExternalStream(g.stream)
+    for _ in range(args.warmup):
+        L.check(L.lib.rrhd_hydro_step(g.handle, tau, None))
+    torch.cuda.synchronize()
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # device-resident timing
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with Clocks(dev) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            L.check(L.lib.rrhd_hydro_step(g.handle, tau, None))
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    st = L.StepStats()
+    L.check(L.lib.rrhd_hydro_step(g.handle, tau, ctypes.byref(st)))
+    ms_t = torch.tensor([ms], device=f"cuda:{dev}")
+    if ws > 1:
+        import torch.distributed as dist
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    per_step = ms / args.steps
+    value = ws * m.n_cells * args.steps / (ms / 1e3)
+
+    # e2e through the host-buffer drop-in
+    Wh = torch.empty((m.n_cells, 5), dtype=torch.float64).pin_memory()
+    Uh = torch.empty((m.n_cells, 5), dtype=torch.float64).pin_memory()
+    L.check(L.lib.rrhd_get_state(g.handle, Wh.data_ptr(), Uh.data_ptr(), 5, L.RRHD_HOST))
+    e2e_steps = max(3, args.steps // 2)
+    L.check(L.lib.rrhd_hydro_step_host(g.handle, tau, Wh.data_ptr(), Uh.data_ptr(), 5, None))
+    barrier()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        L.check(L.lib.rrhd_hydro_step_host(g.handle, tau, Wh.data_ptr(), Uh.data_ptr(), 5, None))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e = torch.tensor([e0.elapsed_time(e1)], device=f"cuda:{dev}")
+    if ws > 1:
+        import torch.distributed as dist
+        dist.all_reduce(ms_e, op=dist.ReduceOp.MAX)
+    e2e_value = ws * m.n_cells * e2e_steps / (float(ms_e.item()) / 1e3)
+    io_bytes = 80 * m.n_cells
+
+    # roofline of the fused step kernel (the only kernel in the step)
+    alg_bytes = 185.0 * m.n_cells + 40.0 * m.n_faces
+    achieved = alg_bytes / (per_step / 1e3) / 1e9
+    pk = peaks()
+    peak = pk["hbm_gbs"] if pk else 6650.0
+    traffic = profile_traffic("hydro_step_jet96.md")
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Kuhn mesh, jet initial state)",
+            "config": {"workload": f"coupled-jet mesh {NHEX}^3x6 tets: RHLLC flux + update + con2prim step",
+                       "cells": m.n_cells, "faces": m.n_faces, "gamma": GAMMA, "tau": tau,
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                       "l2": "state 2 x 425 MB > L2 (126 MB): no flush"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": "measured" if pk else "fallback",
+                         "algorithmic_bytes_per_cell_update": alg_bytes / m.n_cells},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
+            "gpu_launches": args.steps,
+            "clocks": clk.summary(),
+            "step_stats": {"max_speed": st.max_speed, "n_fallback": st.n_fallback, "n_failed": st.n_failed}}
+    g.close()
+    if rank == 0 and not args.no_cpu:
+        import oracle
+        threads = cpu_threads()
+        Wg = W.copy()
+        Wg, Ug = _p2c_fast(Wg)
+        dt, kind = reference_steps(m, Wg, Ug, args.cpu_steps, threads, inflow_conservative())
+        line["cpu_baseline"] = {"value": m.n_cells / dt, "unit": UNIT, "cores": threads, "kind": kind,
+                                "sample": f"{args.cpu_steps} full steps of the {m.n_cells}-cell mesh"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--nhex", type=int, default=96, help="hexes per axis (96 = the benchmark mesh)")
+    args = ap.parse_args()
+    global NHEX
+    NHEX = args.nhex
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()
