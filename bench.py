@@ -210,7 +210,7 @@ def run_ours(args):
     from radrhd_solver_b200 import rhllc
 
     m, W = make_jet()
-    g = rhllc.Grid(m, eos=rhllc.EOS_IDEAL, gamma=GAMMA, device=dev)
+    g = rhllc.Grid(m, eos=rhllc.EOS_IDEAL, gamma=GAMMA, device=dev, cells_per_block=args.cpb)
     g.set_boundary(-3, rhllc.BC_FIXED, INFLOW)
     g.set_state_prim(W)
     tau = CFL * m.h_min
@@ -312,6 +312,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--nhex", type=int, default=96, help="hexes per axis (96 = the benchmark mesh)")
+    ap.add_argument("--cpb", type=int, default=0, help="cells per CTA of the step kernel (0 = library default)")
     args = ap.parse_args()
     global NHEX
     NHEX = args.nhex

@@ -4,8 +4,17 @@ Native library: radrhd_solver_b200/librrhd.so (C ABI: include/rrhd.h).
 Modules mirror the reference's namespaces: `rhllc` (hydro step, con2prim),
 `illum` (scattering integral, moments), `rad_rhd` (radiation 4-force),
 `mesh` (synthetic meshes and direction sets).
+
+Submodules load on first use, so `radrhd_solver_b200.build` runs on a tree
+where the library has not been built yet; every other submodule imports `_lib`,
+which raises ImportError when librrhd.so is missing (there is no fallback).
 """
-from . import _lib  # noqa: F401  (fails loudly if librrhd.so is missing)
-from . import illum, mesh, rad_rhd, rhllc  # noqa: F401
+import importlib
 
 __all__ = ["illum", "mesh", "rad_rhd", "rhllc"]
+
+
+def __getattr__(name):
+    if name in ("illum", "mesh", "rad_rhd", "rhllc", "coupled", "c2p_mlp", "scatter_tc", "sweep", "_lib"):
+        return importlib.import_module(f".{name}", __name__)
+    raise AttributeError(name)

@@ -35,7 +35,9 @@ struct rrhd_ctx {
   int cpb = 256;      // cells per CTA
   int nblocks = 0;
   int max_entries = 0;  // largest per-CTA face list
+  int max_halo = 0;     // largest per-CTA list of neighbour cells owned by other CTAs
   int64_t n_entries = 0;
+  size_t step_smem = 0; // dynamic shared memory of the step kernel
 
   // numbering: perm[new] = caller id, iperm[caller id] = new
   int32_t *d_perm = nullptr, *d_iperm = nullptr;
@@ -43,7 +45,9 @@ struct rrhd_ctx {
 
   // per-CTA face lists
   int32_t *d_bface_off = nullptr;  // [nblocks+1]
-  int2 *d_bface_lr = nullptr;      // [E] (l, r) in the new numbering; r < 0: boundary code
+  int2 *d_bface_lr = nullptr;      // [E] (l, r) as CTA-local state slots; r < 0: boundary code
+  int32_t *d_halo_off = nullptr;   // [nblocks+1]
+  int32_t *d_halo_ids = nullptr;   // neighbour cells (new numbering) staged after the CTA's own
   double4 *d_bface_nS = nullptr;   // [E] (n0, n1, n2, area)
   int32_t *d_bface_gid = nullptr;  // [E] caller face id on the owner CTA, else -1
 

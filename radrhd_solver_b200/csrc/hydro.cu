@@ -6,15 +6,19 @@
 //          two buffers (read one, write the other) so that no CTA overwrites a
 //          neighbour state another CTA still reads.
 //   per CTA (cells_per_block consecutive cells) a list of every face touching
-//   one of its cells: (l, r) int2, (n, area) double4, owner flag.  A face between
-//   two CTAs sits in both lists and is computed by both, bit-identically.
-//   per cell: 4 local face slots (ushort4), sign bits, volume.
-// One kernel does the whole step: face fluxes into shared memory, then each
-// cell sums its 4 faces in the reference's order (id_faces j = 0..3 with
-// sign_n), updates U, runs con2prim with the PhysPressureFix fallback and
-// writes U, W and a status byte.  No atomics touch the state; the max signal
-// speed and the fallback counts are reduced per CTA and combined with one
-// atomic per CTA.
+//   one of its cells: (l, r) as CTA-local state slots (int2), (n, area)
+//   double4, owner flag; and a halo list of the neighbour cells owned by other
+//   CTAs.  A face between two CTAs sits in both lists and is computed by both,
+//   bit-identically.  Per cell: 4 local face slots (ushort4), sign bits, volume.
+// One kernel does the whole step:
+//   phase 0  cp.async stages the CTA's own states (one contiguous range) and
+//            its halo states into shared memory, all requests in flight at once;
+//   phase 1  face fluxes from the staged states into shared memory;
+//   phase 2  each cell sums its 4 faces in the reference's order (id_faces
+//            j = 0..3 with sign_n), updates U, runs con2prim with the
+//            PhysPressureFix fallback and writes U, W and a status byte.
+// No atomics touch the state; the max signal speed and the fallback counts are
+// reduced per CTA and combined with one atomic per CTA.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -34,6 +38,9 @@ struct StepParams {
   int N;
   int cpb;
   const int32_t *__restrict__ off;
+  const int32_t *__restrict__ halo_off;
+  const int32_t *__restrict__ halo_ids;
+  int max_halo;
   const int2 *__restrict__ lr;
   const double4 *__restrict__ nS;
   const int32_t *__restrict__ gid;
@@ -123,16 +130,65 @@ __device__ __forceinline__ void boundary(const BcTable &bc, int code, const doub
 }
 
 constexpr int kStepThreads = 256;
+constexpr int kMaxCellsPerBlock = 1024;  // local cell index fits 12 bits
 
-__global__ void __launch_bounds__(kStepThreads) k_hydro_step(const StepParams P) {
-  extern __shared__ double sflux[];
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void load_state_smem(const double *s, int slot, double *U, double *W) {
+  const double2 *p = reinterpret_cast<const double2 *>(s + 10 * slot);
+  const double2 a = p[0], b = p[1], d = p[2], e = p[3], f = p[4];
+  U[0] = a.x;
+  U[1] = a.y;
+  U[2] = b.x;
+  U[3] = b.y;
+  U[4] = d.x;
+  W[0] = d.y;
+  W[1] = e.x;
+  W[2] = e.y;
+  W[3] = f.x;
+  W[4] = f.y;
+}
+
+#ifndef RRHD_STEP_MIN_BLOCKS
+#define RRHD_STEP_MIN_BLOCKS 3  // CTAs per SM the register budget is sized for
+#endif
+__global__ void __launch_bounds__(kStepThreads, RRHD_STEP_MIN_BLOCKS) k_hydro_step(const StepParams P) {
+  extern __shared__ double2 smem_raw[];
+  double *sstate = reinterpret_cast<double *>(smem_raw);  // [cpb + max_halo][10]
+  double *sflux = sstate + 10 * (P.cpb + P.max_halo);     // [entries][5]
   __shared__ double s_red[kStepThreads / 32];
   __shared__ unsigned long long s_cnt[2];
+  __shared__ unsigned short s_fail[kMaxCellsPerBlock];
+  __shared__ int s_nfail;
   const int b = blockIdx.x;
+  const int c0 = b * P.cpb;
+  const int nc = min(P.cpb, P.N - c0);
   const int e0 = P.off[b], e1 = P.off[b + 1];
+  const int h0 = P.halo_off[b], h1 = P.halo_off[b + 1];
   double tau = P.tau;
   if (P.device_tau) tau = P.cfl_hmin / P.prev->max_speed;
   if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0;
+  if (threadIdx.x == 0) s_nfail = 0;
+
+  // phase 0: stage own (contiguous) and halo states, 16 bytes per request
+  {
+    const char *g = reinterpret_cast<const char *>(P.sin);
+    char *sm = reinterpret_cast<char *>(sstate);
+    for (int q = threadIdx.x; q < nc * 5; q += kStepThreads)
+      cp_async16(sm + 16 * q, g + 80 * (size_t)c0 + 16 * q);
+    for (int q = threadIdx.x; q < (h1 - h0) * 5; q += kStepThreads) {
+      const int h = q / 5, k = q - 5 * h;
+      cp_async16(sm + 80 * (P.cpb + h) + 16 * k, g + 80 * (size_t)P.halo_ids[h0 + h] + 16 * k);
+    }
+    cp_async_wait_all();
+  }
+  __syncthreads();
 
   // phase 1: every face touching this CTA's cells
   double vmax = 0.0;
@@ -140,9 +196,9 @@ __global__ void __launch_bounds__(kStepThreads) k_hydro_step(const StepParams P)
     const int2 lr = P.lr[e];
     const double4 g = P.nS[e];
     double UL[5], WL[5], UR[5], WR[5], Fl[5];
-    load_state(P.sin, lr.x, UL, WL);
+    load_state_smem(sstate, lr.x, UL, WL);
     if (lr.y >= 0)
-      load_state(P.sin, lr.y, UR, WR);
+      load_state_smem(sstate, lr.y, UR, WR);
     else
       boundary(P.bc, lr.y, g, UL, WL, UR, WR);
     const double s = hllc_flux(P.eos, UL, UR, WL, WR, g.x, g.y, g.z, g.w, Fl);
@@ -160,11 +216,11 @@ __global__ void __launch_bounds__(kStepThreads) k_hydro_step(const StepParams P)
   }
   __syncthreads();
 
-  // phase 2: gather, update, con2prim
+  // phase 2: gather, update, con2prim.  Cells whose con2prim fails keep their
+  // updated U and old W in the staging slot for the fallback pass below.
   unsigned n_fb = 0, n_fail = 0;
-  for (int cl = threadIdx.x; cl < P.cpb; cl += kStepThreads) {
-    const int c = b * P.cpb + cl;
-    if (c >= P.N) break;
+  for (int cl = threadIdx.x; cl < nc; cl += kStepThreads) {
+    const int c = c0 + cl;
     const ushort4 sl = P.slot[c];
     const unsigned sg = P.sign[c];
     const unsigned short sls[4] = {sl.x, sl.y, sl.z, sl.w};
@@ -182,14 +238,29 @@ __global__ void __launch_bounds__(kStepThreads) k_hydro_step(const StepParams P)
     }
     const double sc = (tau / P.V[c]);
     double U[5], W[5];
-    load_state(P.sin, c, U, W);
+    load_state_smem(sstate, cl, U, W);
 #pragma unroll
     for (int i = 0; i < 5; i++) U[i] -= sum[i] * sc;
-    const uint8_t st = c2p_with_fix(P.eos, U, W);
-    store_state(P.sout, c, U, W);
-    P.status[c] = st;
-    n_fb += (st & RRHD_STATUS_FALLBACK) ? 1u : 0u;
-    n_fail += (st & RRHD_STATUS_FAILED) ? 1u : 0u;
+    const int code = c2p(P.eos, U, W);
+    if (code) {
+      store_state(sstate, cl, U, W);
+      s_fail[atomicAdd(&s_nfail, 1)] = (unsigned short)(cl | (code << 12));
+    } else {
+      store_state(P.sout, c, U, W);
+      P.status[c] = 0;
+    }
+  }
+  __syncthreads();
+  // fallback pass: rhllc::PhysPressureFix where con2prim failed (rare)
+  for (int i = threadIdx.x; i < s_nfail; i += kStepThreads) {
+    const int cl = s_fail[i] & 0xfff, code = s_fail[i] >> 12;
+    double U[5], W[5];
+    load_state_smem(sstate, cl, U, W);
+    const int fix = pressure_fix(P.eos, U, W);
+    store_state(P.sout, c0 + cl, U, W);
+    P.status[c0 + cl] = (uint8_t)(code | RRHD_STATUS_FALLBACK | (fix ? RRHD_STATUS_FAILED : 0));
+    n_fb += 1;
+    n_fail += fix ? 1u : 0u;
   }
 
   // CTA reduction of the max speed and the counters
@@ -313,7 +384,7 @@ rrhd_status upload(T **dst, const std::vector<T> &src) {
 void free_ctx(rrhd_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
-  void *ptrs[] = {c->d_perm, c->d_iperm, c->d_bface_off, c->d_bface_lr, c->d_bface_nS,
+  void *ptrs[] = {c->d_perm, c->d_iperm, c->d_bface_off, c->d_bface_lr, c->d_bface_nS, c->d_halo_off, c->d_halo_ids,
                   c->d_bface_gid, c->d_cell_slot, c->d_cell_sign, c->d_cell_V, c->d_state[0],
                   c->d_state[1], c->d_status, c->d_scal, c->d_face_flux, c->d_scratch_io};
   for (void *p : ptrs)
@@ -401,10 +472,23 @@ extern "C" rrhd_status rrhd_create(const rrhd_mesh_desc *m, const rrhd_opts *opt
   std::vector<uint8_t> sign(N);
   std::vector<double> vol(N);
   std::vector<int32_t> stamp(F, -1), local(F, 0);
-  int max_e = 0;
+  std::vector<int32_t> hstamp(N, -1), hlocal(N, 0);
+  std::vector<int32_t> hoff(nb + 1, 0), hids;
+  hids.reserve((size_t)(N / 2));
+  int max_e = 0, max_h = 0;
   for (int b = 0; b < nb; b++) {
-    int ne = 0;
+    int ne = 0, nh = 0;
     const int64_t c0 = (int64_t)b * cpb, c1 = std::min<int64_t>(N, c0 + cpb);
+    // CTA-local state slot of a cell: own cells first, then the halo
+    auto slot_of = [&](int32_t x) -> int32_t {
+      if (x >= c0 && x < c1) return (int32_t)(x - c0);
+      if (hstamp[x] != b) {
+        hstamp[x] = b;
+        hlocal[x] = nh++;
+        hids.push_back(x);
+      }
+      return cpb + hlocal[x];
+    };
     for (int64_t cn = c0; cn < c1; cn++) {
       const int32_t co = perm[cn];
       unsigned short s4[4];
@@ -415,7 +499,9 @@ extern "C" rrhd_status rrhd_create(const rrhd_mesh_desc *m, const rrhd_opts *opt
           local[f] = ne++;
           const int32_t l = iperm[m->face_id_l[f]];
           const int32_t r = m->face_id_r[f] >= 0 ? iperm[m->face_id_r[f]] : m->face_id_r[f];
-          lr.push_back(make_int2(l, r));
+          const int32_t ls = slot_of(l);
+          const int32_t rs = r >= 0 ? slot_of(r) : r;
+          lr.push_back(make_int2(ls, rs));
           nS.push_back(make_double4(m->face_n[3 * f], m->face_n[3 * f + 1], m->face_n[3 * f + 2],
                                     m->face_area[f]));
           gid.push_back((l / cpb == b) ? f : -1);
@@ -428,8 +514,11 @@ extern "C" rrhd_status rrhd_create(const rrhd_mesh_desc *m, const rrhd_opts *opt
     }
     if (ne > 65535) return fail(rrhd_fail(RRHD_ERR_LIMIT, "CTA face list too long"));
     max_e = std::max(max_e, ne);
+    max_h = std::max(max_h, nh);
     off[b + 1] = off[b] + ne;
+    hoff[b + 1] = hoff[b] + nh;
   }
+  c->max_halo = max_h;
   c->max_entries = max_e;
   c->n_entries = off[nb];
   c->h_perm = perm;
@@ -437,7 +526,8 @@ extern "C" rrhd_status rrhd_create(const rrhd_mesh_desc *m, const rrhd_opts *opt
       (st = upload(&c->d_bface_off, off)) || (st = upload(&c->d_bface_lr, lr)) ||
       (st = upload(&c->d_bface_nS, nS)) || (st = upload(&c->d_bface_gid, gid)) ||
       (st = upload(&c->d_cell_slot, slot)) || (st = upload(&c->d_cell_sign, sign)) ||
-      (st = upload(&c->d_cell_V, vol)))
+      (st = upload(&c->d_cell_V, vol)) || (st = upload(&c->d_halo_off, hoff)) ||
+      (st = upload(&c->d_halo_ids, hids)))
     return fail(st);
   const size_t ssz = sizeof(double) * 10 * N;
   if (cudaMalloc(&c->d_state[0], ssz) != cudaSuccess || cudaMalloc(&c->d_state[1], ssz) != cudaSuccess ||
@@ -451,10 +541,13 @@ extern "C" rrhd_status rrhd_create(const rrhd_mesh_desc *m, const rrhd_opts *opt
   cudaMemcpy(c->d_scal, init, sizeof init, cudaMemcpyHostToDevice);
   c->scal_cur = 0;
   for (int k = 0; k < 8; k++) c->bc.kind[k] = RRHD_BC_TRANSMISSIVE;
-  const size_t smem = sizeof(double) * 5 * (size_t)max_e;
-  if (smem > 48 * 1024 &&
-      cudaFuncSetAttribute(k_hydro_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-    return fail(rrhd_fail(RRHD_ERR_LIMIT, "CTA face list needs %zu B of shared memory", smem));
+  // staged states (own + halo) and the CTA's face fluxes
+  const size_t smem = sizeof(double) * (10 * (size_t)(cpb + max_h) + 5 * (size_t)max_e);
+  c->step_smem = smem;
+  if (smem > 227 * 1024)
+    return fail(rrhd_fail(RRHD_ERR_LIMIT, "step needs %zu B of shared memory per CTA; lower cells_per_block", smem));
+  if (cudaFuncSetAttribute(k_hydro_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return fail(rrhd_fail(RRHD_ERR_LIMIT, "cannot reserve %zu B of shared memory", smem));
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(rrhd_fail(RRHD_ERR_CUDA, "%s", cudaGetErrorString(cudaGetLastError())));
   *out = c;
   return RRHD_OK;
@@ -583,6 +676,9 @@ extern "C" rrhd_status rrhd_hydro_step(rrhd_ctx *c, double tau, rrhd_step_stats 
   P.N = (int)c->N;
   P.cpb = c->cpb;
   P.off = c->d_bface_off;
+  P.halo_off = c->d_halo_off;
+  P.halo_ids = c->d_halo_ids;
+  P.max_halo = c->max_halo;
   P.lr = c->d_bface_lr;
   P.nS = c->d_bface_nS;
   P.gid = c->d_bface_gid;
@@ -600,8 +696,7 @@ extern "C" rrhd_status rrhd_hydro_step(rrhd_ctx *c, double tau, rrhd_step_stats 
   P.cfl_hmin = c->cfl * c->h_min;
   P.bc = c->bc;
   RRHD_CUDA(cudaMemsetAsync(P.out, 0, sizeof(StepScalars), c->stream));
-  const size_t smem = sizeof(double) * 5 * (size_t)c->max_entries;
-  k_hydro_step<<<c->nblocks, kStepThreads, smem, c->stream>>>(P);
+  k_hydro_step<<<c->nblocks, kStepThreads, c->step_smem, c->stream>>>(P);
   RRHD_CUDA(cudaGetLastError());
   c->cur ^= 1;
   c->scal_cur ^= 1;

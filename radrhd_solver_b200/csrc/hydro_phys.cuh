@@ -117,7 +117,7 @@ __device__ __forceinline__ double dh_fix(const Eos &e, double D, double plor, do
 }
 
 // PhysPressureFix, rhllc_flux_stab.cpp:40-121 (rewrites U[4]).
-__device__ __noinline__ int pressure_fix(const Eos &e, double *U, double *W) {
+__device__ __forceinline__ int pressure_fix(const Eos &e, double *U, double *W) {
   const double p = 1e-12;  // kMinPressure
   const double D = U[0];
   const double m2 = dot3(U[1], U[2], U[3], U[1], U[2], U[3]);

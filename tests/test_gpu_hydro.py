@@ -93,6 +93,25 @@ def test_shock_tube_steps_bitexact(cpb):
     g.close()
 
 
+def test_step_fallback_path_bitexact():
+    """Cells whose con2prim fails inside the step take the PhysPressureFix
+    fallback pass; state and status bytes equal the oracle's."""
+    m, W = shock_tube(24, 3, 3, seed=6)
+    W[:, 1] = 0.5
+    W, U = oracle.port_p2c(W, 1, GAMMA_53)
+    bad = np.arange(0, m.n_cells, 17)
+    U[bad, 4] = np.sqrt((U[bad, 1:4] ** 2).sum(1) + U[bad, 0] ** 2) * 0.97  # no solution after the update
+    g = _grid(m, GAMMA_53)
+    g.set_state(W, U)
+    tau = 0.1 * m.h_min
+    st = rhllc.Hllc3dStab(tau, g)
+    U2, W2, _, status, v = oracle.port_hydro_step(m, U, W, tau, 1, GAMMA_53)
+    assert (status & 0x10).sum() > 0 and st.n_fallback == (status & 0x10).astype(bool).sum()
+    Wg, Ug = g.get_state()
+    assert np.array_equal(Ug, U2) and np.array_equal(Wg, W2)
+    assert np.array_equal(g.cell_status().astype(np.int32), status)
+
+
 def test_taub_eos_steps_bitexact():
     m, W = shock_tube(24, 3, 3, seed=4)
     W[:, 1] = 0.3  # moving gas
