@@ -159,6 +159,24 @@ rrhd_status rrhd_get_cell_status(rrhd_ctx *ctx, uint8_t *status);
  * rewrites U.E as the reference does.  status [n] may be NULL. */
 rrhd_status rrhd_con2prim_batch(int32_t eos, double gamma, double *U, double *W, uint8_t *status,
                                 int64_t n, int32_t fallback, void *stream);
+/* Totals over a con2prim batch. */
+typedef struct {
+  int64_t n_ok;         /* states solved by the Newton iteration                 */
+  int64_t n_fallback;   /* states that went to PhysPressureFix                   */
+  int64_t n_failed;     /* states where the fallback failed too (or no fallback) */
+  int64_t newton_iters; /* Newton iterations summed over all states              */
+  int32_t max_iters;    /* largest Newton iteration count of one state           */
+} rrhd_c2p_stats;
+
+/* rrhd_con2prim_batch plus the totals above, reduced per CTA into a device
+ * scratch buffer (one per device, allocated on first use) and then summed in a
+ * fixed order.  Synchronises `stream` when stats is not NULL.  Same reference
+ * functions as rrhd_con2prim_batch (rhllc::GetPhysValueStab / PhysPressureFix);
+ * the iteration counts are those of the loop at rhllc_flux_stab.cpp:153-183. */
+rrhd_status rrhd_con2prim_batch_stats(int32_t eos, double gamma, double *U, double *W,
+                                      uint8_t *status, int64_t n, int32_t fallback,
+                                      rrhd_c2p_stats *stats, void *stream);
+
 /* prim->cons for n states, device pointers: rhllc::GetConvValueStab. */
 rrhd_status rrhd_prim2con_batch(int32_t eos, double gamma, double *W, double *U, int64_t n,
                                 void *stream);

@@ -55,6 +55,10 @@ class StepStats(C.Structure):
     _fields_ = [("max_speed", D), ("n_fallback", I64), ("n_failed", I64)]
 
 
+class C2pStats(C.Structure):
+    _fields_ = [("n_ok", I64), ("n_fallback", I64), ("n_failed", I64), ("newton_iters", I64), ("max_iters", I32)]
+
+
 class KuhnParams(C.Structure):
     _fields_ = [("nx", I32), ("ny", I32), ("nz", I32), ("lo", D * 3), ("hi", D * 3), ("jitter", D),
                 ("seed", U64), ("bc_code", I32 * 6), ("inflow_radius", D), ("inflow_code", I32)]
@@ -82,6 +86,7 @@ _SIGS = {
     "rrhd_get_cell_status": (I32, [P, P]),
     "rrhd_con2prim_batch": (I32, [I32, D, P, P, P, I64, I32, P]),
     "rrhd_prim2con_batch": (I32, [I32, D, P, P, I64, P]),
+    "rrhd_con2prim_batch_stats": (I32, [I32, D, P, P, P, I64, I32, P, P]),
     "rrhd_dirs_create": (I32, [I32, P, P, D, I32, P]),
     "rrhd_dirs_destroy": (I32, [P]),
     "rrhd_dirs_count": (I32, [P]),

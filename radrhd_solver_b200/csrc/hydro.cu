@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -340,6 +341,106 @@ __global__ void k_c2p_batch(Eos eos, double *U, double *W, uint8_t *status, int6
   }
   for (int k = 0; k < 5; k++) W[5 * i + k] = w[k];
   if (status) status[i] = (uint8_t)code;
+}
+
+// con2prim with per-CTA statistics.  Each CTA handles kC2pPerBlock states and
+// writes one partial record (ok, fallback, failed, Newton iterations, max
+// iterations) to scratch[blockIdx.x]; k_c2p_stats_reduce sums the partials in a
+// fixed order into scratch[nblocks], so the totals do not depend on scheduling.
+constexpr int kC2pThreads = 256;
+constexpr int kC2pPerThread = 8;
+constexpr int kC2pPerBlock = kC2pThreads * kC2pPerThread;
+
+struct C2pPartial {
+  unsigned long long ok, fallback, failed, iters, max_iters;
+};
+
+__global__ void __launch_bounds__(kC2pThreads) k_c2p_stats(Eos eos, double *U, double *W, uint8_t *status,
+                                                          int64_t n, int fallback, C2pPartial *scratch) {
+  unsigned long long ok = 0, fb = 0, failed = 0, iters = 0, mx = 0;
+  const int64_t base = (int64_t)blockIdx.x * kC2pPerBlock;
+  for (int k = 0; k < kC2pPerThread; k++) {
+    const int64_t i = base + k * kC2pThreads + threadIdx.x;
+    if (i >= n) break;
+    double u[5], w[5];
+    for (int q = 0; q < 5; q++) {
+      u[q] = U[5 * i + q];
+      w[q] = W[5 * i + q];
+    }
+    int it = 0;
+    int code = c2p_from(eos, u, w, 0.0, false, &it);
+    iters += (unsigned long long)it;
+    mx = (unsigned long long)it > mx ? (unsigned long long)it : mx;
+    if (code == 0) {
+      ok++;
+    } else if (fallback) {
+      const int fix = pressure_fix(eos, u, w);
+      code = code | 0x10 | (fix ? 0x20 : 0);
+      fb++;
+      failed += fix ? 1 : 0;
+      for (int q = 0; q < 5; q++) U[5 * i + q] = u[q];
+    } else {
+      failed++;
+    }
+    for (int q = 0; q < 5; q++) W[5 * i + q] = w[q];
+    if (status) status[i] = (uint8_t)code;
+  }
+  __shared__ unsigned long long red[5][kC2pThreads / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ok += __shfl_xor_sync(0xffffffffu, ok, o);
+    fb += __shfl_xor_sync(0xffffffffu, fb, o);
+    failed += __shfl_xor_sync(0xffffffffu, failed, o);
+    iters += __shfl_xor_sync(0xffffffffu, iters, o);
+    const unsigned long long m2 = __shfl_xor_sync(0xffffffffu, mx, o);
+    mx = m2 > mx ? m2 : mx;
+  }
+  const int wid = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    red[0][wid] = ok;
+    red[1][wid] = fb;
+    red[2][wid] = failed;
+    red[3][wid] = iters;
+    red[4][wid] = mx;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    C2pPartial p = {0, 0, 0, 0, 0};
+    for (int w2 = 0; w2 < kC2pThreads / 32; w2++) {
+      p.ok += red[0][w2];
+      p.fallback += red[1][w2];
+      p.failed += red[2][w2];
+      p.iters += red[3][w2];
+      p.max_iters = red[4][w2] > p.max_iters ? red[4][w2] : p.max_iters;
+    }
+    scratch[blockIdx.x] = p;
+  }
+}
+
+__global__ void k_c2p_stats_reduce(C2pPartial *scratch, int nblocks) {
+  __shared__ C2pPartial red[256];
+  C2pPartial p = {0, 0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nblocks; b += 256) {
+    const C2pPartial q = scratch[b];
+    p.ok += q.ok;
+    p.fallback += q.fallback;
+    p.failed += q.failed;
+    p.iters += q.iters;
+    p.max_iters = q.max_iters > p.max_iters ? q.max_iters : p.max_iters;
+  }
+  red[threadIdx.x] = p;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    C2pPartial t = {0, 0, 0, 0, 0};
+    for (int k = 0; k < 256; k++) {
+      t.ok += red[k].ok;
+      t.fallback += red[k].fallback;
+      t.failed += red[k].failed;
+      t.iters += red[k].iters;
+      t.max_iters = red[k].max_iters > t.max_iters ? red[k].max_iters : t.max_iters;
+    }
+    scratch[nblocks] = t;
+  }
 }
 
 __global__ void k_p2c_batch(Eos eos, double *W, double *U, int64_t n) {
@@ -758,7 +859,7 @@ extern "C" rrhd_status rrhd_get_cell_status(rrhd_ctx *c, uint8_t *status) {
 
 extern "C" rrhd_status rrhd_con2prim_batch(int32_t eos, double gamma, double *U, double *W, uint8_t *status,
                                            int64_t n, int32_t fallback, void *stream) {
-  RRHD_CHECK_ARG(U && W && n >= 0, "bad arguments");
+  RRHD_CHECK_ARG(n >= 0 && ((U && W) || n == 0), "bad arguments");
   RRHD_CHECK_ARG(eos == RRHD_EOS_IDEAL || eos == RRHD_EOS_TAUB, "bad eos");
   if (n == 0) return RRHD_OK;
   k_c2p_batch<<<grid1d(n, 128), 128, 0, (cudaStream_t)stream>>>(make_eos(eos, gamma), U, W, status, n, fallback);
@@ -768,10 +869,68 @@ extern "C" rrhd_status rrhd_con2prim_batch(int32_t eos, double gamma, double *U,
 
 extern "C" rrhd_status rrhd_prim2con_batch(int32_t eos, double gamma, double *W, double *U, int64_t n,
                                            void *stream) {
-  RRHD_CHECK_ARG(U && W && n >= 0, "bad arguments");
+  RRHD_CHECK_ARG(n >= 0 && ((U && W) || n == 0), "bad arguments");
   RRHD_CHECK_ARG(eos == RRHD_EOS_IDEAL || eos == RRHD_EOS_TAUB, "bad eos");
   if (n == 0) return RRHD_OK;
   k_p2c_batch<<<grid1d(n, 256), 256, 0, (cudaStream_t)stream>>>(make_eos(eos, gamma), W, U, n);
   RRHD_CUDA(cudaGetLastError());
   return RRHD_OK;
+}
+
+// Scratch of rrhd_con2prim_batch_stats: one buffer per device, allocated on
+// first use and grown when a larger batch needs more partial records.
+namespace {
+std::mutex g_c2p_scratch_mu;
+C2pPartial *g_c2p_scratch[64] = {nullptr};
+int64_t g_c2p_scratch_cap[64] = {0};
+
+rrhd_status c2p_stats_launch(Eos eos, double *U, double *W, uint8_t *status, int64_t n, int32_t fallback,
+                             C2pPartial *scratch, rrhd_c2p_stats *stats, cudaStream_t stream) {
+  const int64_t nb = (n + kC2pPerBlock - 1) / kC2pPerBlock;
+  if (nb > 0) {
+    k_c2p_stats<<<(unsigned)nb, kC2pThreads, 0, stream>>>(eos, U, W, status, n, fallback, scratch);
+    RRHD_CUDA(cudaGetLastError());
+  }
+  k_c2p_stats_reduce<<<1, 256, 0, stream>>>(scratch, (int)nb);
+  RRHD_CUDA(cudaGetLastError());
+  if (stats) {
+    C2pPartial t;
+    RRHD_CUDA(cudaMemcpyAsync(&t, scratch + nb, sizeof t, cudaMemcpyDeviceToHost, stream));
+    RRHD_CUDA(cudaStreamSynchronize(stream));
+    stats->n_ok = (int64_t)t.ok;
+    stats->n_fallback = (int64_t)t.fallback;
+    stats->n_failed = (int64_t)t.failed;
+    stats->newton_iters = (int64_t)t.iters;
+    stats->max_iters = (int32_t)t.max_iters;
+  }
+  return RRHD_OK;
+}
+}  // namespace
+
+extern "C" rrhd_status rrhd_con2prim_batch_stats(int32_t eos, double gamma, double *U, double *W,
+                                                 uint8_t *status, int64_t n, int32_t fallback,
+                                                 rrhd_c2p_stats *stats, void *stream) {
+  RRHD_CHECK_ARG(n >= 0 && ((U && W) || n == 0), "bad arguments");
+  RRHD_CHECK_ARG(eos == RRHD_EOS_IDEAL || eos == RRHD_EOS_TAUB, "bad eos");
+  int dev = 0;
+  RRHD_CUDA(cudaGetDevice(&dev));
+  RRHD_CHECK_ARG(dev >= 0 && dev < 64, "device ordinal out of range");
+  const int64_t need = (n + kC2pPerBlock - 1) / kC2pPerBlock + 1;
+  C2pPartial *scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_c2p_scratch_mu);
+    if (g_c2p_scratch_cap[dev] < need) {
+      if (g_c2p_scratch[dev]) {
+        RRHD_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+        cudaFree(g_c2p_scratch[dev]);
+        g_c2p_scratch[dev] = nullptr;
+        g_c2p_scratch_cap[dev] = 0;
+      }
+      const int64_t cap = std::max<int64_t>(need, 1024);
+      RRHD_CUDA(cudaMalloc(&g_c2p_scratch[dev], sizeof(C2pPartial) * cap));
+      g_c2p_scratch_cap[dev] = cap;
+    }
+    scratch = g_c2p_scratch[dev];
+  }
+  return c2p_stats_launch(make_eos(eos, gamma), U, W, status, n, fallback, scratch, stats, (cudaStream_t)stream);
 }

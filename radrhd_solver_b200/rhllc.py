@@ -141,6 +141,16 @@ def GetPhysValueStab(U, W, status=None, eos: int = EOS_IDEAL, gamma: float = 5.0
                                       stream), "GetPhysValueStab")
 
 
+def GetPhysValueStabStats(U, W, status=None, eos: int = EOS_IDEAL, gamma: float = 5.0 / 3.0,
+                          fallback: bool = True, stream=None) -> L.C2pStats:
+    """Batched con2prim with totals (solved, fallbacks, failures, Newton
+    iterations); synchronises the stream."""
+    st = L.C2pStats()
+    L.check(L.lib.rrhd_con2prim_batch_stats(eos, gamma, L.ptr(U), L.ptr(W), L.ptr(status), U.shape[0],
+                                            1 if fallback else 0, C.byref(st), stream), "GetPhysValueStabStats")
+    return st
+
+
 def GetConvValueStab(W, U, eos: int = EOS_IDEAL, gamma: float = 5.0 / 3.0, stream=None):
     """Batched prim->cons on device tensors [n,5] (rhllc_flux_stab.cpp:10-38)."""
     L.check(L.lib.rrhd_prim2con_batch(eos, gamma, L.ptr(W), L.ptr(U), W.shape[0], stream), "GetConvValueStab")

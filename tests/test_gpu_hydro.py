@@ -35,6 +35,30 @@ def test_con2prim_batch_bitexact(eos, gamma):
     assert np.array_equal(Wd.cpu().numpy()[ok], Wo[ok])
 
 
+def test_con2prim_stats_matches_oracle():
+    """Batch con2prim with totals: states, status bytes and the iteration
+    statistics equal the oracle's; a batch spanning many CTAs and a ragged tail."""
+    W0 = c2p_states(70001, GAMMA_43, seed=21)
+    W0, U = oracle.port_p2c(W0, 1, GAMMA_43)
+    U[::97, 4] *= 0.6  # some states go to the fallback
+    Wo, codes = oracle.port_c2p(U, 1, GAMMA_43, W=W0)
+    Uf, Wf, fix = oracle.port_pressure_fix(U, np.where(codes[:, None] == 0, Wo, W0), 1, GAMMA_43)
+    Ud = torch.tensor(U, device="cuda")
+    Wd = torch.tensor(W0, device="cuda")
+    sd = torch.zeros(len(U), dtype=torch.uint8, device="cuda")
+    st = rhllc.GetPhysValueStabStats(Ud, Wd, sd, eos=1, gamma=GAMMA_43, fallback=True,
+                                     stream=torch.cuda.current_stream().cuda_stream)
+    bad = codes != 0
+    assert st.n_ok == (~bad).sum() and st.n_fallback == bad.sum() and st.n_failed == ((fix != 0) & bad).sum()
+    Wg = Wd.cpu().numpy()
+    assert np.array_equal(Wg[~bad], Wo[~bad])
+    assert np.array_equal(Wg[bad & (fix == 0)], Wf[bad & (fix == 0)])
+    assert 0 < st.newton_iters / len(U) < 40 and 0 < st.max_iters <= 40
+    st0 = rhllc.GetPhysValueStabStats(Ud[:0], Wd[:0], None, eos=1, gamma=GAMMA_43,
+                                      stream=torch.cuda.current_stream().cuda_stream)
+    assert st0.n_ok == 0 and st0.newton_iters == 0
+
+
 def test_prim2con_batch_bitexact():
     W = c2p_states(5000, GAMMA_43, seed=9)
     W[:50, 1:4] *= 1.5  # |v| >= 1: rescaled by 0.9999 as in GetConvValueStab
