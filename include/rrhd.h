@@ -177,6 +177,20 @@ rrhd_status rrhd_con2prim_batch_stats(int32_t eos, double gamma, double *U, doub
                                       uint8_t *status, int64_t n, int32_t fallback,
                                       rrhd_c2p_stats *stats, void *stream);
 
+/* The same computation as rrhd_con2prim_batch_stats without allocating any
+ * device memory (no counterpart in the reference).  For callers that cannot
+ * call cudaMalloc: hosts whose memory pool or arena already reserves the GPU,
+ * and latency-critical loops that cannot take cudaMalloc's implicit device
+ * synchronisation.  The per-CTA partial totals live in a fixed file-scope
+ * device array of 320 KiB, held by every GPU that loads the library until the
+ * process exits, so n is limited to 16,777,216 states (RRHD_ERR_LIMIT beyond).
+ * The first call on a device looks up that array's device address (make it
+ * before any stream capture).  Every call shares the array: calls that overlap
+ * on the GPU race and must be serialised by the caller. */
+rrhd_status rrhd_con2prim_batch_stats_noalloc(int32_t eos, double gamma, double *U, double *W,
+                                              uint8_t *status, int64_t n, int32_t fallback,
+                                              rrhd_c2p_stats *stats, void *stream);
+
 /* prim->cons for n states, device pointers: rhllc::GetConvValueStab. */
 rrhd_status rrhd_prim2con_batch(int32_t eos, double gamma, double *W, double *U, int64_t n,
                                 void *stream);

@@ -934,3 +934,53 @@ extern "C" rrhd_status rrhd_con2prim_batch_stats(int32_t eos, double gamma, doub
   }
   return c2p_stats_launch(make_eos(eos, gamma), U, W, status, n, fallback, scratch, stats, (cudaStream_t)stream);
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of rrhd_con2prim_batch_stats.
+//
+// For callers that must not allocate device memory themselves: hosts whose
+// memory pool or arena reserves the whole GPU (a cudaMalloc would fail or
+// bypass their accounting), and latency-critical loops that cannot accept
+// cudaMalloc's implicit device synchronisation.  The per-CTA partial records
+// live in the file-scope array below, which every GPU that loads this library
+// holds until the process exits.
+//
+// Host code cannot use the array's name as a device address (it is a host-side
+// stand-in), so the first call on each device looks the address up with
+// cudaGetSymbolAddress while that device is current and caches it; make that
+// first call before any stream capture.  All calls share the array and it keeps
+// the last call's contents: every call rewrites all the records it reads (one
+// per CTA, then the total), so nothing has to be cleared, but calls that
+// overlap on the GPU (concurrent streams) race on it and must be serialised.
+constexpr int kNoallocMaxBlocks = 8192;
+constexpr int64_t kNoallocMaxStates = (int64_t)kNoallocMaxBlocks * kC2pPerBlock;  // 16,777,216
+static __device__ __align__(256) C2pPartial g_c2p_noalloc_scratch[kNoallocMaxBlocks + 1];  // 320 KiB
+
+namespace {
+std::mutex g_noalloc_mu;
+C2pPartial *g_noalloc_addr[64] = {nullptr};
+}  // namespace
+
+extern "C" rrhd_status rrhd_con2prim_batch_stats_noalloc(int32_t eos, double gamma, double *U, double *W,
+                                                         uint8_t *status, int64_t n, int32_t fallback,
+                                                         rrhd_c2p_stats *stats, void *stream) {
+  RRHD_CHECK_ARG(n >= 0 && ((U && W) || n == 0), "bad arguments");
+  RRHD_CHECK_ARG(eos == RRHD_EOS_IDEAL || eos == RRHD_EOS_TAUB, "bad eos");
+  if (n > kNoallocMaxStates)
+    return rrhd_fail(RRHD_ERR_LIMIT, "rrhd_con2prim_batch_stats_noalloc: %lld states exceed the fixed maximum of %lld",
+                     (long long)n, (long long)kNoallocMaxStates);
+  int dev = 0;
+  RRHD_CUDA(cudaGetDevice(&dev));
+  RRHD_CHECK_ARG(dev >= 0 && dev < 64, "device ordinal out of range");
+  C2pPartial *scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void *addr = nullptr;
+      RRHD_CUDA(cudaGetSymbolAddress(&addr, g_c2p_noalloc_scratch));
+      g_noalloc_addr[dev] = reinterpret_cast<C2pPartial *>(addr);
+    }
+    scratch = g_noalloc_addr[dev];
+  }
+  return c2p_stats_launch(make_eos(eos, gamma), U, W, status, n, fallback, scratch, stats, (cudaStream_t)stream);
+}
