@@ -231,6 +231,32 @@ const double *rrhd_dirs_device_kernel(const rrhd_dirs *d);
 rrhd_status rrhd_moments_fp64(const rrhd_dirs *d, const double *I, double *E, double *F,
                               double *T, int64_t rows, void *stream);
 
+/* Scattering integral and moments on the tensor cores (tcgen05), FP32 in/out.
+ * The same contraction as rrhd_scatter_fp64 plus the moments as 16 extra
+ * output columns, with the kernel matrix split into 16-bit parts once at
+ * creation.  Forms (error against FP64 measured by the tests):
+ *   RRHD_TC_BF16X3 : bf16 hi/lo split of I and K, three products
+ *   RRHD_TC_F16X3  : per-row power-of-two scaled fp16 hi/lo split, three products
+ *   RRHD_TC_F16    : per-row scaled fp16, one product
+ *   RRHD_TC_BF16   : bf16, one product
+ * M must be 64, 128, 192, 256 or a multiple of 256 (<= 1024).  Stands behind
+ * CalculateIntScatteringAsync + CalculateAllParamAsync (cuda_multi_interface.h:69, :81). */
+#define RRHD_TC_BF16X3 0
+#define RRHD_TC_F16X3 1
+#define RRHD_TC_F16 2
+#define RRHD_TC_BF16 3
+typedef struct rrhd_scatter_tc rrhd_scatter_tc;
+rrhd_status rrhd_scatter_tc_create(const rrhd_dirs *d, int32_t form, rrhd_scatter_tc **out);
+rrhd_status rrhd_scatter_tc_destroy(rrhd_scatter_tc *t);
+/* I [rows][M] FP32 -> S [rows][M] FP32 and, when moments is not NULL, moments
+ * [rows][16] FP32 = {E, Fx, Fy, Fz, Txx, Txy, Txz, Tyy, Tyz, Tzz, 0...}.  All
+ * device pointers, 16-byte aligned. */
+rrhd_status rrhd_scatter_tc_run(const rrhd_scatter_tc *t, const float *I, float *S, float *moments,
+                                int64_t rows, void *stream);
+/* Reads (and with clear != 0 resets) the error word of the tensor-core kernels:
+ * RRHD_ERR_CUDA if a bounded pipeline wait timed out.  Synchronises `stream`. */
+rrhd_status rrhd_scatter_tc_check(const rrhd_scatter_tc *t, void *stream, int32_t clear);
+
 /* Emission constants of rad_rhd::GetRadSource: T = temp_coef*p/rho,
  * B = T^4*sigma_sb/pi, q = -alpha*rho*B/rad_unit (lib/physics/src/plunk.cpp:87-90,
  * lib/physics/include/gas_state.h:22-27).  rrhd_emission_reference() gives the

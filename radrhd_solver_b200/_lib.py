@@ -37,6 +37,10 @@ RRHD_EOS_TAUB = 2
 RRHD_BC_TRANSMISSIVE = 0
 RRHD_BC_FIXED = 1
 RRHD_BC_REFLECT = 2
+RRHD_TC_BF16X3 = 0
+RRHD_TC_F16X3 = 1
+RRHD_TC_F16 = 2
+RRHD_TC_BF16 = 3
 STATUS_FALLBACK = 0x10
 STATUS_FAILED = 0x20
 
@@ -94,6 +98,10 @@ _SIGS = {
     "rrhd_scatter_fp64": (I32, [P, P, P, I64, P]),
     "rrhd_scatter_fp64_fma": (I32, [P, P, P, I64, P]),
     "rrhd_moments_fp64": (I32, [P, P, P, P, P, I64, P]),
+    "rrhd_scatter_tc_create": (I32, [P, I32, P]),
+    "rrhd_scatter_tc_destroy": (I32, [P]),
+    "rrhd_scatter_tc_run": (I32, [P, P, P, P, I64, P]),
+    "rrhd_scatter_tc_check": (I32, [P, P, I32]),
     "rrhd_emission_reference": (Emission, []),
     "rrhd_rad_source": (I32, [P, P, P, P, P, P, P, P, I64, P]),
     "rrhd_last_error": (C.c_char_p, []),

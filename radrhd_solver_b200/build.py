@@ -31,6 +31,7 @@ SOURCES = {
     "mesh.cpp": [],
     "hydro.cu": ["--fmad=false"],
     "radiation_fp64.cu": ["--fmad=false"],
+    "scatter_tc.cu": [],
 }
 
 

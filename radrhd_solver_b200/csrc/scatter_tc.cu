@@ -1,0 +1,601 @@
+// Scattering integral and moments on the 5th-generation tensor cores (tcgen05).
+//
+// C[r][n] = sum_d I[r][d] B[n][d] with, for n < M, B[n][d] = K[d][n] =
+// Gamma(w_d . w_n) a_d / full_area (the FP64 kernel of
+// cuda/src/short_characteristics/cuda_scattering.cu:82-105 and
+// cuda_integrator.cu:10-13) and, for n = M..M+9, the moment weights
+// a_d / full_area * {1, wx, wy, wz, wx^2, wx wy, wx wz, wy^2, wy wz, wz^2}
+// (cuda_illum_sep_param.cu:9-69; T is symmetric so 6 columns carry it).
+// Rows r are cells x frequency groups; I and the outputs are FP32.
+//
+// Precision forms (A = I, B = the kernel; FP32 accumulation in TMEM):
+//   BF16X3 : A = Ah + Al, B = Bh + Bl in bf16; Ah Bh + Ah Bl + Al Bh
+//   F16X3  : per-row power-of-two scale s_r (max |s_r I| in [2^14, 2^15)),
+//            the same three products in fp16; B pre-scaled by 2^8
+//   F16    : per-row scaled fp16, one product
+//   BF16   : bf16, one product
+//
+// The tensor core's FP32 accumulation truncates, so an accumulator that takes
+// every MMA of a long K loop drifts by about one ulp per MMA.  Each chunk of
+// 64 directions is therefore accumulated in a fresh TMEM accumulator (two,
+// alternating), and the chunks are summed in FP32 registers with
+// round-to-nearest adds by the accumulator warps.
+//
+// CTA (448 threads, one per SM; 128 rows x 128 output directions, plus the 16
+// moment columns in the first direction tile): warp 0 issues the TMA loads of
+// B (bf16/fp16, 128-byte swizzle, no multicast), warp 1 owns TMEM and issues
+// the MMAs from one thread, warps 2-5 load the FP32 intensity tile and split it
+// into hi/lo 16-bit tiles written in the UMMA K-major 128B-swizzled layout,
+// warps 6-13 drain the chunk accumulators (tcgen05.ld), sum, unscale and store.
+// Three smem stages of K = 64 directions.  Every mbarrier wait is bounded: on
+// a timeout the kernel records an error word, skips the remaining work, frees
+// its TMEM and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "rrhd_internal.h"
+
+#include "dirs.h"
+
+namespace {
+
+constexpr int kForms = 4;
+enum { FORM_BF16X3 = 0, FORM_F16X3 = 1, FORM_F16 = 2, FORM_BF16 = 3 };
+
+constexpr int BM = 128;      // rows per CTA (UMMA M)
+constexpr int BK = 64;       // directions per stage (one 128-byte swizzle row of 16-bit values)
+constexpr int NT = 128;      // output directions per CTA (UMMA N)
+constexpr int NMOM = 16;     // moment columns (10 used)
+constexpr int STAGES = 3;
+constexpr int THREADS = 448; // 14 warps: TMA, MMA, 4 converters, 8 accumulators
+constexpr int A_BYTES = BM * BK * 2;                   // 16 KiB
+constexpr int B_ROWS = NT + NMOM;                      // 144
+constexpr int B_BYTES = B_ROWS * BK * 2;               // 18 KiB
+constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES; // hi + lo
+constexpr int ACC_STRIDE = 256;                        // TMEM columns between the two chunk accumulators
+constexpr int MAX_HALF = (NT + NMOM) / 2;              // accumulator columns per thread
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + BM * 4;
+constexpr float kF16BScale = 256.0f;
+constexpr long long kSpinLimit = 1ll << 22;  // polls before a wait is declared timed out
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("{\n.reg .b64 st;\nmbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("{\n.reg .b64 st;\nmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// Bounded wait for the phase with the given parity; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (long long i = 0; i < kSpinLimit; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr & 0x3FFFF) >> 4);
+  d |= (uint64_t)1 << 16;            // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;  // stride byte offset
+  d |= (uint64_t)1 << 46;            // descriptor version for sm_100
+  d |= (uint64_t)2 << 61;            // SWIZZLE_128B
+  return d;
+}
+
+// Instruction descriptor, kind::f16: D f32, A/B bf16 (fmt 1) or f16 (fmt 0), both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc(int fmt, int n) {
+  return (1u << 4) | ((uint32_t)fmt << 7) | ((uint32_t)fmt << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                     uint32_t accumulate) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+template <int FORM>
+struct Split;
+template <>
+struct Split<FORM_BF16X3> {
+  __device__ static void run(float x, uint16_t &h, uint16_t &l) {
+    const __nv_bfloat16 a = __float2bfloat16_rn(x);
+    const __nv_bfloat16 b = __float2bfloat16_rn(x - __bfloat162float(a));
+    h = __bfloat16_as_ushort(a);
+    l = __bfloat16_as_ushort(b);
+  }
+};
+template <>
+struct Split<FORM_BF16> {
+  __device__ static void run(float x, uint16_t &h, uint16_t &l) {
+    h = __bfloat16_as_ushort(__float2bfloat16_rn(x));
+    l = 0;
+  }
+};
+template <>
+struct Split<FORM_F16X3> {
+  __device__ static void run(float x, uint16_t &h, uint16_t &l) {
+    const __half a = __float2half_rn(x);
+    const __half b = __float2half_rn(x - __half2float(a));
+    h = __half_as_ushort(a);
+    l = __half_as_ushort(b);
+  }
+};
+template <>
+struct Split<FORM_F16> {
+  __device__ static void run(float x, uint16_t &h, uint16_t &l) {
+    h = __half_as_ushort(__float2half_rn(x));
+    l = 0;
+  }
+};
+
+struct TcParams {
+  const float *I;
+  float *S;
+  float *mom;  // [rows][16] or null
+  int64_t rows;
+  int M;
+  float b_unscale;
+  int *err;
+};
+
+template <int FORM>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_scatter_tc(const __grid_constant__ CUtensorMap tm_bh, const __grid_constant__ CUtensorMap tm_bl,
+                 const __grid_constant__ CUtensorMap tm_mh, const __grid_constant__ CUtensorMap tm_ml,
+                 const TcParams P) {
+  constexpr bool THREE = (FORM == FORM_BF16X3 || FORM == FORM_F16X3);
+  constexpr bool SCALED = (FORM == FORM_F16X3 || FORM == FORM_F16);
+  constexpr int FMT = (FORM == FORM_BF16X3 || FORM == FORM_BF16) ? 1 : 0;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+  uint64_t *full_a = bars, *full_b = bars + STAGES, *empty = bars + 2 * STAGES;
+  uint64_t *acc_full = bars + 3 * STAGES, *acc_empty = bars + 3 * STAGES + 2;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 3 * STAGES + 4);
+  int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+  float *row_scale = reinterpret_cast<float *>(smem + STAGES * STAGE_BYTES + 256);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t r0 = (int64_t)blockIdx.x * BM;
+  const int nt = blockIdx.y;                   // output-direction tile
+  const bool with_mom = (nt == 0) && P.mom != nullptr;
+  const int nk = P.M / BK;
+  const int nS = P.M < NT ? P.M : NT;  // output directions of this tile (M <= 256 or M % 256 == 0)
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full_a[s], 128);
+      mbar_init(&full_b[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 8);
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;\n" ::"r"(smem_u32(tmem_slot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  auto fail = [&]() {
+    *abort_flag = 1;
+    atomicOr(P.err, 1);
+  };
+
+  if (warp == 0) {
+    // ---------------- B producer (TMA)
+    if (lane == 0) {
+      const uint32_t bytes = (uint32_t)((THREE ? 2 : 1) * (nS + (with_mom ? NMOM : 0)) * BK * 2);
+      int issued[STAGES] = {0};
+      for (int k = 0; k < nk; k++) {
+        const int s = k % STAGES;
+        if (k >= STAGES && !mbar_wait(&empty[s], ((k / STAGES) - 1) & 1)) {
+          fail();
+          break;
+        }
+        if (*abort_flag) break;
+        uint8_t *st = smem + s * STAGE_BYTES;
+        uint8_t *bh = st + 2 * A_BYTES, *bl = bh + B_BYTES;
+        mbar_arrive_expect_tx(&full_b[s], bytes);
+        tma_load_2d(bh, &tm_bh, k * BK, nt * NT, &full_b[s]);
+        if (THREE) tma_load_2d(bl, &tm_bl, k * BK, nt * NT, &full_b[s]);
+        if (with_mom) {
+          tma_load_2d(bh + NT * 128, &tm_mh, k * BK, 0, &full_b[s]);
+          if (THREE) tma_load_2d(bl + NT * 128, &tm_ml, k * BK, 0, &full_b[s]);
+        }
+        issued[s]++;
+      }
+      // make sure no copy is still in flight when the CTA retires (bounded)
+      for (int s = 0; s < STAGES; s++)
+        if (issued[s] && !mbar_wait(&full_b[s], (issued[s] - 1) & 1)) fail();
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer: chunk k goes to accumulator k % 2, fresh each chunk
+    if (lane == 0) {
+      const uint32_t idN = umma_idesc(FMT, nS);
+      constexpr uint32_t idM = umma_idesc(FMT, NMOM);
+      for (int k = 0; k < nk; k++) {
+        const int s = k % STAGES, ab = k & 1;
+        const uint32_t par = (k / STAGES) & 1;
+        if (!mbar_wait(&full_a[s], par) || !mbar_wait(&full_b[s], par) ||
+            (k >= 2 && !mbar_wait(&acc_empty[ab], ((k >> 1) - 1) & 1))) {
+          fail();
+          break;
+        }
+        if (*abort_flag) break;
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        uint8_t *st = smem + s * STAGE_BYTES;
+        const uint32_t ah = smem_u32(st), al = ah + A_BYTES;
+        const uint32_t bh = al + A_BYTES, bl = bh + B_BYTES;
+        const uint32_t acc_s = tmem + ab * ACC_STRIDE, acc_m = acc_s + nS;
+#pragma unroll
+        for (int kk = 0; kk < BK / 16; kk++) {
+          const uint32_t acc = kk > 0 ? 1u : 0u;
+          const uint32_t o = kk * 32;
+          umma(acc_s, umma_desc(ah + o), umma_desc(bh + o), idN, acc);
+          if (THREE) {
+            umma(acc_s, umma_desc(ah + o), umma_desc(bl + o), idN, 1u);
+            umma(acc_s, umma_desc(al + o), umma_desc(bh + o), idN, 1u);
+          }
+          if (with_mom) {
+            umma(acc_m, umma_desc(ah + o), umma_desc(bh + NT * 128 + o), idM, acc);
+            if (THREE) {
+              umma(acc_m, umma_desc(ah + o), umma_desc(bl + NT * 128 + o), idM, 1u);
+              umma(acc_m, umma_desc(al + o), umma_desc(bh + NT * 128 + o), idM, 1u);
+            }
+          }
+        }
+        umma_commit(&empty[s]);
+        umma_commit(&acc_full[ab]);
+      }
+    }
+  } else if (warp < 6) {
+    // ---------------- A converters (warps 2-5)
+    const int t = threadIdx.x - 64;  // 0..127
+    if (SCALED) {
+      // per-row power-of-two scale from the row maximum over all directions
+      float rmax[16];
+#pragma unroll
+      for (int i = 0; i < 16; i++) rmax[i] = 0.f;
+      for (int k = 0; k < nk; k++) {
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+          const int e = i * 128 + t, row = e >> 4, c4 = e & 15;
+          const int64_t gr = r0 + row;
+          if (gr < P.rows) {
+            const float4 v = __ldg(reinterpret_cast<const float4 *>(P.I + gr * P.M + k * BK) + c4);
+            rmax[i] = fmaxf(rmax[i], fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+          }
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        float m = rmax[i];
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((t & 15) == 0) {
+          const int row = (i * 128 + t) >> 4;
+          float sc = 1.f;
+          if (m > 0.f && isfinite(m)) sc = ldexpf(1.f, 14 - ilogbf(m));
+          row_scale[row] = sc;
+        }
+      }
+      asm volatile("bar.sync 1, 128;\n" ::: "memory");
+      asm volatile("bar.arrive 2, 384;\n" ::: "memory");  // row scales ready for the accumulator warps
+    }
+    for (int k = 0; k < nk; k++) {
+      const int s = k % STAGES;
+      if (k >= STAGES && !mbar_wait(&empty[s], ((k / STAGES) - 1) & 1)) {
+        fail();
+        break;
+      }
+      if (*abort_flag) break;
+      uint8_t *ah = smem + s * STAGE_BYTES, *al = ah + A_BYTES;
+      float4 v[16];
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        const int e = i * 128 + t, row = e >> 4, c4 = e & 15;
+        const int64_t gr = r0 + row;
+        v[i] = gr < P.rows ? __ldg(reinterpret_cast<const float4 *>(P.I + gr * P.M + k * BK) + c4)
+                           : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        const int e = i * 128 + t, row = e >> 4, c4 = e & 15;
+        float x[4] = {v[i].x, v[i].y, v[i].z, v[i].w};
+        if (SCALED) {
+          const float sc = row_scale[row];
+#pragma unroll
+          for (int q = 0; q < 4; q++) x[q] *= sc;
+        }
+        uint16_t h[4], l[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) Split<FORM>::run(x[q], h[q], l[q]);
+        const uint32_t off = row * 128 + ((((c4 >> 1) ^ (row & 7))) << 4) + ((c4 & 1) << 3);
+        *reinterpret_cast<uint2 *>(ah + off) =
+            make_uint2((uint32_t)h[0] | ((uint32_t)h[1] << 16), (uint32_t)h[2] | ((uint32_t)h[3] << 16));
+        if (THREE)
+          *reinterpret_cast<uint2 *>(al + off) =
+              make_uint2((uint32_t)l[0] | ((uint32_t)l[1] << 16), (uint32_t)l[2] | ((uint32_t)l[3] << 16));
+      }
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      mbar_arrive(&full_a[s]);
+    }
+  } else {
+    // ---------------- accumulator warps 6-13: warp w reads TMEM lanes 32*(w%4)..+31
+    // (one row per thread); warps 6-9 take the first half of the columns, 10-13 the second
+    const int q = warp & 3, hf = (warp - 6) >> 2;
+    const int row = q * 32 + lane;
+    const int64_t gr = r0 + row;
+    const int width = nS + (with_mom ? NMOM : 0);
+    const int half = width >> 1;  // multiple of 8
+    const int c0 = hf * half;
+    if (SCALED) asm volatile("bar.sync 2, 384;\n" ::: "memory");
+    float run[MAX_HALF];
+#pragma unroll
+    for (int j = 0; j < MAX_HALF; j++) run[j] = 0.f;
+    bool ok = true;
+    for (int k = 0; k < nk && ok; k++) {
+      const int ab = k & 1;
+      if (!mbar_wait(&acc_full[ab], (k >> 1) & 1)) {
+        fail();
+        ok = false;
+        break;
+      }
+      if (*abort_flag) {
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * ACC_STRIDE + c0);
+#pragma unroll
+      for (int j = 0; j < MAX_HALF / 8; j++) {
+        if (j * 8 < half) {
+          uint32_t r[8];
+          asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                         "=r"(r[7])
+                       : "r"(base + j * 8));
+          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+          for (int i = 0; i < 8; i++) run[j * 8 + i] = __fadd_rn(run[j * 8 + i], __uint_as_float(r[i]));
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[ab]);
+    }
+    if (ok && gr < P.rows) {
+      const float inv = (SCALED ? 1.f / row_scale[row] : 1.f) * P.b_unscale;
+#pragma unroll
+      for (int j = 0; j < MAX_HALF / 4; j++) {
+        const int col = c0 + 4 * j;
+        if (4 * j < half) {
+          const float4 v = make_float4(run[4 * j] * inv, run[4 * j + 1] * inv, run[4 * j + 2] * inv,
+                                       run[4 * j + 3] * inv);
+          if (col < nS)
+            *reinterpret_cast<float4 *>(P.S + gr * P.M + nt * NT + col) = v;
+          else
+            *reinterpret_cast<float4 *>(P.mom + gr * NMOM + (col - nS)) = v;
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(tmem));
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    cudaDriverEntryPointQueryResult q;
+    void *p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+}  // namespace
+
+struct rrhd_scatter_tc {
+  int device = 0;
+  int form = 0;
+  int M = 0;
+  uint16_t *d_bh = nullptr, *d_bl = nullptr;  // [M + 16][M] 16-bit, row n = output column n
+  CUtensorMap tm_bh, tm_bl, tm_mh, tm_ml;
+  float b_unscale = 1.f;
+  int *d_err = nullptr;
+};
+
+static uint16_t to_bf16(double x) {
+  const __nv_bfloat16 b = __float2bfloat16_rn((float)x);  // x is representable in float range here
+  return __bfloat16_as_ushort(b);
+}
+
+extern "C" rrhd_status rrhd_scatter_tc_create(const rrhd_dirs *d, int32_t form, rrhd_scatter_tc **out) {
+  RRHD_CHECK_ARG(d && out, "null argument");
+  RRHD_CHECK_ARG(form >= 0 && form < kForms, "unknown tensor-core form %d", form);
+  RRHD_CHECK_ARG(d->M % BK == 0 && d->M >= BK && d->M <= 1024 && (d->M <= NT || d->M % NT == 0),
+                 "tensor-core scattering needs M = 64 or a multiple of 128 (<= 1024)");
+  *out = nullptr;
+  auto enc = get_encode();
+  if (!enc) return rrhd_fail(RRHD_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  RRHD_CUDA(cudaSetDevice(d->device));
+  const int M = d->M, NB = M + NMOM;
+  const double A = d->full_area;
+  const bool f16 = (form == FORM_F16X3 || form == FORM_F16);
+  const double bscale = f16 ? kF16BScale : 1.0;
+  std::vector<uint16_t> bh((size_t)NB * M), bl((size_t)NB * M);
+  for (int n = 0; n < NB; n++)
+    for (int dd = 0; dd < M; dd++) {
+      const double *w = &d->h_w[3 * dd];
+      double v = 0.0;
+      if (n < M) {
+        const double *wn = &d->h_w[3 * n];
+        const double mu = (w[0] * wn[0] + w[1] * wn[1]) + w[2] * wn[2];
+        v = (3. * (1. + mu * mu)) / 4. * d->h_a[dd] / A;
+      } else {
+        const double f[10] = {1.0, w[0], w[1], w[2], w[0] * w[0], w[0] * w[1], w[0] * w[2], w[1] * w[1], w[1] * w[2], w[2] * w[2]};
+        const int j = n - M;
+        v = j < 10 ? f[j] * d->h_a[dd] / A : 0.0;
+      }
+      v *= bscale;
+      uint16_t h, l;
+      if (f16) {
+        const __half a = __float2half_rn((float)v);
+        const __half b = __float2half_rn((float)(v - (double)__half2float(a)));
+        h = __half_as_ushort(a);
+        l = __half_as_ushort(b);
+      } else {
+        h = to_bf16(v);
+        const double hv = (double)__bfloat162float(__ushort_as_bfloat16(h));
+        l = to_bf16(v - hv);
+      }
+      bh[(size_t)n * M + dd] = h;
+      bl[(size_t)n * M + dd] = l;
+    }
+  rrhd_scatter_tc *t = new rrhd_scatter_tc();
+  t->device = d->device;
+  t->form = form;
+  t->M = M;
+  t->b_unscale = (float)(1.0 / bscale);
+  const size_t bytes = sizeof(uint16_t) * bh.size();
+  if (cudaMalloc(&t->d_bh, bytes) != cudaSuccess || cudaMalloc(&t->d_bl, bytes) != cudaSuccess ||
+      cudaMalloc(&t->d_err, sizeof(int)) != cudaSuccess) {
+    cudaFree(t->d_bh);
+    cudaFree(t->d_bl);
+    cudaFree(t->d_err);
+    delete t;
+    return rrhd_fail(RRHD_ERR_OOM, "tensor-core operand allocation failed");
+  }
+  cudaMemcpy(t->d_bh, bh.data(), bytes, cudaMemcpyHostToDevice);
+  cudaMemcpy(t->d_bl, bl.data(), bytes, cudaMemcpyHostToDevice);
+  cudaMemset(t->d_err, 0, sizeof(int));
+  const CUtensorMapDataType dt = f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+  auto make = [&](CUtensorMap *m, uint16_t *base, int rows_total, int box_rows, int row0) -> bool {
+    cuuint64_t dims[2] = {(cuuint64_t)M, (cuuint64_t)rows_total};
+    cuuint64_t strides[1] = {(cuuint64_t)M * 2};
+    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+    cuuint32_t es[2] = {1, 1};
+    return enc(m, dt, 2, base + (size_t)row0 * M, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  const int box_n = M < NT ? M : NT;
+  if (!make(&t->tm_bh, t->d_bh, M, box_n, 0) || !make(&t->tm_bl, t->d_bl, M, box_n, 0) ||
+      !make(&t->tm_mh, t->d_bh, NMOM, NMOM, M) || !make(&t->tm_ml, t->d_bl, NMOM, NMOM, M)) {
+    cudaFree(t->d_bh);
+    cudaFree(t->d_bl);
+    cudaFree(t->d_err);
+    delete t;
+    return rrhd_fail(RRHD_ERR_CUDA, "tensor map encoding failed");
+  }
+  *out = t;
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_scatter_tc_destroy(rrhd_scatter_tc *t) {
+  if (!t) return RRHD_OK;
+  cudaSetDevice(t->device);
+  cudaFree(t->d_bh);
+  cudaFree(t->d_bl);
+  cudaFree(t->d_err);
+  delete t;
+  return RRHD_OK;
+}
+
+template <int FORM>
+static rrhd_status launch_tc(const rrhd_scatter_tc *t, const float *I, float *S, float *mom, int64_t rows,
+                             cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    RRHD_CUDA(cudaFuncSetAttribute(k_scatter_tc<FORM>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    attr = true;
+  }
+  TcParams P{I, S, mom, rows, t->M, t->b_unscale, t->d_err};
+  dim3 grid((unsigned)((rows + BM - 1) / BM), (unsigned)((t->M + NT - 1) / NT));
+  k_scatter_tc<FORM><<<grid, THREADS, SMEM_BYTES, st>>>(t->tm_bh, t->tm_bl, t->tm_mh, t->tm_ml, P);
+  RRHD_CUDA(cudaGetLastError());
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_scatter_tc_run(const rrhd_scatter_tc *t, const float *I, float *S, float *mom,
+                                           int64_t rows, void *stream) {
+  RRHD_CHECK_ARG(t && rows >= 0, "bad arguments");
+  if (rows == 0) return RRHD_OK;
+  RRHD_CHECK_ARG(I && S, "null I or S");
+  RRHD_CHECK_ARG(((uintptr_t)I & 15) == 0 && ((uintptr_t)S & 15) == 0 && ((uintptr_t)mom & 15) == 0,
+                 "I, S and moments must be 16-byte aligned");
+  if (rows == 0) return RRHD_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (t->form) {
+    case FORM_BF16X3: return launch_tc<FORM_BF16X3>(t, I, S, mom, rows, st);
+    case FORM_F16X3: return launch_tc<FORM_F16X3>(t, I, S, mom, rows, st);
+    case FORM_F16: return launch_tc<FORM_F16>(t, I, S, mom, rows, st);
+    default: return launch_tc<FORM_BF16>(t, I, S, mom, rows, st);
+  }
+}
+
+// Error word of the tensor-core kernels (non-zero after a bounded wait timed
+// out); reading it synchronises the stream, clear resets it.
+extern "C" rrhd_status rrhd_scatter_tc_check(const rrhd_scatter_tc *t, void *stream, int32_t clear) {
+  RRHD_CHECK_ARG(t, "null argument");
+  int e = 0;
+  RRHD_CUDA(cudaMemcpyAsync(&e, t->d_err, sizeof e, cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+  RRHD_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  if (clear) RRHD_CUDA(cudaMemsetAsync(t->d_err, 0, sizeof(int), (cudaStream_t)stream));
+  if (e) return rrhd_fail(RRHD_ERR_CUDA, "tensor-core scattering: a pipeline wait timed out");
+  return RRHD_OK;
+}

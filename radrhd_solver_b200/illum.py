@@ -70,3 +70,52 @@ def CalculateAllParam(dg: DirectionGrid, I, stream=None):
     L.check(L.lib.rrhd_moments_fp64(dg.handle, L.ptr(I), L.ptr(E), L.ptr(F), L.ptr(T), rows, _stream(stream)),
             "CalculateAllParam")
     return E, F, T
+
+
+TC_FORMS = {"bf16x3": L.RRHD_TC_BF16X3, "f16x3": L.RRHD_TC_F16X3, "f16": L.RRHD_TC_F16, "bf16": L.RRHD_TC_BF16}
+
+
+class ScatterTC:
+    """Tensor-core (tcgen05) scattering integral + moments for one direction set
+    and precision form ("bf16x3", "f16x3", "f16", "bf16"); FP32 in/out."""
+
+    def __init__(self, dg: DirectionGrid, form: str = "f16x3"):
+        self.dg = dg
+        self.form = form
+        h = C.c_void_p()
+        L.check(L.lib.rrhd_scatter_tc_create(dg.handle, TC_FORMS[form], C.byref(h)), "rrhd_scatter_tc_create")
+        self._h = h
+
+    def __call__(self, I, S=None, moments=True, stream=None):
+        import torch
+        rows = I.shape[0]
+        if S is None:
+            S = torch.empty_like(I)
+        mom = torch.empty(rows, 16, dtype=torch.float32, device=I.device) if moments else None
+        L.check(L.lib.rrhd_scatter_tc_run(self._h, L.ptr(I), L.ptr(S), L.ptr(mom), rows, _stream(stream)),
+                "rrhd_scatter_tc_run")
+        return S, mom
+
+    def check(self, clear=True, stream=None):
+        L.check(L.lib.rrhd_scatter_tc_check(self._h, _stream(stream), 1 if clear else 0), "rrhd_scatter_tc_check")
+
+    def close(self):
+        if self._h:
+            L.lib.rrhd_scatter_tc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def moments_from_tc(mom):
+    """Expands the 16-column moment block to E [n], F [n,3], T [n,3,3] (float64)."""
+    import torch
+    m = mom.to(torch.float64)
+    E = m[:, 0].clone()
+    F = m[:, 1:4].clone()
+    T = torch.stack([m[:, 4], m[:, 5], m[:, 6], m[:, 5], m[:, 7], m[:, 8], m[:, 6], m[:, 8], m[:, 9]], 1).view(-1, 3, 3)
+    return E, F, T

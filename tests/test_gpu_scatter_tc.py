@@ -1,0 +1,80 @@
+"""Tensor-core (tcgen05) scattering + moments against the FP64 oracle.
+
+The tensor-core forms are mixed precision, so the bar is an error bound per
+form, stated below as max and rms relative error of S (and of the moments,
+relative to the energy moment E of the same row), on FP32 inputs whose FP64
+copies feed the oracle.
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from cases import intensity
+from radrhd_solver_b200 import illum
+from radrhd_solver_b200.mesh import fibonacci_directions
+
+pytestmark = pytest.mark.gpu
+
+# max / rms relative error bounds per form (measured on B200: f16x3 7.0e-7 / 3.3e-7,
+# bf16x3 1.9e-6 / 3.8e-7, f16 1.0e-4 / 2.0e-5, bf16 8.1e-4 / 1.8e-4 at M=256)
+BOUND = {"f16x3": (1.2e-6, 5e-7), "bf16x3": (4e-6, 8e-7), "f16": (3e-4, 6e-5), "bf16": (2e-3, 5e-4)}
+
+
+def _errors(S, Mom, So, Eo, Fo, To):
+    rel = np.abs(S - So) / np.abs(So)
+    E, F, T = (x.cpu().numpy() for x in illum.moments_from_tc(torch.tensor(Mom)))
+    den = Eo[:, None]
+    mrel = np.concatenate([np.abs(E - Eo)[:, None] / den, np.abs(F - Fo) / den,
+                           np.abs(T - To).reshape(len(Eo), 9) / den], 1)
+    return rel.max(), np.sqrt((rel ** 2).mean()), mrel.max()
+
+
+def _config2_rows(cells, groups, M, seed):
+    """Config-2 style rows (cell x group): scale 10^(-6+6g/15) * lognormal(0, 1)."""
+    rng = np.random.default_rng(seed)
+    g = np.tile(np.arange(groups), cells)
+    return (10.0 ** (-6 + 6 * g / 15.0))[:, None] * np.exp(rng.normal(0, 1, (cells * groups, M)))
+
+
+@pytest.mark.parametrize("form", ["f16x3", "bf16x3", "f16", "bf16"])
+@pytest.mark.parametrize("M,rows,kind", [(256, 3001, "c1"), (512, 777, "c2"), (64, 260, "c1"), (128, 129, "c2")])
+def test_scatter_tc_error_bounds(form, M, rows, kind):
+    d = fibonacci_directions(M)
+    if kind == "c1":
+        I = intensity(rows, M, seed=M + rows)
+    else:
+        I = _config2_rows((rows + 15) // 16, 16, M, seed=M)[:rows]
+    I32 = I.astype(np.float32)
+    I64 = I32.astype(np.float64)
+    So = oracle.port_scatter(I64, d.dirs, d.areas, d.full_area)
+    Eo, Fo, To = oracle.port_moments(I64, d.dirs, d.areas, d.full_area)
+    dg = illum.DirectionGrid(d)
+    tc = illum.ScatterTC(dg, form)
+    S, Mom = tc(torch.tensor(I32, device="cuda"))
+    torch.cuda.synchronize()
+    tc.check()
+    mx, rms, mom_mx = _errors(S.cpu().numpy().astype(np.float64), Mom.cpu().numpy().astype(np.float64),
+                              So, Eo, Fo, To)
+    print(f"\n{form} M={M} rows={rows} {kind}: S max rel {mx:.3e} rms {rms:.3e}; moments max {mom_mx:.3e}")
+    bmax, brms = BOUND[form]
+    assert mx <= bmax and rms <= brms, (mx, rms)
+    assert mom_mx <= 4 * bmax
+    # the padding columns of the moment block are zero
+    assert np.all(Mom.cpu().numpy()[:, 10:] == 0)
+    tc.close()
+    dg.close()
+
+
+def test_scatter_tc_without_moments_and_empty():
+    M = 256
+    d = fibonacci_directions(M)
+    dg = illum.DirectionGrid(d)
+    tc = illum.ScatterTC(dg, "bf16x3")
+    I = torch.tensor(intensity(300, M, seed=5).astype(np.float32), device="cuda")
+    S1, _ = tc(I, moments=False)
+    S2, _ = tc(I, moments=True)
+    torch.cuda.synchronize()
+    assert torch.equal(S1, S2)
+    S0, _ = tc(I[:0])
+    tc.check()
