@@ -194,6 +194,72 @@ def profile_traffic(name):
     return None
 
 
+def _time(fn, reps, stream, warm=2):
+    import torch
+    for _ in range(warm):
+        fn()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def scatter_component(dev, nhex=48, M=256, groups=1, kind=0, sigma=0.5, reps=5, fp64=True):
+    """Scattering integral + moments, plain FP64 and tensor-core forms.
+    nhex=48, M=256, groups=1: 663,552 cells x 256 directions (lognormal(0,0.5) x
+    exp(-|x|^2/0.2)); inputs 0.68 GB (FP32) / 1.36 GB (FP64) > L2, no flush."""
+    import torch
+    from radrhd_solver_b200 import _lib as L
+    from radrhd_solver_b200 import illum
+    from radrhd_solver_b200 import mesh as Mm
+    m = Mm.kuhn_box(nhex, nhex, nhex, lo=(-1, -1, -1), hi=(1, 1, 1), jitter=0.15, seed=7)
+    rows = m.n_cells * groups
+    d = Mm.fibonacci_directions(M)
+    dg = illum.DirectionGrid(d, dev)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    centers = torch.tensor(m.cell_center, device=f"cuda:{dev}")
+    out = {"workload": f"{m.n_cells} cells x {groups} groups x {M} directions", "rows": rows, "M": M}
+    flop = 2.0 * rows * M * (M + 10)  # algorithmic: S plus the 10 moment columns
+    cd = rows * M
+    I32 = torch.empty(rows, M, dtype=torch.float32, device=f"cuda:{dev}")
+    L.check(L.lib.rrhd_fill_intensity_f32(I32.data_ptr(), rows, M, groups, kind, sigma, centers.data_ptr(), 11, sp))
+    if fp64:
+        I64 = torch.empty(rows, M, dtype=torch.float64, device=f"cuda:{dev}")
+        L.check(L.lib.rrhd_fill_intensity_f64(I64.data_ptr(), rows, M, groups, kind, sigma, centers.data_ptr(), 11, sp))
+        S64 = torch.empty_like(I64)
+        E = torch.empty(rows, dtype=torch.float64, device=I64.device)
+        F = torch.empty(rows, 3, dtype=torch.float64, device=I64.device)
+        T = torch.empty(rows, 3, 3, dtype=torch.float64, device=I64.device)
+        for name, fn in (("fp64_exact", L.lib.rrhd_scatter_fp64), ("fp64_fma", L.lib.rrhd_scatter_fp64_fma)):
+            def run(fn=fn):
+                L.check(fn(dg.handle, I64.data_ptr(), S64.data_ptr(), rows, sp))
+                L.check(L.lib.rrhd_moments_fp64(dg.handle, I64.data_ptr(), E.data_ptr(), F.data_ptr(), T.data_ptr(),
+                                                rows, sp))
+            ms = _time(run, reps, stream)
+            out[name] = {"ms": ms, "cell_dir_per_s": cd / (ms / 1e3), "tflops": flop / (ms / 1e3) / 1e12}
+        del I64, S64
+    S32 = torch.empty_like(I32)
+    mom = torch.empty(rows, 16, dtype=torch.float32, device=I32.device)
+    for form in ("f16x3", "bf16x3", "f16"):
+        tc = illum.ScatterTC(dg, form)
+
+        def run(tc=tc):
+            L.check(L.lib.rrhd_scatter_tc_run(tc._h, I32.data_ptr(), S32.data_ptr(), mom.data_ptr(), rows, sp))
+        ms = _time(run, reps, stream)
+        tc.check()
+        nbytes = rows * M * 8 + rows * 64
+        out["tc_" + form] = {"ms": ms, "cell_dir_per_s": cd / (ms / 1e3), "tflops": flop / (ms / 1e3) / 1e12,
+                             "gbs": nbytes / (ms / 1e3) / 1e9}
+        tc.close()
+    dg.close()
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -270,7 +336,7 @@ def run_ours(args):
     achieved = alg_bytes / (per_step / 1e3) / 1e9
     pk = peaks()
     peak = pk["hbm_gbs"] if pk else 6650.0
-    traffic = profile_traffic("hydro_step_jet96.md")
+    traffic = profile_traffic("hydro_step_jet96.md") if NHEX == 96 else None
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
@@ -296,6 +362,11 @@ def run_ours(args):
         dt, kind = reference_steps(m, Wg, Ug, args.cpu_steps, threads, inflow_conservative())
         line["cpu_baseline"] = {"value": m.n_cells / dt, "unit": UNIT, "cores": threads, "kind": kind,
                                 "sample": f"{args.cpu_steps} full steps of the {m.n_cells}-cell mesh"}
+    if rank == 0 and not args.no_scatter:
+        line["scatter"] = scatter_component(dev)
+        sc = line["scatter"]
+        if "fp64_fma" in sc:
+            line["chosen_vs_plain"] = {"scatter_moments": sc["fp64_fma"]["ms"] / sc["tc_f16x3"]["ms"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -313,9 +384,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--nhex", type=int, default=96, help="hexes per axis (96 = the benchmark mesh)")
     ap.add_argument("--cpb", type=int, default=0, help="cells per CTA of the step kernel (0 = library default)")
+    ap.add_argument("--no-scatter", action="store_true", help="skip the scattering component")
+    ap.add_argument("--scatter-only", type=int, default=0, metavar="NHEX",
+                    help="only time the scattering component on an NHEX^3 x 6 mesh (profiling runs)")
     args = ap.parse_args()
     global NHEX
     NHEX = args.nhex
+    if args.scatter_only:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(scatter_component(0, nhex=args.scatter_only, reps=args.steps)), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -50,6 +50,15 @@ rrhd_status rrhd_mesh_kuhn_build(const rrhd_kuhn_params *p, int32_t *face_id_l,
 /* Fibonacci sphere with equal weights 4 pi / M and full_area = 4 pi. */
 rrhd_status rrhd_directions_fibonacci(int32_t M, double *dirs, double *areas, double *full_area);
 
+/* Synthetic intensity I [rows][M] on the device (rows = cells x groups, cell-major):
+ *   kind 0: exp(sigma z) * exp(-|x_c|^2 / 0.2), x_c from centers [cells][3] (device; NULL: no envelope)
+ *   kind 1: 10^(-6 + 6 g / (groups - 1)) * exp(sigma z), g = row % groups
+ * z standard normal (Box-Muller on the counter-based RNG), a pure function of (seed, row, k). */
+rrhd_status rrhd_fill_intensity_f32(float *I, int64_t rows, int32_t M, int32_t groups, int32_t kind,
+                                    double sigma, const double *centers, uint64_t seed, void *stream);
+rrhd_status rrhd_fill_intensity_f64(double *I, int64_t rows, int32_t M, int32_t groups, int32_t kind,
+                                    double sigma, const double *centers, uint64_t seed, void *stream);
+
 /* Counter-based uniform [0,1) variate: the same value on host and device. */
 double rrhd_rng_u01(uint64_t seed, uint64_t stream, uint64_t index);
 

@@ -110,6 +110,8 @@ _SIGS = {
     "rrhd_mesh_kuhn_build": (I32, [P, P, P, P, P, P, P, P, P, P, P, P]),
     "rrhd_directions_fibonacci": (I32, [I32, P, P, P]),
     "rrhd_rng_u01": (D, [U64, U64, U64]),
+    "rrhd_fill_intensity_f32": (I32, [P, I64, I32, I32, I32, D, P, U64, P]),
+    "rrhd_fill_intensity_f64": (I32, [P, I64, I32, I32, I32, D, P, U64, P]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

@@ -32,6 +32,7 @@ SOURCES = {
     "hydro.cu": ["--fmad=false"],
     "radiation_fp64.cu": ["--fmad=false"],
     "scatter_tc.cu": [],
+    "synth.cu": [],
 }
 
 

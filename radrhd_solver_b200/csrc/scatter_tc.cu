@@ -21,21 +21,23 @@
 // alternating), and the chunks are summed in FP32 registers with
 // round-to-nearest adds by the accumulator warps.
 //
-// CTA (448 threads, one per SM; 128 rows x 128 output directions, plus the 16
-// moment columns in the first direction tile): warp 0 issues the TMA loads of
-// B (bf16/fp16, 128-byte swizzle, no multicast), warp 1 owns TMEM and issues
-// the MMAs from one thread, warps 2-5 load the FP32 intensity tile and split it
-// into hi/lo 16-bit tiles written in the UMMA K-major 128B-swizzled layout,
-// warps 6-13 drain the chunk accumulators (tcgen05.ld), sum, unscale and store.
-// Three smem stages of K = 64 directions.  Every mbarrier wait is bounded: on
-// a timeout the kernel records an error word, skips the remaining work, frees
-// its TMEM and returns.
+// Persistent CTAs (576 threads, one per SM) loop over tiles of 128 rows x 128
+// output directions (plus the 16 moment columns in the first direction tile):
+// warp 0 issues the TMA loads of B (bf16/fp16, 128-byte swizzle, no multicast),
+// warp 1 owns TMEM and issues the MMAs from one thread, warps 2-9 split the
+// FP32 intensity tile (brought in by TMA, two chunks ahead) into hi/lo 16-bit
+// tiles written in the UMMA K-major 128B-swizzled layout, warps 10-17 drain
+// the chunk accumulators (tcgen05.ld), sum, unscale and store.  Two smem stages
+// of K = 64 directions.  The row scales of the FP16 forms come from k_row_scale.
+// Every mbarrier wait is bounded: on a timeout the kernel records an error
+// word, skips the remaining work, frees its TMEM and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -53,15 +55,21 @@ constexpr int BM = 128;      // rows per CTA (UMMA M)
 constexpr int BK = 64;       // directions per stage (one 128-byte swizzle row of 16-bit values)
 constexpr int NT = 128;      // output directions per CTA (UMMA N)
 constexpr int NMOM = 16;     // moment columns (10 used)
-constexpr int STAGES = 3;
-constexpr int THREADS = 448; // 14 warps: TMA, MMA, 4 converters, 8 accumulators
+constexpr int STAGES = 2;
+constexpr int A32_STAGES = 2;
+constexpr int CONV_WARPS = 8;
+constexpr int ACC_WARPS = 8;
+constexpr int THREADS = 32 * (2 + CONV_WARPS + ACC_WARPS);  // TMA, MMA, converters, accumulators
+constexpr int CONV_THREADS = 32 * CONV_WARPS;
+constexpr int CONV_ITERS = BM * BK / 4 / CONV_THREADS;     // float4 per converter thread per chunk
 constexpr int A_BYTES = BM * BK * 2;                   // 16 KiB
 constexpr int B_ROWS = NT + NMOM;                      // 144
 constexpr int B_BYTES = B_ROWS * BK * 2;               // 18 KiB
 constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES; // hi + lo
 constexpr int ACC_STRIDE = 256;                        // TMEM columns between the two chunk accumulators
 constexpr int MAX_HALF = (NT + NMOM) / 2;              // accumulator columns per thread
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + BM * 4;
+constexpr int A32_BYTES = BM * BK * 4;                  // 32 KiB FP32 intensity tile
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + A32_STAGES * A32_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 constexpr float kF16BScale = 256.0f;
 constexpr long long kSpinLimit = 1ll << 22;  // polls before a wait is declared timed out
 
@@ -170,46 +178,74 @@ struct Split<FORM_F16> {
 struct TcParams {
   const float *I;
   float *S;
-  float *mom;  // [rows][16] or null
+  float *mom;          // [rows][16] or null
+  const float *scale;  // [rows] power-of-two row scales (scaled forms)
   int64_t rows;
   int M;
   float b_unscale;
   int *err;
 };
 
+// Row scale for the scaled FP16 forms: 2^(14 - floor(log2(max_d |I[r][d]|))),
+// so that max |s_r I| lies in [2^14, 2^15).  One warp per row, streaming.
+__global__ void k_row_scale(const float *__restrict__ I, int64_t rows, int M, float *__restrict__ scale) {
+  const int64_t r = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (r >= rows) return;
+  const float4 *row = reinterpret_cast<const float4 *>(I + r * M);
+  float m = 0.f;
+  for (int c = lane; c < M / 4; c += 32) {
+    const float4 v = __ldg(row + c);
+    m = fmaxf(m, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) scale[r] = (m > 0.f && isfinite(m)) ? ldexpf(1.f, 14 - ilogbf(m)) : 1.f;
+}
+
+// Persistent: CTA b takes tiles b, b + gridDim.x, ...; tile t covers rows
+// 128 (t / n_nt) .. +127 and output directions 128 (t % n_nt) .. +127.  The
+// chunk counter g runs on across tiles, so smem stages and TMEM accumulators
+// keep cycling and the accumulator warps store one tile while the next is
+// being multiplied.
 template <int FORM>
 __global__ void __launch_bounds__(THREADS, 1)
     k_scatter_tc(const __grid_constant__ CUtensorMap tm_bh, const __grid_constant__ CUtensorMap tm_bl,
                  const __grid_constant__ CUtensorMap tm_mh, const __grid_constant__ CUtensorMap tm_ml,
-                 const TcParams P) {
+                 const __grid_constant__ CUtensorMap tm_a, const TcParams P) {
   constexpr bool THREE = (FORM == FORM_BF16X3 || FORM == FORM_F16X3);
   constexpr bool SCALED = (FORM == FORM_F16X3 || FORM == FORM_F16);
   constexpr int FMT = (FORM == FORM_BF16X3 || FORM == FORM_BF16) ? 1 : 0;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+  uint8_t *a32 = smem + STAGES * STAGE_BYTES;  // [A32_STAGES][128][64] FP32
+  uint64_t *bars = reinterpret_cast<uint64_t *>(a32 + A32_STAGES * A32_BYTES);
   uint64_t *full_a = bars, *full_b = bars + STAGES, *empty = bars + 2 * STAGES;
   uint64_t *acc_full = bars + 3 * STAGES, *acc_empty = bars + 3 * STAGES + 2;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 3 * STAGES + 4);
-  int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
-  float *row_scale = reinterpret_cast<float *>(smem + STAGES * STAGE_BYTES + 256);
+  uint64_t *a32_full = bars + 3 * STAGES + 4, *a32_empty = a32_full + A32_STAGES;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 3 * STAGES + 4 + 2 * A32_STAGES);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t r0 = (int64_t)blockIdx.x * BM;
-  const int nt = blockIdx.y;                   // output-direction tile
-  const bool with_mom = (nt == 0) && P.mom != nullptr;
   const int nk = P.M / BK;
-  const int nS = P.M < NT ? P.M : NT;  // output directions of this tile (M <= 256 or M % 256 == 0)
+  const int nS = P.M < NT ? P.M : NT;  // output directions per tile (M <= 128 or M % 128 == 0)
+  const int n_nt = P.M / nS;
+  const int64_t n_rt = (P.rows + BM - 1) / BM;
+  const int64_t tiles = n_rt * n_nt;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; s++) {
-      mbar_init(&full_a[s], 128);
+      mbar_init(&full_a[s], CONV_THREADS);
       mbar_init(&full_b[s], 1);
       mbar_init(&empty[s], 1);
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(&acc_full[b], 1);
-      mbar_init(&acc_empty[b], 8);
+      mbar_init(&acc_empty[b], ACC_WARPS);
+    }
+    for (int b = 0; b < A32_STAGES; b++) {
+      mbar_init(&a32_full[b], 1);
+      mbar_init(&a32_empty[b], CONV_THREADS);
     }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -231,198 +267,210 @@ __global__ void __launch_bounds__(THREADS, 1)
   if (warp == 0) {
     // ---------------- B producer (TMA)
     if (lane == 0) {
-      const uint32_t bytes = (uint32_t)((THREE ? 2 : 1) * (nS + (with_mom ? NMOM : 0)) * BK * 2);
       int issued[STAGES] = {0};
-      for (int k = 0; k < nk; k++) {
-        const int s = k % STAGES;
-        if (k >= STAGES && !mbar_wait(&empty[s], ((k / STAGES) - 1) & 1)) {
-          fail();
-          break;
+      int64_t g = 0;
+      for (int64_t tile = blockIdx.x; tile < tiles && !*abort_flag; tile += gridDim.x) {
+        const int nt = (int)(tile % n_nt);
+        const bool with_mom = (nt == 0) && P.mom != nullptr;
+        const uint32_t bytes = (uint32_t)((THREE ? 2 : 1) * (nS + (with_mom ? NMOM : 0)) * BK * 2);
+        for (int k = 0; k < nk; k++, g++) {
+          const int s = (int)(g % STAGES);
+          if (g >= STAGES && !mbar_wait(&empty[s], (uint32_t)((g / STAGES) - 1) & 1)) {
+            fail();
+            break;
+          }
+          if (*abort_flag) break;
+          uint8_t *st = smem + s * STAGE_BYTES;
+          uint8_t *bh = st + 2 * A_BYTES, *bl = bh + B_BYTES;
+          mbar_arrive_expect_tx(&full_b[s], bytes);
+          tma_load_2d(bh, &tm_bh, k * BK, nt * NT, &full_b[s]);
+          if (THREE) tma_load_2d(bl, &tm_bl, k * BK, nt * NT, &full_b[s]);
+          if (with_mom) {
+            tma_load_2d(bh + NT * 128, &tm_mh, k * BK, 0, &full_b[s]);
+            if (THREE) tma_load_2d(bl + NT * 128, &tm_ml, k * BK, 0, &full_b[s]);
+          }
+          issued[s]++;
         }
-        if (*abort_flag) break;
-        uint8_t *st = smem + s * STAGE_BYTES;
-        uint8_t *bh = st + 2 * A_BYTES, *bl = bh + B_BYTES;
-        mbar_arrive_expect_tx(&full_b[s], bytes);
-        tma_load_2d(bh, &tm_bh, k * BK, nt * NT, &full_b[s]);
-        if (THREE) tma_load_2d(bl, &tm_bl, k * BK, nt * NT, &full_b[s]);
-        if (with_mom) {
-          tma_load_2d(bh + NT * 128, &tm_mh, k * BK, 0, &full_b[s]);
-          if (THREE) tma_load_2d(bl + NT * 128, &tm_ml, k * BK, 0, &full_b[s]);
-        }
-        issued[s]++;
       }
-      // make sure no copy is still in flight when the CTA retires (bounded)
+      // no copy may still be in flight when the CTA retires (bounded)
       for (int s = 0; s < STAGES; s++)
         if (issued[s] && !mbar_wait(&full_b[s], (issued[s] - 1) & 1)) fail();
     }
   } else if (warp == 1) {
-    // ---------------- MMA issuer: chunk k goes to accumulator k % 2, fresh each chunk
+    // ---------------- MMA issuer: chunk g goes to accumulator g % 2, fresh each chunk
     if (lane == 0) {
       const uint32_t idN = umma_idesc(FMT, nS);
       constexpr uint32_t idM = umma_idesc(FMT, NMOM);
-      for (int k = 0; k < nk; k++) {
-        const int s = k % STAGES, ab = k & 1;
-        const uint32_t par = (k / STAGES) & 1;
-        if (!mbar_wait(&full_a[s], par) || !mbar_wait(&full_b[s], par) ||
-            (k >= 2 && !mbar_wait(&acc_empty[ab], ((k >> 1) - 1) & 1))) {
+      int64_t g = 0;
+      for (int64_t tile = blockIdx.x; tile < tiles && !*abort_flag; tile += gridDim.x) {
+        const bool with_mom = (tile % n_nt == 0) && P.mom != nullptr;
+        for (int k = 0; k < nk; k++, g++) {
+          const int s = (int)(g % STAGES), ab = (int)(g & 1);
+          const uint32_t par = (uint32_t)(g / STAGES) & 1;
+          if (!mbar_wait(&full_a[s], par) || !mbar_wait(&full_b[s], par) ||
+              (g >= 2 && !mbar_wait(&acc_empty[ab], (uint32_t)((g >> 1) - 1) & 1))) {
+            fail();
+            break;
+          }
+          if (*abort_flag) break;
+          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+          uint8_t *st = smem + s * STAGE_BYTES;
+          const uint32_t ah = smem_u32(st), al = ah + A_BYTES;
+          const uint32_t bh = al + A_BYTES, bl = bh + B_BYTES;
+          const uint32_t acc_s = tmem + ab * ACC_STRIDE, acc_m = acc_s + nS;
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; kk++) {
+            const uint32_t acc = kk > 0 ? 1u : 0u;
+            const uint32_t o = kk * 32;
+            umma(acc_s, umma_desc(ah + o), umma_desc(bh + o), idN, acc);
+            if (THREE) {
+              umma(acc_s, umma_desc(ah + o), umma_desc(bl + o), idN, 1u);
+              umma(acc_s, umma_desc(al + o), umma_desc(bh + o), idN, 1u);
+            }
+            if (with_mom) {
+              umma(acc_m, umma_desc(ah + o), umma_desc(bh + NT * 128 + o), idM, acc);
+              if (THREE) {
+                umma(acc_m, umma_desc(ah + o), umma_desc(bl + NT * 128 + o), idM, 1u);
+                umma(acc_m, umma_desc(al + o), umma_desc(bh + NT * 128 + o), idM, 1u);
+              }
+            }
+          }
+          umma_commit(&empty[s]);
+          umma_commit(&acc_full[ab]);
+        }
+      }
+    }
+  } else if (warp < 2 + CONV_WARPS) {
+    // ---------------- A converters: FP32 tile (TMA-staged) -> hi/lo 16-bit tiles in the
+    // UMMA K-major 128B-swizzled layout.  Every converter arrives on a32_empty
+    // once it has read chunk g; converter thread 0 waits for that (bounded) and
+    // issues the TMA of chunk g + 2 into the same staging slot, so the intensity
+    // stream runs two chunks ahead.
+    const int t = threadIdx.x - 64;
+    const int64_t my_chunks = (tiles > blockIdx.x ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0) * nk;
+    auto issue_a = [&](int64_t gg) {
+      const int64_t tile = blockIdx.x + (gg / nk) * gridDim.x;
+      const int kk = (int)(gg % nk);
+      const int sa = (int)(gg % A32_STAGES);
+      mbar_arrive_expect_tx(&a32_full[sa], A32_BYTES);
+      tma_load_2d(a32 + sa * A32_BYTES, &tm_a, kk * BK, (int)((tile / n_nt) * BM), &a32_full[sa]);
+    };
+    if (t == 0)
+      for (int64_t gg = 0; gg < A32_STAGES && gg < my_chunks; gg++) issue_a(gg);
+    int64_t g = 0;
+    for (int64_t tile = blockIdx.x; tile < tiles && !*abort_flag; tile += gridDim.x) {
+      const int64_t r0 = (tile / n_nt) * BM;
+      for (int k = 0; k < nk; k++, g++) {
+        const int s = (int)(g % STAGES), sa = (int)(g % A32_STAGES);
+        if (!mbar_wait(&a32_full[sa], (uint32_t)(g / A32_STAGES) & 1)) {
+          fail();
+          break;
+        }
+        float4 v[CONV_ITERS];
+        const float4 *src = reinterpret_cast<const float4 *>(a32 + sa * A32_BYTES);
+#pragma unroll
+        for (int i = 0; i < CONV_ITERS; i++) v[i] = src[i * CONV_THREADS + t];
+        mbar_arrive(&a32_empty[sa]);
+        if (t == 0 && g + A32_STAGES < my_chunks) {
+          if (!mbar_wait(&a32_empty[sa], (uint32_t)(g / A32_STAGES) & 1)) {
+            fail();
+            break;
+          }
+          issue_a(g + A32_STAGES);
+        }
+        if (g >= STAGES && !mbar_wait(&empty[s], (uint32_t)((g / STAGES) - 1) & 1)) {
           fail();
           break;
         }
         if (*abort_flag) break;
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        uint8_t *st = smem + s * STAGE_BYTES;
-        const uint32_t ah = smem_u32(st), al = ah + A_BYTES;
-        const uint32_t bh = al + A_BYTES, bl = bh + B_BYTES;
-        const uint32_t acc_s = tmem + ab * ACC_STRIDE, acc_m = acc_s + nS;
+        uint8_t *ah = smem + s * STAGE_BYTES, *al = ah + A_BYTES;
 #pragma unroll
-        for (int kk = 0; kk < BK / 16; kk++) {
-          const uint32_t acc = kk > 0 ? 1u : 0u;
-          const uint32_t o = kk * 32;
-          umma(acc_s, umma_desc(ah + o), umma_desc(bh + o), idN, acc);
-          if (THREE) {
-            umma(acc_s, umma_desc(ah + o), umma_desc(bl + o), idN, 1u);
-            umma(acc_s, umma_desc(al + o), umma_desc(bh + o), idN, 1u);
+        for (int i = 0; i < CONV_ITERS; i++) {
+          const int e = i * CONV_THREADS + t, row = e >> 4, c4 = e & 15;
+          float x[4] = {v[i].x, v[i].y, v[i].z, v[i].w};
+          if (SCALED) {
+            const int64_t gr = r0 + row;
+            const float sc = gr < P.rows ? __ldg(P.scale + gr) : 1.f;
+#pragma unroll
+            for (int q = 0; q < 4; q++) x[q] *= sc;
           }
-          if (with_mom) {
-            umma(acc_m, umma_desc(ah + o), umma_desc(bh + NT * 128 + o), idM, acc);
-            if (THREE) {
-              umma(acc_m, umma_desc(ah + o), umma_desc(bl + NT * 128 + o), idM, 1u);
-              umma(acc_m, umma_desc(al + o), umma_desc(bh + NT * 128 + o), idM, 1u);
-            }
-          }
+          uint16_t h[4], l[4];
+#pragma unroll
+          for (int q = 0; q < 4; q++) Split<FORM>::run(x[q], h[q], l[q]);
+          const uint32_t off = row * 128 + ((((c4 >> 1) ^ (row & 7))) << 4) + ((c4 & 1) << 3);
+          *reinterpret_cast<uint2 *>(ah + off) =
+              make_uint2((uint32_t)h[0] | ((uint32_t)h[1] << 16), (uint32_t)h[2] | ((uint32_t)h[3] << 16));
+          if (THREE)
+            *reinterpret_cast<uint2 *>(al + off) =
+                make_uint2((uint32_t)l[0] | ((uint32_t)l[1] << 16), (uint32_t)l[2] | ((uint32_t)l[3] << 16));
         }
-        umma_commit(&empty[s]);
-        umma_commit(&acc_full[ab]);
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_arrive(&full_a[s]);
       }
     }
-  } else if (warp < 6) {
-    // ---------------- A converters (warps 2-5)
-    const int t = threadIdx.x - 64;  // 0..127
-    if (SCALED) {
-      // per-row power-of-two scale from the row maximum over all directions
-      float rmax[16];
-#pragma unroll
-      for (int i = 0; i < 16; i++) rmax[i] = 0.f;
-      for (int k = 0; k < nk; k++) {
-#pragma unroll
-        for (int i = 0; i < 16; i++) {
-          const int e = i * 128 + t, row = e >> 4, c4 = e & 15;
-          const int64_t gr = r0 + row;
-          if (gr < P.rows) {
-            const float4 v = __ldg(reinterpret_cast<const float4 *>(P.I + gr * P.M + k * BK) + c4);
-            rmax[i] = fmaxf(rmax[i], fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
-          }
-        }
-      }
-#pragma unroll
-      for (int i = 0; i < 16; i++) {
-        float m = rmax[i];
-#pragma unroll
-        for (int o = 8; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if ((t & 15) == 0) {
-          const int row = (i * 128 + t) >> 4;
-          float sc = 1.f;
-          if (m > 0.f && isfinite(m)) sc = ldexpf(1.f, 14 - ilogbf(m));
-          row_scale[row] = sc;
-        }
-      }
-      asm volatile("bar.sync 1, 128;\n" ::: "memory");
-      asm volatile("bar.arrive 2, 384;\n" ::: "memory");  // row scales ready for the accumulator warps
-    }
-    for (int k = 0; k < nk; k++) {
-      const int s = k % STAGES;
-      if (k >= STAGES && !mbar_wait(&empty[s], ((k / STAGES) - 1) & 1)) {
-        fail();
-        break;
-      }
-      if (*abort_flag) break;
-      uint8_t *ah = smem + s * STAGE_BYTES, *al = ah + A_BYTES;
-      float4 v[16];
-#pragma unroll
-      for (int i = 0; i < 16; i++) {
-        const int e = i * 128 + t, row = e >> 4, c4 = e & 15;
-        const int64_t gr = r0 + row;
-        v[i] = gr < P.rows ? __ldg(reinterpret_cast<const float4 *>(P.I + gr * P.M + k * BK) + c4)
-                           : make_float4(0.f, 0.f, 0.f, 0.f);
-      }
-#pragma unroll
-      for (int i = 0; i < 16; i++) {
-        const int e = i * 128 + t, row = e >> 4, c4 = e & 15;
-        float x[4] = {v[i].x, v[i].y, v[i].z, v[i].w};
-        if (SCALED) {
-          const float sc = row_scale[row];
-#pragma unroll
-          for (int q = 0; q < 4; q++) x[q] *= sc;
-        }
-        uint16_t h[4], l[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) Split<FORM>::run(x[q], h[q], l[q]);
-        const uint32_t off = row * 128 + ((((c4 >> 1) ^ (row & 7))) << 4) + ((c4 & 1) << 3);
-        *reinterpret_cast<uint2 *>(ah + off) =
-            make_uint2((uint32_t)h[0] | ((uint32_t)h[1] << 16), (uint32_t)h[2] | ((uint32_t)h[3] << 16));
-        if (THREE)
-          *reinterpret_cast<uint2 *>(al + off) =
-              make_uint2((uint32_t)l[0] | ((uint32_t)l[1] << 16), (uint32_t)l[2] | ((uint32_t)l[3] << 16));
-      }
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      mbar_arrive(&full_a[s]);
-    }
+    // drain: every issued intensity copy has landed before the CTA retires (bounded)
+    if (t == 0)
+      for (int64_t gg = g; gg < my_chunks && gg < g + A32_STAGES; gg++)
+        if (!mbar_wait(&a32_full[gg % A32_STAGES], (uint32_t)(gg / A32_STAGES) & 1)) fail();
   } else {
-    // ---------------- accumulator warps 6-13: warp w reads TMEM lanes 32*(w%4)..+31
-    // (one row per thread); warps 6-9 take the first half of the columns, 10-13 the second
-    const int q = warp & 3, hf = (warp - 6) >> 2;
+    // ---------------- accumulator warps: warp w reads TMEM lanes 32*(w%4)..+31 (one row
+    // per thread); the first four take the first half of the columns, the others the second
+    const int q = warp & 3, hf = (warp - 2 - CONV_WARPS) >> 2;
     const int row = q * 32 + lane;
-    const int64_t gr = r0 + row;
-    const int width = nS + (with_mom ? NMOM : 0);
-    const int half = width >> 1;  // multiple of 8
-    const int c0 = hf * half;
-    if (SCALED) asm volatile("bar.sync 2, 384;\n" ::: "memory");
-    float run[MAX_HALF];
-#pragma unroll
-    for (int j = 0; j < MAX_HALF; j++) run[j] = 0.f;
+    int64_t g = 0;
     bool ok = true;
-    for (int k = 0; k < nk && ok; k++) {
-      const int ab = k & 1;
-      if (!mbar_wait(&acc_full[ab], (k >> 1) & 1)) {
-        fail();
-        ok = false;
-        break;
-      }
-      if (*abort_flag) {
-        ok = false;
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * ACC_STRIDE + c0);
+    for (int64_t tile = blockIdx.x; tile < tiles && ok && !*abort_flag; tile += gridDim.x) {
+      const int nt = (int)(tile % n_nt);
+      const bool with_mom = (nt == 0) && P.mom != nullptr;
+      const int64_t gr = (tile / n_nt) * BM + row;
+      const int half = (nS + (with_mom ? NMOM : 0)) >> 1;  // multiple of 8
+      const int c0 = hf * half;
+      float run[MAX_HALF];
 #pragma unroll
-      for (int j = 0; j < MAX_HALF / 8; j++) {
-        if (j * 8 < half) {
-          uint32_t r[8];
-          asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
-                       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-                         "=r"(r[7])
-                       : "r"(base + j * 8));
-          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-          for (int i = 0; i < 8; i++) run[j * 8 + i] = __fadd_rn(run[j * 8 + i], __uint_as_float(r[i]));
+      for (int j = 0; j < MAX_HALF; j++) run[j] = 0.f;
+      for (int k = 0; k < nk; k++, g++) {
+        const int ab = (int)(g & 1);
+        if (!mbar_wait(&acc_full[ab], (uint32_t)(g >> 1) & 1)) {
+          fail();
+          ok = false;
+          break;
         }
-      }
-      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&acc_empty[ab]);
-    }
-    if (ok && gr < P.rows) {
-      const float inv = (SCALED ? 1.f / row_scale[row] : 1.f) * P.b_unscale;
+        if (*abort_flag) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * ACC_STRIDE + c0);
 #pragma unroll
-      for (int j = 0; j < MAX_HALF / 4; j++) {
-        const int col = c0 + 4 * j;
-        if (4 * j < half) {
-          const float4 v = make_float4(run[4 * j] * inv, run[4 * j + 1] * inv, run[4 * j + 2] * inv,
-                                       run[4 * j + 3] * inv);
-          if (col < nS)
-            *reinterpret_cast<float4 *>(P.S + gr * P.M + nt * NT + col) = v;
-          else
-            *reinterpret_cast<float4 *>(P.mom + gr * NMOM + (col - nS)) = v;
+        for (int j = 0; j < MAX_HALF / 8; j++) {
+          if (j * 8 < half) {
+            uint32_t r[8];
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7])
+                         : "r"(base + j * 8));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+            for (int i = 0; i < 8; i++) run[j * 8 + i] = __fadd_rn(run[j * 8 + i], __uint_as_float(r[i]));
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[ab]);
+      }
+      if (ok && gr < P.rows) {
+        const float inv = (SCALED ? 1.f / __ldg(P.scale + gr) : 1.f) * P.b_unscale;
+#pragma unroll
+        for (int j = 0; j < MAX_HALF / 4; j++) {
+          const int col = c0 + 4 * j;
+          if (4 * j < half) {
+            const float4 v = make_float4(run[4 * j] * inv, run[4 * j + 1] * inv, run[4 * j + 2] * inv,
+                                         run[4 * j + 3] * inv);
+            if (col < nS)
+              *reinterpret_cast<float4 *>(P.S + gr * P.M + nt * NT + col) = v;
+            else
+              *reinterpret_cast<float4 *>(P.mom + gr * NMOM + (col - nS)) = v;
+          }
         }
       }
     }
@@ -457,6 +505,9 @@ struct rrhd_scatter_tc {
   CUtensorMap tm_bh, tm_bl, tm_mh, tm_ml;
   float b_unscale = 1.f;
   int *d_err = nullptr;
+  float *d_scale = nullptr;  // row scales of the FP16 forms (grown on demand)
+  int64_t scale_cap = 0;
+  int num_sms = 148;
 };
 
 static uint16_t to_bf16(double x) {
@@ -511,6 +562,7 @@ extern "C" rrhd_status rrhd_scatter_tc_create(const rrhd_dirs *d, int32_t form, 
   t->form = form;
   t->M = M;
   t->b_unscale = (float)(1.0 / bscale);
+  cudaDeviceGetAttribute(&t->num_sms, cudaDevAttrMultiProcessorCount, d->device);
   const size_t bytes = sizeof(uint16_t) * bh.size();
   if (cudaMalloc(&t->d_bh, bytes) != cudaSuccess || cudaMalloc(&t->d_bl, bytes) != cudaSuccess ||
       cudaMalloc(&t->d_err, sizeof(int)) != cudaSuccess) {
@@ -552,6 +604,7 @@ extern "C" rrhd_status rrhd_scatter_tc_destroy(rrhd_scatter_tc *t) {
   cudaFree(t->d_bh);
   cudaFree(t->d_bl);
   cudaFree(t->d_err);
+  cudaFree(t->d_scale);
   delete t;
   return RRHD_OK;
 }
@@ -564,9 +617,27 @@ static rrhd_status launch_tc(const rrhd_scatter_tc *t, const float *I, float *S,
     RRHD_CUDA(cudaFuncSetAttribute(k_scatter_tc<FORM>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
     attr = true;
   }
-  TcParams P{I, S, mom, rows, t->M, t->b_unscale, t->d_err};
-  dim3 grid((unsigned)((rows + BM - 1) / BM), (unsigned)((t->M + NT - 1) / NT));
-  k_scatter_tc<FORM><<<grid, THREADS, SMEM_BYTES, st>>>(t->tm_bh, t->tm_bl, t->tm_mh, t->tm_ml, P);
+  constexpr bool SCALED = (FORM == FORM_F16X3 || FORM == FORM_F16);
+  if (SCALED) {
+    k_row_scale<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(I, rows, t->M, t->d_scale);
+    RRHD_CUDA(cudaGetLastError());
+  }
+  TcParams P{I, S, mom, t->d_scale, rows, t->M, t->b_unscale, t->d_err};
+  CUtensorMap tm_a;
+  {
+    auto enc = get_encode();
+    cuuint64_t dims[2] = {(cuuint64_t)t->M, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)t->M * 4};
+    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BM};
+    cuuint32_t es[2] = {1, 1};
+    if (!enc || enc(&tm_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(I), dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return rrhd_fail(RRHD_ERR_CUDA, "tensor map encoding for the intensity failed");
+  }
+  const int64_t tiles = ((rows + BM - 1) / BM) * (int64_t)(t->M < NT ? 1 : t->M / NT);
+  const unsigned grid = (unsigned)std::min<int64_t>(tiles, t->num_sms);
+  k_scatter_tc<FORM><<<grid, THREADS, SMEM_BYTES, st>>>(t->tm_bh, t->tm_bl, t->tm_mh, t->tm_ml, tm_a, P);
   RRHD_CUDA(cudaGetLastError());
   return RRHD_OK;
 }
@@ -576,6 +647,15 @@ extern "C" rrhd_status rrhd_scatter_tc_run(const rrhd_scatter_tc *t, const float
   RRHD_CHECK_ARG(t && rows >= 0, "bad arguments");
   if (rows == 0) return RRHD_OK;
   RRHD_CHECK_ARG(I && S, "null I or S");
+  if ((t->form == FORM_F16X3 || t->form == FORM_F16) && t->scale_cap < rows) {
+    rrhd_scatter_tc *tm = const_cast<rrhd_scatter_tc *>(t);
+    RRHD_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    cudaFree(tm->d_scale);
+    tm->d_scale = nullptr;
+    tm->scale_cap = 0;
+    RRHD_CUDA(cudaMalloc(&tm->d_scale, sizeof(float) * rows));
+    tm->scale_cap = rows;
+  }
   RRHD_CHECK_ARG(((uintptr_t)I & 15) == 0 && ((uintptr_t)S & 15) == 0 && ((uintptr_t)mom & 15) == 0,
                  "I, S and moments must be 16-byte aligned");
   if (rows == 0) return RRHD_OK;
