@@ -260,6 +260,63 @@ def scatter_component(dev, nhex=48, M=256, groups=1, kind=0, sigma=0.5, reps=5, 
     return out
 
 
+def c2p_component(dev, n=8_000_000, epochs=8, reps=5):
+    """Config 3: 8M states (rho, p/rho, W log-uniform; isotropic v; Gamma 4/3),
+    network trained on the first 4M, plain vs learned-guess con2prim timed on the
+    other 4M (inputs 160 MB U + 160 MB W > L2)."""
+    import torch
+    from radrhd_solver_b200 import _lib as L
+    from radrhd_solver_b200 import rhllc
+    from radrhd_solver_b200.c2p_mlp import LearnedGuess
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    W = torch.empty(n, 5, dtype=torch.float64, device=f"cuda:{dev}")
+    L.check(L.lib.rrhd_fill_c2p_states(W.data_ptr(), n, 2024, sp))
+    U = torch.empty_like(W)
+    rhllc.GetConvValueStab(W, U, eos=1, gamma=GAMMA, stream=sp)
+    h = n // 2
+    Utr, ptr_ = U[:h].contiguous(), W[:h, 4].contiguous()
+    Ute = U[h:].contiguous()
+    net = LearnedGuess(device=dev, seed=1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist = net.train(Utr, ptr_, epochs=epochs, batch=4096, lr=2e-3, seed=3, stream=sp)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    Wo = torch.empty_like(Ute)
+    Uw = torch.empty_like(Ute)
+    out = {"workload": f"{n} states (train {h}, test {n - h})", "train_s": t_train,
+           "train_loss_first_last": [float(hist[0]), float(hist[-1])]}
+    st_box = {}
+
+    def plain():
+        Uw.copy_(Ute)
+        st_box["p"] = L.C2pStats()
+        L.check(L.lib.rrhd_con2prim_batch_stats(1, GAMMA, Uw.data_ptr(), Wo.data_ptr(), None, n - h, 1,
+                                                ctypes.byref(st_box["p"]), sp))
+
+    def learned():
+        Uw.copy_(Ute)
+        st_box["l"] = L.C2pStats()
+        st_box["nb"] = ctypes.c_int64()
+        L.check(L.lib.rrhd_con2prim_batch_mlp(net.handle, 1, GAMMA, Uw.data_ptr(), Wo.data_ptr(), None, n - h, 1, 8,
+                                              ctypes.byref(st_box["l"]), ctypes.byref(st_box["nb"]), None, sp))
+
+    def copy_only():
+        Uw.copy_(Ute)
+    t_copy = _time(copy_only, reps, stream)
+    for name, fn in (("plain_guess", plain), ("learned_guess", learned)):
+        ms = _time(fn, reps, stream) - t_copy
+        key = "p" if name == "plain_guess" else "l"
+        st = st_box[key]
+        out[name] = {"ms": ms, "states_per_s": (n - h) / (ms / 1e3), "newton_iters_per_state": st.newton_iters / (n - h),
+                     "max_iters": st.max_iters, "pressure_fix_fallbacks": st.n_fallback, "failed": st.n_failed}
+        if key == "l":
+            out[name]["guess_fallbacks"] = st_box["nb"].value
+    net.close()
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -362,6 +419,8 @@ def run_ours(args):
         dt, kind = reference_steps(m, Wg, Ug, args.cpu_steps, threads, inflow_conservative())
         line["cpu_baseline"] = {"value": m.n_cells / dt, "unit": UNIT, "cores": threads, "kind": kind,
                                 "sample": f"{args.cpu_steps} full steps of the {m.n_cells}-cell mesh"}
+    if rank == 0 and not args.no_c2p:
+        line["c2p"] = c2p_component(dev)
     if rank == 0 and not args.no_scatter:
         line["scatter"] = scatter_component(dev)
         sc = line["scatter"]
@@ -385,6 +444,7 @@ def main():
     ap.add_argument("--nhex", type=int, default=96, help="hexes per axis (96 = the benchmark mesh)")
     ap.add_argument("--cpb", type=int, default=0, help="cells per CTA of the step kernel (0 = library default)")
     ap.add_argument("--no-scatter", action="store_true", help="skip the scattering component")
+    ap.add_argument("--no-c2p", action="store_true", help="skip the con2prim (learned guess) component")
     ap.add_argument("--scatter-only", type=int, default=0, metavar="NHEX",
                     help="only time the scattering component on an NHEX^3 x 6 mesh (profiling runs)")
     args = ap.parse_args()

@@ -191,6 +191,42 @@ rrhd_status rrhd_con2prim_batch_stats_noalloc(int32_t eos, double gamma, double 
                                               uint8_t *status, int64_t n, int32_t fallback,
                                               rrhd_c2p_stats *stats, void *stream);
 
+/* ------------------------------------------------ learned con2prim guess
+ * A 3-64-64-1 ReLU network predicting log(p/tau), tau = E - D, from
+ * (log(Q/tau), log(|S|/tau), log(tau/D)), Q = E - sqrt(|S|^2 + D^2) (all built in
+ * FP64 from D, |S|/tau, tau/D); trained on the device by this library's
+ * own forward/backward/Adam kernels; its prediction seeds the Newton solve of
+ * rhllc::GetPhysValueStab (rhllc_flux_stab.cpp:123-220), which has no learned
+ * part of its own.  Parameters: 4481 floats = W1[64][3], b1[64], W2[64][64]
+ * (row = output), b2[64], W3[64], b3; normalisation: 8 floats = mu[3],
+ * sigma[3] of the features, mu, sigma of the target. */
+typedef struct rrhd_mlp rrhd_mlp;
+int32_t rrhd_mlp_num_params(void);
+rrhd_status rrhd_mlp_create(int32_t device, uint64_t seed, rrhd_mlp **out);
+rrhd_status rrhd_mlp_destroy(rrhd_mlp *m);
+/* host copies of the parameters / normalisation (either pointer may be NULL) */
+rrhd_status rrhd_mlp_set(rrhd_mlp *m, const float *theta, const float *norm);
+rrhd_status rrhd_mlp_get(const rrhd_mlp *m, float *theta, float *norm);
+/* Adam on labelled states U [n][5], p [n] (device): mini-batches of `batch`
+ * (multiple of 128) in a seeded order; lr halved at 50 % and 75 % of the epochs;
+ * set_norm != 0 derives the normalisation from the data; loss_hist (host
+ * [epochs], may be NULL) gets each epoch's mean squared normalised error. */
+rrhd_status rrhd_mlp_train(rrhd_mlp *m, const double *U, const double *p, int64_t n, int32_t epochs,
+                           int32_t batch, float lr, uint64_t seed, int32_t set_norm, float *loss_hist,
+                           void *stream);
+/* Gradient (host [4481]) and loss of the mean squared normalised error over
+ * all n labelled states at the current parameters. */
+rrhd_status rrhd_mlp_gradient(rrhd_mlp *m, const double *U, const double *p, int64_t n, float *grad,
+                              float *loss);
+/* con2prim batch seeded by the network: Newton from the learned guess for at
+ * most k_stall iterations, else the reference solve from its own guess, then
+ * PhysPressureFix when fallback != 0.  stats / n_guess_fallback (host) and
+ * guess (device [n], the learned initial pressures) may be NULL. */
+rrhd_status rrhd_con2prim_batch_mlp(const rrhd_mlp *m, int32_t eos, double gamma, double *U, double *W,
+                                    uint8_t *status, int64_t n, int32_t fallback, int32_t k_stall,
+                                    rrhd_c2p_stats *stats, int64_t *n_guess_fallback, double *guess,
+                                    void *stream);
+
 /* prim->cons for n states, device pointers: rhllc::GetConvValueStab. */
 rrhd_status rrhd_prim2con_batch(int32_t eos, double gamma, double *W, double *U, int64_t n,
                                 void *stream);

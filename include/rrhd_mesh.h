@@ -59,6 +59,11 @@ rrhd_status rrhd_fill_intensity_f32(float *I, int64_t rows, int32_t M, int32_t g
 rrhd_status rrhd_fill_intensity_f64(double *I, int64_t rows, int32_t M, int32_t groups, int32_t kind,
                                     double sigma, const double *centers, uint64_t seed, void *stream);
 
+/* Primitive states W [n][5] on the device for the con2prim benchmark: rho
+ * log-uniform [1e-4, 1e2], p/rho log-uniform [1e-6, 1e2], Lorentz factor
+ * log-uniform [1, 50], isotropic velocity direction (counter-based RNG). */
+rrhd_status rrhd_fill_c2p_states(double *W, int64_t n, uint64_t seed, void *stream);
+
 /* Counter-based uniform [0,1) variate: the same value on host and device. */
 double rrhd_rng_u01(uint64_t seed, uint64_t stream, uint64_t index);
 

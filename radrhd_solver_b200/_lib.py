@@ -112,6 +112,15 @@ _SIGS = {
     "rrhd_rng_u01": (D, [U64, U64, U64]),
     "rrhd_fill_intensity_f32": (I32, [P, I64, I32, I32, I32, D, P, U64, P]),
     "rrhd_fill_intensity_f64": (I32, [P, I64, I32, I32, I32, D, P, U64, P]),
+    "rrhd_fill_c2p_states": (I32, [P, I64, U64, P]),
+    "rrhd_mlp_num_params": (I32, []),
+    "rrhd_mlp_create": (I32, [I32, U64, P]),
+    "rrhd_mlp_destroy": (I32, [P]),
+    "rrhd_mlp_set": (I32, [P, P, P]),
+    "rrhd_mlp_get": (I32, [P, P, P]),
+    "rrhd_mlp_train": (I32, [P, P, P, I64, I32, I32, C.c_float, U64, I32, P, P]),
+    "rrhd_mlp_gradient": (I32, [P, P, P, I64, P, P]),
+    "rrhd_con2prim_batch_mlp": (I32, [P, I32, D, P, P, P, I64, I32, I32, P, P, P, P]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

@@ -33,6 +33,7 @@ SOURCES = {
     "radiation_fp64.cu": ["--fmad=false"],
     "scatter_tc.cu": [],
     "synth.cu": [],
+    "c2p_mlp.cu": ["--fmad=false"],
 }
 
 

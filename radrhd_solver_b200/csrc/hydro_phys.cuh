@@ -164,7 +164,7 @@ __device__ __forceinline__ int pressure_fix(const Eos &e, double *U, double *W) 
 // the initial guess p0; returns the reference's code (5 where it would abort).
 // W is written only on success.  iters (if non-null) gets the Newton count.
 __device__ __forceinline__ int c2p_from(const Eos &e, const double *U, double *W, double p0,
-                                        bool use_guess, int *iters) {
+                                        bool use_guess, int *iters, int max_iter = RRHD_MAX_ITER) {
   const double tol = 1.e-11;
   const double eps2 = 1.e-12;
   const double D = U[0];
@@ -180,7 +180,7 @@ __device__ __forceinline__ int c2p_from(const Eos &e, const double *U, double *W
   p = smax(p, pmin);
   double alpha, alpha2, lor2, lor, tau, theta, h, dh_dp, dh_dtau, yp = 0, dp, dyp;
   int iter;
-  for (iter = 0; iter < RRHD_MAX_ITER; iter++) {
+  for (iter = 0; iter < max_iter; iter++) {
     alpha = E + p;
     alpha2 = alpha * alpha;
     lor2 = 1.0 - m2 / alpha2;
@@ -212,7 +212,7 @@ __device__ __forceinline__ int c2p_from(const Eos &e, const double *U, double *W
   if (iters) *iters = iter;
   if (p < 0.0) return 2;
   if (isnan(p)) return 4;
-  if (iter >= RRHD_MAX_ITER || fabs(yp / (E + p)) > 1.e-4 || p < (m - E)) return 3;
+  if (iter >= max_iter || fabs(yp / (E + p)) > 1.e-4 || p < (m - E)) return 3;
   alpha = E + p;
   alpha2 = alpha * alpha;
   lor2 = alpha2 / (alpha2 - m2);

@@ -32,7 +32,37 @@ __global__ void k_fill(T *I, int64_t rows, int M, int groups, int kind, double s
   I[i] = (T)v;
 }
 
+// Config-3 primitive states: rho log-uniform [1e-4, 1e2], p/rho log-uniform
+// [1e-6, 1e2], Lorentz factor log-uniform [1, 50], isotropic velocity direction.
+__global__ void k_fill_states(double *W, int64_t n, uint64_t seed) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double u0 = rrhd_u01(seed, 101, (uint64_t)i), u1 = rrhd_u01(seed, 102, (uint64_t)i);
+  const double u2 = rrhd_u01(seed, 103, (uint64_t)i), u3 = rrhd_u01(seed, 104, (uint64_t)i);
+  const double u4 = rrhd_u01(seed, 105, (uint64_t)i);
+  const double rho = exp10(-4.0 + 6.0 * u0);
+  const double p = rho * exp10(-6.0 + 8.0 * u1);
+  const double lor = exp10(u2 * log10(50.0));
+  const double v = sqrt(1.0 - 1.0 / (lor * lor));
+  const double mu = 2.0 * u3 - 1.0, s = sqrt(fmax(0.0, 1.0 - mu * mu));
+  const double ph = 2.0 * u4;  // in units of pi
+  double *w = W + 5 * i;
+  w[0] = rho;
+  w[1] = v * s * cospi(ph);
+  w[2] = v * s * sinpi(ph);
+  w[3] = v * mu;
+  w[4] = p;
+}
+
 }  // namespace
+
+extern "C" rrhd_status rrhd_fill_c2p_states(double *W, int64_t n, uint64_t seed, void *stream) {
+  RRHD_CHECK_ARG(n >= 0 && (W || n == 0), "bad arguments");
+  if (n == 0) return RRHD_OK;
+  k_fill_states<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(W, n, seed);
+  RRHD_CUDA(cudaGetLastError());
+  return RRHD_OK;
+}
 
 template <class T>
 static rrhd_status fill(T *I, int64_t rows, int32_t M, int32_t groups, int32_t kind, double sigma,
