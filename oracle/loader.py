@@ -40,6 +40,11 @@ class OrcBc(C.Structure):
     _fields_ = [("kind", I32 * 8), ("W", (D * 5) * 8), ("U", (D * 5) * 8)]
 
 
+class OrcSweepMesh(C.Structure):
+    _fields_ = [("n_cells", I64), ("n_faces", I64), ("cell_volume", P), ("cell_faces", P), ("cell_nbr", P),
+                ("cell_sign", P), ("face_n", P), ("face_area", P)]
+
+
 class OrcEmission(C.Structure):
     _fields_ = [("temp_coef", D), ("sigma_sb", D), ("pi", D), ("rad_unit", D)]
 
@@ -57,6 +62,9 @@ def port() -> C.CDLL:
             "orc_scatter": (None, [I64, I32, P, P, P, D, P, C.c_int]),
             "orc_moments": (None, [I64, I32, P, P, P, D, P, P, P, C.c_int]),
             "orc_rad_source": (None, [I64, P, P, P, P, P, P, P, P]),
+            "orc_get_illum": (D, [P, P, D, D]), "orc_get_rhs": (D, [D, D, D, D, P]),
+            "orc_recalc_illum": (D, [I64, P, P, P, I32, I32, P]),
+            "orc_sweep": (I64, [P, I32, P, I32, P, P, P, P, D, P]),
         }
         for n, (r, a) in sig.items():
             f = getattr(lib, n)
@@ -90,6 +98,8 @@ def ref(variant: str) -> C.CDLL | None:
         "ref_moments": (None, [I64, I32, P, P, P, D, P, P, P, C.c_int]),
         "ref_rad_source": (None, [I64, P, P, P, P, P, P, P]), "ref_rad_constants": (None, [P]),
         "ref_eos": (C.c_int, []),
+        "ref_get_illum": (D, [P, P, D, D]), "ref_get_rhs": (D, [D, D, D, D, P]),
+        "ref_recalc_illum": (D, [I64, I64, P, P, P, I32, I32, P]),
     }
     for n, (r, a) in sig.items():
         f = getattr(lib, n, None)
@@ -335,3 +345,82 @@ def ref_rad_source(W, alpha, sigma, E, F, T, variant="rad_ideal_4_3"):
     arrs = [np.ascontiguousarray(a, np.float64) for a in (W, alpha, sigma, E, F, T)]
     lib.ref_rad_source(N, *(_p(a) for a in arrs), _p(G))
     return G
+
+
+def port_get_illum(I0, s, k, rhs):
+    I0 = np.ascontiguousarray(I0, np.float64)
+    s = np.ascontiguousarray(s, np.float64)
+    return port().orc_get_illum(_p(I0), _p(s), k, rhs)
+
+
+def port_get_rhs(alpha, betta, Q, S):
+    k = C.c_double()
+    r = port().orc_get_rhs(alpha, betta, Q, S, C.byref(k))
+    return r, k.value
+
+
+def port_recalc_illum(cell_faces, face_area, face_values, Illum, direction):
+    """Rewrites column `direction` of Illum [N][M] in place; returns the norm."""
+    cf = np.ascontiguousarray(cell_faces, np.int32)
+    fa = np.ascontiguousarray(face_area, np.float64)
+    fv = np.ascontiguousarray(face_values, np.float64)
+    assert Illum.flags.c_contiguous and Illum.dtype == np.float64
+    return port().orc_recalc_illum(len(cf), _p(cf), _p(fa), _p(fv), Illum.shape[1], direction, _p(Illum))
+
+
+def sweep_neighbours(mesh):
+    """[N][4] neighbour across each local face (-1 on the boundary) of a Mesh."""
+    cf = np.asarray(mesh.cell_faces)
+    l, r = np.asarray(mesh.face_id_l), np.asarray(mesh.face_id_r)
+    own = np.arange(len(cf))[:, None]
+    nl, nr = l[cf], r[cf]
+    nb = np.where(nl == own, nr, nl)
+    return np.where(nb < 0, -1, nb).astype(np.int32)
+
+
+def port_sweep(mesh, dirs, alpha, betta, Q, S, bc=0.0, I=None):
+    """orc_sweep on a Mesh: returns (I [N*G][M], unswept pairs).  I (optional) is the
+    previous intensity; only the relative-change norm would read it."""
+    N, F = mesh.n_cells, mesh.n_faces
+    Q = np.ascontiguousarray(Q, np.float64).reshape(N, -1)
+    G = Q.shape[1]
+    dirs = np.ascontiguousarray(dirs, np.float64)
+    M = len(dirs)
+    S = np.ascontiguousarray(S, np.float64).reshape(N * G, M)
+    keep = [np.ascontiguousarray(mesh.cell_volume, np.float64),
+            np.ascontiguousarray(mesh.cell_faces, np.int32), sweep_neighbours(mesh),
+            np.ascontiguousarray(mesh.cell_sign, np.uint8), np.ascontiguousarray(mesh.face_n, np.float64),
+            np.ascontiguousarray(mesh.face_area, np.float64)]
+    sm = OrcSweepMesh(N, F, *(_p(a) for a in keep))
+    a = np.ascontiguousarray(alpha, np.float64)
+    b = np.ascontiguousarray(betta, np.float64)
+    I = np.zeros((N * G, M)) if I is None else np.array(I, np.float64, order="C")
+    missing = port().orc_sweep(C.byref(sm), M, _p(dirs), G, _p(a), _p(b), _p(Q), _p(S), bc, _p(I))
+    return I, missing
+
+
+def ref_get_illum(I0, s, k, rhs, variant="rad_ideal_4_3"):
+    I0 = np.ascontiguousarray(I0, np.float64)
+    s = np.ascontiguousarray(s, np.float64)
+    return ref(variant).ref_get_illum(_p(I0), _p(s), k, rhs)
+
+
+def ref_get_rhs(alpha, betta, T, S, variant="rad_ideal_4_3"):
+    k = C.c_double()
+    r = ref(variant).ref_get_rhs(alpha, betta, T, S, C.byref(k))
+    return r, k.value
+
+
+def ref_recalc_illum(cell_faces, face_area, face_values, Illum, direction, variant="rad_ideal_4_3"):
+    cf = np.ascontiguousarray(cell_faces, np.int32)
+    fa = np.ascontiguousarray(face_area, np.float64)
+    fv = np.ascontiguousarray(face_values, np.float64)
+    assert Illum.flags.c_contiguous and Illum.dtype == np.float64
+    return ref(variant).ref_recalc_illum(len(cf), len(fa), _p(cf), _p(fa), _p(fv), Illum.shape[1], direction,
+                                         _p(Illum))
+
+
+def ref_rad_constants(variant="rad_ideal_4_3"):
+    out = np.zeros(4)
+    ref(variant).ref_rad_constants(_p(out))
+    return out

@@ -39,6 +39,7 @@
 #include "radRHD_utils.h"
 #include "plunk.h"
 #include "gas_state.h"
+#include "illum_utils.h"
 #endif
 
 namespace {
@@ -364,6 +365,13 @@ void ref_moments(int64_t N, int32_t M, const double *I, const double *dirs, cons
 #endif  // RRHD_SHIM_ILLUM
 
 #if defined RRHD_SHIM_RAD
+}  // extern "C"
+// Definitions that lib/grids/src/solvers_struct.cpp normally provides; that file
+// does not compile with ILLUM, and none of the entry points below reach these.
+solve_mode_t _solve_mode;
+Type TableFunc::operator()(Type, Type) { return 0.0; }
+extern "C" {
+
 // rad_rhd::GetRadSource (solvers/RadRHD/src/radRHD_utils.cpp:44-101) for each
 // cell.  W [N][5] primitive state, alpha/sigma [N] opacities, E [N], F [N][3],
 // T [N][3][3] row-major radiation moments.  G [N][4].
@@ -401,6 +409,55 @@ void ref_rad_source(int64_t N, const double *W, const double *alpha, const doubl
   g->stream = nullptr;
   g->impuls = nullptr;
   g->cells.clear();
+}
+
+// Out-face intensity of one short characteristic: illum::GetIllum(I0, s, k, rhs)
+// (solvers/illum/src/illum_utils.cpp:454-490); I0 and s hold 3 values each.
+double ref_get_illum(const double *I0, const double *s, double k, double rhs) {
+  alignas(32) double i0[4] = {I0[0], I0[1], I0[2], 0.0};
+  alignas(32) double ss[4] = {s[0], s[1], s[2], 0.0};
+  return illum::GetIllum(i0, ss, k, rhs);
+}
+
+// Source function of the transfer equation: illum::GetRhsOpt
+// (illum_utils.cpp:631-646) for a cell with opacities alpha, betta and
+// temperature T; returns rhs, k_out = alpha + betta.
+double ref_get_rhs(double alpha, double betta, double T, double S, double *k_out) {
+  elem_t cell;
+  full_phys_data_t data;
+  data.alpha = alpha;
+  data.betta = betta;
+  data.T = T;
+  cell.cell_data = &data;
+  Type k = 0;
+  const double r = illum::GetRhsOpt(Vector3(0, 0, 0), S, cell, k);
+  cell.cell_data = nullptr;
+  *k_out = k;
+  return r;
+}
+
+// Cell intensities from face values for one direction:
+// illum::separate_gpu::ReCalcIllumOpt (illum_utils.cpp:377-433).  Illum [N][M]
+// in/out (column `dir` is rewritten); returns the norm it computes.
+double ref_recalc_illum(int64_t N, int64_t F, const int32_t *cell_faces, const double *face_area,
+                        const double *face_values, int32_t M, int32_t dir, double *Illum) {
+  static grid_t *g = new grid_t();  // see ref_rad_source for why it is kept
+  g->cells.clear();
+  g->faces.clear();
+  g->size = N;
+  g->size_dir = M;
+  g->cells.resize(N);
+  g->faces.resize(F);
+  for (int64_t c = 0; c < N; c++)
+    for (int j = 0; j < 4; j++) g->cells[c].geo.id_faces[j] = cell_faces[4 * c + j];
+  for (int64_t f = 0; f < F; f++) g->faces[f].geo.S = face_area[f];
+  std::vector<Type> coef(face_values, face_values + F);
+  g->Illum = Illum;
+  const double norm = illum::separate_gpu::ReCalcIllumOpt(dir, coef, *g, 0);
+  g->Illum = nullptr;
+  g->cells.clear();
+  g->faces.clear();
+  return norm;
 }
 
 // The emission constants the reference compiles in: GetTemperature's

@@ -12,6 +12,7 @@
 
 #include <math.h>
 #include <stddef.h>
+#include <stdlib.h>
 #include <string.h>
 
 #define MAX_ITER 40 /* solvers/rhllc/src/rhllc_flux_stab.cpp:8 */
@@ -519,4 +520,163 @@ void orc_rad_source(int64_t N, const orc_emission *em, const double *W, const do
       G[4 * c + i + 1] = q * u[i] - rho * (tot_op * uD[i] + scat_op * u[i] * (gamma2 + uuD)) * Ur +
                          rhogamma * (tot_op * Fr[i] + scat_op * 2.0 * uF * u[i]);
   }
+}
+
+/* ------------------------------------------------------------------ sweep */
+
+/* illum::GetIllum, solvers/illum/src/illum_utils.cpp:454-490 (TRANSFER_CELL_TO_FACE) */
+double orc_get_illum(const double *I0, const double *s, double k, double rhs) {
+  double Icur = exp(-k * s[0]) * (I0[0] - rhs) + rhs;
+  Icur += (exp(-k * s[1]) * (I0[1] - rhs) + rhs);
+  Icur += (exp(-k * s[2]) * (I0[2] - rhs) + rhs);
+  return (Icur * 0.3333333333333333);
+}
+
+/* illum::GetRhsOpt, illum_utils.cpp:631-646 (Q = B_Plank(T) / kRadiation given) */
+double orc_get_rhs(double alpha, double betta, double Q, double S, double *k) {
+  *k = alpha + betta;
+  return (alpha * Q + betta * S) / *k;
+}
+
+/* illum::separate_gpu::ReCalcIllumOpt, illum_utils.cpp:377-433: area-weighted face
+ * mean for every cell but the last, plain mean for the last one. */
+double orc_recalc_illum(int64_t N, const int32_t *cell_faces, const double *face_area,
+                        const double *fv, int32_t M, int32_t dir, double *Illum) {
+  double norm = -1;
+  for (int64_t c = 0; c < N - 1; c++) {
+    const size_t id = (size_t)c * M + dir;
+    double curI = 0, S = 0;
+    for (int j = 0; j < 4; j++) {
+      const int32_t f = cell_faces[4 * c + j];
+      curI += fv[f] * face_area[f];
+      S += face_area[f];
+    }
+    curI /= S;
+    norm = smax(norm, fabs((Illum[id] - curI) / curI));
+    Illum[id] = curI;
+  }
+  {
+    const int64_t c = N - 1;
+    const size_t id = (size_t)c * M + dir;
+    double curI = 0;
+    for (int j = 0; j < 4; j++) curI += fv[cell_faces[4 * c + j]];
+    curI /= 4;
+    norm = smax(norm, fabs((Illum[id] - curI) / curI));
+    Illum[id] = curI;
+  }
+  return norm;
+}
+
+/* Short characteristics of the out-face j of a cell for direction w.  The three
+ * interpolation nodes of the face (barycentric weight 2/3 at one face vertex and
+ * 1/6 at the other two: the nodes of BaseTetra_t, lib/geometry/include/geo_types.h:163-212)
+ * are traced back along -w to the in-face the ray leaves the cell through: the
+ * in-face h (cos_h = n_h.w < 0) with the smallest ray parameter
+ *     t_h = lam_h * (H_h / -cos_h),
+ * lam_h the node's barycentric weight of vertex h (the vertex opposite face h) and
+ * H_h = 3 V / A_h that vertex's height over face h, since the signed distance of a
+ * point to the plane of face h is -lam_h H_h.  First in face order on ties.
+ * Output: in-face index h[3] and distance s[3]. */
+static void trace_face(const double *H, const double *cosf, int j, int *h, double *s) {
+  double r[4];
+  for (int f = 0; f < 4; f++) r[f] = cosf[f] < 0 ? H[f] / -cosf[f] : 0.0;
+  for (int q = 0; q < 3; q++) {
+    const int vq = (j + 1 + q) & 3;
+    double tmin = 0;
+    int hmin = -1;
+    for (int f = 0; f < 4; f++) {
+      if (!(cosf[f] < 0)) continue;
+      const double lam = f == vq ? 2.0 / 3.0 : 1.0 / 6.0;
+      const double t = lam * r[f];
+      if (hmin < 0 || t < tmin) {
+        tmin = t;
+        hmin = f;
+      }
+    }
+    h[q] = hmin;
+    s[q] = tmin;
+  }
+}
+
+/* Outward normal of local face j of cell c: the mesh face normal signed by the
+ * cell's orientation bit, so two neighbours classify a shared face consistently. */
+static void cell_normal(const orc_sweep_mesh *m, int64_t c, int j, double *n) {
+  const double *fn = m->face_n + 3 * (int64_t)m->cell_faces[4 * c + j];
+  if ((m->cell_sign[c] >> j) & 1) {
+    n[0] = fn[0];
+    n[1] = fn[1];
+    n[2] = fn[2];
+  } else {
+    n[0] = -fn[0];
+    n[1] = -fn[1];
+    n[2] = -fn[2];
+  }
+}
+
+int64_t orc_sweep(const orc_sweep_mesh *m, int32_t M, const double *dirs, int32_t G, const double *alpha,
+                  const double *betta, const double *Q, const double *S, double bc, double *I) {
+  const int64_t N = m->n_cells, F = m->n_faces;
+  double *geo = (double *)malloc(sizeof(double) * 16 * N); /* n_j[3], then H_j */
+  for (int64_t c = 0; c < N; c++) {
+    for (int j = 0; j < 4; j++) {
+      cell_normal(m, c, j, geo + 16 * c + 3 * j);
+      geo[16 * c + 12 + j] = 3.0 * m->cell_volume[c] / m->face_area[m->cell_faces[4 * c + j]];
+    }
+  }
+  double *fv = (double *)malloc(sizeof(double) * F * G);
+  double *col = (double *)malloc(sizeof(double) * N * M);
+  double *fvg = (double *)malloc(sizeof(double) * F);
+  int32_t *indeg = (int32_t *)malloc(sizeof(int32_t) * N);
+  int64_t *queue = (int64_t *)malloc(sizeof(int64_t) * N);
+  int64_t missing = 0;
+  for (int32_t dd = 0; dd < M; dd++) {
+    const double *w = dirs + 3 * dd;
+    /* faces nobody writes in this direction (boundary in-faces, faces parallel to w)
+     * hold the boundary value */
+    for (int64_t i = 0; i < F * G; i++) fv[i] = bc;
+    int64_t qh = 0, qt = 0;
+    for (int64_t c = 0; c < N; c++) {
+      int cnt = 0;
+      for (int j = 0; j < 4; j++)
+        if (dot3(geo + 16 * c + 3 * j, w) < 0 && m->cell_nbr[4 * c + j] >= 0) cnt++;
+      indeg[c] = cnt;
+      if (cnt == 0) queue[qt++] = c;
+    }
+    while (qh < qt) {
+      const int64_t c = queue[qh++];
+      double cosf[4];
+      for (int j = 0; j < 4; j++) cosf[j] = dot3(geo + 16 * c + 3 * j, w);
+      for (int j = 0; j < 4; j++) {
+        if (!(cosf[j] > 0)) continue;
+        int h[3];
+        double sdist[3];
+        trace_face(geo + 16 * c + 12, cosf, j, h, sdist);
+        for (int g = 0; g < G; g++) {
+          double I0[3], k, rhs;
+          for (int q = 0; q < 3; q++) {
+            const int hf = h[q];
+            I0[q] = (hf >= 0 && m->cell_nbr[4 * c + hf] >= 0) ? fv[(int64_t)m->cell_faces[4 * c + hf] * G + g] : bc;
+          }
+          rhs = orc_get_rhs(alpha[c], betta[c], Q[c * G + g], S[((size_t)c * G + g) * M + dd], &k);
+          fv[(int64_t)m->cell_faces[4 * c + j] * G + g] = orc_get_illum(I0, sdist, k, rhs);
+        }
+        const int32_t nb = m->cell_nbr[4 * c + j];
+        if (nb >= 0 && --indeg[nb] == 0) queue[qt++] = nb;
+      }
+    }
+    missing += N - qt;
+    for (int g = 0; g < G; g++) {
+      for (int64_t f = 0; f < F; f++) fvg[f] = fv[f * G + g];
+      for (int64_t c = 0; c < N; c++) col[(size_t)c * M + dd] = I[((size_t)c * G + g) * M + dd];
+      orc_recalc_illum(N, m->cell_faces, m->face_area, fvg, M, dd, col);
+      for (int64_t c = 0; c < N; c++) I[((size_t)c * G + g) * M + dd] = col[(size_t)c * M + dd];
+    }
+  }
+  free(geo);
+  free(fv);
+  free(col);
+  free(fvg);
+  free(indeg);
+  free(queue);
+  return missing;
 }

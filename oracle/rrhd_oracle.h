@@ -84,6 +84,37 @@ void orc_rad_source(int64_t N, const orc_emission *em, const double *W, const do
                     const double *sigma, const double *E, const double *F, const double *T,
                     double *G);
 
+/* ---------------------------------------------------------------- transport sweep
+ * Short-characteristics sweep of solvers/illum/src/mpi/multi_gpu/illum_multi_gpu_face_calc.cpp:91-190
+ * on a tetrahedral mesh.  Local face j of a cell is the face opposite its vertex j
+ * (cell_faces[c][j], the ConvertBinToGeo order); cell_nbr[c][j] is the cell across
+ * it or -1 on the boundary (intensity bc there).  The outward normal of a cell's
+ * face is the mesh face normal signed by cell_sign, so two neighbours always
+ * classify their shared face consistently (in for one, out for the other). */
+typedef struct {
+  int64_t n_cells, n_faces;
+  const double *cell_volume;    /* [N] */
+  const int32_t *cell_faces;    /* [N][4] */
+  const int32_t *cell_nbr;      /* [N][4] */
+  const uint8_t *cell_sign;     /* [N] bit j: face j's normal is outward for this cell */
+  const double *face_n;         /* [F][3] */
+  const double *face_area;      /* [F] */
+} orc_sweep_mesh;
+
+/* illum::GetIllum (solvers/illum/src/illum_utils.cpp:454-490) */
+double orc_get_illum(const double *I0, const double *s, double k, double rhs);
+/* illum::GetRhsOpt (illum_utils.cpp:631-646) with the emission Q given */
+double orc_get_rhs(double alpha, double betta, double Q, double S, double *k);
+/* illum::separate_gpu::ReCalcIllumOpt (illum_utils.cpp:377-433): writes column dir
+ * of Illum [N][M] from face values [F]; returns the relative-change norm. */
+double orc_recalc_illum(int64_t N, const int32_t *cell_faces, const double *face_area,
+                        const double *face_values, int32_t M, int32_t dir, double *Illum);
+/* One sweep of all M directions and G groups: S [N*G][M] (rows cell*G+g) in,
+ * I [N*G][M] out.  alpha, betta [N]; Q [N][G] emission per group.  Returns the
+ * number of (cell, direction) pairs a dependency cycle left unswept (0 normally). */
+int64_t orc_sweep(const orc_sweep_mesh *m, int32_t M, const double *dirs, int32_t G, const double *alpha,
+               const double *betta, const double *Q, const double *S, double bc, double *I);
+
 #ifdef __cplusplus
 }
 #endif
