@@ -309,6 +309,73 @@ rrhd_status rrhd_rad_source(const rrhd_emission *em, const double *W, const doub
                             const double *sigma, const double *E, const double *F, const double *T,
                             double *G, int64_t n, void *stream);
 
+/* ------------------------------------------------------------ transport sweep
+ * Short-characteristics sweep of illum::separate_gpu::CalculateIllum
+ * (solvers/illum/src/mpi/multi_gpu/illum_multi_gpu_face_calc.cpp:20-190, one
+ * iteration of its direction loop): for every direction, cells in upwind order;
+ * each out-face value is the mean over its three interpolation nodes of
+ * illum::GetIllum (illum_utils.cpp:454-490) with the source illum::GetRhsOpt
+ * (illum_utils.cpp:631-646); each cell value is illum::separate_gpu::ReCalcIllumOpt
+ * (illum_utils.cpp:377-433), area-weighted face mean (plain mean for the last
+ * cell).  The upwind order (the reference's sorted_graph, made offline by its
+ * graph/ and make_trace/ tools) is built on the device at setup as levels of
+ * cells whose upwind neighbours are all done; one level is one kernel launch,
+ * all launches of a sweep are one CUDA graph. */
+#define RRHD_RAD_FP64 0 /* sweep arithmetic and storage in double */
+#define RRHD_RAD_FP32 1 /* in float (input of the tensor-core scattering) */
+typedef struct {
+  int32_t groups;         /* frequency groups G >= 1 (grey copies, rows cell * G + g)           */
+  int32_t precision;      /* RRHD_RAD_FP64 or RRHD_RAD_FP32                                     */
+  int32_t dirs_per_batch; /* directions swept together: power of two <= 64; 0 = min(64, M)      */
+  double boundary_value;  /* intensity entering through boundary faces (illum::BoundaryConditions
+                             returns 0 for free, lock and outer boundaries, illum_utils.cpp:52-65) */
+} rrhd_rad_opts;
+/* Builds the sweep geometry and plan for ctx's mesh and the direction set (which
+ * must outlive the context's radiation use).  RRHD_ERR_STATE if the mesh has a
+ * dependency cycle for some direction. */
+rrhd_status rrhd_rad_setup(rrhd_ctx *ctx, const rrhd_dirs *dirs, const rrhd_rad_opts *opts);
+/* Levels summed over direction batches and the largest level (items). */
+rrhd_status rrhd_rad_plan_info(const rrhd_ctx *ctx, int64_t *levels, int64_t *max_level_items);
+/* One sweep of all directions and groups on ctx's stream.  Device pointers of the
+ * setup's precision (double or float), caller cell numbering: alpha, betta [N]
+ * absorption and scattering coefficients, Q [N][G] emission B / kRadiation per
+ * group, S [N*G][M] scattering integral in, I [N*G][M] intensity out. */
+rrhd_status rrhd_sweep(rrhd_ctx *ctx, const void *alpha, const void *betta, const void *Q, const void *S, void *I);
+
+/* ------------------------------------------------------------ coupled step
+ * One step of the RadRHD loop (solvers/RadRHD/src/radRHD_main.cpp:96-139):
+ * rhllc::Hllc3dStab; opacities alpha = absorption rho, betta = scattering rho and
+ * emission Q = B(T) / kRadiation / G from the new primitives; the sweep with the
+ * scattering integral of the previous step; the 4-force rad_rhd::GetRadSource
+ * from the moments of the previous step's intensity (the reference computes them
+ * asynchronously at the start of each radiation iteration, before the sweep,
+ * illum_multi_gpu_face_calc.cpp:59-66) added as U.E += tau G0, U.S += tau G,
+ * then con2prim without fallback; finally the scattering integral and moments
+ * of the new intensity for the next step. */
+#define RRHD_SCATTER_FP64 (-1) /* rrhd_scatter_fp64_fma + rrhd_moments_fp64 (RRHD_RAD_FP64) */
+typedef struct {
+  int32_t scatter;        /* RRHD_SCATTER_FP64, or an RRHD_TC_* form (RRHD_RAD_FP32)             */
+  const rrhd_mlp *guess;  /* NULL: the reference's initial guess in the source con2prim; else the
+                             learned guess (Newton for at most k_stall iterations from it)        */
+  int32_t k_stall;        /* 0 = 12                                                             */
+  double absorption;      /* alpha = absorption * rho                                           */
+  double scattering;      /* betta = scattering * rho                                           */
+  rrhd_emission emission;
+} rrhd_coupled_opts;
+/* tau > 0.  hydro / source (host, may be NULL): statistics of the hydro step and
+ * of the source con2prim; either one synchronises the stream. */
+rrhd_status rrhd_coupled_step(rrhd_ctx *ctx, double tau, const rrhd_coupled_opts *opts, rrhd_step_stats *hydro,
+                              rrhd_c2p_stats *source);
+/* Host copies (caller cell numbering, double) of the coupled step's radiation
+ * arrays: RRHD_RAD_I / RRHD_RAD_S [N*G][M], RRHD_RAD_G4 [N][4] (4-force of the
+ * last step); rrhd_rad_set writes I or S (e.g. the scattering integral of a
+ * previous run). */
+#define RRHD_RAD_I 0
+#define RRHD_RAD_S 1
+#define RRHD_RAD_G4 2
+rrhd_status rrhd_rad_get(rrhd_ctx *ctx, int32_t what, double *out);
+rrhd_status rrhd_rad_set(rrhd_ctx *ctx, int32_t what, const double *in);
+
 /* ------------------------------------------------------------ misc */
 const char *rrhd_last_error(void);
 const char *rrhd_version(void);

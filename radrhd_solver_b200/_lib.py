@@ -72,6 +72,23 @@ class Emission(C.Structure):
     _fields_ = [("temp_coef", D), ("sigma_sb", D), ("pi", D), ("rad_unit", D)]
 
 
+RRHD_RAD_FP64 = 0
+RRHD_RAD_FP32 = 1
+RRHD_SCATTER_FP64 = -1
+RRHD_RAD_I = 0
+RRHD_RAD_S = 1
+RRHD_RAD_G4 = 2
+
+
+class RadOpts(C.Structure):
+    _fields_ = [("groups", I32), ("precision", I32), ("dirs_per_batch", I32), ("boundary_value", D)]
+
+
+class CoupledOpts(C.Structure):
+    _fields_ = [("scatter", I32), ("guess", P), ("k_stall", I32), ("absorption", D), ("scattering", D),
+                ("emission", Emission)]
+
+
 _SIGS = {
     "rrhd_create": (I32, [P, P, P]),
     "rrhd_destroy": (I32, [P]),
@@ -121,6 +138,12 @@ _SIGS = {
     "rrhd_mlp_train": (I32, [P, P, P, I64, I32, I32, C.c_float, U64, I32, P, P]),
     "rrhd_mlp_gradient": (I32, [P, P, P, I64, P, P]),
     "rrhd_con2prim_batch_mlp": (I32, [P, I32, D, P, P, P, I64, I32, I32, P, P, P, P]),
+    "rrhd_rad_setup": (I32, [P, P, P]),
+    "rrhd_rad_plan_info": (I32, [P, P, P]),
+    "rrhd_sweep": (I32, [P, P, P, P, P, P]),
+    "rrhd_coupled_step": (I32, [P, D, P, P, P]),
+    "rrhd_rad_get": (I32, [P, I32, P]),
+    "rrhd_rad_set": (I32, [P, I32, P]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

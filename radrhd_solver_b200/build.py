@@ -34,6 +34,7 @@ SOURCES = {
     "scatter_tc.cu": [],
     "synth.cu": [],
     "c2p_mlp.cu": ["--fmad=false"],
+    "sweep.cu": ["--fmad=false"],
 }
 
 

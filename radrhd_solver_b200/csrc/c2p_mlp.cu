@@ -33,6 +33,7 @@
 
 #include "hydro_phys.cuh"
 #include "rng.h"
+#include "coupled.h"
 #include "rrhd_internal.h"
 
 using namespace rrhd;
@@ -280,8 +281,12 @@ __device__ __forceinline__ float mlp_warp(const float *xs, const float *sW1, con
   return y + b3;
 }
 
-__global__ void __launch_bounds__(IT) k_c2p_mlp(Eos eos, double *U, double *W, uint8_t *status, int64_t n,
-                                                int fallback, int k_stall, const float *__restrict__ theta,
+// States i live at U + stride*i and W + stride*i (stride 5 for separate arrays,
+// 10 for a solver state [n][10] = U, W).  With G4 != NULL the radiation source
+// is added first, U.E += tau G0 and U.S += tau G[1..3] (radRHD_main.cpp:117-126).
+__global__ void __launch_bounds__(IT) k_c2p_mlp(Eos eos, double *U, double *W, int64_t stride, const double *G4,
+                                                double tau_src, uint8_t *status, int64_t n, int fallback,
+                                                int k_stall, const float *__restrict__ theta,
                                                 const uint32_t *__restrict__ frag, Norm nm, MlpPartial *scratch,
                                                 double *guess_out) {
   __shared__ float sW1[H * 3], sb1[H], sb2[H], sW3[H];
@@ -303,11 +308,18 @@ __global__ void __launch_bounds__(IT) k_c2p_mlp(Eos eos, double *U, double *W, u
     const int64_t i = w * 32 + lane;
     const bool live = i < n;
     double u[5] = {0, 0, 0, 0, 0}, wv[5] = {0, 0, 0, 0, 0};
-    if (live)
+    if (live) {
       for (int q = 0; q < 5; q++) {
-        u[q] = U[5 * i + q];
-        wv[q] = W[5 * i + q];
+        u[q] = U[stride * i + q];
+        wv[q] = W[stride * i + q];
       }
+      if (G4) {
+        u[4] += tau_src * G4[4 * i];
+        u[1] += tau_src * G4[4 * i + 1];
+        u[2] += tau_src * G4[4 * i + 2];
+        u[3] += tau_src * G4[4 * i + 3];
+      }
+    }
     float f[3] = {0.f, 0.f, 0.f};
     double tau = 0.0;
     const bool feat = live && features(u, f, tau);
@@ -317,6 +329,7 @@ __global__ void __launch_bounds__(IT) k_c2p_mlp(Eos eos, double *U, double *W, u
     const float y = mlp_warp(xs, sW1, sb1, sb2, sW3, b3, sfrag);
     if (!live) continue;
     int it1 = 0, it2 = 0, code = 1;
+    bool u_dirty = G4 != nullptr;
     if (feat) {
       const double p0 = tau * exp((double)(y * nm.sig_t + nm.mu_t));
       if (guess_out) guess_out[i] = p0;
@@ -338,12 +351,14 @@ __global__ void __launch_bounds__(IT) k_c2p_mlp(Eos eos, double *U, double *W, u
         code = code | 0x10 | (fix ? 0x20 : 0);
         fb++;
         failed += fix ? 1 : 0;
-        for (int q = 0; q < 5; q++) U[5 * i + q] = u[q];
+        u_dirty = true;
       } else {
         failed++;
       }
     }
-    for (int q = 0; q < 5; q++) W[5 * i + q] = wv[q];
+    if (u_dirty)
+      for (int q = 0; q < 5; q++) U[stride * i + q] = u[q];
+    for (int q = 0; q < 5; q++) W[stride * i + q] = wv[q];
     if (status) status[i] = (uint8_t)code;
   }
 #pragma unroll
@@ -685,17 +700,9 @@ extern "C" rrhd_status rrhd_mlp_gradient(rrhd_mlp *m, const double *U, const dou
   return s;
 }
 
-// con2prim batch seeded by the network: Newton from the learned guess for at
-// most k_stall iterations, then (if needed) the reference solve from its own
-// guess, then PhysPressureFix when fallback != 0.  stats (host, may be NULL).
-// guess (device [n], may be NULL) receives the learned initial pressures.
-extern "C" rrhd_status rrhd_con2prim_batch_mlp(const rrhd_mlp *m, int32_t eos, double gamma, double *U, double *W,
-                                               uint8_t *status, int64_t n, int32_t fallback, int32_t k_stall,
-                                               rrhd_c2p_stats *stats, int64_t *n_guess_fallback, double *guess,
-                                               void *stream) {
-  RRHD_CHECK_ARG(m && n >= 0 && ((U && W) || n == 0) && k_stall > 0 && k_stall <= 40, "bad arguments");
-  RRHD_CHECK_ARG(eos == RRHD_EOS_IDEAL || eos == RRHD_EOS_TAUB, "bad eos");
-  cudaStream_t st = (cudaStream_t)stream;
+rrhd_status rrhd::mlp_c2p(const rrhd_mlp *m, int eos, double gamma, double *U, double *W, int64_t stride,
+                          const double *G4, double tau_src, uint8_t *status, int64_t n, int fallback, int k_stall,
+                          rrhd_c2p_stats *stats, int64_t *n_guess_fallback, double *guess, cudaStream_t st) {
   rrhd_mlp *mm = const_cast<rrhd_mlp *>(m);
   const int64_t warps = (n + 31) / 32;
   const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>((warps + IT / 32 - 1) / (IT / 32), 8 * m->num_sms));
@@ -706,8 +713,8 @@ extern "C" rrhd_status rrhd_con2prim_batch_mlp(const rrhd_mlp *m, int32_t eos, d
     RRHD_CUDA(cudaMalloc(&mm->d_stats, sizeof(MlpPartial) * (nblk + 1)));
     mm->stats_cap = nblk + 1;
   }
-  k_c2p_mlp<<<nblk, IT, 0, st>>>(make_eos(eos, gamma), U, W, status, n, fallback, k_stall, m->d_theta, m->d_frag,
-                                 m->norm, mm->d_stats, guess);
+  k_c2p_mlp<<<nblk, IT, 0, st>>>(make_eos(eos, gamma), U, W, stride, G4, tau_src, status, n, fallback, k_stall,
+                                 m->d_theta, m->d_frag, m->norm, mm->d_stats, guess);
   RRHD_CUDA(cudaGetLastError());
   k_mlp_stats_reduce<<<1, 32, 0, st>>>(mm->d_stats, nblk);
   RRHD_CUDA(cudaGetLastError());
@@ -725,4 +732,18 @@ extern "C" rrhd_status rrhd_con2prim_batch_mlp(const rrhd_mlp *m, int32_t eos, d
     if (n_guess_fallback) *n_guess_fallback = (int64_t)t.guess_fallback;
   }
   return RRHD_OK;
+}
+
+// con2prim batch seeded by the network: Newton from the learned guess for at
+// most k_stall iterations, then (if needed) the reference solve from its own
+// guess, then PhysPressureFix when fallback != 0.  stats (host, may be NULL).
+// guess (device [n], may be NULL) receives the learned initial pressures.
+extern "C" rrhd_status rrhd_con2prim_batch_mlp(const rrhd_mlp *m, int32_t eos, double gamma, double *U, double *W,
+                                               uint8_t *status, int64_t n, int32_t fallback, int32_t k_stall,
+                                               rrhd_c2p_stats *stats, int64_t *n_guess_fallback, double *guess,
+                                               void *stream) {
+  RRHD_CHECK_ARG(m && n >= 0 && ((U && W) || n == 0) && k_stall > 0 && k_stall <= 40, "bad arguments");
+  RRHD_CHECK_ARG(eos == RRHD_EOS_IDEAL || eos == RRHD_EOS_TAUB, "bad eos");
+  return rrhd::mlp_c2p(m, eos, gamma, U, W, 5, nullptr, 0.0, status, n, fallback, k_stall, stats, n_guess_fallback,
+                       guess, (cudaStream_t)stream);
 }

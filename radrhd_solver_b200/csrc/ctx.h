@@ -26,6 +26,49 @@ struct BcTable {
 
 }  // namespace rrhd
 
+struct rrhd_dirs;
+struct rrhd_scatter_tc;
+
+namespace rrhd {
+// Pointers a sweep reads and writes, kept in device memory so that one captured
+// graph of level launches serves every call.
+struct SweepIO {
+  const void *alpha, *betta, *Q, *S;  // [N], [N], [N][G], [N*G][M]
+  void *I;                            // [N*G][M]
+  const int32_t *row_of;              // context cell -> caller cell, or NULL (context rows)
+};
+
+// Radiation part of a context: the transport sweep and the coupled step.
+struct RadState {
+  bool ready = false;
+  const rrhd_dirs *dirs = nullptr;  // not owned
+  int M = 0, G = 1, DB = 64, shift = 6, nbatch = 0;
+  int prec = 0;  // RRHD_RAD_FP64 or RRHD_RAD_FP32: storage and arithmetic of the sweep
+  double bc = 0.0;
+  int64_t last_cell = 0;  // context index of the caller's last cell (plain-mean quirk)
+  void *d_w = nullptr;     // [M][3] directions in the sweep precision
+  void *d_geo = nullptr;   // [N][16] per local face j: outward normal (3 j..3 j+2), then heights H_j at 12+j
+  void *d_area = nullptr;  // [N][4] face areas
+  int4 *d_fid = nullptr;   // [N] caller face ids of the local faces
+  int4 *d_nbr = nullptr;   // [N] neighbour (context numbering) or -1
+  uint32_t *d_plan = nullptr;               // all batches: items (cell << shift | d) in level order
+  std::vector<std::vector<int64_t>> lvl;    // per batch: level offsets into d_plan
+  int64_t levels = 0, max_level = 0;
+  cudaGraphExec_t graph = nullptr;          // every level launch of one sweep
+  SweepIO *d_io = nullptr;
+  void *d_fv = nullptr;  // [F][DB][G] face values
+  // coupled step (context numbering, rows cell * G + g)
+  void *d_I = nullptr, *d_S = nullptr;                      // [N*G][M]
+  void *d_alpha = nullptr, *d_betta = nullptr, *d_Q = nullptr;  // [N], [N], [N][G]
+  double *d_G4 = nullptr;                                    // [N][4] radiation 4-force of the last step
+  double *d_mE = nullptr, *d_mF = nullptr, *d_mT = nullptr;  // FP64 moments per row [N*G], [N*G][3], [N*G][9]
+  float *d_mom = nullptr;                                    // FP32 moments per row [N*G][16]
+  unsigned long long *d_cnt = nullptr;                       // [8] counters of the source con2prim
+  rrhd_scatter_tc *tc = nullptr;
+  int tc_form = -1;
+};
+}  // namespace rrhd
+
 struct rrhd_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -72,4 +115,13 @@ struct rrhd_ctx {
 
   double *d_scratch_io = nullptr;  // [N][5] staging for strided host/device transfers
   double *h_pinned = nullptr;      // pinned staging for host transfers, N*10 doubles
+
+  // mesh arrays kept for the radiation set-up (caller numbering)
+  std::vector<int32_t> h_cell_faces, h_face_l, h_face_r;
+  std::vector<uint8_t> h_cell_sign;
+  std::vector<double> h_face_n, h_face_area, h_cell_V;
+
+  rrhd::RadState rad;
 };
+
+void rrhd_rad_release(rrhd_ctx *c);

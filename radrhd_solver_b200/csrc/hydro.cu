@@ -485,6 +485,7 @@ rrhd_status upload(T **dst, const std::vector<T> &src) {
 void free_ctx(rrhd_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
+  rrhd_rad_release(c);
   void *ptrs[] = {c->d_perm, c->d_iperm, c->d_bface_off, c->d_bface_lr, c->d_bface_nS, c->d_halo_off, c->d_halo_ids,
                   c->d_bface_gid, c->d_cell_slot, c->d_cell_sign, c->d_cell_V, c->d_state[0],
                   c->d_state[1], c->d_status, c->d_scal, c->d_face_flux, c->d_scratch_io};
@@ -620,6 +621,13 @@ extern "C" rrhd_status rrhd_create(const rrhd_mesh_desc *m, const rrhd_opts *opt
     hoff[b + 1] = hoff[b] + nh;
   }
   c->max_halo = max_h;
+  c->h_cell_faces.assign(m->cell_faces, m->cell_faces + 4 * N);
+  c->h_cell_sign.assign(m->cell_sign, m->cell_sign + N);
+  c->h_face_l.assign(m->face_id_l, m->face_id_l + F);
+  c->h_face_r.assign(m->face_id_r, m->face_id_r + F);
+  c->h_face_n.assign(m->face_n, m->face_n + 3 * F);
+  c->h_face_area.assign(m->face_area, m->face_area + F);
+  c->h_cell_V.assign(m->cell_volume, m->cell_volume + N);
   c->max_entries = max_e;
   c->n_entries = off[nb];
   c->h_perm = perm;

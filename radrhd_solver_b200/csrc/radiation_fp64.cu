@@ -17,6 +17,7 @@
 #include "rrhd_internal.h"
 
 #include "dirs.h"
+#include "rad_phys.cuh"
 
 namespace {
 
@@ -157,58 +158,23 @@ __global__ void __launch_bounds__(MR) k_moments(int64_t rows, int M, const doubl
   }
 }
 
-struct Emission {
-  double temp_coef, sigma_sb, pi, rad_unit;
-};
-
 // rad_rhd::GetRadSource, solvers/RadRHD/src/radRHD_utils.cpp:44-101
-__global__ void k_rad_source(int64_t n, Emission em, const double *__restrict__ W,
+__global__ void k_rad_source(int64_t n, rrhd::Emission em, const double *__restrict__ W,
                              const double *__restrict__ alpha, const double *__restrict__ sigma,
                              const double *__restrict__ E, const double *__restrict__ F,
                              const double *__restrict__ T, double *__restrict__ G) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= n) return;
-  const double abs_op = alpha[c];
-  const double scat_op = sigma[c];
-  const double tot_op = abs_op + scat_op;
-  const double rho = W[5 * c + 0];
-  const double prs = W[5 * c + 4];
-  const double v[3] = {W[5 * c + 1], W[5 * c + 2], W[5 * c + 3]};
-  const double Ur = E[c];
-  const double Fr[3] = {F[3 * c], F[3 * c + 1], F[3 * c + 2]};
-  double Tr[9];
+  double w[5], Fr[3], Tr[9], g[4];
+#pragma unroll
+  for (int i = 0; i < 5; i++) w[i] = W[5 * c + i];
+#pragma unroll
+  for (int i = 0; i < 3; i++) Fr[i] = F[3 * c + i];
 #pragma unroll
   for (int i = 0; i < 9; i++) Tr[i] = T[9 * c + i];
-  double gamma = (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2];
-  double u2 = gamma;
-  const double gamma2 = 1.0 / (1.0 - gamma);
-  u2 *= gamma2;
-  gamma = sqrt(gamma2);
-  const double u[3] = {gamma * v[0], gamma * v[1], gamma * v[2]};
-  double uuD = 0.;
-  const double uF = (u[0] * Fr[0] + u[1] * Fr[1]) + u[2] * Fr[2];
-  double uD[3];
+  rrhd::rad_source_cell(em, w, alpha[c], sigma[c], E[c], Fr, Tr, g);
 #pragma unroll
-  for (int i = 0; i < 3; i++) {
-    uD[i] = 0.;
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-      const double D = Tr[3 * j + i];
-      uD[i] += u[j] * D;
-      uuD += u[i] * u[j] * D;
-    }
-  }
-  const double rhogamma = rho * gamma;
-  const double Tg = em.temp_coef * prs / rho;
-  const double T2 = Tg * Tg;
-  const double B = (T2 * T2) * em.sigma_sb / em.pi;
-  const double q = -abs_op * rho * B / em.rad_unit;
-  G[4 * c + 0] = q * gamma + rhogamma * (abs_op - scat_op * (u2 + uuD)) * Ur -
-                 rho * (abs_op - scat_op * (u2 + gamma2)) * uF;
-#pragma unroll
-  for (int i = 0; i < 3; i++)
-    G[4 * c + i + 1] = q * u[i] - rho * (tot_op * uD[i] + scat_op * u[i] * (gamma2 + uuD)) * Ur +
-                       rhogamma * (tot_op * Fr[i] + scat_op * 2.0 * uF * u[i]);
+  for (int i = 0; i < 4; i++) G[4 * c + i] = g[i];
 }
 
 }  // namespace
@@ -311,7 +277,7 @@ extern "C" rrhd_status rrhd_rad_source(const rrhd_emission *em, const double *W,
                                        double *G, int64_t n, void *stream) {
   RRHD_CHECK_ARG(em && W && alpha && sigma && E && F && T && G && n >= 0, "bad arguments");
   if (n == 0) return RRHD_OK;
-  Emission e{em->temp_coef, em->sigma_sb, em->pi, em->rad_unit};
+  rrhd::Emission e{em->temp_coef, em->sigma_sb, em->pi, em->rad_unit};
   k_rad_source<<<(unsigned)((n + 127) / 128), 128, 0, (cudaStream_t)stream>>>(n, e, W, alpha, sigma, E, F, T, G);
   RRHD_CUDA(cudaGetLastError());
   return RRHD_OK;

@@ -1,0 +1,765 @@
+// Transport sweep (short characteristics) and the coupled radiation-hydro step.
+//
+// The reference sweeps every direction on the CPU in the order of a precomputed
+// graph (sorted_graph: (cell, out-face) pairs) with precomputed node distances
+// (vec_x0), solvers/illum/src/mpi/multi_gpu/illum_multi_gpu_face_calc.cpp:91-190.
+// Here the order is built on the device once per mesh and direction set as
+// levels: level 0 holds the (cell, direction) pairs whose in-faces are all on
+// the boundary, level L+1 those whose last upwind neighbour is in level L.  All
+// pairs of a level are independent, so one level is one kernel launch with one
+// thread per pair, and a sweep is one CUDA graph of all level launches.  A batch
+// of DB directions is swept together, so the face values of one batch,
+// [F][DB][G], are the only scratch.
+//
+// Per pair the kernel classifies the four faces by the sign of n_j . w, traces
+// the three nodes of each out-face back to the in-face they came through (the
+// smallest t_h = lam_h H_h / -cos_h, H_h the height of the cell over face h and
+// lam_h the node's barycentric weight of the vertex opposite h: no vertex data
+// is needed), evaluates GetIllum per group with one set of exponentials shared by
+// all groups (the opacity k = alpha + betta does not depend on the group), and
+// folds the four face values into the cell value (ReCalcIllumOpt) in the same
+// thread, so face values are read once.  Compiled with --fmad=false: in double
+// precision every value is the oracle's operation for operation, exp aside.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <cub/device/device_radix_sort.cuh>
+#include <vector>
+
+#include "coupled.h"
+#include "ctx.h"
+#include "dirs.h"
+#include "hydro_phys.cuh"
+#include "rad_phys.cuh"
+#include "rrhd_internal.h"
+
+using namespace rrhd;
+
+namespace {
+
+constexpr int kSweepThreads = 128;
+
+template <class T>
+struct SweepArgs {
+  const SweepIO *io;
+  const uint32_t *items;
+  int64_t n;  // items of this level
+  int shift, DB, d0, M, G;
+  const T *w;     // [M][3]
+  const T *geo;   // [N][16]
+  const T *area;  // [N][4]
+  const int4 *fid, *nbr;
+  T *fv;  // [F][DB][G]
+  T bc;
+  int64_t last;
+};
+
+__device__ __forceinline__ double ex(double x) { return exp(x); }
+__device__ __forceinline__ float ex(float x) { return expf(x); }
+
+template <class T>
+__device__ __forceinline__ void load_geo(const T *g, T *out) {
+#pragma unroll
+  for (int q = 0; q < 16; q++) out[q] = g[q];
+}
+template <>
+__device__ __forceinline__ void load_geo<double>(const double *g, double *out) {
+  const double2 *g2 = reinterpret_cast<const double2 *>(g);
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const double2 v = __ldg(g2 + q);
+    out[2 * q] = v.x;
+    out[2 * q + 1] = v.y;
+  }
+}
+template <>
+__device__ __forceinline__ void load_geo<float>(const float *g, float *out) {
+  const float4 *g4 = reinterpret_cast<const float4 *>(g);
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const float4 v = __ldg(g4 + q);
+    out[4 * q] = v.x;
+    out[4 * q + 1] = v.y;
+    out[4 * q + 2] = v.z;
+    out[4 * q + 3] = v.w;
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void face_cos(const T *g, T wx, T wy, T wz, T *cosf) {
+#pragma unroll
+  for (int j = 0; j < 4; j++) cosf[j] = (g[3 * j] * wx + g[3 * j + 1] * wy) + g[3 * j + 2] * wz;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  const uint32_t it = a.items[i];
+  const int64_t c = it >> a.shift;
+  const int dl = (int)(it & (uint32_t)(a.DB - 1));
+  const int d = a.d0 + dl;
+  const SweepIO io = *a.io;
+  const T *alpha = (const T *)io.alpha, *betta = (const T *)io.betta, *Qv = (const T *)io.Q, *Sv = (const T *)io.S;
+  T *I = (T *)io.I;
+  const int64_t p = io.row_of ? (int64_t)io.row_of[c] : c;
+  const T wx = a.w[3 * d], wy = a.w[3 * d + 1], wz = a.w[3 * d + 2];
+  T g[16];
+  load_geo<T>(a.geo + 16 * c, g);
+  T cosf[4];
+  face_cos(g, wx, wy, wz, cosf);
+  const int4 f4 = a.fid[c], n4 = a.nbr[c];
+  const int fid[4] = {f4.x, f4.y, f4.z, f4.w};
+  const int nbr[4] = {n4.x, n4.y, n4.z, n4.w};
+  const T al = alpha[p], be = betta[p];
+  const T k = al + be;
+  T r[4];
+#pragma unroll
+  for (int f = 0; f < 4; f++) r[f] = cosf[f] < 0 ? g[12 + f] / -cosf[f] : (T)0;
+  // in-face of each node and its exponential, per out-face
+  int hq[4][3];
+  T e[4][3];
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      hq[j][q] = -1;
+      e[j][q] = (T)0;
+    }
+    if (!(cosf[j] > 0)) continue;
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const int vq = (j + 1 + q) & 3;
+      T tmin = 0;
+      int hmin = -1;
+#pragma unroll
+      for (int f = 0; f < 4; f++) {
+        if (!(cosf[f] < 0)) continue;
+        const T lam = f == vq ? (T)(2.0 / 3.0) : (T)(1.0 / 6.0);
+        const T t = lam * r[f];
+        if (hmin < 0 || t < tmin) {
+          tmin = t;
+          hmin = f;
+        }
+      }
+      hq[j][q] = hmin;
+      e[j][q] = ex(-k * tmin);
+    }
+  }
+  const bool last = c == a.last;
+  T A[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) A[j] = a.area[4 * c + j];
+  for (int gg = 0; gg < a.G; gg++) {
+    const int64_t row = p * a.G + gg;
+    const T rhs = (al * Qv[row] + be * Sv[row * a.M + d]) / k;
+    T fvals[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      if (cosf[j] < 0)
+        fvals[j] = nbr[j] >= 0 ? a.fv[((int64_t)fid[j] * a.DB + dl) * a.G + gg] : a.bc;
+      else
+        fvals[j] = a.bc;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      if (!(cosf[j] > 0)) continue;
+      T I0[3];
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        const int h = hq[j][q];
+        I0[q] = a.bc;
+#pragma unroll
+        for (int f = 0; f < 4; f++)
+          if (h == f) I0[q] = fvals[f];
+      }
+      T Icur = e[j][0] * (I0[0] - rhs) + rhs;
+      Icur += (e[j][1] * (I0[1] - rhs) + rhs);
+      Icur += (e[j][2] * (I0[2] - rhs) + rhs);
+      const T v = Icur * (T)0.3333333333333333;
+      a.fv[((int64_t)fid[j] * a.DB + dl) * a.G + gg] = v;
+      fvals[j] = v;
+    }
+    T curI = 0;
+    if (!last) {
+      T Ssum = 0;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        curI += fvals[j] * A[j];
+        Ssum += A[j];
+      }
+      curI /= Ssum;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; j++) curI += fvals[j];
+      curI /= (T)4;
+    }
+    I[row * a.M + d] = curI;
+  }
+}
+
+// ---------------------------------------------------------------- plan
+template <class T>
+__global__ void k_plan_init(int64_t N, int nbd, int shift, int d0, const T *w, const T *geo, const int4 *nbr4,
+                            uint32_t *indeg, uint32_t *plan, unsigned long long *tail) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= N * nbd) return;
+  const int64_t c = i / nbd;
+  const int dl = (int)(i - c * nbd);
+  const int d = d0 + dl;
+  T g[16];
+  load_geo<T>(geo + 16 * c, g);
+  T cosf[4];
+  face_cos(g, w[3 * d], w[3 * d + 1], w[3 * d + 2], cosf);
+  const int4 n4 = nbr4[c];
+  const int nbr[4] = {n4.x, n4.y, n4.z, n4.w};
+  uint32_t cnt = 0;
+#pragma unroll
+  for (int j = 0; j < 4; j++) cnt += (cosf[j] < 0 && nbr[j] >= 0) ? 1u : 0u;
+  indeg[i] = cnt;
+  if (cnt == 0) plan[atomicAdd(tail, 1ull)] = ((uint32_t)c << shift) | (uint32_t)dl;
+}
+
+template <class T>
+__global__ void k_plan_expand(const uint32_t *cur, int64_t n, int nbd, int shift, int d0, const T *w, const T *geo,
+                              const int4 *nbr4, uint32_t *indeg, uint32_t *plan, unsigned long long *tail) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t it = cur[i];
+  const int64_t c = it >> shift;
+  const int dl = (int)(it & ((1u << shift) - 1));
+  const int d = d0 + dl;
+  T g[16];
+  load_geo<T>(geo + 16 * c, g);
+  T cosf[4];
+  face_cos(g, w[3 * d], w[3 * d + 1], w[3 * d + 2], cosf);
+  const int4 n4 = nbr4[c];
+  const int nbr[4] = {n4.x, n4.y, n4.z, n4.w};
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    if (!(cosf[j] > 0) || nbr[j] < 0) continue;
+    const int64_t q = (int64_t)nbr[j] * nbd + dl;
+    if (atomicSub(indeg + q, 1u) == 1u) plan[atomicAdd(tail, 1ull)] = ((uint32_t)nbr[j] << shift) | (uint32_t)dl;
+  }
+}
+
+// ---------------------------------------------------------------- coupled step
+template <class T>
+__global__ void k_opacity(int64_t N, int G, const double *state, double a_coef, double b_coef, Emission em,
+                          T *alpha, T *betta, T *Q) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  const double rho = state[10 * c + 5], prs = state[10 * c + 9];
+  alpha[c] = (T)(a_coef * rho);
+  betta[c] = (T)(b_coef * rho);
+  const double q = planck_B(em, rho, prs) / em.rad_unit / (double)G;
+  for (int g = 0; g < G; g++) Q[c * G + g] = (T)q;
+}
+
+// 4-force from the moments summed over the groups.  FP64 moments per row: E
+// [rows], F [rows][3], T [rows][9]; FP32 moments: [rows][16] = {E, F, Txx, Txy,
+// Txz, Tyy, Tyz, Tzz, ...}.
+__global__ void k_source(int64_t N, int G, const double *state, double a_coef, double b_coef, Emission em,
+                         const double *mE, const double *mF, const double *mT, const float *mom, double *G4) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  double E = 0, F[3] = {0, 0, 0}, Tm[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int g = 0; g < G; g++) {
+    const int64_t r = c * G + g;
+    if (mom) {
+      const float4 *m4 = reinterpret_cast<const float4 *>(mom + 16 * r);
+      const float4 a = m4[0], b = m4[1], cc = m4[2];
+      const double t9[9] = {b.x, b.y, b.z, b.y, b.w, cc.x, b.z, cc.x, cc.y};
+      E += a.x;
+      F[0] += a.y;
+      F[1] += a.z;
+      F[2] += a.w;
+#pragma unroll
+      for (int q = 0; q < 9; q++) Tm[q] += t9[q];
+    } else {
+      E += mE[r];
+#pragma unroll
+      for (int q = 0; q < 3; q++) F[q] += mF[3 * r + q];
+#pragma unroll
+      for (int q = 0; q < 9; q++) Tm[q] += mT[9 * r + q];
+    }
+  }
+  double w[5];
+#pragma unroll
+  for (int q = 0; q < 5; q++) w[q] = state[10 * c + 5 + q];
+  double out[4];
+  rad_source_cell(em, w, a_coef * w[0], b_coef * w[0], E, F, Tm, out);
+#pragma unroll
+  for (int q = 0; q < 4; q++) G4[4 * c + q] = out[q];
+}
+
+// U.E += tau G0, U.S += tau G (radRHD_main.cpp:117-126), then GetPhysValueStab
+// from its own guess without fallback (its status is ignored there as well).
+// cnt: {ok, failed, newton iterations, max iterations}.
+__global__ void k_source_c2p(int64_t N, Eos eos, double *state, const double *G4, double tau,
+                             unsigned long long *cnt) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  unsigned long long ok = 0, failed = 0, iters = 0;
+  if (c < N) {
+    double u[5], w[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+      u[q] = state[10 * c + q];
+      w[q] = state[10 * c + 5 + q];
+    }
+    u[4] += tau * G4[4 * c];
+    u[1] += tau * G4[4 * c + 1];
+    u[2] += tau * G4[4 * c + 2];
+    u[3] += tau * G4[4 * c + 3];
+    int it = 0;
+    const int code = c2p_from(eos, u, w, 0.0, false, &it);
+    ok = code == 0;
+    failed = code != 0;
+    iters = (unsigned long long)it;
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+      state[10 * c + q] = u[q];
+      state[10 * c + 5 + q] = w[q];
+    }
+  }
+  unsigned long long mx = iters;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ok += __shfl_xor_sync(0xffffffffu, ok, o);
+    failed += __shfl_xor_sync(0xffffffffu, failed, o);
+    iters += __shfl_xor_sync(0xffffffffu, iters, o);
+    const unsigned long long m2 = __shfl_xor_sync(0xffffffffu, mx, o);
+    mx = m2 > mx ? m2 : mx;
+  }
+  if ((threadIdx.x & 31) == 0 && (ok | failed)) {
+    atomicAdd(cnt + 0, ok);
+    atomicAdd(cnt + 1, failed);
+    atomicAdd(cnt + 2, iters);
+    atomicMax(cnt + 3, mx);
+  }
+}
+
+template <class T>
+__global__ void k_rows_to_host_order(int64_t N, int64_t width, const int32_t *perm, const T *src, double *dst) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= N * width) return;
+  const int64_t c = i / width, k = i - c * width;
+  dst[(int64_t)perm[c] * width + k] = (double)src[i];
+}
+
+template <class T>
+__global__ void k_rows_from_host_order(int64_t N, int64_t width, const int32_t *perm, const double *src, T *dst) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= N * width) return;
+  const int64_t c = i / width, k = i - c * width;
+  dst[i] = (T)src[(int64_t)perm[c] * width + k];
+}
+
+unsigned grid_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+Eos eos_of(const rrhd_ctx *c) {
+  Eos e;
+  e.eos = c->eos;
+  e.g1 = c->gamma;
+  e.gg = c->gamma / (c->gamma - 1.0);
+  return e;
+}
+
+template <class T>
+rrhd_status build_plan(rrhd_ctx *c) {
+  RadState &R = c->rad;
+  const int64_t N = c->N;
+  const int64_t total = N * (int64_t)R.M;
+  cudaStream_t st = c->stream;
+  uint32_t *indeg = nullptr, *tmp = nullptr;
+  unsigned long long *d_tail = nullptr;
+  void *sort_tmp = nullptr;
+  size_t sort_bytes = 0;
+  auto cleanup = [&]() {
+    cudaFree(indeg);
+    cudaFree(tmp);
+    cudaFree(d_tail);
+    cudaFree(sort_tmp);
+  };
+  const int64_t bmax = N * (int64_t)R.DB;
+  if (cudaMalloc(&R.d_plan, sizeof(uint32_t) * total) != cudaSuccess ||
+      cudaMalloc(&indeg, sizeof(uint32_t) * bmax) != cudaSuccess ||
+      cudaMalloc(&tmp, sizeof(uint32_t) * bmax) != cudaSuccess ||
+      cudaMalloc(&d_tail, sizeof(unsigned long long)) != cudaSuccess) {
+    cleanup();
+    return rrhd_fail(RRHD_ERR_OOM, "sweep plan allocation failed");
+  }
+  int end_bit = R.shift;
+  while ((int64_t(1) << (end_bit - R.shift)) < N) end_bit++;
+  cub::DeviceRadixSort::SortKeys(nullptr, sort_bytes, (const uint32_t *)nullptr, (uint32_t *)nullptr, bmax, 0,
+                                 end_bit, st);
+  if (cudaMalloc(&sort_tmp, sort_bytes) != cudaSuccess) {
+    cleanup();
+    return rrhd_fail(RRHD_ERR_OOM, "sweep plan allocation failed");
+  }
+  R.lvl.assign(R.nbatch, {});
+  R.levels = 0;
+  R.max_level = 0;
+  int64_t base = 0;
+  for (int b = 0; b < R.nbatch; b++) {
+    const int d0 = b * R.DB;
+    const int nbd = std::min(R.DB, R.M - d0);
+    uint32_t *plan = R.d_plan + base;
+    const unsigned long long zero = 0;
+    RRHD_CUDA(cudaMemcpyAsync(d_tail, &zero, sizeof zero, cudaMemcpyHostToDevice, st));
+    k_plan_init<T><<<grid_for(N * nbd, 256), 256, 0, st>>>(N, nbd, R.shift, d0, (const T *)R.d_w,
+                                                            (const T *)R.d_geo, R.d_nbr, indeg, plan, d_tail);
+    RRHD_CUDA(cudaGetLastError());
+    std::vector<int64_t> &off = R.lvl[b];
+    off.assign(1, 0);
+    int64_t lo = 0;
+    for (;;) {
+      unsigned long long hi_u = 0;
+      RRHD_CUDA(cudaMemcpyAsync(&hi_u, d_tail, sizeof hi_u, cudaMemcpyDeviceToHost, st));
+      RRHD_CUDA(cudaStreamSynchronize(st));
+      const int64_t hi = (int64_t)hi_u;
+      if (hi == lo) break;
+      // items of a level in ascending (cell, direction) order: deterministic
+      // launches and neighbouring cells' rows close together
+      cub::DeviceRadixSort::SortKeys(sort_tmp, sort_bytes, plan + lo, tmp, hi - lo, 0, end_bit, st);
+      RRHD_CUDA(cudaMemcpyAsync(plan + lo, tmp, sizeof(uint32_t) * (hi - lo), cudaMemcpyDeviceToDevice, st));
+      off.push_back(hi);
+      R.max_level = std::max(R.max_level, hi - lo);
+      k_plan_expand<T><<<grid_for(hi - lo, 256), 256, 0, st>>>(plan + lo, hi - lo, nbd, R.shift, d0,
+                                                                (const T *)R.d_w, (const T *)R.d_geo, R.d_nbr,
+                                                                indeg, plan, d_tail);
+      RRHD_CUDA(cudaGetLastError());
+      lo = hi;
+    }
+    if (lo != N * nbd) {
+      cleanup();
+      return rrhd_fail(RRHD_ERR_STATE, "sweep dependency cycle: %lld of %lld (cell, direction) pairs of batch %d "
+                                       "have an upwind neighbour that depends on them",
+                       (long long)(N * nbd - lo), (long long)(N * nbd), b);
+    }
+    R.levels += (int64_t)off.size() - 1;
+    base += N * nbd;
+  }
+  cleanup();
+  return RRHD_OK;
+}
+
+template <class T>
+rrhd_status capture_sweep(rrhd_ctx *c) {
+  RadState &R = c->rad;
+  cudaStream_t cs = nullptr;
+  RRHD_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    SweepArgs<T> a;
+    a.io = R.d_io;
+    a.shift = R.shift;
+    a.DB = R.DB;
+    a.M = R.M;
+    a.G = R.G;
+    a.w = (const T *)R.d_w;
+    a.geo = (const T *)R.d_geo;
+    a.area = (const T *)R.d_area;
+    a.fid = R.d_fid;
+    a.nbr = R.d_nbr;
+    a.fv = (T *)R.d_fv;
+    a.bc = (T)R.bc;
+    a.last = R.last_cell;
+    int64_t base = 0;
+    for (int b = 0; b < R.nbatch; b++) {
+      a.d0 = b * R.DB;
+      const int nbd = std::min(R.DB, R.M - a.d0);
+      const std::vector<int64_t> &off = R.lvl[b];
+      for (size_t L = 0; L + 1 < off.size(); L++) {
+        a.items = R.d_plan + base + off[L];
+        a.n = off[L + 1] - off[L];
+        k_sweep_level<T><<<grid_for(a.n, kSweepThreads), kSweepThreads, 0, cs>>>(a);
+      }
+      base += c->N * nbd;
+    }
+    e = cudaStreamEndCapture(cs, &g);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&R.graph, g, 0);
+  if (g) cudaGraphDestroy(g);
+  cudaStreamDestroy(cs);
+  RRHD_CUDA(e);
+  return RRHD_OK;
+}
+
+}  // namespace
+
+void rrhd_rad_release(rrhd_ctx *c) {
+  RadState &R = c->rad;
+  if (R.graph) cudaGraphExecDestroy(R.graph);
+  void *ptrs[] = {R.d_w, R.d_geo, R.d_area, R.d_fid, R.d_nbr, R.d_plan, R.d_io, R.d_fv, R.d_I, R.d_S, R.d_alpha,
+                  R.d_betta, R.d_Q, R.d_G4, R.d_mE, R.d_mF, R.d_mT, R.d_mom, R.d_cnt};
+  for (void *p : ptrs) cudaFree(p);
+  if (R.tc) rrhd_scatter_tc_destroy(R.tc);
+  R = RadState();
+}
+
+template <class T>
+static rrhd_status rad_setup_t(rrhd_ctx *c) {
+  RadState &R = c->rad;
+  const int64_t N = c->N;
+  // geometry in context numbering
+  std::vector<T> geo(16 * N), area(4 * N), w(3 * R.M);
+  std::vector<int4> fid(N), nbr(N);
+  std::vector<int32_t> iperm(N);
+  for (int64_t i = 0; i < N; i++) iperm[c->h_perm[i]] = (int32_t)i;
+  for (int64_t cn = 0; cn < N; cn++) {
+    const int64_t p = c->h_perm[cn];
+    int f[4], nb[4];
+    for (int j = 0; j < 4; j++) {
+      const int32_t fc = c->h_cell_faces[4 * p + j];
+      f[j] = fc;
+      const bool out = (c->h_cell_sign[p] >> j) & 1;
+      for (int x = 0; x < 3; x++) {
+        const double v = c->h_face_n[3 * (int64_t)fc + x];
+        geo[16 * cn + 3 * j + x] = (T)(out ? v : -v);
+      }
+      geo[16 * cn + 12 + j] = (T)(3.0 * c->h_cell_V[p] / c->h_face_area[fc]);
+      area[4 * cn + j] = (T)c->h_face_area[fc];
+      const int32_t l = c->h_face_l[fc], r = c->h_face_r[fc];
+      const int32_t o = (l == p) ? r : l;
+      nb[j] = o < 0 ? -1 : iperm[o];
+    }
+    fid[cn] = make_int4(f[0], f[1], f[2], f[3]);
+    nbr[cn] = make_int4(nb[0], nb[1], nb[2], nb[3]);
+  }
+  for (int q = 0; q < 3 * R.M; q++) w[q] = (T)R.dirs->h_w[q];
+  R.last_cell = iperm[N - 1];
+  auto up = [&](void **dst, const void *src, size_t bytes) -> rrhd_status {
+    if (cudaMalloc(dst, bytes) != cudaSuccess) return rrhd_fail(RRHD_ERR_OOM, "sweep allocation failed");
+    RRHD_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+    return RRHD_OK;
+  };
+  rrhd_status s;
+  if ((s = up(&R.d_geo, geo.data(), sizeof(T) * geo.size())) || (s = up(&R.d_area, area.data(), sizeof(T) * area.size())) ||
+      (s = up(&R.d_w, w.data(), sizeof(T) * w.size())) || (s = up((void **)&R.d_fid, fid.data(), sizeof(int4) * N)) ||
+      (s = up((void **)&R.d_nbr, nbr.data(), sizeof(int4) * N)))
+    return s;
+  if (cudaMalloc(&R.d_io, sizeof(SweepIO)) != cudaSuccess ||
+      cudaMalloc(&R.d_fv, sizeof(T) * (size_t)c->F * R.DB * R.G) != cudaSuccess)
+    return rrhd_fail(RRHD_ERR_OOM, "sweep face-value allocation failed");
+  if ((s = build_plan<T>(c))) return s;
+  return capture_sweep<T>(c);
+}
+
+extern "C" rrhd_status rrhd_rad_setup(rrhd_ctx *c, const rrhd_dirs *dirs, const rrhd_rad_opts *o) {
+  RRHD_CHECK_ARG(c && dirs && o, "null argument");
+  RRHD_CHECK_ARG(o->groups >= 1 && o->groups <= 64, "groups must be in [1, 64]");
+  RRHD_CHECK_ARG(o->precision == RRHD_RAD_FP64 || o->precision == RRHD_RAD_FP32, "bad precision");
+  RRHD_CHECK_ARG(dirs->device == c->device, "direction set lives on another device");
+  int DB = o->dirs_per_batch;
+  RRHD_CHECK_ARG(DB == 0 || (DB > 0 && DB <= 64 && (DB & (DB - 1)) == 0), "dirs_per_batch: power of two <= 64");
+  RRHD_CUDA(cudaSetDevice(c->device));
+  RRHD_CUDA(cudaStreamSynchronize(c->stream));
+  rrhd_rad_release(c);
+  RadState &R = c->rad;
+  R.dirs = dirs;
+  R.M = dirs->M;
+  R.G = o->groups;
+  if (DB == 0) {
+    DB = 1;
+    while (DB < std::min(R.M, 64)) DB <<= 1;
+  }
+  R.DB = DB;
+  R.shift = 0;
+  while ((1 << R.shift) < DB) R.shift++;
+  if ((c->N << R.shift) > (int64_t)UINT32_MAX)
+    return rrhd_fail(RRHD_ERR_LIMIT, "sweep items are 32-bit: cells x dirs_per_batch must stay below 2^32");
+  R.nbatch = (R.M + DB - 1) / DB;
+  R.prec = o->precision;
+  R.bc = o->boundary_value;
+  const rrhd_status s = R.prec == RRHD_RAD_FP64 ? rad_setup_t<double>(c) : rad_setup_t<float>(c);
+  if (s) {
+    rrhd_rad_release(c);
+    return s;
+  }
+  R.ready = true;
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_rad_plan_info(const rrhd_ctx *c, int64_t *levels, int64_t *max_level_items) {
+  RRHD_CHECK_ARG(c, "null context");
+  if (!c->rad.ready) return rrhd_fail(RRHD_ERR_STATE, "rrhd_rad_setup has not run");
+  if (levels) *levels = c->rad.levels;
+  if (max_level_items) *max_level_items = c->rad.max_level;
+  return RRHD_OK;
+}
+
+static rrhd_status launch_sweep(rrhd_ctx *c, const SweepIO &io) {
+  RadState &R = c->rad;
+  RRHD_CUDA(cudaMemcpyAsync(R.d_io, &io, sizeof io, cudaMemcpyHostToDevice, c->stream));
+  RRHD_CUDA(cudaGraphLaunch(R.graph, c->stream));
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_sweep(rrhd_ctx *c, const void *alpha, const void *betta, const void *Q, const void *S,
+                                  void *I) {
+  RRHD_CHECK_ARG(c && alpha && betta && Q && S && I, "null argument");
+  if (!c->rad.ready) return rrhd_fail(RRHD_ERR_STATE, "rrhd_rad_setup has not run");
+  RRHD_CUDA(cudaSetDevice(c->device));
+  SweepIO io{alpha, betta, Q, S, I, c->d_perm};
+  return launch_sweep(c, io);
+}
+
+// ---------------------------------------------------------------- coupled step
+template <class T>
+static rrhd_status alloc_coupled(rrhd_ctx *c) {
+  RadState &R = c->rad;
+  const int64_t N = c->N, rows = N * R.G;
+  const size_t big = sizeof(T) * (size_t)rows * R.M;
+  if (cudaMalloc(&R.d_I, big) != cudaSuccess || cudaMalloc(&R.d_S, big) != cudaSuccess ||
+      cudaMalloc(&R.d_alpha, sizeof(T) * N) != cudaSuccess || cudaMalloc(&R.d_betta, sizeof(T) * N) != cudaSuccess ||
+      cudaMalloc(&R.d_Q, sizeof(T) * rows) != cudaSuccess || cudaMalloc(&R.d_G4, sizeof(double) * 4 * N) != cudaSuccess ||
+      cudaMalloc(&R.d_cnt, sizeof(unsigned long long) * 8) != cudaSuccess)
+    return rrhd_fail(RRHD_ERR_OOM, "coupled-step allocation failed");
+  RRHD_CUDA(cudaMemsetAsync(R.d_I, 0, big, c->stream));
+  RRHD_CUDA(cudaMemsetAsync(R.d_S, 0, big, c->stream));
+  RRHD_CUDA(cudaMemsetAsync(R.d_G4, 0, sizeof(double) * 4 * N, c->stream));
+  if (R.prec == RRHD_RAD_FP64) {
+    if (cudaMalloc(&R.d_mE, sizeof(double) * rows) != cudaSuccess ||
+        cudaMalloc(&R.d_mF, sizeof(double) * 3 * rows) != cudaSuccess ||
+        cudaMalloc(&R.d_mT, sizeof(double) * 9 * rows) != cudaSuccess)
+      return rrhd_fail(RRHD_ERR_OOM, "coupled-step allocation failed");
+    RRHD_CUDA(cudaMemsetAsync(R.d_mE, 0, sizeof(double) * rows, c->stream));
+    RRHD_CUDA(cudaMemsetAsync(R.d_mF, 0, sizeof(double) * 3 * rows, c->stream));
+    RRHD_CUDA(cudaMemsetAsync(R.d_mT, 0, sizeof(double) * 9 * rows, c->stream));
+  } else {
+    if (cudaMalloc(&R.d_mom, sizeof(float) * 16 * rows) != cudaSuccess)
+      return rrhd_fail(RRHD_ERR_OOM, "coupled-step allocation failed");
+    RRHD_CUDA(cudaMemsetAsync(R.d_mom, 0, sizeof(float) * 16 * rows, c->stream));
+  }
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_coupled_opts *o, rrhd_step_stats *hs,
+                                         rrhd_c2p_stats *ss) {
+  RRHD_CHECK_ARG(c && o, "null argument");
+  RRHD_CHECK_ARG(tau > 0, "tau must be > 0");
+  RadState &R = c->rad;
+  if (!R.ready) return rrhd_fail(RRHD_ERR_STATE, "rrhd_rad_setup has not run");
+  const bool fp64 = R.prec == RRHD_RAD_FP64;
+  RRHD_CHECK_ARG(fp64 ? o->scatter == RRHD_SCATTER_FP64 : (o->scatter >= RRHD_TC_BF16X3 && o->scatter <= RRHD_TC_BF16),
+                 "scatter form does not match the sweep precision");
+  const int k_stall = o->k_stall ? o->k_stall : 12;
+  RRHD_CHECK_ARG(k_stall > 0 && k_stall <= 40, "k_stall must be in [1, 40]");
+  RRHD_CUDA(cudaSetDevice(c->device));
+  rrhd_status s;
+  if (!R.d_I && (s = fp64 ? alloc_coupled<double>(c) : alloc_coupled<float>(c))) return s;
+  if (!fp64 && (!R.tc || R.tc_form != o->scatter)) {
+    if (R.tc) rrhd_scatter_tc_destroy(R.tc);
+    R.tc = nullptr;
+    if ((s = rrhd_scatter_tc_create(R.dirs, o->scatter, &R.tc))) return s;
+    R.tc_form = o->scatter;
+  }
+  cudaStream_t st = c->stream;
+  const int64_t N = c->N, rows = N * R.G;
+  // 1. hydro step (flux, update, con2prim with fallback)
+  rrhd_step_stats hst;
+  const rrhd_status hstat = rrhd_hydro_step(c, tau, hs ? &hst : nullptr);
+  if (hstat && hstat != RRHD_ERR_C2P) return hstat;
+  if (hs) *hs = hst;
+  double *state = c->d_state[c->cur];
+  const Emission em{o->emission.temp_coef, o->emission.sigma_sb, o->emission.pi, o->emission.rad_unit};
+  // 2. opacities and emission from the new primitives
+  if (fp64)
+    k_opacity<double><<<grid_for(N, 256), 256, 0, st>>>(N, R.G, state, o->absorption, o->scattering, em,
+                                                         (double *)R.d_alpha, (double *)R.d_betta, (double *)R.d_Q);
+  else
+    k_opacity<float><<<grid_for(N, 256), 256, 0, st>>>(N, R.G, state, o->absorption, o->scattering, em,
+                                                        (float *)R.d_alpha, (float *)R.d_betta, (float *)R.d_Q);
+  RRHD_CUDA(cudaGetLastError());
+  // 3. sweep with the previous scattering integral
+  SweepIO io{R.d_alpha, R.d_betta, R.d_Q, R.d_S, R.d_I, nullptr};
+  if ((s = launch_sweep(c, io))) return s;
+  // 4. 4-force from the previous intensity's moments, source con2prim
+  k_source<<<grid_for(N, 128), 128, 0, st>>>(N, R.G, state, o->absorption, o->scattering, em, R.d_mE, R.d_mF, R.d_mT,
+                                              R.d_mom, R.d_G4);
+  RRHD_CUDA(cudaGetLastError());
+  if (o->guess) {
+    if ((s = mlp_c2p(o->guess, c->eos, c->gamma, state, state + 5, 10, R.d_G4, tau, nullptr, N, 0, k_stall, ss,
+                     nullptr, nullptr, st)))
+      return s;
+  } else {
+    RRHD_CUDA(cudaMemsetAsync(R.d_cnt, 0, sizeof(unsigned long long) * 8, st));
+    k_source_c2p<<<grid_for(N, 256), 256, 0, st>>>(N, eos_of(c), state, R.d_G4, tau, R.d_cnt);
+    RRHD_CUDA(cudaGetLastError());
+    if (ss) {
+      unsigned long long h[8];
+      RRHD_CUDA(cudaMemcpyAsync(h, R.d_cnt, sizeof h, cudaMemcpyDeviceToHost, st));
+      RRHD_CUDA(cudaStreamSynchronize(st));
+      ss->n_ok = (int64_t)h[0];
+      ss->n_fallback = 0;
+      ss->n_failed = (int64_t)h[1];
+      ss->newton_iters = (int64_t)h[2];
+      ss->max_iters = (int32_t)h[3];
+    }
+  }
+  // 5. scattering integral and moments of the new intensity, for the next step
+  if (fp64) {
+    if ((s = rrhd_scatter_fp64_fma(R.dirs, (const double *)R.d_I, (double *)R.d_S, rows, st))) return s;
+    if ((s = rrhd_moments_fp64(R.dirs, (const double *)R.d_I, R.d_mE, R.d_mF, R.d_mT, rows, st))) return s;
+  } else {
+    if ((s = rrhd_scatter_tc_run(R.tc, (const float *)R.d_I, (float *)R.d_S, R.d_mom, rows, st))) return s;
+  }
+  return hstat;
+}
+
+extern "C" rrhd_status rrhd_rad_get(rrhd_ctx *c, int32_t what, double *out) {
+  RRHD_CHECK_ARG(c && out, "null argument");
+  RadState &R = c->rad;
+  RRHD_CHECK_ARG(what == RRHD_RAD_I || what == RRHD_RAD_S || what == RRHD_RAD_G4, "bad array id");
+  if (!R.ready || !R.d_I) return rrhd_fail(RRHD_ERR_STATE, "no coupled step has run");
+  RRHD_CUDA(cudaSetDevice(c->device));
+  const int64_t N = c->N;
+  const int64_t width = what == RRHD_RAD_G4 ? 4 : (int64_t)R.G * R.M;
+  double *tmp = nullptr;
+  RRHD_CUDA(cudaMalloc(&tmp, sizeof(double) * N * width));
+  const void *src = what == RRHD_RAD_I ? R.d_I : what == RRHD_RAD_S ? R.d_S : (const void *)R.d_G4;
+  if (what == RRHD_RAD_G4 || R.prec == RRHD_RAD_FP64)
+    k_rows_to_host_order<double><<<grid_for(N * width, 256), 256, 0, c->stream>>>(N, width, c->d_perm,
+                                                                                  (const double *)src, tmp);
+  else
+    k_rows_to_host_order<float><<<grid_for(N * width, 256), 256, 0, c->stream>>>(N, width, c->d_perm,
+                                                                                 (const float *)src, tmp);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, sizeof(double) * N * width, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(tmp);
+  RRHD_CUDA(e);
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_rad_set(rrhd_ctx *c, int32_t what, const double *in) {
+  RRHD_CHECK_ARG(c && in, "null argument");
+  RadState &R = c->rad;
+  RRHD_CHECK_ARG(what == RRHD_RAD_I || what == RRHD_RAD_S, "bad array id");
+  if (!R.ready) return rrhd_fail(RRHD_ERR_STATE, "rrhd_rad_setup has not run");
+  RRHD_CUDA(cudaSetDevice(c->device));
+  rrhd_status s;
+  if (!R.d_I && (s = R.prec == RRHD_RAD_FP64 ? alloc_coupled<double>(c) : alloc_coupled<float>(c))) return s;
+  const int64_t N = c->N, width = (int64_t)R.G * R.M;
+  double *tmp = nullptr;
+  RRHD_CUDA(cudaMalloc(&tmp, sizeof(double) * N * width));
+  void *dst = what == RRHD_RAD_I ? R.d_I : R.d_S;
+  cudaError_t e = cudaMemcpyAsync(tmp, in, sizeof(double) * N * width, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) {
+    if (R.prec == RRHD_RAD_FP64)
+      k_rows_from_host_order<double><<<grid_for(N * width, 256), 256, 0, c->stream>>>(N, width, c->d_perm, tmp,
+                                                                                      (double *)dst);
+    else
+      k_rows_from_host_order<float><<<grid_for(N * width, 256), 256, 0, c->stream>>>(N, width, c->d_perm, tmp,
+                                                                                     (float *)dst);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(tmp);
+  RRHD_CUDA(e);
+  return RRHD_OK;
+}

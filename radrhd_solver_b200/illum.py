@@ -4,6 +4,8 @@
     dg = DirectionGrid(fibonacci_directions(256))          # InitDevice (directions)
     S = CalculateIntScattering(dg, I)                      # GetS_MPI_multi_device
     E, F, T = CalculateAllParam(dg, I)                     # MakeIllumParam
+    sw = TransportSweep(grid, dg, groups=1)                # sweep plan (graph/ + make_trace/)
+    CalculateIllum(sw, alpha, betta, Q, S, I)              # one sweep of separate_gpu::CalculateIllum
 
 I is a CUDA tensor [rows, M] with rows = cells x groups (cell-major, the
 layout of grid.Illum, solvers/illum/src/illum_utils.cpp:362).
@@ -119,3 +121,37 @@ def moments_from_tc(mom):
     F = m[:, 1:4].clone()
     T = torch.stack([m[:, 4], m[:, 5], m[:, 6], m[:, 5], m[:, 7], m[:, 8], m[:, 6], m[:, 8], m[:, 9]], 1).view(-1, 3, 3)
     return E, F, T
+
+
+class TransportSweep:
+    """Device sweep plan for a hydro Grid's mesh and a DirectionGrid: the
+    upwind order the reference reads from its offline graph/ and make_trace/
+    outputs (sorted_graph, vec_x0), built on the GPU as levels.  precision:
+    "fp64" or "fp32" (storage and arithmetic of alpha, betta, Q, S, I)."""
+
+    def __init__(self, grid, dg: DirectionGrid, groups: int = 1, precision: str = "fp64", dirs_per_batch: int = 0,
+                 boundary_value: float = 0.0):
+        prec = {"fp64": L.RRHD_RAD_FP64, "fp32": L.RRHD_RAD_FP32}[precision]
+        o = L.RadOpts(groups, prec, dirs_per_batch, boundary_value)
+        L.check(L.lib.rrhd_rad_setup(grid.handle, dg.handle, C.byref(o)), "rrhd_rad_setup")
+        self.grid, self.dg, self.groups, self.precision = grid, dg, groups, precision
+
+    def plan_info(self):
+        lv, mx = C.c_int64(), C.c_int64()
+        L.check(L.lib.rrhd_rad_plan_info(self.grid.handle, C.byref(lv), C.byref(mx)), "rrhd_rad_plan_info")
+        return lv.value, mx.value
+
+
+def CalculateIllum(sw: TransportSweep, alpha, betta, Q, S, I=None):
+    """One sweep of all directions and groups (the direction loop of
+    solvers/illum/src/mpi/multi_gpu/illum_multi_gpu_face_calc.cpp:91-190) on the
+    grid's stream.  CUDA tensors in the sweep precision, caller cell numbering:
+    alpha, betta [N], Q [N, G], S [N*G, M]; returns I [N*G, M]."""
+    import torch
+    if I is None:
+        I = torch.empty_like(S)
+    for t in (alpha, betta, Q, S, I):
+        assert t.is_contiguous() and t.dtype == (torch.float64 if sw.precision == "fp64" else torch.float32)
+    L.check(L.lib.rrhd_sweep(sw.grid.handle, L.ptr(alpha), L.ptr(betta), L.ptr(Q), L.ptr(S), L.ptr(I)),
+            "CalculateIllum")
+    return I

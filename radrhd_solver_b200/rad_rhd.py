@@ -1,5 +1,14 @@
-"""Radiation-hydro coupling, mirroring the reference's `rad_rhd` namespace."""
+"""Radiation-hydro coupling, mirroring the reference's `rad_rhd` namespace.
+
+    sw = illum.TransportSweep(grid, dg, groups=4, precision="fp64")
+    step = RadRHDStep(sw, absorption=1.0, scattering=0.5, em=emission(1, 1))
+    step(tau)                                      # one pass of radRHD_main.cpp:96-139
+"""
 from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
 
 from . import _lib as L
 
@@ -34,3 +43,49 @@ def GetRadSource(W, alpha, sigma, E, F, T, em=None, G=None, stream=None):
 def C_ref(em):
     import ctypes
     return ctypes.byref(em)
+
+
+class RadRHDStep:
+    """The coupled step of solvers/RadRHD/src/radRHD_main.cpp:96-139 on the Grid
+    of a TransportSweep.  scatter: "fp64" (plain form, needs an fp64 sweep) or a
+    tensor-core form "bf16x3" / "f16x3" / "f16" / "bf16" (fp32 sweep); guess: a
+    LearnedGuess for the source con2prim, or None for the reference guess."""
+
+    FORMS = {"fp64": L.RRHD_SCATTER_FP64, "bf16x3": L.RRHD_TC_BF16X3, "f16x3": L.RRHD_TC_F16X3,
+             "f16": L.RRHD_TC_F16, "bf16": L.RRHD_TC_BF16}
+
+    def __init__(self, sweep, absorption: float = 1.0, scattering: float = 0.5, em=None, scatter: str = "fp64",
+                 guess=None, k_stall: int = 0):
+        self.sweep = sweep
+        self.grid = sweep.grid
+        self.guess = guess
+        em = em if em is not None else emission(1.0, 1.0)
+        self.opts = L.CoupledOpts(self.FORMS[scatter], guess.handle.value if guess is not None else None, k_stall,
+                                  absorption, scattering, em)
+
+    def __call__(self, tau: float, stats: bool = False):
+        """One coupled step; with stats=True returns (hydro StepStats, source C2pStats)."""
+        if not stats:
+            L.check(L.lib.rrhd_coupled_step(self.grid.handle, tau, C.byref(self.opts), None, None), "coupled step")
+            return None
+        hs, ss = L.StepStats(), L.C2pStats()
+        L.check(L.lib.rrhd_coupled_step(self.grid.handle, tau, C.byref(self.opts), C.byref(hs), C.byref(ss)),
+                "coupled step")
+        return hs, ss
+
+    _KEYS = {"I": L.RRHD_RAD_I, "S": L.RRHD_RAD_S, "G4": L.RRHD_RAD_G4}
+
+    def get(self, what: str):
+        """Host copy, caller numbering: "I" / "S" [N*G, M], "G4" [N, 4]."""
+        n = self.grid.size
+        shape = (n, 4) if what == "G4" else (n * self.sweep.groups, self.sweep.dg.size)
+        out = np.zeros(shape)
+        L.check(L.lib.rrhd_rad_get(self.grid.handle, self._KEYS[what], L.ptr(out)), "rrhd_rad_get")
+        return out
+
+    def set(self, what: str, values):
+        """Writes "I" or "S" [N*G, M] (caller numbering)."""
+        assert what in ("I", "S")
+        v = np.ascontiguousarray(values, np.float64)
+        assert v.shape == (self.grid.size * self.sweep.groups, self.sweep.dg.size)
+        L.check(L.lib.rrhd_rad_set(self.grid.handle, self._KEYS[what], L.ptr(v)), "rrhd_rad_set")
