@@ -317,6 +317,126 @@ def c2p_component(dev, n=8_000_000, epochs=8, reps=5):
     return out
 
 
+EM_JET = (1.0, 10.0, float(np.pi), 1.0)  # temp_coef, a_R, pi, kRadiation in code units: T = p / rho, B = a_R T^4 / pi
+
+
+def coupled_component(dev, m, W, steps=3, warm=1, M=256, G=4, train_epochs=2, forms=("plain", "chosen")):
+    """Config-4 coupled radiation-hydro jet step (radRHD_main.cpp:96-139) on the
+    benchmark mesh: hydro step, opacities alpha = rho, betta = 0.5 rho, emission
+    Q = a_R T^4 / pi / G per grey group, sweep of M directions x G groups,
+    4-force + source con2prim, scattering integral + moments.  Plain form: FP64
+    sweep, FP64 scattering (one FMA per term), reference con2prim guess.  Chosen
+    form: FP32 sweep, tensor-core F16X3 scattering, learned con2prim guess
+    trained on the plain run's own states.  Both forms start from the same state;
+    the intensity arrays (N*G*M = 5.4e9 values) are far larger than L2."""
+    import torch
+    from radrhd_solver_b200 import illum, rad_rhd, rhllc
+    from radrhd_solver_b200 import mesh as Mm
+    from radrhd_solver_b200.c2p_mlp import LearnedGuess
+    d = Mm.fibonacci_directions(M)
+    tau = CFL * m.h_min
+    out = {"workload": f"coupled jet {m.n_cells} cells x {M} directions x {G} groups", "cells": m.n_cells,
+           "directions": M, "groups": G, "emission": {"temp_coef": EM_JET[0], "a_R": EM_JET[1], "rad_unit": EM_JET[3]},
+           "tau": tau, "steps": steps}
+    states = {}
+    net = None
+    for form in forms:
+        torch.cuda.empty_cache()
+        g = rhllc.Grid(m, eos=rhllc.EOS_IDEAL, gamma=GAMMA, device=dev)
+        g.set_boundary(-3, rhllc.BC_FIXED, INFLOW)
+        g.set_state_prim(W)
+        dg = illum.DirectionGrid(d, dev)
+        t0 = time.perf_counter()
+        sw = illum.TransportSweep(g, dg, groups=G, precision="fp64" if form == "plain" else "fp32")
+        t_plan = time.perf_counter() - t0
+        if form == "chosen" and "plain_dump" in states:
+            Wp, Up = states["plain_dump"]
+            net = LearnedGuess(device=dev, seed=1)
+            Ut = torch.tensor(Up, device=f"cuda:{dev}")
+            pt = torch.tensor(Wp[:, 4], device=f"cuda:{dev}")
+            net.train(Ut, pt, epochs=train_epochs, batch=4096, lr=2e-3, seed=3)
+            del Ut, pt
+        step = rad_rhd.RadRHDStep(sw, absorption=1.0, scattering=0.5, em=rad_rhd.emission(*EM_JET),
+                                  scatter="fp64" if form == "plain" else "f16x3",
+                                  guess=None if form == "plain" else net)
+        stream = torch.cuda.ExternalStream(g.stream)
+        warm_stats = [step(tau, stats=True) for _ in range(warm)]
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps - 1):
+            step(tau)
+        hs, ss = step(tau, stats=True)  # the last step reads its statistics back
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        ph = step.phase_ms()
+        levels, biggest = sw.plan_info()
+        Wg, Ug = g.get_state()
+        states[form] = Ug
+        if form == "plain":
+            states["plain_dump"] = (Wg, Ug)
+        bpv = 8 if form == "plain" else 4
+        sweep_alg = (2.0 * m.n_cells + 2.0 * m.n_faces) * M * G * bpv + m.n_cells * (20 * bpv + 32.0)
+        out[form] = {"ms_per_step": ms, "steps_per_s": 1e3 / ms, "cell_updates_per_s": m.n_cells / (ms / 1e3),
+                     "cell_dir_group_per_s": m.n_cells * M * G / (ms / 1e3), "phase_ms_last_step": ph,
+                     "sweep_levels": levels, "largest_level": biggest, "plan_build_s": t_plan,
+                     "sweep_alg_gbs": sweep_alg / (ph["sweep"] / 1e3) / 1e9,
+                     "source_c2p": {"newton_iters_per_state": ss.newton_iters / m.n_cells, "failed": ss.n_failed},
+                     "hydro": {"n_fallback": hs.n_fallback, "n_failed": hs.n_failed},
+                     "warmup_failures": [[h.n_failed, s_.n_failed] for h, s_ in warm_stats]}
+        g.close()
+        dg.close()
+        del step, sw
+    if net is not None:
+        net.close()
+    if "plain" in states and "chosen" in states:
+        up, uc = states["plain"], states["chosen"]
+        out["state_max_rel_diff"] = float(np.max(np.abs(uc - up) / np.maximum(np.abs(up).max(0), 1e-300)))
+        out["chosen_vs_plain"] = out["plain"]["ms_per_step"] / out["chosen"]["ms_per_step"]
+    return out
+
+
+def sweep_component(dev, nhex=32, M=256, G=4, reps=3, precisions=("fp64", "fp32")):
+    """Standalone transport sweep (rrhd_sweep) on the jet mesh with seeded
+    opacities and sources: alpha log-uniform [0.1, 30], betta = alpha / 2, Q and S
+    log-uniform; the unit is one (cell, direction) pair with all G groups."""
+    import torch
+    from radrhd_solver_b200 import illum, rhllc
+    from radrhd_solver_b200 import mesh as Mm
+    m, _ = make_jet(nhex)
+    d = Mm.fibonacci_directions(M)
+    out = {"workload": f"sweep {m.n_cells} cells x {M} directions x {G} groups", "cells": m.n_cells, "faces": m.n_faces}
+    for prec in precisions:
+        torch.cuda.empty_cache()
+        g = rhllc.Grid(m, eos=rhllc.EOS_IDEAL, gamma=GAMMA, device=dev)
+        dg = illum.DirectionGrid(d, dev)
+        t0 = time.perf_counter()
+        sw = illum.TransportSweep(g, dg, groups=G, precision=prec)
+        t_plan = time.perf_counter() - t0
+        dt = torch.float64 if prec == "fp64" else torch.float32
+        gen = torch.Generator(device=f"cuda:{dev}").manual_seed(5)
+        rnd = lambda *shape, lo, hi: (10 ** (lo + (hi - lo) * torch.rand(*shape, generator=gen, device=f"cuda:{dev}",
+                                                                        dtype=torch.float64))).to(dt)
+        alpha = rnd(m.n_cells, lo=-1, hi=1.5)
+        betta = (0.5 * alpha).contiguous()
+        Q = rnd(m.n_cells, G, lo=-2, hi=0)
+        S = rnd(m.n_cells * G, M, lo=-3, hi=-1)
+        I = torch.empty_like(S)
+        torch.cuda.synchronize()
+        stream = torch.cuda.ExternalStream(g.stream)
+        ms = _time(lambda: illum.CalculateIllum(sw, alpha, betta, Q, S, I), reps, stream, warm=1)
+        levels, biggest = sw.plan_info()
+        bpv = 8 if prec == "fp64" else 4
+        alg = (2.0 * m.n_cells + 2.0 * m.n_faces) * M * G * bpv + m.n_cells * (20 * bpv + 32.0)
+        out[prec] = {"ms": ms, "cell_dir_per_s": m.n_cells * M / (ms / 1e3), "levels": levels,
+                     "largest_level": biggest, "plan_build_s": t_plan, "alg_gbs": alg / (ms / 1e3) / 1e9}
+        del alpha, betta, Q, S, I
+        g.close()
+        dg.close()
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -411,6 +531,8 @@ def run_ours(args):
             "clocks": clk.summary(),
             "step_stats": {"max_speed": st.max_speed, "n_fallback": st.n_fallback, "n_failed": st.n_failed}}
     g.close()
+    if rank == 0 and not args.no_coupled:
+        line["coupled"] = coupled_component(dev, m, W, steps=args.coupled_steps)
     if rank == 0 and not args.no_cpu:
         import oracle
         threads = cpu_threads()
@@ -425,7 +547,9 @@ def run_ours(args):
         line["scatter"] = scatter_component(dev)
         sc = line["scatter"]
         if "fp64_fma" in sc:
-            line["chosen_vs_plain"] = {"scatter_moments": sc["fp64_fma"]["ms"] / sc["tc_f16x3"]["ms"]}
+            line.setdefault("chosen_vs_plain", {})["scatter_moments"] = sc["fp64_fma"]["ms"] / sc["tc_f16x3"]["ms"]
+    if rank == 0 and "coupled" in line:
+        line.setdefault("chosen_vs_plain", {})["coupled_step"] = line["coupled"]["chosen_vs_plain"]
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -445,8 +569,16 @@ def main():
     ap.add_argument("--cpb", type=int, default=0, help="cells per CTA of the step kernel (0 = library default)")
     ap.add_argument("--no-scatter", action="store_true", help="skip the scattering component")
     ap.add_argument("--no-c2p", action="store_true", help="skip the con2prim (learned guess) component")
+    ap.add_argument("--no-coupled", action="store_true", help="skip the coupled radiation-hydro step component")
+    ap.add_argument("--coupled-steps", type=int, default=3, help="timed coupled steps per form")
     ap.add_argument("--scatter-only", type=int, default=0, metavar="NHEX",
                     help="only time the scattering component on an NHEX^3 x 6 mesh (profiling runs)")
+    ap.add_argument("--sweep-only", type=int, default=0, metavar="NHEX",
+                    help="only time the standalone sweep on an NHEX^3 x 6 jet mesh (profiling runs)")
+    ap.add_argument("--sweep-prec", default="fp64,fp32", help="precisions of --sweep-only")
+    ap.add_argument("--coupled-only", type=int, default=0, metavar="NHEX",
+                    help="only time the coupled step on an NHEX^3 x 6 jet mesh (profiling runs)")
+    ap.add_argument("--coupled-forms", default="plain,chosen", help="forms of --coupled-only")
     args = ap.parse_args()
     global NHEX
     NHEX = args.nhex
@@ -454,6 +586,19 @@ def main():
         import torch
         torch.cuda.set_device(0)
         print(json.dumps(scatter_component(0, nhex=args.scatter_only, reps=args.steps)), flush=True)
+        return
+    if args.coupled_only:
+        import torch
+        torch.cuda.set_device(0)
+        m, W = make_jet(args.coupled_only)
+        print(json.dumps(coupled_component(0, m, W, steps=args.coupled_steps,
+                                           forms=tuple(args.coupled_forms.split(",")))), flush=True)
+        return
+    if args.sweep_only:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(sweep_component(0, nhex=args.sweep_only, reps=args.steps,
+                                         precisions=tuple(args.sweep_prec.split(",")))), flush=True)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -289,6 +289,16 @@ rrhd_status rrhd_scatter_tc_destroy(rrhd_scatter_tc *t);
  * device pointers, 16-byte aligned. */
 rrhd_status rrhd_scatter_tc_run(const rrhd_scatter_tc *t, const float *I, float *S, float *moments,
                                 int64_t rows, void *stream);
+/* The same three contractions on the cell-direction-group layout the coupled
+ * step keeps its intensity in: I, S [cells][M][groups] (row cell * groups + g of
+ * the row-layout calls above; moments stay [rows][...]).  groups divides 64 for
+ * the FP64 calls and is 1, 2 or 4 for the tensor cores. */
+rrhd_status rrhd_scatter_fp64_cdg(const rrhd_dirs *d, const double *I, double *S, int64_t cells, int32_t groups,
+                                  int32_t exact, void *stream);
+rrhd_status rrhd_moments_fp64_cdg(const rrhd_dirs *d, const double *I, double *E, double *F, double *T,
+                                  int64_t cells, int32_t groups, void *stream);
+rrhd_status rrhd_scatter_tc_run_cdg(const rrhd_scatter_tc *t, const float *I, float *S, float *moments,
+                                    int64_t cells, int32_t groups, void *stream);
 /* Reads (and with clear != 0 resets) the error word of the tensor-core kernels:
  * RRHD_ERR_CUDA if a bounded pipeline wait timed out.  Synchronises `stream`. */
 rrhd_status rrhd_scatter_tc_check(const rrhd_scatter_tc *t, void *stream, int32_t clear);
@@ -366,6 +376,9 @@ typedef struct {
  * of the source con2prim; either one synchronises the stream. */
 rrhd_status rrhd_coupled_step(rrhd_ctx *ctx, double tau, const rrhd_coupled_opts *opts, rrhd_step_stats *hydro,
                               rrhd_c2p_stats *source);
+/* Device time (ms) of the phases of the last coupled step: hydro step; opacities
+ * + sweep; 4-force + source con2prim; scattering + moments.  Synchronises. */
+rrhd_status rrhd_coupled_phase_ms(rrhd_ctx *ctx, float *ms4);
 /* Host copies (caller cell numbering, double) of the coupled step's radiation
  * arrays: RRHD_RAD_I / RRHD_RAD_S [N*G][M], RRHD_RAD_G4 [N][4] (4-force of the
  * last step); rrhd_rad_set writes I or S (e.g. the scattering integral of a

@@ -15,4 +15,14 @@ rrhd_status mlp_c2p(const rrhd_mlp *m, int eos, double gamma, double *U, double 
                     const double *G4, double tau_src, uint8_t *status, int64_t n, int fallback, int k_stall,
                     rrhd_c2p_stats *stats, int64_t *n_guess_fallback, double *guess, cudaStream_t st);
 
+// Scattering integral / moments with I and S in the cell-direction-group layout
+// [cells][M][G] (rows cell * G + g of the row-layout entry points); G divides 64
+// (FP64) or is 1, 2 or 4 (tensor cores).
+rrhd_status scatter_fp64_cdg(const rrhd_dirs *d, const double *I, double *S, int64_t cells, int G, bool exact,
+                             cudaStream_t st);
+rrhd_status moments_fp64_cdg(const rrhd_dirs *d, const double *I, double *E, double *F, double *T, int64_t cells,
+                             int G, cudaStream_t st);
+rrhd_status scatter_tc_cdg(const rrhd_scatter_tc *t, const float *I, float *S, float *mom, int64_t cells, int G,
+                           cudaStream_t st);
+
 }  // namespace rrhd

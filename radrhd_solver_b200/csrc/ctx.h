@@ -33,9 +33,10 @@ namespace rrhd {
 // Pointers a sweep reads and writes, kept in device memory so that one captured
 // graph of level launches serves every call.
 struct SweepIO {
-  const void *alpha, *betta, *Q, *S;  // [N], [N], [N][G], [N*G][M]
-  void *I;                            // [N*G][M]
-  const int32_t *row_of;              // context cell -> caller cell, or NULL (context rows)
+  const void *S;          // scattering integral
+  void *I;                // intensity
+  const int32_t *row_of;  // layout 0: context cell -> caller cell
+  int32_t layout;         // 0: rows (cell * G + g) x M in caller numbering; 1: [N][M][G], context numbering
 };
 
 // Radiation part of a context: the transport sweep and the coupled step.
@@ -44,22 +45,28 @@ struct RadState {
   const rrhd_dirs *dirs = nullptr;  // not owned
   int M = 0, G = 1, DB = 64, shift = 6, nbatch = 0;
   int prec = 0;  // RRHD_RAD_FP64 or RRHD_RAD_FP32: storage and arithmetic of the sweep
+  int DS = 0;    // stride (values) of the per-cell source record
+  int GS = 0;    // stride (values) of one face-value slot: G rounded up to a 32-byte sector
   double bc = 0.0;
   int64_t last_cell = 0;  // context index of the caller's last cell (plain-mean quirk)
-  void *d_w = nullptr;     // [M][3] directions in the sweep precision
-  void *d_geo = nullptr;   // [N][16] per local face j: outward normal (3 j..3 j+2), then heights H_j at 12+j
-  void *d_area = nullptr;  // [N][4] face areas
-  int4 *d_fid = nullptr;   // [N] caller face ids of the local faces
-  int4 *d_nbr = nullptr;   // [N] neighbour (context numbering) or -1
+  void *d_w = nullptr;    // [M][3] directions in the sweep precision
+  // per-cell record (context numbering): outward normals n_j (12), heights H_j = 3 V / A_j (4),
+  // areas A_j (4), then face-value slots of the faces (4 x int32) and neighbours (4 x int32, context
+  // numbering or -1);
+  // 192 B in double, 128 B in float
+  void *d_rec = nullptr;
+  void *d_dyn = nullptr;  // [N][DS] per-cell source record: k = alpha + betta, betta, alpha Q_g
   uint32_t *d_plan = nullptr;               // all batches: items (cell << shift | d) in level order
   std::vector<std::vector<int64_t>> lvl;    // per batch: level offsets into d_plan
   int64_t levels = 0, max_level = 0;
   cudaGraphExec_t graph = nullptr;          // every level launch of one sweep
   SweepIO *d_io = nullptr;
-  void *d_fv = nullptr;  // [F][DB][G] face values
-  // coupled step (context numbering, rows cell * G + g)
-  void *d_I = nullptr, *d_S = nullptr;                      // [N*G][M]
-  void *d_alpha = nullptr, *d_betta = nullptr, *d_Q = nullptr;  // [N], [N], [N][G]
+  SweepIO h_io{};       // last pointers uploaded to d_io
+  bool io_valid = false;
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // phase marks of the last coupled step
+  void *d_fv = nullptr;  // [F][DB][GS] face values
+  // coupled step (context numbering, [N][M][G])
+  void *d_I = nullptr, *d_S = nullptr;
   double *d_G4 = nullptr;                                    // [N][4] radiation 4-force of the last step
   double *d_mE = nullptr, *d_mF = nullptr, *d_mT = nullptr;  // FP64 moments per row [N*G], [N*G][3], [N*G][9]
   float *d_mom = nullptr;                                    // FP32 moments per row [N*G][16]

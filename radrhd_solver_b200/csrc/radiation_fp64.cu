@@ -17,6 +17,7 @@
 #include "rrhd_internal.h"
 
 #include "dirs.h"
+#include "coupled.h"
 #include "rad_phys.cuh"
 
 namespace {
@@ -34,13 +35,34 @@ __global__ void k_build_gamma(int M, const double *w, const double *a, double A,
   K[(size_t)d * M + k] = g * a[d] / A;
 }
 
+// Element (row r, direction d) of a [rows][M] array (lg < 0) or of a
+// cell-direction-group array [rows >> lg][M][1 << lg] (row r = cell * 2^lg + group).
+__device__ __forceinline__ int64_t elem(int64_t r, int d, int M, int lg) {
+  return lg >= 0 ? (((r >> lg) * M + d) << lg) + (r & ((1 << lg) - 1)) : r * M + d;
+}
+
+// Tile element t of a (rows) x (nd directions) tile in memory order: row r, direction d.
+__device__ __forceinline__ void tile_rd(int t, int nd, int lg, int &r, int &d) {
+  if (lg >= 0) {
+    const int g = t & ((1 << lg) - 1), q = t >> lg;
+    d = q % nd;
+    r = ((q / nd) << lg) + g;
+  } else {
+    r = t / nd;
+    d = t % nd;
+  }
+}
+
 template <bool EXACT>
-__global__ void __launch_bounds__(256) k_scatter(int64_t rows, int M, const double *__restrict__ I,
+__global__ void __launch_bounds__(256) k_scatter(int64_t rows, int M, int lg, const double *__restrict__ I,
                                                  const double *__restrict__ G,
                                                  const double *__restrict__ a, double A,
                                                  double *__restrict__ S) {
-  __shared__ double sI[TR][TD + 1];
-  __shared__ double sG[TD][TK];
+  // the input tiles, then (after the loop) the output tile staged for coalesced stores
+  __shared__ double buf[TR * (TD + 1) + TD * TK];
+  static_assert(TR * (TD + 1) + TD * TK >= TR * (TK + 1), "output tile must fit");
+  double(*sI)[TD + 1] = reinterpret_cast<double(*)[TD + 1]>(buf);
+  double(*sG)[TK] = reinterpret_cast<double(*)[TK]>(buf + TR * (TD + 1));
   __shared__ double sa[TD];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int64_t r0 = (int64_t)blockIdx.x * TR;
@@ -54,9 +76,10 @@ __global__ void __launch_bounds__(256) k_scatter(int64_t rows, int M, const doub
   for (int d0 = 0; d0 < M; d0 += TD) {
     // I tile: 64 rows x 32 directions
     for (int t = threadIdx.x; t < TR * TD; t += 256) {
-      const int r = t / TD, d = t % TD;
+      int r, d;
+      tile_rd(t, TD, lg, r, d);
       const int64_t gr = r0 + r;
-      sI[r][d] = (gr < rows && d0 + d < M) ? I[gr * M + d0 + d] : 0.0;
+      sI[r][d] = (gr < rows && d0 + d < M) ? I[elem(gr, d0 + d, M, lg)] : 0.0;
     }
     for (int t = threadIdx.x; t < TD * TK; t += 256) {
       const int d = t / TK, k = t % TK;
@@ -90,22 +113,25 @@ __global__ void __launch_bounds__(256) k_scatter(int64_t rows, int M, const doub
     }
     __syncthreads();
   }
+  double(*sO)[TK + 1] = reinterpret_cast<double(*)[TK + 1]>(buf);
 #pragma unroll
-  for (int i = 0; i < 4; i++) {
-    const int64_t gr = r0 + ty + 16 * i;
-    if (gr >= rows) continue;
+  for (int i = 0; i < 4; i++)
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int k = k0 + tx + 16 * j;
-      if (k < M) S[gr * M + k] = EXACT ? acc[i][j] / A : acc[i][j];
-    }
+    for (int j = 0; j < 4; j++) sO[ty + 16 * i][tx + 16 * j] = EXACT ? acc[i][j] / A : acc[i][j];
+  __syncthreads();
+  // stores in memory order of the layout (consecutive threads, consecutive addresses)
+  for (int t = threadIdx.x; t < TR * TK; t += 256) {
+    int r, k;
+    tile_rd(t, TK, lg, r, k);
+    const int64_t gr = r0 + r;
+    if (gr < rows && k0 + k < M) S[elem(gr, k0 + k, M, lg)] = sO[r][k];
   }
 }
 
 // cuda_sep::device::MakeEnergy / MakeStream / MakeImpuls
 // (cuda_illum_sep_param.cu:9-69), one thread per row.
 constexpr int MR = 128, MD = 32;
-__global__ void __launch_bounds__(MR) k_moments(int64_t rows, int M, const double *__restrict__ I,
+__global__ void __launch_bounds__(MR) k_moments(int64_t rows, int M, int lg, const double *__restrict__ I,
                                                 const double *__restrict__ w,
                                                 const double *__restrict__ a, double A,
                                                 double *__restrict__ E, double *__restrict__ Fo,
@@ -121,8 +147,9 @@ __global__ void __launch_bounds__(MR) k_moments(int64_t rows, int M, const doubl
   for (int i = 0; i < 9; i++) t[i] = 0;
   for (int d0 = 0; d0 < M; d0 += MD) {
     for (int q = threadIdx.x; q < MR * MD; q += MR) {
-      const int rr = q / MD, d = q % MD;
-      sI[rr][d] = (r0 + rr < rows && d0 + d < M) ? I[(r0 + rr) * M + d0 + d] : 0.0;
+      int rr, d;
+      tile_rd(q, MD, lg, rr, d);
+      sI[rr][d] = (r0 + rr < rows && d0 + d < M) ? I[elem(r0 + rr, d0 + d, M, lg)] : 0.0;
     }
     if (threadIdx.x < MD) {
       const int d = d0 + threadIdx.x;
@@ -226,7 +253,7 @@ extern "C" rrhd_status rrhd_scatter_fp64(const rrhd_dirs *d, const double *I, do
   RRHD_CHECK_ARG(d && I && S && rows >= 0, "bad arguments");
   if (rows == 0) return RRHD_OK;
   dim3 grid((unsigned)((rows + TR - 1) / TR), (d->M + TK - 1) / TK);
-  k_scatter<true><<<grid, 256, 0, (cudaStream_t)stream>>>(rows, d->M, I, d->d_G, d->d_a, d->full_area, S);
+  k_scatter<true><<<grid, 256, 0, (cudaStream_t)stream>>>(rows, d->M, -1, I, d->d_G, d->d_a, d->full_area, S);
   RRHD_CUDA(cudaGetLastError());
   return RRHD_OK;
 }
@@ -238,7 +265,7 @@ extern "C" rrhd_status rrhd_scatter_fp64_fma(const rrhd_dirs *d, const double *I
   RRHD_CHECK_ARG(d && I && S && rows >= 0, "bad arguments");
   if (rows == 0) return RRHD_OK;
   dim3 grid((unsigned)((rows + TR - 1) / TR), (d->M + TK - 1) / TK);
-  k_scatter<false><<<grid, 256, 0, (cudaStream_t)stream>>>(rows, d->M, I, d->d_K, d->d_a, d->full_area, S);
+  k_scatter<false><<<grid, 256, 0, (cudaStream_t)stream>>>(rows, d->M, -1, I, d->d_K, d->d_a, d->full_area, S);
   RRHD_CUDA(cudaGetLastError());
   return RRHD_OK;
 }
@@ -247,8 +274,37 @@ extern "C" rrhd_status rrhd_moments_fp64(const rrhd_dirs *d, const double *I, do
                                          double *T, int64_t rows, void *stream) {
   RRHD_CHECK_ARG(d && I && E && F && T && rows >= 0, "bad arguments");
   if (rows == 0) return RRHD_OK;
-  k_moments<<<(unsigned)((rows + MR - 1) / MR), MR, 0, (cudaStream_t)stream>>>(rows, d->M, I, d->d_w, d->d_a,
+  k_moments<<<(unsigned)((rows + MR - 1) / MR), MR, 0, (cudaStream_t)stream>>>(rows, d->M, -1, I, d->d_w, d->d_a,
                                                                                d->full_area, E, F, T);
+  RRHD_CUDA(cudaGetLastError());
+  return RRHD_OK;
+}
+
+rrhd_status rrhd::scatter_fp64_cdg(const rrhd_dirs *d, const double *I, double *S, int64_t cells, int ng, bool exact,
+                                   cudaStream_t st) {
+  RRHD_CHECK_ARG(d && I && S && cells >= 0 && ng > 0 && TR % ng == 0, "bad arguments");
+  const int64_t rows = cells * ng;
+  if (rows == 0) return RRHD_OK;
+  int lg = 0;
+  while ((1 << lg) < ng) lg++;
+  dim3 grid((unsigned)((rows + TR - 1) / TR), (d->M + TK - 1) / TK);
+  if (exact)
+    k_scatter<true><<<grid, 256, 0, st>>>(rows, d->M, lg, I, d->d_G, d->d_a, d->full_area, S);
+  else
+    k_scatter<false><<<grid, 256, 0, st>>>(rows, d->M, lg, I, d->d_K, d->d_a, d->full_area, S);
+  RRHD_CUDA(cudaGetLastError());
+  return RRHD_OK;
+}
+
+rrhd_status rrhd::moments_fp64_cdg(const rrhd_dirs *d, const double *I, double *E, double *F, double *T,
+                                   int64_t cells, int ng, cudaStream_t st) {
+  RRHD_CHECK_ARG(d && I && E && F && T && cells >= 0 && ng > 0 && MR % ng == 0, "bad arguments");
+  const int64_t rows = cells * ng;
+  if (rows == 0) return RRHD_OK;
+  int lg = 0;
+  while ((1 << lg) < ng) lg++;
+  k_moments<<<(unsigned)((rows + MR - 1) / MR), MR, 0, st>>>(rows, d->M, lg, I, d->d_w, d->d_a, d->full_area, E, F,
+                                                             T);
   RRHD_CUDA(cudaGetLastError());
   return RRHD_OK;
 }
@@ -281,4 +337,14 @@ extern "C" rrhd_status rrhd_rad_source(const rrhd_emission *em, const double *W,
   k_rad_source<<<(unsigned)((n + 127) / 128), 128, 0, (cudaStream_t)stream>>>(n, e, W, alpha, sigma, E, F, T, G);
   RRHD_CUDA(cudaGetLastError());
   return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_scatter_fp64_cdg(const rrhd_dirs *d, const double *I, double *S, int64_t cells,
+                                             int32_t groups, int32_t exact, void *stream) {
+  return rrhd::scatter_fp64_cdg(d, I, S, cells, groups, exact != 0, (cudaStream_t)stream);
+}
+
+extern "C" rrhd_status rrhd_moments_fp64_cdg(const rrhd_dirs *d, const double *I, double *E, double *F, double *T,
+                                             int64_t cells, int32_t groups, void *stream) {
+  return rrhd::moments_fp64_cdg(d, I, E, F, T, cells, groups, (cudaStream_t)stream);
 }

@@ -42,6 +42,7 @@
 #include <cstring>
 #include <vector>
 
+#include "coupled.h"
 #include "rrhd_internal.h"
 
 #include "dirs.h"
@@ -203,12 +204,39 @@ __global__ void k_row_scale(const float *__restrict__ I, int64_t rows, int M, fl
   if (lane == 0) scale[r] = (m > 0.f && isfinite(m)) ? ldexpf(1.f, 14 - ilogbf(m)) : 1.f;
 }
 
+// The same for a cell-direction-group array [cells][M][ng]: one warp per cell,
+// scale[cell * ng + g] from the maximum over the cell's group-g values.
+__global__ void k_row_scale_cdg(const float *__restrict__ I, int64_t cells, int M, int ng,
+                                float *__restrict__ scale) {
+  const int64_t c = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (c >= cells) return;
+  const float4 *blk = reinterpret_cast<const float4 *>(I + c * (int64_t)M * ng);
+  float m[4] = {0.f, 0.f, 0.f, 0.f};  // per float4 component; component q holds group q % ng
+  for (int i = lane; i < M * ng / 4; i += 32) {
+    const float4 v = __ldg(blk + i);
+    m[0] = fmaxf(m[0], fabsf(v.x));
+    m[1] = fmaxf(m[1], fabsf(v.y));
+    m[2] = fmaxf(m[2], fabsf(v.z));
+    m[3] = fmaxf(m[3], fabsf(v.w));
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m[q] = fmaxf(m[q], __shfl_xor_sync(0xffffffffu, m[q], o));
+  if (lane < ng) {
+    float mg = 0.f;
+    for (int q = lane; q < 4; q += ng) mg = fmaxf(mg, m[q]);
+    scale[c * ng + lane] = (mg > 0.f && isfinite(mg)) ? ldexpf(1.f, 14 - ilogbf(mg)) : 1.f;
+  }
+}
+
 // Persistent: CTA b takes tiles b, b + gridDim.x, ...; tile t covers rows
 // 128 (t / n_nt) .. +127 and output directions 128 (t % n_nt) .. +127.  The
 // chunk counter g runs on across tiles, so smem stages and TMEM accumulators
 // keep cycling and the accumulator warps store one tile while the next is
 // being multiplied.
-template <int FORM>
+template <int FORM, int NG>
 __global__ void __launch_bounds__(THREADS, 1)
     k_scatter_tc(const __grid_constant__ CUtensorMap tm_bh, const __grid_constant__ CUtensorMap tm_bl,
                  const __grid_constant__ CUtensorMap tm_mh, const __grid_constant__ CUtensorMap tm_ml,
@@ -353,7 +381,8 @@ __global__ void __launch_bounds__(THREADS, 1)
       const int kk = (int)(gg % nk);
       const int sa = (int)(gg % A32_STAGES);
       mbar_arrive_expect_tx(&a32_full[sa], A32_BYTES);
-      tma_load_2d(a32 + sa * A32_BYTES, &tm_a, kk * BK, (int)((tile / n_nt) * BM), &a32_full[sa]);
+      // NG > 1: box {BK * NG, BM / NG} of the [cells][M * NG] view
+      tma_load_2d(a32 + sa * A32_BYTES, &tm_a, kk * BK * NG, (int)((tile / n_nt) * (BM / NG)), &a32_full[sa]);
     };
     if (t == 0)
       for (int64_t gg = 0; gg < A32_STAGES && gg < my_chunks; gg++) issue_a(gg);
@@ -368,8 +397,13 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         float4 v[CONV_ITERS];
         const float4 *src = reinterpret_cast<const float4 *>(a32 + sa * A32_BYTES);
+        // rows layout: float4 i*CONV_THREADS + t; [cells][64][ng]: the ng float4s of unit i/ng*CONV_THREADS + t
+        constexpr int ush = NG == 4 ? 2 : (NG == 2 ? 1 : 0);
 #pragma unroll
-        for (int i = 0; i < CONV_ITERS; i++) v[i] = src[i * CONV_THREADS + t];
+        for (int i = 0; i < CONV_ITERS; i++)
+          v[i] = src[((((i >> ush) * CONV_THREADS) + t) << ush) + (i & ((1 << ush) - 1))];
+        // the next TMA into this slot (async proxy) must not overtake these generic-proxy reads
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         mbar_arrive(&a32_empty[sa]);
         if (t == 0 && g + A32_STAGES < my_chunks) {
           if (!mbar_wait(&a32_empty[sa], (uint32_t)(g / A32_STAGES) & 1)) {
@@ -384,10 +418,9 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         if (*abort_flag) break;
         uint8_t *ah = smem + s * STAGE_BYTES, *al = ah + A_BYTES;
-#pragma unroll
-        for (int i = 0; i < CONV_ITERS; i++) {
-          const int e = i * CONV_THREADS + t, row = e >> 4, c4 = e & 15;
-          float x[4] = {v[i].x, v[i].y, v[i].z, v[i].w};
+        // (row, c4) of the unit each converted quad belongs to, and its 4 values
+        auto put = [&](int row, int c4, float x0, float x1, float x2, float x3) {
+          float x[4] = {x0, x1, x2, x3};
           if (SCALED) {
             const int64_t gr = r0 + row;
             const float sc = gr < P.rows ? __ldg(P.scale + gr) : 1.f;
@@ -403,6 +436,33 @@ __global__ void __launch_bounds__(THREADS, 1)
           if (THREE)
             *reinterpret_cast<uint2 *>(al + off) =
                 make_uint2((uint32_t)l[0] | ((uint32_t)l[1] << 16), (uint32_t)l[2] | ((uint32_t)l[3] << 16));
+        };
+        if constexpr (NG == 4) {
+          // staged tile [32 cells][64 directions][4 groups]: unit (cell, c4) = float4s 4u..4u+3, one per direction
+#pragma unroll
+          for (int iu = 0; iu < CONV_ITERS / 4; iu++) {
+            const int u = iu * CONV_THREADS + t, cl = u >> 4, c4 = u & 15;
+            const float4 d0 = v[4 * iu], d1 = v[4 * iu + 1], d2 = v[4 * iu + 2], d3 = v[4 * iu + 3];
+            put(cl * 4 + 0, c4, d0.x, d1.x, d2.x, d3.x);
+            put(cl * 4 + 1, c4, d0.y, d1.y, d2.y, d3.y);
+            put(cl * 4 + 2, c4, d0.z, d1.z, d2.z, d3.z);
+            put(cl * 4 + 3, c4, d0.w, d1.w, d2.w, d3.w);
+          }
+        } else if constexpr (NG == 2) {
+          // [64 cells][64 directions][2 groups]: unit (cell, c4) = 2 float4s {d0 g0, d0 g1, d1 g0, d1 g1}, {d2 .., d3 ..}
+#pragma unroll
+          for (int iu = 0; iu < CONV_ITERS / 2; iu++) {
+            const int u = iu * CONV_THREADS + t, cl = u >> 4, c4 = u & 15;
+            const float4 a = v[2 * iu], b = v[2 * iu + 1];
+            put(cl * 2 + 0, c4, a.x, a.z, b.x, b.z);
+            put(cl * 2 + 1, c4, a.y, a.w, b.y, b.w);
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < CONV_ITERS; i++) {
+            const int e = i * CONV_THREADS + t;
+            put(e >> 4, e & 15, v[i].x, v[i].y, v[i].z, v[i].w);
+          }
         }
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         mbar_arrive(&full_a[s]);
@@ -466,9 +526,17 @@ __global__ void __launch_bounds__(THREADS, 1)
           if (4 * j < half) {
             const float4 v = make_float4(run[4 * j] * inv, run[4 * j + 1] * inv, run[4 * j + 2] * inv,
                                          run[4 * j + 3] * inv);
-            if (col < nS)
-              *reinterpret_cast<float4 *>(P.S + gr * P.M + nt * NT + col) = v;
-            else
+            if (col < nS) {
+              if constexpr (NG > 1) {
+                float *o = P.S + ((gr / NG) * P.M + nt * NT + col) * NG + gr % NG;
+                o[0] = v.x;
+                o[NG] = v.y;
+                o[2 * NG] = v.z;
+                o[3 * NG] = v.w;
+              } else {
+                *reinterpret_cast<float4 *>(P.S + gr * P.M + nt * NT + col) = v;
+              }
+            } else
               *reinterpret_cast<float4 *>(P.mom + gr * NMOM + (col - nS)) = v;
           }
         }
@@ -609,26 +677,33 @@ extern "C" rrhd_status rrhd_scatter_tc_destroy(rrhd_scatter_tc *t) {
   return RRHD_OK;
 }
 
-template <int FORM>
+// NG = 1: I, S are [rows][M]; NG = 2, 4: [rows / NG][M][NG] (row = cell * NG + group)
+template <int FORM, int NG>
 static rrhd_status launch_tc(const rrhd_scatter_tc *t, const float *I, float *S, float *mom, int64_t rows,
                              cudaStream_t st) {
+  constexpr int ng = NG;
   static bool attr = false;
   if (!attr) {
-    RRHD_CUDA(cudaFuncSetAttribute(k_scatter_tc<FORM>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    RRHD_CUDA(cudaFuncSetAttribute(k_scatter_tc<FORM, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
     attr = true;
   }
   constexpr bool SCALED = (FORM == FORM_F16X3 || FORM == FORM_F16);
   if (SCALED) {
-    k_row_scale<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(I, rows, t->M, t->d_scale);
+    if (ng > 1)
+      k_row_scale_cdg<<<(unsigned)((rows / ng + 7) / 8), 256, 0, st>>>(I, rows / ng, t->M, ng, t->d_scale);
+    else
+      k_row_scale<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(I, rows, t->M, t->d_scale);
     RRHD_CUDA(cudaGetLastError());
   }
   TcParams P{I, S, mom, t->d_scale, rows, t->M, t->b_unscale, t->d_err};
   CUtensorMap tm_a;
   {
     auto enc = get_encode();
-    cuuint64_t dims[2] = {(cuuint64_t)t->M, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)t->M * 4};
-    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BM};
+    // rows layout: [rows][M], box {BK, BM}; cell-direction-group: [cells][M * ng], box {BK * ng, BM / ng}
+    const int u = ng > 1 ? ng : 1;
+    cuuint64_t dims[2] = {(cuuint64_t)t->M * u, (cuuint64_t)(rows / u)};
+    cuuint64_t strides[1] = {(cuuint64_t)t->M * u * 4};
+    cuuint32_t box[2] = {(cuuint32_t)(BK * u), (cuuint32_t)(BM / u)};
     cuuint32_t es[2] = {1, 1};
     if (!enc || enc(&tm_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(I), dims, strides, box, es,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -637,19 +712,16 @@ static rrhd_status launch_tc(const rrhd_scatter_tc *t, const float *I, float *S,
   }
   const int64_t tiles = ((rows + BM - 1) / BM) * (int64_t)(t->M < NT ? 1 : t->M / NT);
   const unsigned grid = (unsigned)std::min<int64_t>(tiles, t->num_sms);
-  k_scatter_tc<FORM><<<grid, THREADS, SMEM_BYTES, st>>>(t->tm_bh, t->tm_bl, t->tm_mh, t->tm_ml, tm_a, P);
+  k_scatter_tc<FORM, NG><<<grid, THREADS, SMEM_BYTES, st>>>(t->tm_bh, t->tm_bl, t->tm_mh, t->tm_ml, tm_a, P);
   RRHD_CUDA(cudaGetLastError());
   return RRHD_OK;
 }
 
-extern "C" rrhd_status rrhd_scatter_tc_run(const rrhd_scatter_tc *t, const float *I, float *S, float *mom,
-                                           int64_t rows, void *stream) {
-  RRHD_CHECK_ARG(t && rows >= 0, "bad arguments");
-  if (rows == 0) return RRHD_OK;
-  RRHD_CHECK_ARG(I && S, "null I or S");
+static rrhd_status run_tc(const rrhd_scatter_tc *t, const float *I, float *S, float *mom, int64_t rows, int ng,
+                          cudaStream_t st) {
   if ((t->form == FORM_F16X3 || t->form == FORM_F16) && t->scale_cap < rows) {
     rrhd_scatter_tc *tm = const_cast<rrhd_scatter_tc *>(t);
-    RRHD_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    RRHD_CUDA(cudaStreamSynchronize(st));
     cudaFree(tm->d_scale);
     tm->d_scale = nullptr;
     tm->scale_cap = 0;
@@ -658,14 +730,39 @@ extern "C" rrhd_status rrhd_scatter_tc_run(const rrhd_scatter_tc *t, const float
   }
   RRHD_CHECK_ARG(((uintptr_t)I & 15) == 0 && ((uintptr_t)S & 15) == 0 && ((uintptr_t)mom & 15) == 0,
                  "I, S and moments must be 16-byte aligned");
-  if (rows == 0) return RRHD_OK;
-  cudaStream_t st = (cudaStream_t)stream;
-  switch (t->form) {
-    case FORM_BF16X3: return launch_tc<FORM_BF16X3>(t, I, S, mom, rows, st);
-    case FORM_F16X3: return launch_tc<FORM_F16X3>(t, I, S, mom, rows, st);
-    case FORM_F16: return launch_tc<FORM_F16>(t, I, S, mom, rows, st);
-    default: return launch_tc<FORM_BF16>(t, I, S, mom, rows, st);
+  switch (t->form * 3 + (ng == 4 ? 2 : ng == 2 ? 1 : 0)) {
+#define RRHD_TC_CASE(F)                                                        \
+  case 3 * F + 0: return launch_tc<F, 1>(t, I, S, mom, rows, st);           \
+  case 3 * F + 1: return launch_tc<F, 2>(t, I, S, mom, rows, st);           \
+  case 3 * F + 2: return launch_tc<F, 4>(t, I, S, mom, rows, st);
+    RRHD_TC_CASE(FORM_BF16X3)
+    RRHD_TC_CASE(FORM_F16X3)
+    RRHD_TC_CASE(FORM_F16)
+    RRHD_TC_CASE(FORM_BF16)
+#undef RRHD_TC_CASE
+    default: return rrhd_fail(RRHD_ERR_INVALID, "bad tensor-core form");
   }
+}
+
+rrhd_status rrhd::scatter_tc_cdg(const rrhd_scatter_tc *t, const float *I, float *S, float *mom, int64_t cells,
+                                 int ng, cudaStream_t st) {
+  RRHD_CHECK_ARG(t && cells >= 0 && (ng == 1 || ng == 2 || ng == 4), "bad arguments");
+  if (cells == 0) return RRHD_OK;
+  RRHD_CHECK_ARG(I && S, "null I or S");
+  return run_tc(t, I, S, mom, cells * ng, ng, st);
+}
+
+extern "C" rrhd_status rrhd_scatter_tc_run(const rrhd_scatter_tc *t, const float *I, float *S, float *mom,
+                                           int64_t rows, void *stream) {
+  RRHD_CHECK_ARG(t && rows >= 0, "bad arguments");
+  if (rows == 0) return RRHD_OK;
+  RRHD_CHECK_ARG(I && S, "null I or S");
+  return run_tc(t, I, S, mom, rows, 0, (cudaStream_t)stream);
+}
+
+extern "C" rrhd_status rrhd_scatter_tc_run_cdg(const rrhd_scatter_tc *t, const float *I, float *S, float *mom,
+                                               int64_t cells, int32_t groups, void *stream) {
+  return rrhd::scatter_tc_cdg(t, I, S, mom, cells, groups, (cudaStream_t)stream);
 }
 
 // Error word of the tensor-core kernels (non-zero after a bounded wait timed

@@ -41,17 +41,70 @@ namespace {
 
 constexpr int kSweepThreads = 128;
 
+// Per-cell record: words 0-11 outward normals n_j, 12-15 heights H_j, 16-19 areas
+// A_j, then the caller face ids and the neighbours as int32 (4 + 4).
+template <class T>
+struct Rec;
+template <>
+struct Rec<double> {
+  static constexpr int WORDS = 24;  // 192 B
+};
+template <>
+struct Rec<float> {
+  static constexpr int WORDS = 32;  // 128 B (4 words of padding)
+};
+
+template <class T>
+__device__ __forceinline__ void load_rec(const T *r, T *g, int *fid, int *nbr);
+template <>
+__device__ __forceinline__ void load_rec<double>(const double *r, double *g, int *fid, int *nbr) {
+  const double2 *r2 = reinterpret_cast<const double2 *>(r);
+#pragma unroll
+  for (int q = 0; q < 10; q++) {
+    const double2 v = __ldg(r2 + q);
+    g[2 * q] = v.x;
+    g[2 * q + 1] = v.y;
+  }
+  const int4 *r4 = reinterpret_cast<const int4 *>(r + 20);
+  const int4 f = __ldg(r4), n = __ldg(r4 + 1);
+  fid[0] = f.x, fid[1] = f.y, fid[2] = f.z, fid[3] = f.w;
+  nbr[0] = n.x, nbr[1] = n.y, nbr[2] = n.z, nbr[3] = n.w;
+}
+template <>
+__device__ __forceinline__ void load_rec<float>(const float *r, float *g, int *fid, int *nbr) {
+  const float4 *r4 = reinterpret_cast<const float4 *>(r);
+#pragma unroll
+  for (int q = 0; q < 5; q++) {
+    const float4 v = __ldg(r4 + q);
+    g[4 * q] = v.x;
+    g[4 * q + 1] = v.y;
+    g[4 * q + 2] = v.z;
+    g[4 * q + 3] = v.w;
+  }
+  const int4 *i4 = reinterpret_cast<const int4 *>(r + 20);
+  const int4 f = __ldg(i4), n = __ldg(i4 + 1);
+  fid[0] = f.x, fid[1] = f.y, fid[2] = f.z, fid[3] = f.w;
+  nbr[0] = n.x, nbr[1] = n.y, nbr[2] = n.z, nbr[3] = n.w;
+}
+// normals and neighbours only (the plan kernels)
+template <class T>
+__device__ __forceinline__ void load_normals(const T *r, T *g, int *nbr) {
+#pragma unroll
+  for (int q = 0; q < 12; q++) g[q] = __ldg(r + q);
+  const int4 n = __ldg(reinterpret_cast<const int4 *>(r + 20) + 1);
+  nbr[0] = n.x, nbr[1] = n.y, nbr[2] = n.z, nbr[3] = n.w;
+}
+
 template <class T>
 struct SweepArgs {
   const SweepIO *io;
   const uint32_t *items;
   int64_t n;  // items of this level
-  int shift, DB, d0, M, G;
-  const T *w;     // [M][3]
-  const T *geo;   // [N][16]
-  const T *area;  // [N][4]
-  const int4 *fid, *nbr;
-  T *fv;  // [F][DB][G]
+  int shift, DB, d0, M, G, DS, GS, nbd;
+  const T *w;    // [M][3]
+  const T *rec;  // [N][Rec<T>::WORDS]
+  const T *dyn;  // [N][DS]
+  T *fv;         // [F][DB][GS] face values (GS >= G, full 32-byte sectors)
   T bc;
   int64_t last;
 };
@@ -60,40 +113,49 @@ __device__ __forceinline__ double ex(double x) { return exp(x); }
 __device__ __forceinline__ float ex(float x) { return expf(x); }
 
 template <class T>
-__device__ __forceinline__ void load_geo(const T *g, T *out) {
-#pragma unroll
-  for (int q = 0; q < 16; q++) out[q] = g[q];
-}
-template <>
-__device__ __forceinline__ void load_geo<double>(const double *g, double *out) {
-  const double2 *g2 = reinterpret_cast<const double2 *>(g);
-#pragma unroll
-  for (int q = 0; q < 8; q++) {
-    const double2 v = __ldg(g2 + q);
-    out[2 * q] = v.x;
-    out[2 * q + 1] = v.y;
-  }
-}
-template <>
-__device__ __forceinline__ void load_geo<float>(const float *g, float *out) {
-  const float4 *g4 = reinterpret_cast<const float4 *>(g);
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const float4 v = __ldg(g4 + q);
-    out[4 * q] = v.x;
-    out[4 * q + 1] = v.y;
-    out[4 * q + 2] = v.z;
-    out[4 * q + 3] = v.w;
-  }
-}
-
-template <class T>
 __device__ __forceinline__ void face_cos(const T *g, T wx, T wy, T wz, T *cosf) {
 #pragma unroll
   for (int j = 0; j < 4; j++) cosf[j] = (g[3 * j] * wx + g[3 * j + 1] * wy) + g[3 * j + 2] * wz;
 }
 
-template <class T>
+
+// G values at p (contiguous), vectorised for 2 and 4 groups
+template <class T, int G>
+__device__ __forceinline__ void ld_groups(const T *p, T *v) {
+  if constexpr (sizeof(T) == 8 && G % 2 == 0) {
+#pragma unroll
+    for (int q = 0; q < G / 2; q++) {
+      const double2 x = reinterpret_cast<const double2 *>(p)[q];
+      v[2 * q] = x.x;
+      v[2 * q + 1] = x.y;
+    }
+  } else if constexpr (sizeof(T) == 4 && G == 4) {
+    const float4 x = *reinterpret_cast<const float4 *>(p);
+    v[0] = x.x, v[1] = x.y, v[2] = x.z, v[3] = x.w;
+  } else {
+#pragma unroll
+    for (int q = 0; q < G; q++) v[q] = p[q];
+  }
+}
+// G values to a face-value slot of GS values; float slots of 4 groups are padded to 8 so
+// that every store fills a whole 32-byte sector
+template <class T, int G>
+__device__ __forceinline__ void st_slot(T *p, const T *v) {
+  if constexpr (sizeof(T) == 8 && G % 2 == 0) {
+#pragma unroll
+    for (int q = 0; q < G / 2; q++) reinterpret_cast<double2 *>(p)[q] = make_double2(v[2 * q], v[2 * q + 1]);
+  } else if constexpr (sizeof(T) == 4 && G == 4) {
+    reinterpret_cast<float4 *>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
+    reinterpret_cast<float4 *>(p)[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+  } else {
+#pragma unroll
+    for (int q = 0; q < G; q++) p[q] = v[q];
+  }
+}
+
+// One thread per (cell, direction) pair of a level: the out-face values of all
+// groups.  GT: compile-time group count (1, 2 or 4), 0 for any other (loop).
+template <class T, int GT>
 __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= a.n) return;
@@ -101,24 +163,28 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
   const int64_t c = it >> a.shift;
   const int dl = (int)(it & (uint32_t)(a.DB - 1));
   const int d = a.d0 + dl;
+  T g[20];
+  int fid[4], nbr[4];
+  load_rec<T>(a.rec + (int64_t)Rec<T>::WORDS * c, g, fid, nbr);
+  const T *dy = a.dyn + (int64_t)a.DS * c;
+  const T k = dy[0], be = dy[1];
   const SweepIO io = *a.io;
-  const T *alpha = (const T *)io.alpha, *betta = (const T *)io.betta, *Qv = (const T *)io.Q, *Sv = (const T *)io.S;
-  T *I = (T *)io.I;
-  const int64_t p = io.row_of ? (int64_t)io.row_of[c] : c;
+  const T *Sv = (const T *)io.S;
+  // S element (group gg) of this cell and direction: base + gg * gs
+  int64_t base, gs;
+  if (io.layout) {
+    base = (c * a.M + d) * a.G;
+    gs = 1;
+  } else {
+    base = (int64_t)io.row_of[c] * a.G * a.M + d;
+    gs = a.M;
+  }
   const T wx = a.w[3 * d], wy = a.w[3 * d + 1], wz = a.w[3 * d + 2];
-  T g[16];
-  load_geo<T>(a.geo + 16 * c, g);
   T cosf[4];
   face_cos(g, wx, wy, wz, cosf);
-  const int4 f4 = a.fid[c], n4 = a.nbr[c];
-  const int fid[4] = {f4.x, f4.y, f4.z, f4.w};
-  const int nbr[4] = {n4.x, n4.y, n4.z, n4.w};
-  const T al = alpha[p], be = betta[p];
-  const T k = al + be;
   T r[4];
 #pragma unroll
   for (int f = 0; f < 4; f++) r[f] = cosf[f] < 0 ? g[12 + f] / -cosf[f] : (T)0;
-  // in-face of each node and its exponential, per out-face
   int hq[4][3];
   T e[4][3];
 #pragma unroll
@@ -148,73 +214,143 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
       e[j][q] = ex(-k * tmin);
     }
   }
-  const bool last = c == a.last;
-  T A[4];
+  if constexpr (GT > 0) {
+    T rhs[GT], fin[4][GT];
+    if (io.layout) {
+      ld_groups<T, GT>(Sv + base, rhs);
+    } else {
 #pragma unroll
-  for (int j = 0; j < 4; j++) A[j] = a.area[4 * c + j];
-  for (int gg = 0; gg < a.G; gg++) {
-    const int64_t row = p * a.G + gg;
-    const T rhs = (al * Qv[row] + be * Sv[row * a.M + d]) / k;
-    T fvals[4];
+      for (int q = 0; q < GT; q++) rhs[q] = Sv[base + q * gs];
+    }
+#pragma unroll
+    for (int q = 0; q < GT; q++) rhs[q] = (dy[2 + q] + be * rhs[q]) / k;
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-      if (cosf[j] < 0)
-        fvals[j] = nbr[j] >= 0 ? a.fv[((int64_t)fid[j] * a.DB + dl) * a.G + gg] : a.bc;
-      else
-        fvals[j] = a.bc;
+      if (cosf[j] < 0 && nbr[j] >= 0) {
+        ld_groups<T, GT>(a.fv + ((int64_t)fid[j] * a.DB + dl) * a.GS, fin[j]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < GT; q++) fin[j][q] = a.bc;
+      }
     }
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       if (!(cosf[j] > 0)) continue;
-      T I0[3];
+      T out[GT];
 #pragma unroll
-      for (int q = 0; q < 3; q++) {
-        const int h = hq[j][q];
-        I0[q] = a.bc;
+      for (int q = 0; q < GT; q++) {
+        T I0[3];
 #pragma unroll
-        for (int f = 0; f < 4; f++)
-          if (h == f) I0[q] = fvals[f];
+        for (int n = 0; n < 3; n++) {
+          const int h = hq[j][n];
+          I0[n] = a.bc;
+#pragma unroll
+          for (int f = 0; f < 4; f++)
+            if (h == f) I0[n] = fin[f][q];
+        }
+        T Icur = e[j][0] * (I0[0] - rhs[q]) + rhs[q];
+        Icur += (e[j][1] * (I0[1] - rhs[q]) + rhs[q]);
+        Icur += (e[j][2] * (I0[2] - rhs[q]) + rhs[q]);
+        out[q] = Icur * (T)0.3333333333333333;
       }
-      T Icur = e[j][0] * (I0[0] - rhs) + rhs;
-      Icur += (e[j][1] * (I0[1] - rhs) + rhs);
-      Icur += (e[j][2] * (I0[2] - rhs) + rhs);
-      const T v = Icur * (T)0.3333333333333333;
-      a.fv[((int64_t)fid[j] * a.DB + dl) * a.G + gg] = v;
-      fvals[j] = v;
+      st_slot<T, GT>(a.fv + ((int64_t)fid[j] * a.DB + dl) * a.GS, out);
     }
+  } else {
+    for (int gg = 0; gg < a.G; gg++) {
+      const T rhs = (dy[2 + gg] + be * Sv[base + gg * gs]) / k;
+      T fvals[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        fvals[j] = (cosf[j] < 0 && nbr[j] >= 0) ? a.fv[((int64_t)fid[j] * a.DB + dl) * a.GS + gg] : a.bc;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        if (!(cosf[j] > 0)) continue;
+        T I0[3];
+#pragma unroll
+        for (int n = 0; n < 3; n++) {
+          const int h = hq[j][n];
+          I0[n] = a.bc;
+#pragma unroll
+          for (int f = 0; f < 4; f++)
+            if (h == f) I0[n] = fvals[f];
+        }
+        T Icur = e[j][0] * (I0[0] - rhs) + rhs;
+        Icur += (e[j][1] * (I0[1] - rhs) + rhs);
+        Icur += (e[j][2] * (I0[2] - rhs) + rhs);
+        a.fv[((int64_t)fid[j] * a.DB + dl) * a.GS + gg] = Icur * (T)0.3333333333333333;
+      }
+    }
+  }
+}
+
+// Cell values of one direction batch from its face values: ReCalcIllumOpt
+// (illum_utils.cpp:377-433), the area-weighted face mean, a plain mean for the
+// caller's last cell.  Faces nobody wrote for a direction (inflow boundary,
+// parallel to it) hold the boundary value.  One thread per (cell, direction);
+// consecutive threads take consecutive directions of a cell, so face-value reads
+// and intensity writes are contiguous.
+template <class T>
+__global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= N * a.nbd) return;
+  const int64_t c = t / a.nbd;
+  const int dl = (int)(t - c * a.nbd);
+  const int d = a.d0 + dl;
+  T g[20];
+  int fid[4], nbr[4];
+  load_rec<T>(a.rec + (int64_t)Rec<T>::WORDS * c, g, fid, nbr);
+  T cosf[4];
+  face_cos(g, a.w[3 * d], a.w[3 * d + 1], a.w[3 * d + 2], cosf);
+  const SweepIO io = *a.io;
+  T *I = (T *)io.I;
+  int64_t base, gs;
+  if (io.layout) {
+    base = (c * a.M + d) * a.G;
+    gs = 1;
+  } else {
+    base = (int64_t)io.row_of[c] * a.G * a.M + d;
+    gs = a.M;
+  }
+  const bool last = c == a.last;
+  bool have[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) have[j] = cosf[j] > 0 || (cosf[j] < 0 && nbr[j] >= 0);
+  for (int gg = 0; gg < a.G; gg++) {
+    T fv[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) fv[j] = have[j] ? a.fv[((int64_t)fid[j] * a.DB + dl) * a.GS + gg] : a.bc;
     T curI = 0;
     if (!last) {
       T Ssum = 0;
 #pragma unroll
       for (int j = 0; j < 4; j++) {
-        curI += fvals[j] * A[j];
-        Ssum += A[j];
+        curI += fv[j] * g[16 + j];
+        Ssum += g[16 + j];
       }
       curI /= Ssum;
     } else {
 #pragma unroll
-      for (int j = 0; j < 4; j++) curI += fvals[j];
+      for (int j = 0; j < 4; j++) curI += fv[j];
       curI /= (T)4;
     }
-    I[row * a.M + d] = curI;
+    I[base + gg * gs] = curI;
   }
 }
 
 // ---------------------------------------------------------------- plan
 template <class T>
-__global__ void k_plan_init(int64_t N, int nbd, int shift, int d0, const T *w, const T *geo, const int4 *nbr4,
-                            uint32_t *indeg, uint32_t *plan, unsigned long long *tail) {
+__global__ void k_plan_init(int64_t N, int nbd, int shift, int d0, const T *w, const T *rec, uint32_t *indeg,
+                            uint32_t *plan, unsigned long long *tail) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= N * nbd) return;
   const int64_t c = i / nbd;
   const int dl = (int)(i - c * nbd);
   const int d = d0 + dl;
-  T g[16];
-  load_geo<T>(geo + 16 * c, g);
+  T g[12];
+  int nbr[4];
+  load_normals<T>(rec + (int64_t)Rec<T>::WORDS * c, g, nbr);
   T cosf[4];
   face_cos(g, w[3 * d], w[3 * d + 1], w[3 * d + 2], cosf);
-  const int4 n4 = nbr4[c];
-  const int nbr[4] = {n4.x, n4.y, n4.z, n4.w};
   uint32_t cnt = 0;
 #pragma unroll
   for (int j = 0; j < 4; j++) cnt += (cosf[j] < 0 && nbr[j] >= 0) ? 1u : 0u;
@@ -223,20 +359,19 @@ __global__ void k_plan_init(int64_t N, int nbd, int shift, int d0, const T *w, c
 }
 
 template <class T>
-__global__ void k_plan_expand(const uint32_t *cur, int64_t n, int nbd, int shift, int d0, const T *w, const T *geo,
-                              const int4 *nbr4, uint32_t *indeg, uint32_t *plan, unsigned long long *tail) {
+__global__ void k_plan_expand(const uint32_t *cur, int64_t n, int nbd, int shift, int d0, const T *w, const T *rec,
+                              uint32_t *indeg, uint32_t *plan, unsigned long long *tail) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t it = cur[i];
   const int64_t c = it >> shift;
   const int dl = (int)(it & ((1u << shift) - 1));
   const int d = d0 + dl;
-  T g[16];
-  load_geo<T>(geo + 16 * c, g);
+  T g[12];
+  int nbr[4];
+  load_normals<T>(rec + (int64_t)Rec<T>::WORDS * c, g, nbr);
   T cosf[4];
   face_cos(g, w[3 * d], w[3 * d + 1], w[3 * d + 2], cosf);
-  const int4 n4 = nbr4[c];
-  const int nbr[4] = {n4.x, n4.y, n4.z, n4.w};
 #pragma unroll
   for (int j = 0; j < 4; j++) {
     if (!(cosf[j] > 0) || nbr[j] < 0) continue;
@@ -245,19 +380,38 @@ __global__ void k_plan_expand(const uint32_t *cur, int64_t n, int nbd, int shift
   }
 }
 
-// ---------------------------------------------------------------- coupled step
+// Source record {k = alpha + betta, betta, alpha Q_g} of each context cell from
+// caller arrays (caller numbering) ...
 template <class T>
-__global__ void k_opacity(int64_t N, int G, const double *state, double a_coef, double b_coef, Emission em,
-                          T *alpha, T *betta, T *Q) {
+__global__ void k_dyn_from_arrays(int64_t N, int G, int DS, const int32_t *perm, const T *alpha, const T *betta,
+                                  const T *Q, T *dyn) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  const int64_t p = perm[c];
+  const T al = alpha[p], be = betta[p];
+  T *o = dyn + (int64_t)DS * c;
+  o[0] = al + be;
+  o[1] = be;
+  for (int g = 0; g < G; g++) o[2 + g] = al * Q[p * G + g];
+}
+
+// ... or from the solver state: alpha = a rho, betta = b rho, Q_g = B(T) / kRadiation / G.
+template <class T>
+__global__ void k_dyn_from_state(int64_t N, int G, int DS, const double *state, double a_coef, double b_coef,
+                                 Emission em, T *dyn) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= N) return;
   const double rho = state[10 * c + 5], prs = state[10 * c + 9];
-  alpha[c] = (T)(a_coef * rho);
-  betta[c] = (T)(b_coef * rho);
-  const double q = planck_B(em, rho, prs) / em.rad_unit / (double)G;
-  for (int g = 0; g < G; g++) Q[c * G + g] = (T)q;
+  const T al = (T)(a_coef * rho), be = (T)(b_coef * rho);
+  const T q = (T)(planck_B(em, rho, prs) / em.rad_unit / (double)G);
+  T *o = dyn + (int64_t)DS * c;
+  o[0] = al + be;
+  o[1] = be;
+  const T aq = al * q;
+  for (int g = 0; g < G; g++) o[2 + g] = aq;
 }
 
+// ---------------------------------------------------------------- coupled step
 // 4-force from the moments summed over the groups.  FP64 moments per row: E
 // [rows], F [rows][3], T [rows][9]; FP32 moments: [rows][16] = {E, F, Txx, Txy,
 // Txz, Tyy, Tyz, Tzz, ...}.
@@ -349,14 +503,6 @@ __global__ void k_rows_to_host_order(int64_t N, int64_t width, const int32_t *pe
   dst[(int64_t)perm[c] * width + k] = (double)src[i];
 }
 
-template <class T>
-__global__ void k_rows_from_host_order(int64_t N, int64_t width, const int32_t *perm, const double *src, T *dst) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= N * width) return;
-  const int64_t c = i / width, k = i - c * width;
-  dst[i] = (T)src[(int64_t)perm[c] * width + k];
-}
-
 unsigned grid_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 Eos eos_of(const rrhd_ctx *c) {
@@ -410,7 +556,7 @@ rrhd_status build_plan(rrhd_ctx *c) {
     const unsigned long long zero = 0;
     RRHD_CUDA(cudaMemcpyAsync(d_tail, &zero, sizeof zero, cudaMemcpyHostToDevice, st));
     k_plan_init<T><<<grid_for(N * nbd, 256), 256, 0, st>>>(N, nbd, R.shift, d0, (const T *)R.d_w,
-                                                            (const T *)R.d_geo, R.d_nbr, indeg, plan, d_tail);
+                                                            (const T *)R.d_rec, indeg, plan, d_tail);
     RRHD_CUDA(cudaGetLastError());
     std::vector<int64_t> &off = R.lvl[b];
     off.assign(1, 0);
@@ -428,8 +574,8 @@ rrhd_status build_plan(rrhd_ctx *c) {
       off.push_back(hi);
       R.max_level = std::max(R.max_level, hi - lo);
       k_plan_expand<T><<<grid_for(hi - lo, 256), 256, 0, st>>>(plan + lo, hi - lo, nbd, R.shift, d0,
-                                                                (const T *)R.d_w, (const T *)R.d_geo, R.d_nbr,
-                                                                indeg, plan, d_tail);
+                                                                (const T *)R.d_w, (const T *)R.d_rec, indeg,
+                                                                plan, d_tail);
       RRHD_CUDA(cudaGetLastError());
       lo = hi;
     }
@@ -460,24 +606,32 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
     a.DB = R.DB;
     a.M = R.M;
     a.G = R.G;
+    a.DS = R.DS;
     a.w = (const T *)R.d_w;
-    a.geo = (const T *)R.d_geo;
-    a.area = (const T *)R.d_area;
-    a.fid = R.d_fid;
-    a.nbr = R.d_nbr;
+    a.rec = (const T *)R.d_rec;
+    a.dyn = (const T *)R.d_dyn;
     a.fv = (T *)R.d_fv;
     a.bc = (T)R.bc;
     a.last = R.last_cell;
+    a.GS = R.GS;
     int64_t base = 0;
     for (int b = 0; b < R.nbatch; b++) {
       a.d0 = b * R.DB;
       const int nbd = std::min(R.DB, R.M - a.d0);
+      a.nbd = nbd;
       const std::vector<int64_t> &off = R.lvl[b];
       for (size_t L = 0; L + 1 < off.size(); L++) {
         a.items = R.d_plan + base + off[L];
         a.n = off[L + 1] - off[L];
-        k_sweep_level<T><<<grid_for(a.n, kSweepThreads), kSweepThreads, 0, cs>>>(a);
+        const unsigned nb = grid_for(a.n, kSweepThreads);
+        switch (R.G) {
+          case 1: k_sweep_level<T, 1><<<nb, kSweepThreads, 0, cs>>>(a); break;
+          case 2: k_sweep_level<T, 2><<<nb, kSweepThreads, 0, cs>>>(a); break;
+          case 4: k_sweep_level<T, 4><<<nb, kSweepThreads, 0, cs>>>(a); break;
+          default: k_sweep_level<T, 0><<<nb, kSweepThreads, 0, cs>>>(a); break;
+        }
       }
+      k_recalc<T><<<grid_for(c->N * nbd, 256), 256, 0, cs>>>(a, c->N);
       base += c->N * nbd;
     }
     e = cudaStreamEndCapture(cs, &g);
@@ -494,9 +648,11 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
 void rrhd_rad_release(rrhd_ctx *c) {
   RadState &R = c->rad;
   if (R.graph) cudaGraphExecDestroy(R.graph);
-  void *ptrs[] = {R.d_w, R.d_geo, R.d_area, R.d_fid, R.d_nbr, R.d_plan, R.d_io, R.d_fv, R.d_I, R.d_S, R.d_alpha,
-                  R.d_betta, R.d_Q, R.d_G4, R.d_mE, R.d_mF, R.d_mT, R.d_mom, R.d_cnt};
+  void *ptrs[] = {R.d_w, R.d_rec, R.d_dyn, R.d_plan, R.d_io, R.d_fv, R.d_I, R.d_S, R.d_G4, R.d_mE, R.d_mF, R.d_mT,
+                  R.d_mom, R.d_cnt};
   for (void *p : ptrs) cudaFree(p);
+  for (cudaEvent_t e : R.ev)
+    if (e) cudaEventDestroy(e);
   if (R.tc) rrhd_scatter_tc_destroy(R.tc);
   R = RadState();
 }
@@ -505,46 +661,55 @@ template <class T>
 static rrhd_status rad_setup_t(rrhd_ctx *c) {
   RadState &R = c->rad;
   const int64_t N = c->N;
-  // geometry in context numbering
-  std::vector<T> geo(16 * N), area(4 * N), w(3 * R.M);
-  std::vector<int4> fid(N), nbr(N);
+  constexpr int W = Rec<T>::WORDS;
+  std::vector<T> rec((size_t)W * N, (T)0), w(3 * R.M);
   std::vector<int32_t> iperm(N);
   for (int64_t i = 0; i < N; i++) iperm[c->h_perm[i]] = (int32_t)i;
+  // face-value slots numbered in order of first use by context cells, so that the
+  // faces of neighbouring cells sit close together
+  std::vector<int32_t> fslot(c->F, -1);
+  int32_t nslot = 0;
+  for (int64_t cn = 0; cn < N; cn++)
+    for (int j = 0; j < 4; j++) {
+      const int32_t fc = c->h_cell_faces[4 * c->h_perm[cn] + j];
+      if (fslot[fc] < 0) fslot[fc] = nslot++;
+    }
   for (int64_t cn = 0; cn < N; cn++) {
     const int64_t p = c->h_perm[cn];
-    int f[4], nb[4];
+    T *r = rec.data() + (size_t)W * cn;
+    int32_t ids[8];
     for (int j = 0; j < 4; j++) {
       const int32_t fc = c->h_cell_faces[4 * p + j];
-      f[j] = fc;
       const bool out = (c->h_cell_sign[p] >> j) & 1;
       for (int x = 0; x < 3; x++) {
         const double v = c->h_face_n[3 * (int64_t)fc + x];
-        geo[16 * cn + 3 * j + x] = (T)(out ? v : -v);
+        r[3 * j + x] = (T)(out ? v : -v);
       }
-      geo[16 * cn + 12 + j] = (T)(3.0 * c->h_cell_V[p] / c->h_face_area[fc]);
-      area[4 * cn + j] = (T)c->h_face_area[fc];
-      const int32_t l = c->h_face_l[fc], r = c->h_face_r[fc];
-      const int32_t o = (l == p) ? r : l;
-      nb[j] = o < 0 ? -1 : iperm[o];
+      r[12 + j] = (T)(3.0 * c->h_cell_V[p] / c->h_face_area[fc]);
+      r[16 + j] = (T)c->h_face_area[fc];
+      const int32_t l = c->h_face_l[fc], rr = c->h_face_r[fc];
+      const int32_t o = (l == p) ? rr : l;
+      ids[j] = fslot[fc];
+      ids[4 + j] = o < 0 ? -1 : iperm[o];
     }
-    fid[cn] = make_int4(f[0], f[1], f[2], f[3]);
-    nbr[cn] = make_int4(nb[0], nb[1], nb[2], nb[3]);
+    std::memcpy(r + 20, ids, sizeof ids);
   }
   for (int q = 0; q < 3 * R.M; q++) w[q] = (T)R.dirs->h_w[q];
   R.last_cell = iperm[N - 1];
+  R.DS = sizeof(T) == 8 ? ((2 + R.G + 1) & ~1) : ((2 + R.G + 3) & ~3);
+  R.GS = sizeof(T) == 8 ? ((R.G + 3) & ~3) : ((R.G + 7) & ~7);
   auto up = [&](void **dst, const void *src, size_t bytes) -> rrhd_status {
     if (cudaMalloc(dst, bytes) != cudaSuccess) return rrhd_fail(RRHD_ERR_OOM, "sweep allocation failed");
     RRHD_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
     return RRHD_OK;
   };
   rrhd_status s;
-  if ((s = up(&R.d_geo, geo.data(), sizeof(T) * geo.size())) || (s = up(&R.d_area, area.data(), sizeof(T) * area.size())) ||
-      (s = up(&R.d_w, w.data(), sizeof(T) * w.size())) || (s = up((void **)&R.d_fid, fid.data(), sizeof(int4) * N)) ||
-      (s = up((void **)&R.d_nbr, nbr.data(), sizeof(int4) * N)))
+  if ((s = up(&R.d_rec, rec.data(), sizeof(T) * rec.size())) || (s = up(&R.d_w, w.data(), sizeof(T) * w.size())))
     return s;
   if (cudaMalloc(&R.d_io, sizeof(SweepIO)) != cudaSuccess ||
-      cudaMalloc(&R.d_fv, sizeof(T) * (size_t)c->F * R.DB * R.G) != cudaSuccess)
-    return rrhd_fail(RRHD_ERR_OOM, "sweep face-value allocation failed");
+      cudaMalloc(&R.d_dyn, sizeof(T) * (size_t)R.DS * N) != cudaSuccess ||
+      cudaMalloc(&R.d_fv, sizeof(T) * (size_t)c->F * R.DB * R.GS) != cudaSuccess)
+    return rrhd_fail(RRHD_ERR_OOM, "sweep allocation failed");
   if ((s = build_plan<T>(c))) return s;
   return capture_sweep<T>(c);
 }
@@ -594,7 +759,13 @@ extern "C" rrhd_status rrhd_rad_plan_info(const rrhd_ctx *c, int64_t *levels, in
 
 static rrhd_status launch_sweep(rrhd_ctx *c, const SweepIO &io) {
   RadState &R = c->rad;
-  RRHD_CUDA(cudaMemcpyAsync(R.d_io, &io, sizeof io, cudaMemcpyHostToDevice, c->stream));
+  // the graph reads its pointers from d_io; upload only when they change
+  if (!R.io_valid || std::memcmp(&io, &R.h_io, sizeof io) != 0) {
+    R.h_io = io;
+    RRHD_CUDA(cudaMemcpyAsync(R.d_io, &R.h_io, sizeof io, cudaMemcpyHostToDevice, c->stream));
+    RRHD_CUDA(cudaStreamSynchronize(c->stream));
+    R.io_valid = true;
+  }
   RRHD_CUDA(cudaGraphLaunch(R.graph, c->stream));
   return RRHD_OK;
 }
@@ -602,23 +773,54 @@ static rrhd_status launch_sweep(rrhd_ctx *c, const SweepIO &io) {
 extern "C" rrhd_status rrhd_sweep(rrhd_ctx *c, const void *alpha, const void *betta, const void *Q, const void *S,
                                   void *I) {
   RRHD_CHECK_ARG(c && alpha && betta && Q && S && I, "null argument");
-  if (!c->rad.ready) return rrhd_fail(RRHD_ERR_STATE, "rrhd_rad_setup has not run");
+  RadState &R = c->rad;
+  if (!R.ready) return rrhd_fail(RRHD_ERR_STATE, "rrhd_rad_setup has not run");
   RRHD_CUDA(cudaSetDevice(c->device));
-  SweepIO io{alpha, betta, Q, S, I, c->d_perm};
+  const int64_t N = c->N;
+  if (R.prec == RRHD_RAD_FP64)
+    k_dyn_from_arrays<double><<<grid_for(N, 256), 256, 0, c->stream>>>(
+        N, R.G, R.DS, c->d_perm, (const double *)alpha, (const double *)betta, (const double *)Q, (double *)R.d_dyn);
+  else
+    k_dyn_from_arrays<float><<<grid_for(N, 256), 256, 0, c->stream>>>(
+        N, R.G, R.DS, c->d_perm, (const float *)alpha, (const float *)betta, (const float *)Q, (float *)R.d_dyn);
+  RRHD_CUDA(cudaGetLastError());
+  SweepIO io{S, I, c->d_perm, 0};
   return launch_sweep(c, io);
 }
 
 // ---------------------------------------------------------------- coupled step
+namespace {
+template <class T>
+__global__ void k_cdg_to_rows(int64_t N, int M, int G, const int32_t *perm, const T *src, double *dst) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t per = (int64_t)M * G;
+  if (i >= N * per) return;
+  const int64_t c = i / per, rem = i - c * per;
+  const int d = (int)(rem / G), g = (int)(rem - (int64_t)d * G);
+  dst[((int64_t)perm[c] * G + g) * M + d] = (double)src[i];
+}
+
+template <class T>
+__global__ void k_rows_to_cdg(int64_t N, int M, int G, const int32_t *perm, const double *src, T *dst) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t per = (int64_t)M * G;
+  if (i >= N * per) return;
+  const int64_t c = i / per, rem = i - c * per;
+  const int d = (int)(rem / G), g = (int)(rem - (int64_t)d * G);
+  dst[i] = (T)src[((int64_t)perm[c] * G + g) * M + d];
+}
+}  // namespace
+
 template <class T>
 static rrhd_status alloc_coupled(rrhd_ctx *c) {
   RadState &R = c->rad;
   const int64_t N = c->N, rows = N * R.G;
   const size_t big = sizeof(T) * (size_t)rows * R.M;
   if (cudaMalloc(&R.d_I, big) != cudaSuccess || cudaMalloc(&R.d_S, big) != cudaSuccess ||
-      cudaMalloc(&R.d_alpha, sizeof(T) * N) != cudaSuccess || cudaMalloc(&R.d_betta, sizeof(T) * N) != cudaSuccess ||
-      cudaMalloc(&R.d_Q, sizeof(T) * rows) != cudaSuccess || cudaMalloc(&R.d_G4, sizeof(double) * 4 * N) != cudaSuccess ||
+      cudaMalloc(&R.d_G4, sizeof(double) * 4 * N) != cudaSuccess ||
       cudaMalloc(&R.d_cnt, sizeof(unsigned long long) * 8) != cudaSuccess)
     return rrhd_fail(RRHD_ERR_OOM, "coupled-step allocation failed");
+  for (cudaEvent_t &e : R.ev) RRHD_CUDA(cudaEventCreate(&e));
   RRHD_CUDA(cudaMemsetAsync(R.d_I, 0, big, c->stream));
   RRHD_CUDA(cudaMemsetAsync(R.d_S, 0, big, c->stream));
   RRHD_CUDA(cudaMemsetAsync(R.d_G4, 0, sizeof(double) * 4 * N, c->stream));
@@ -647,6 +849,8 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
   const bool fp64 = R.prec == RRHD_RAD_FP64;
   RRHD_CHECK_ARG(fp64 ? o->scatter == RRHD_SCATTER_FP64 : (o->scatter >= RRHD_TC_BF16X3 && o->scatter <= RRHD_TC_BF16),
                  "scatter form does not match the sweep precision");
+  RRHD_CHECK_ARG(fp64 ? (64 % R.G == 0) : (R.G == 1 || R.G == 2 || R.G == 4),
+                 "coupled step groups: a divisor of 64 (FP64) or 1, 2, 4 (tensor cores)");
   const int k_stall = o->k_stall ? o->k_stall : 12;
   RRHD_CHECK_ARG(k_stall > 0 && k_stall <= 40, "k_stall must be in [1, 40]");
   RRHD_CUDA(cudaSetDevice(c->device));
@@ -659,25 +863,27 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
     R.tc_form = o->scatter;
   }
   cudaStream_t st = c->stream;
-  const int64_t N = c->N, rows = N * R.G;
+  const int64_t N = c->N;
+  RRHD_CUDA(cudaEventRecord(R.ev[0], st));
   // 1. hydro step (flux, update, con2prim with fallback)
   rrhd_step_stats hst;
   const rrhd_status hstat = rrhd_hydro_step(c, tau, hs ? &hst : nullptr);
   if (hstat && hstat != RRHD_ERR_C2P) return hstat;
   if (hs) *hs = hst;
+  RRHD_CUDA(cudaEventRecord(R.ev[1], st));
   double *state = c->d_state[c->cur];
   const Emission em{o->emission.temp_coef, o->emission.sigma_sb, o->emission.pi, o->emission.rad_unit};
-  // 2. opacities and emission from the new primitives
+  // 2. opacities and emission from the new primitives, 3. sweep with the previous scattering integral
   if (fp64)
-    k_opacity<double><<<grid_for(N, 256), 256, 0, st>>>(N, R.G, state, o->absorption, o->scattering, em,
-                                                         (double *)R.d_alpha, (double *)R.d_betta, (double *)R.d_Q);
+    k_dyn_from_state<double><<<grid_for(N, 256), 256, 0, st>>>(N, R.G, R.DS, state, o->absorption, o->scattering,
+                                                                em, (double *)R.d_dyn);
   else
-    k_opacity<float><<<grid_for(N, 256), 256, 0, st>>>(N, R.G, state, o->absorption, o->scattering, em,
-                                                        (float *)R.d_alpha, (float *)R.d_betta, (float *)R.d_Q);
+    k_dyn_from_state<float><<<grid_for(N, 256), 256, 0, st>>>(N, R.G, R.DS, state, o->absorption, o->scattering, em,
+                                                               (float *)R.d_dyn);
   RRHD_CUDA(cudaGetLastError());
-  // 3. sweep with the previous scattering integral
-  SweepIO io{R.d_alpha, R.d_betta, R.d_Q, R.d_S, R.d_I, nullptr};
+  SweepIO io{R.d_S, R.d_I, nullptr, 1};
   if ((s = launch_sweep(c, io))) return s;
+  RRHD_CUDA(cudaEventRecord(R.ev[2], st));
   // 4. 4-force from the previous intensity's moments, source con2prim
   k_source<<<grid_for(N, 128), 128, 0, st>>>(N, R.G, state, o->absorption, o->scattering, em, R.d_mE, R.d_mF, R.d_mT,
                                               R.d_mom, R.d_G4);
@@ -701,14 +907,26 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
       ss->max_iters = (int32_t)h[3];
     }
   }
+  RRHD_CUDA(cudaEventRecord(R.ev[3], st));
   // 5. scattering integral and moments of the new intensity, for the next step
   if (fp64) {
-    if ((s = rrhd_scatter_fp64_fma(R.dirs, (const double *)R.d_I, (double *)R.d_S, rows, st))) return s;
-    if ((s = rrhd_moments_fp64(R.dirs, (const double *)R.d_I, R.d_mE, R.d_mF, R.d_mT, rows, st))) return s;
+    if ((s = scatter_fp64_cdg(R.dirs, (const double *)R.d_I, (double *)R.d_S, N, R.G, false, st))) return s;
+    if ((s = moments_fp64_cdg(R.dirs, (const double *)R.d_I, R.d_mE, R.d_mF, R.d_mT, N, R.G, st))) return s;
   } else {
-    if ((s = rrhd_scatter_tc_run(R.tc, (const float *)R.d_I, (float *)R.d_S, R.d_mom, rows, st))) return s;
+    if ((s = scatter_tc_cdg(R.tc, (const float *)R.d_I, (float *)R.d_S, R.d_mom, N, R.G, st))) return s;
   }
+  RRHD_CUDA(cudaEventRecord(R.ev[4], st));
   return hstat;
+}
+
+extern "C" rrhd_status rrhd_coupled_phase_ms(rrhd_ctx *c, float *ms) {
+  RRHD_CHECK_ARG(c && ms, "null argument");
+  RadState &R = c->rad;
+  if (!R.ev[0]) return rrhd_fail(RRHD_ERR_STATE, "no coupled step has run");
+  RRHD_CUDA(cudaSetDevice(c->device));
+  RRHD_CUDA(cudaEventSynchronize(R.ev[4]));
+  for (int k = 0; k < 4; k++) RRHD_CUDA(cudaEventElapsedTime(ms + k, R.ev[k], R.ev[k + 1]));
+  return RRHD_OK;
 }
 
 extern "C" rrhd_status rrhd_rad_get(rrhd_ctx *c, int32_t what, double *out) {
@@ -721,13 +939,14 @@ extern "C" rrhd_status rrhd_rad_get(rrhd_ctx *c, int32_t what, double *out) {
   const int64_t width = what == RRHD_RAD_G4 ? 4 : (int64_t)R.G * R.M;
   double *tmp = nullptr;
   RRHD_CUDA(cudaMalloc(&tmp, sizeof(double) * N * width));
-  const void *src = what == RRHD_RAD_I ? R.d_I : what == RRHD_RAD_S ? R.d_S : (const void *)R.d_G4;
-  if (what == RRHD_RAD_G4 || R.prec == RRHD_RAD_FP64)
-    k_rows_to_host_order<double><<<grid_for(N * width, 256), 256, 0, c->stream>>>(N, width, c->d_perm,
-                                                                                  (const double *)src, tmp);
+  if (what == RRHD_RAD_G4)
+    k_rows_to_host_order<double><<<grid_for(N * width, 256), 256, 0, c->stream>>>(N, width, c->d_perm, R.d_G4, tmp);
+  else if (R.prec == RRHD_RAD_FP64)
+    k_cdg_to_rows<double><<<grid_for(N * width, 256), 256, 0, c->stream>>>(
+        N, R.M, R.G, c->d_perm, (const double *)(what == RRHD_RAD_I ? R.d_I : R.d_S), tmp);
   else
-    k_rows_to_host_order<float><<<grid_for(N * width, 256), 256, 0, c->stream>>>(N, width, c->d_perm,
-                                                                                 (const float *)src, tmp);
+    k_cdg_to_rows<float><<<grid_for(N * width, 256), 256, 0, c->stream>>>(
+        N, R.M, R.G, c->d_perm, (const float *)(what == RRHD_RAD_I ? R.d_I : R.d_S), tmp);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, sizeof(double) * N * width, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -751,11 +970,11 @@ extern "C" rrhd_status rrhd_rad_set(rrhd_ctx *c, int32_t what, const double *in)
   cudaError_t e = cudaMemcpyAsync(tmp, in, sizeof(double) * N * width, cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess) {
     if (R.prec == RRHD_RAD_FP64)
-      k_rows_from_host_order<double><<<grid_for(N * width, 256), 256, 0, c->stream>>>(N, width, c->d_perm, tmp,
-                                                                                      (double *)dst);
+      k_rows_to_cdg<double><<<grid_for(N * width, 256), 256, 0, c->stream>>>(N, R.M, R.G, c->d_perm, tmp,
+                                                                             (double *)dst);
     else
-      k_rows_from_host_order<float><<<grid_for(N * width, 256), 256, 0, c->stream>>>(N, width, c->d_perm, tmp,
-                                                                                     (float *)dst);
+      k_rows_to_cdg<float><<<grid_for(N * width, 256), 256, 0, c->stream>>>(N, R.M, R.G, c->d_perm, tmp,
+                                                                            (float *)dst);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);

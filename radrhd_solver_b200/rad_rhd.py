@@ -64,14 +64,25 @@ class RadRHDStep:
                                   absorption, scattering, em)
 
     def __call__(self, tau: float, stats: bool = False):
-        """One coupled step; with stats=True returns (hydro StepStats, source C2pStats)."""
+        """One coupled step; with stats=True returns (hydro StepStats, source C2pStats).
+        Cells where the hydro con2prim failed even after PhysPressureFix are
+        counted in the hydro statistics (the step itself completes)."""
         if not stats:
-            L.check(L.lib.rrhd_coupled_step(self.grid.handle, tau, C.byref(self.opts), None, None), "coupled step")
+            st = L.lib.rrhd_coupled_step(self.grid.handle, tau, C.byref(self.opts), None, None)
+            if st != L.RRHD_ERR_C2P:
+                L.check(st, "coupled step")
             return None
         hs, ss = L.StepStats(), L.C2pStats()
-        L.check(L.lib.rrhd_coupled_step(self.grid.handle, tau, C.byref(self.opts), C.byref(hs), C.byref(ss)),
-                "coupled step")
+        st = L.lib.rrhd_coupled_step(self.grid.handle, tau, C.byref(self.opts), C.byref(hs), C.byref(ss))
+        if st != L.RRHD_ERR_C2P:
+            L.check(st, "coupled step")
         return hs, ss
+
+    def phase_ms(self):
+        """Device ms of the last step's phases: hydro, sweep, source, scattering."""
+        ms = (C.c_float * 4)()
+        L.check(L.lib.rrhd_coupled_phase_ms(self.grid.handle, ms), "rrhd_coupled_phase_ms")
+        return dict(zip(("hydro", "sweep", "source_c2p", "scatter_moments"), list(ms)))
 
     _KEYS = {"I": L.RRHD_RAD_I, "S": L.RRHD_RAD_S, "G4": L.RRHD_RAD_G4}
 

@@ -78,3 +78,43 @@ def test_scatter_tc_without_moments_and_empty():
     assert torch.equal(S1, S2)
     S0, _ = tc(I[:0])
     tc.check()
+
+
+@pytest.mark.parametrize("groups", [2, 4])
+@pytest.mark.parametrize("form", ["f16x3", "bf16x3"])
+def test_cell_direction_group_layout_bitwise(form, groups):
+    """The coupled step keeps I and S as [cells][M][groups]; the tensor-core and
+    FP64 kernels read and write that layout directly and give the same values as
+    on the row layout, bit for bit."""
+    import ctypes
+    from radrhd_solver_b200 import _lib as L
+    M, cells = 256, 1000  # cells * groups not a multiple of the 128-row tile
+    d = fibonacci_directions(M)
+    dg = illum.DirectionGrid(d)
+    rows = cells * groups
+    I = torch.tensor(intensity(rows, M, seed=17), dtype=torch.float32, device="cuda")
+    I_cdg = I.view(cells, groups, M).transpose(1, 2).contiguous()
+    s = torch.cuda.current_stream().cuda_stream
+    tc = illum.ScatterTC(dg, form)
+    S, mom = torch.empty_like(I), torch.empty(rows, 16, device="cuda")
+    L.check(L.lib.rrhd_scatter_tc_run(tc._h, I.data_ptr(), S.data_ptr(), mom.data_ptr(), rows, s))
+    S2, mom2 = torch.empty_like(I_cdg), torch.empty(rows, 16, device="cuda")
+    L.check(L.lib.rrhd_scatter_tc_run_cdg(tc._h, I_cdg.data_ptr(), S2.data_ptr(), mom2.data_ptr(), cells, groups, s))
+    tc.check()
+    assert torch.equal(S2.transpose(1, 2).reshape(rows, M), S)
+    assert torch.equal(mom2, mom)
+    I64 = I.double()
+    I64_cdg = I64.view(cells, groups, M).transpose(1, 2).contiguous()
+    S64 = torch.empty_like(I64)
+    L.check(L.lib.rrhd_scatter_fp64_fma(dg.handle, I64.data_ptr(), S64.data_ptr(), rows, s))
+    S64c = torch.empty_like(I64_cdg)
+    L.check(L.lib.rrhd_scatter_fp64_cdg(dg.handle, I64_cdg.data_ptr(), S64c.data_ptr(), cells, groups, 0, s))
+    assert torch.equal(S64c.transpose(1, 2).reshape(rows, M), S64)
+    E, F, T = (torch.empty(rows, k, dtype=torch.float64, device="cuda") for k in (1, 3, 9))
+    L.check(L.lib.rrhd_moments_fp64(dg.handle, I64.data_ptr(), E.data_ptr(), F.data_ptr(), T.data_ptr(), rows, s))
+    E2, F2, T2 = (torch.empty_like(x) for x in (E, F, T))
+    L.check(L.lib.rrhd_moments_fp64_cdg(dg.handle, I64_cdg.data_ptr(), E2.data_ptr(), F2.data_ptr(), T2.data_ptr(),
+                                        cells, groups, s))
+    torch.cuda.synchronize()
+    assert torch.equal(E2, E) and torch.equal(F2, F) and torch.equal(T2, T)
+    del ctypes
