@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstring>
 #include <cub/device/device_radix_sort.cuh>
+#include <type_traits>
 #include <vector>
 
 #include "coupled.h"
@@ -110,7 +111,9 @@ struct SweepArgs {
 };
 
 __device__ __forceinline__ double ex(double x) { return exp(x); }
-__device__ __forceinline__ float ex(float x) { return expf(x); }
+__device__ __forceinline__ float ex(float x) { return __expf(x); }
+__device__ __forceinline__ double dv(double a, double b) { return a / b; }
+__device__ __forceinline__ float dv(float a, float b) { return __fdividef(a, b); }
 
 template <class T>
 __device__ __forceinline__ void face_cos(const T *g, T wx, T wy, T wz, T *cosf) {
@@ -121,7 +124,7 @@ __device__ __forceinline__ void face_cos(const T *g, T wx, T wy, T wz, T *cosf) 
 
 // G values at p (contiguous), vectorised for 2 and 4 groups
 template <class T, int G>
-__device__ __forceinline__ void ld_groups(const T *p, T *v) {
+__device__ __forceinline__ void ld_groups(const T *p, T (&v)[G]) {
   if constexpr (sizeof(T) == 8 && G % 2 == 0) {
 #pragma unroll
     for (int q = 0; q < G / 2; q++) {
@@ -140,7 +143,7 @@ __device__ __forceinline__ void ld_groups(const T *p, T *v) {
 // G values to a face-value slot of GS values; float slots of 4 groups are padded to 8 so
 // that every store fills a whole 32-byte sector
 template <class T, int G>
-__device__ __forceinline__ void st_slot(T *p, const T *v) {
+__device__ __forceinline__ void st_slot(T *p, const T (&v)[G]) {
   if constexpr (sizeof(T) == 8 && G % 2 == 0) {
 #pragma unroll
     for (int q = 0; q < G / 2; q++) reinterpret_cast<double2 *>(p)[q] = make_double2(v[2 * q], v[2 * q + 1]);
@@ -155,6 +158,12 @@ __device__ __forceinline__ void st_slot(T *p, const T *v) {
 
 // One thread per (cell, direction) pair of a level: the out-face values of all
 // groups.  GT: compile-time group count (1, 2 or 4), 0 for any other (loop).
+//
+// Node distances: node q of out-face j is traced to the in-face f with the
+// smallest t = lam r_f (r_f = H_f / -cos_f, lam = 2/3 when f is opposite the
+// node's own vertex, 1/6 otherwise), compared exactly as in the restatement.
+// The attenuations need only one exponential per in-face: E1_f = exp(-k r_f / 6)
+// and exp(-k 2 r_f / 3) = E1_f^4 (equal to a few ulp).
 template <class T, int GT>
 __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -167,7 +176,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
   int fid[4], nbr[4];
   load_rec<T>(a.rec + (int64_t)Rec<T>::WORDS * c, g, fid, nbr);
   const T *dy = a.dyn + (int64_t)a.DS * c;
-  const T k = dy[0], be = dy[1];
+  const T k = dy[0], bk = dy[1];
   const SweepIO io = *a.io;
   const T *Sv = (const T *)io.S;
   // S element (group gg) of this cell and direction: base + gg * gs
@@ -182,18 +191,24 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
   const T wx = a.w[3 * d], wy = a.w[3 * d + 1], wz = a.w[3 * d + 2];
   T cosf[4];
   face_cos(g, wx, wy, wz, cosf);
-  T r[4];
+  T t1[4], t4[4], E1[4], E4[4];
 #pragma unroll
-  for (int f = 0; f < 4; f++) r[f] = cosf[f] < 0 ? g[12 + f] / -cosf[f] : (T)0;
-  int hq[4][3];
-  T e[4][3];
+  for (int f = 0; f < 4; f++) {
+    t1[f] = t4[f] = (T)0;
+    E1[f] = E4[f] = (T)1;
+    if (cosf[f] < 0) {
+      const T r = dv(g[12 + f], -cosf[f]);
+      t1[f] = (T)(1.0 / 6.0) * r;
+      t4[f] = (T)(2.0 / 3.0) * r;
+      E1[f] = ex(-k * t1[f]);
+      const T e2 = E1[f] * E1[f];
+      E4[f] = e2 * e2;
+    }
+  }
+  // node selection: 3 bits per node (bit 2: no in-face; bit 3 of the pair: lam = 2/3)
+  uint64_t sel = 0;  // 4 bits per (out-face, node)
 #pragma unroll
   for (int j = 0; j < 4; j++) {
-#pragma unroll
-    for (int q = 0; q < 3; q++) {
-      hq[j][q] = -1;
-      e[j][q] = (T)0;
-    }
     if (!(cosf[j] > 0)) continue;
 #pragma unroll
     for (int q = 0; q < 3; q++) {
@@ -203,19 +218,20 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
 #pragma unroll
       for (int f = 0; f < 4; f++) {
         if (!(cosf[f] < 0)) continue;
-        const T lam = f == vq ? (T)(2.0 / 3.0) : (T)(1.0 / 6.0);
-        const T t = lam * r[f];
+        const T t = f == vq ? t4[f] : t1[f];
         if (hmin < 0 || t < tmin) {
           tmin = t;
           hmin = f;
         }
       }
-      hq[j][q] = hmin;
-      e[j][q] = ex(-k * tmin);
+      const uint32_t code = hmin < 0 ? 8u : (uint32_t)hmin | (hmin == vq ? 4u : 0u);
+      sel |= (uint64_t)code << (12 * j + 4 * q);
     }
   }
   if constexpr (GT > 0) {
-    T rhs[GT], fin[4][GT];
+    // separate per-face arrays (not one [4][GT] array), selected by comparisons, so that
+    // no selection turns into an indexed local-memory access
+    T rhs[GT], f0[GT], f1[GT], f2[GT], f3[GT];
     if (io.layout) {
       ld_groups<T, GT>(Sv + base, rhs);
     } else {
@@ -223,41 +239,56 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
       for (int q = 0; q < GT; q++) rhs[q] = Sv[base + q * gs];
     }
 #pragma unroll
-    for (int q = 0; q < GT; q++) rhs[q] = (dy[2 + q] + be * rhs[q]) / k;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
+    for (int q = 0; q < GT; q++) rhs[q] = dy[2 + q] + bk * rhs[q];
+    auto in_face = [&](int j, T (&fj)[GT]) {
       if (cosf[j] < 0 && nbr[j] >= 0) {
-        ld_groups<T, GT>(a.fv + ((int64_t)fid[j] * a.DB + dl) * a.GS, fin[j]);
+        ld_groups<T, GT>(a.fv + ((int64_t)fid[j] * a.DB + dl) * a.GS, fj);
       } else {
 #pragma unroll
-        for (int q = 0; q < GT; q++) fin[j][q] = a.bc;
+        for (int q = 0; q < GT; q++) fj[q] = a.bc;
       }
-    }
+    };
+    in_face(0, f0);
+    in_face(1, f1);
+    in_face(2, f2);
+    in_face(3, f3);
+    const T E1_0 = E1[0], E1_1 = E1[1], E1_2 = E1[2], E1_3 = E1[3];
+    const T E4_0 = E4[0], E4_1 = E4[1], E4_2 = E4[2], E4_3 = E4[3];
+    auto out_face = [&](int j) {
+      if (!(cosf[j] > 0)) return;
+      T e[3];
+      int h[3];
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      if (!(cosf[j] > 0)) continue;
+      for (int n = 0; n < 3; n++) {
+        const uint32_t code = (uint32_t)(sel >> (12 * j + 4 * n)) & 15u;
+        h[n] = code & 8u ? -1 : (int)(code & 3u);
+        const bool four = code & 4u;
+        e[n] = h[n] == 0 ? (four ? E4_0 : E1_0)
+             : h[n] == 1 ? (four ? E4_1 : E1_1)
+             : h[n] == 2 ? (four ? E4_2 : E1_2)
+             : h[n] == 3 ? (four ? E4_3 : E1_3) : (T)1;
+      }
       T out[GT];
 #pragma unroll
       for (int q = 0; q < GT; q++) {
         T I0[3];
 #pragma unroll
-        for (int n = 0; n < 3; n++) {
-          const int h = hq[j][n];
-          I0[n] = a.bc;
-#pragma unroll
-          for (int f = 0; f < 4; f++)
-            if (h == f) I0[n] = fin[f][q];
-        }
-        T Icur = e[j][0] * (I0[0] - rhs[q]) + rhs[q];
-        Icur += (e[j][1] * (I0[1] - rhs[q]) + rhs[q]);
-        Icur += (e[j][2] * (I0[2] - rhs[q]) + rhs[q]);
+        for (int n = 0; n < 3; n++)
+          I0[n] = h[n] == 0 ? f0[q] : h[n] == 1 ? f1[q] : h[n] == 2 ? f2[q] : h[n] == 3 ? f3[q] : a.bc;
+        T Icur = e[0] * (I0[0] - rhs[q]) + rhs[q];
+        Icur += (e[1] * (I0[1] - rhs[q]) + rhs[q]);
+        Icur += (e[2] * (I0[2] - rhs[q]) + rhs[q]);
         out[q] = Icur * (T)0.3333333333333333;
       }
       st_slot<T, GT>(a.fv + ((int64_t)fid[j] * a.DB + dl) * a.GS, out);
-    }
+    };
+    out_face(0);
+    out_face(1);
+    out_face(2);
+    out_face(3);
   } else {
     for (int gg = 0; gg < a.G; gg++) {
-      const T rhs = (dy[2 + gg] + be * Sv[base + gg * gs]) / k;
+      const T rhs = dy[2 + gg] + bk * Sv[base + gg * gs];
       T fvals[4];
 #pragma unroll
       for (int j = 0; j < 4; j++)
@@ -265,18 +296,23 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         if (!(cosf[j] > 0)) continue;
-        T I0[3];
+        T I0[3], e[3];
 #pragma unroll
         for (int n = 0; n < 3; n++) {
-          const int h = hq[j][n];
+          const uint32_t code = (uint32_t)(sel >> (12 * j + 4 * n)) & 15u;
+          const int h = code & 8u ? -1 : (int)(code & 3u);
           I0[n] = a.bc;
+          e[n] = (T)1;
 #pragma unroll
           for (int f = 0; f < 4; f++)
-            if (h == f) I0[n] = fvals[f];
+            if (h == f) {
+              I0[n] = fvals[f];
+              e[n] = code & 4u ? E4[f] : E1[f];
+            }
         }
-        T Icur = e[j][0] * (I0[0] - rhs) + rhs;
-        Icur += (e[j][1] * (I0[1] - rhs) + rhs);
-        Icur += (e[j][2] * (I0[2] - rhs) + rhs);
+        T Icur = e[0] * (I0[0] - rhs) + rhs;
+        Icur += (e[1] * (I0[1] - rhs) + rhs);
+        Icur += (e[2] * (I0[2] - rhs) + rhs);
         a.fv[((int64_t)fid[j] * a.DB + dl) * a.GS + gg] = Icur * (T)0.3333333333333333;
       }
     }
@@ -380,8 +416,9 @@ __global__ void k_plan_expand(const uint32_t *cur, int64_t n, int nbd, int shift
   }
 }
 
-// Source record {k = alpha + betta, betta, alpha Q_g} of each context cell from
-// caller arrays (caller numbering) ...
+// Source record {k = alpha + betta, betta / k, alpha Q_g / k} of each context cell
+// (rhs_g = alpha Q_g / k + (betta / k) S_g, GetRhsOpt with the division by k
+// distributed) from caller arrays (caller numbering) ...
 template <class T>
 __global__ void k_dyn_from_arrays(int64_t N, int G, int DS, const int32_t *perm, const T *alpha, const T *betta,
                                   const T *Q, T *dyn) {
@@ -390,9 +427,10 @@ __global__ void k_dyn_from_arrays(int64_t N, int G, int DS, const int32_t *perm,
   const int64_t p = perm[c];
   const T al = alpha[p], be = betta[p];
   T *o = dyn + (int64_t)DS * c;
-  o[0] = al + be;
-  o[1] = be;
-  for (int g = 0; g < G; g++) o[2 + g] = al * Q[p * G + g];
+  const T k = al + be;
+  o[0] = k;
+  o[1] = be / k;
+  for (int g = 0; g < G; g++) o[2 + g] = (al * Q[p * G + g]) / k;
 }
 
 // ... or from the solver state: alpha = a rho, betta = b rho, Q_g = B(T) / kRadiation / G.
@@ -405,9 +443,10 @@ __global__ void k_dyn_from_state(int64_t N, int G, int DS, const double *state, 
   const T al = (T)(a_coef * rho), be = (T)(b_coef * rho);
   const T q = (T)(planck_B(em, rho, prs) / em.rad_unit / (double)G);
   T *o = dyn + (int64_t)DS * c;
-  o[0] = al + be;
-  o[1] = be;
-  const T aq = al * q;
+  const T k = al + be;
+  o[0] = k;
+  o[1] = be / k;
+  const T aq = (al * q) / k;
   for (int g = 0; g < G; g++) o[2 + g] = aq;
 }
 
