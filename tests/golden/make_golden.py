@@ -86,7 +86,10 @@ def step_fixtures(out):
     W[:, 0] = 1.0
     W[:, 4] = 1e-3
     W, U = oracle.ref_p2c(W, variant)
-    _, ubc = oracle.ref_p2c(JET_INFLOW[None, :], variant)
+    # inflow boundary state as BoundConditions makes it: rhllc::GetConvValue (rhllc_flux.cpp:7-16)
+    win = np.ascontiguousarray(JET_INFLOW[None, :], np.float64)
+    ubc = np.zeros_like(win)
+    oracle.ref(variant).ref_p2c_plain(win.ctypes.data, ubc.ctypes.data, 1)
     h = oracle.HydroRef(m, variant)
     h.set_bc(-3, 1, JET_INFLOW, ubc[0])
     h.set_state(W, U)
