@@ -45,17 +45,16 @@ struct RadState {
   const rrhd_dirs *dirs = nullptr;  // not owned
   int M = 0, G = 1, DB = 64, shift = 6, nbatch = 0;
   int prec = 0;  // RRHD_RAD_FP64 or RRHD_RAD_FP32: storage and arithmetic of the sweep
-  int DS = 0;    // stride (values) of the per-cell source record
+  int RW = 0;    // stride (values) of the per-cell record
   int GS = 0;    // stride (values) of one face-value slot: G rounded up to a 32-byte sector
   double bc = 0.0;
   int64_t last_cell = 0;  // context index of the caller's last cell (plain-mean quirk)
   void *d_w = nullptr;    // [M][3] directions in the sweep precision
-  // per-cell record (context numbering): outward normals n_j (12), heights H_j = 3 V / A_j (4),
-  // areas A_j (4), then face-value slots of the faces (4 x int32) and neighbours (4 x int32, context
-  // numbering or -1);
-  // 192 B in double, 128 B in float
+  // per-cell record (context numbering, RW values): outward normals n_j (12), heights
+  // H_j = 3 V / A_j (4), face-value slots of the faces (4 x int32) and neighbours (4 x int32,
+  // context numbering or -1), then the step's source record {k, betta/k, alpha Q_g/k}
   void *d_rec = nullptr;
-  void *d_dyn = nullptr;  // [N][DS] per-cell source record: k = alpha + betta, betta, alpha Q_g
+  void *d_area = nullptr;  // [N][4] face areas
   uint32_t *d_plan = nullptr;               // all batches: items (cell << shift | d) in level order
   std::vector<std::vector<int64_t>> lvl;    // per batch: level offsets into d_plan
   int64_t levels = 0, max_level = 0;

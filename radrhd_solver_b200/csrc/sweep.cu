@@ -42,48 +42,36 @@ namespace {
 
 constexpr int kSweepThreads = 128;
 
-// Per-cell record: words 0-11 outward normals n_j, 12-15 heights H_j, 16-19 areas
-// A_j, then the caller face ids and the neighbours as int32 (4 + 4).
+// Per-cell record (RW words): 0-11 outward normals n_j, 12-15 heights H_j, then the
+// face-value slots and the neighbours as int32 (4 + 4: 4 doubles or 8 floats), then the
+// source record {k, betta/k, alpha Q_g/k} of the step.  RW makes a record a whole number
+// of 128-byte lines (G = 4: 256 B in double, 128 B in float), so one item touches one or
+// two lines for everything it needs of its cell.
 template <class T>
-struct Rec;
-template <>
-struct Rec<double> {
-  static constexpr int WORDS = 24;  // 192 B
-};
-template <>
-struct Rec<float> {
-  static constexpr int WORDS = 32;  // 128 B (4 words of padding)
+struct Rec {
+  static constexpr int IDS = 16;                       // word offset of the ids
+  static constexpr int DYN = sizeof(T) == 8 ? 20 : 24;  // word offset of the source record
+  static constexpr int LINE = 128 / (int)sizeof(T);      // words per 128-byte line
 };
 
 template <class T>
-__device__ __forceinline__ void load_rec(const T *r, T *g, int *fid, int *nbr);
-template <>
-__device__ __forceinline__ void load_rec<double>(const double *r, double *g, int *fid, int *nbr) {
-  const double2 *r2 = reinterpret_cast<const double2 *>(r);
+__device__ __forceinline__ void load_rec(const T *r, T *g, int *fid, int *nbr) {
 #pragma unroll
-  for (int q = 0; q < 10; q++) {
-    const double2 v = __ldg(r2 + q);
-    g[2 * q] = v.x;
-    g[2 * q + 1] = v.y;
+  for (int q = 0; q < 16; q += 16 / (int)sizeof(T)) {
+    if constexpr (sizeof(T) == 8) {
+      const double2 v = __ldg(reinterpret_cast<const double2 *>(r) + q / 2);
+      g[q] = v.x;
+      g[q + 1] = v.y;
+    } else {
+      const float4 v = __ldg(reinterpret_cast<const float4 *>(r) + q / 4);
+      g[q] = v.x;
+      g[q + 1] = v.y;
+      g[q + 2] = v.z;
+      g[q + 3] = v.w;
+    }
   }
-  const int4 *r4 = reinterpret_cast<const int4 *>(r + 20);
+  const int4 *r4 = reinterpret_cast<const int4 *>(r + Rec<T>::IDS);
   const int4 f = __ldg(r4), n = __ldg(r4 + 1);
-  fid[0] = f.x, fid[1] = f.y, fid[2] = f.z, fid[3] = f.w;
-  nbr[0] = n.x, nbr[1] = n.y, nbr[2] = n.z, nbr[3] = n.w;
-}
-template <>
-__device__ __forceinline__ void load_rec<float>(const float *r, float *g, int *fid, int *nbr) {
-  const float4 *r4 = reinterpret_cast<const float4 *>(r);
-#pragma unroll
-  for (int q = 0; q < 5; q++) {
-    const float4 v = __ldg(r4 + q);
-    g[4 * q] = v.x;
-    g[4 * q + 1] = v.y;
-    g[4 * q + 2] = v.z;
-    g[4 * q + 3] = v.w;
-  }
-  const int4 *i4 = reinterpret_cast<const int4 *>(r + 20);
-  const int4 f = __ldg(i4), n = __ldg(i4 + 1);
   fid[0] = f.x, fid[1] = f.y, fid[2] = f.z, fid[3] = f.w;
   nbr[0] = n.x, nbr[1] = n.y, nbr[2] = n.z, nbr[3] = n.w;
 }
@@ -92,7 +80,7 @@ template <class T>
 __device__ __forceinline__ void load_normals(const T *r, T *g, int *nbr) {
 #pragma unroll
   for (int q = 0; q < 12; q++) g[q] = __ldg(r + q);
-  const int4 n = __ldg(reinterpret_cast<const int4 *>(r + 20) + 1);
+  const int4 n = __ldg(reinterpret_cast<const int4 *>(r + Rec<T>::IDS) + 1);
   nbr[0] = n.x, nbr[1] = n.y, nbr[2] = n.z, nbr[3] = n.w;
 }
 
@@ -101,10 +89,10 @@ struct SweepArgs {
   const SweepIO *io;
   const uint32_t *items;
   int64_t n;  // items of this level
-  int shift, DB, d0, M, G, DS, GS, nbd;
-  const T *w;    // [M][3]
-  const T *rec;  // [N][Rec<T>::WORDS]
-  const T *dyn;  // [N][DS]
+  int shift, DB, d0, M, G, RW, GS, nbd;
+  const T *w;     // [M][3]
+  const T *rec;   // [N][RW]
+  const T *area;  // [N][4] face areas (cell values)
   T *fv;         // [F][DB][GS] face values (GS >= G, full 32-byte sectors)
   T bc;
   int64_t last;
@@ -172,10 +160,11 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
   const int64_t c = it >> a.shift;
   const int dl = (int)(it & (uint32_t)(a.DB - 1));
   const int d = a.d0 + dl;
-  T g[20];
+  T g[16];
   int fid[4], nbr[4];
-  load_rec<T>(a.rec + (int64_t)Rec<T>::WORDS * c, g, fid, nbr);
-  const T *dy = a.dyn + (int64_t)a.DS * c;
+  const T *rc = a.rec + (int64_t)a.RW * c;
+  load_rec<T>(rc, g, fid, nbr);
+  const T *dy = rc + Rec<T>::DYN;
   const T k = dy[0], bk = dy[1];
   const SweepIO io = *a.io;
   const T *Sv = (const T *)io.S;
@@ -332,11 +321,14 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
   const int64_t c = t / a.nbd;
   const int dl = (int)(t - c * a.nbd);
   const int d = a.d0 + dl;
-  T g[20];
+  T g[16];
   int fid[4], nbr[4];
-  load_rec<T>(a.rec + (int64_t)Rec<T>::WORDS * c, g, fid, nbr);
+  load_rec<T>(a.rec + (int64_t)a.RW * c, g, fid, nbr);
   T cosf[4];
   face_cos(g, a.w[3 * d], a.w[3 * d + 1], a.w[3 * d + 2], cosf);
+  T A[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) A[j] = __ldg(a.area + 4 * c + j);
   const SweepIO io = *a.io;
   T *I = (T *)io.I;
   int64_t base, gs;
@@ -360,8 +352,8 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
       T Ssum = 0;
 #pragma unroll
       for (int j = 0; j < 4; j++) {
-        curI += fv[j] * g[16 + j];
-        Ssum += g[16 + j];
+        curI += fv[j] * A[j];
+        Ssum += A[j];
       }
       curI /= Ssum;
     } else {
@@ -375,7 +367,7 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
 
 // ---------------------------------------------------------------- plan
 template <class T>
-__global__ void k_plan_init(int64_t N, int nbd, int shift, int d0, const T *w, const T *rec, uint32_t *indeg,
+__global__ void k_plan_init(int64_t N, int nbd, int shift, int d0, const T *w, const T *rec, int RW, uint32_t *indeg,
                             uint32_t *plan, unsigned long long *tail) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= N * nbd) return;
@@ -384,7 +376,7 @@ __global__ void k_plan_init(int64_t N, int nbd, int shift, int d0, const T *w, c
   const int d = d0 + dl;
   T g[12];
   int nbr[4];
-  load_normals<T>(rec + (int64_t)Rec<T>::WORDS * c, g, nbr);
+  load_normals<T>(rec + (int64_t)RW * c, g, nbr);
   T cosf[4];
   face_cos(g, w[3 * d], w[3 * d + 1], w[3 * d + 2], cosf);
   uint32_t cnt = 0;
@@ -396,7 +388,7 @@ __global__ void k_plan_init(int64_t N, int nbd, int shift, int d0, const T *w, c
 
 template <class T>
 __global__ void k_plan_expand(const uint32_t *cur, int64_t n, int nbd, int shift, int d0, const T *w, const T *rec,
-                              uint32_t *indeg, uint32_t *plan, unsigned long long *tail) {
+                              int RW, uint32_t *indeg, uint32_t *plan, unsigned long long *tail) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t it = cur[i];
@@ -405,7 +397,7 @@ __global__ void k_plan_expand(const uint32_t *cur, int64_t n, int nbd, int shift
   const int d = d0 + dl;
   T g[12];
   int nbr[4];
-  load_normals<T>(rec + (int64_t)Rec<T>::WORDS * c, g, nbr);
+  load_normals<T>(rec + (int64_t)RW * c, g, nbr);
   T cosf[4];
   face_cos(g, w[3 * d], w[3 * d + 1], w[3 * d + 2], cosf);
 #pragma unroll
@@ -420,13 +412,13 @@ __global__ void k_plan_expand(const uint32_t *cur, int64_t n, int nbd, int shift
 // (rhs_g = alpha Q_g / k + (betta / k) S_g, GetRhsOpt with the division by k
 // distributed) from caller arrays (caller numbering) ...
 template <class T>
-__global__ void k_dyn_from_arrays(int64_t N, int G, int DS, const int32_t *perm, const T *alpha, const T *betta,
-                                  const T *Q, T *dyn) {
+__global__ void k_dyn_from_arrays(int64_t N, int G, int RW, const int32_t *perm, const T *alpha, const T *betta,
+                                  const T *Q, T *rec) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= N) return;
   const int64_t p = perm[c];
   const T al = alpha[p], be = betta[p];
-  T *o = dyn + (int64_t)DS * c;
+  T *o = rec + (int64_t)RW * c + Rec<T>::DYN;
   const T k = al + be;
   o[0] = k;
   o[1] = be / k;
@@ -435,14 +427,14 @@ __global__ void k_dyn_from_arrays(int64_t N, int G, int DS, const int32_t *perm,
 
 // ... or from the solver state: alpha = a rho, betta = b rho, Q_g = B(T) / kRadiation / G.
 template <class T>
-__global__ void k_dyn_from_state(int64_t N, int G, int DS, const double *state, double a_coef, double b_coef,
-                                 Emission em, T *dyn) {
+__global__ void k_dyn_from_state(int64_t N, int G, int RW, const double *state, double a_coef, double b_coef,
+                                 Emission em, T *rec) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= N) return;
   const double rho = state[10 * c + 5], prs = state[10 * c + 9];
   const T al = (T)(a_coef * rho), be = (T)(b_coef * rho);
   const T q = (T)(planck_B(em, rho, prs) / em.rad_unit / (double)G);
-  T *o = dyn + (int64_t)DS * c;
+  T *o = rec + (int64_t)RW * c + Rec<T>::DYN;
   const T k = al + be;
   o[0] = k;
   o[1] = be / k;
@@ -595,7 +587,7 @@ rrhd_status build_plan(rrhd_ctx *c) {
     const unsigned long long zero = 0;
     RRHD_CUDA(cudaMemcpyAsync(d_tail, &zero, sizeof zero, cudaMemcpyHostToDevice, st));
     k_plan_init<T><<<grid_for(N * nbd, 256), 256, 0, st>>>(N, nbd, R.shift, d0, (const T *)R.d_w,
-                                                            (const T *)R.d_rec, indeg, plan, d_tail);
+                                                            (const T *)R.d_rec, R.RW, indeg, plan, d_tail);
     RRHD_CUDA(cudaGetLastError());
     std::vector<int64_t> &off = R.lvl[b];
     off.assign(1, 0);
@@ -613,8 +605,8 @@ rrhd_status build_plan(rrhd_ctx *c) {
       off.push_back(hi);
       R.max_level = std::max(R.max_level, hi - lo);
       k_plan_expand<T><<<grid_for(hi - lo, 256), 256, 0, st>>>(plan + lo, hi - lo, nbd, R.shift, d0,
-                                                                (const T *)R.d_w, (const T *)R.d_rec, indeg,
-                                                                plan, d_tail);
+                                                                (const T *)R.d_w, (const T *)R.d_rec, R.RW,
+                                                                indeg, plan, d_tail);
       RRHD_CUDA(cudaGetLastError());
       lo = hi;
     }
@@ -645,10 +637,10 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
     a.DB = R.DB;
     a.M = R.M;
     a.G = R.G;
-    a.DS = R.DS;
+    a.RW = R.RW;
     a.w = (const T *)R.d_w;
     a.rec = (const T *)R.d_rec;
-    a.dyn = (const T *)R.d_dyn;
+    a.area = (const T *)R.d_area;
     a.fv = (T *)R.d_fv;
     a.bc = (T)R.bc;
     a.last = R.last_cell;
@@ -687,7 +679,7 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
 void rrhd_rad_release(rrhd_ctx *c) {
   RadState &R = c->rad;
   if (R.graph) cudaGraphExecDestroy(R.graph);
-  void *ptrs[] = {R.d_w, R.d_rec, R.d_dyn, R.d_plan, R.d_io, R.d_fv, R.d_I, R.d_S, R.d_G4, R.d_mE, R.d_mF, R.d_mT,
+  void *ptrs[] = {R.d_w, R.d_rec, R.d_area, R.d_plan, R.d_io, R.d_fv, R.d_I, R.d_S, R.d_G4, R.d_mE, R.d_mF, R.d_mT,
                   R.d_mom, R.d_cnt};
   for (void *p : ptrs) cudaFree(p);
   for (cudaEvent_t e : R.ev)
@@ -700,8 +692,9 @@ template <class T>
 static rrhd_status rad_setup_t(rrhd_ctx *c) {
   RadState &R = c->rad;
   const int64_t N = c->N;
-  constexpr int W = Rec<T>::WORDS;
-  std::vector<T> rec((size_t)W * N, (T)0), w(3 * R.M);
+  const int W = ((Rec<T>::DYN + 2 + R.G + Rec<T>::LINE - 1) / Rec<T>::LINE) * Rec<T>::LINE;
+  R.RW = W;
+  std::vector<T> rec((size_t)W * N, (T)0), area(4 * (size_t)N), w(3 * R.M);
   std::vector<int32_t> iperm(N);
   for (int64_t i = 0; i < N; i++) iperm[c->h_perm[i]] = (int32_t)i;
   // face-value slots numbered in order of first use by context cells, so that the
@@ -725,17 +718,16 @@ static rrhd_status rad_setup_t(rrhd_ctx *c) {
         r[3 * j + x] = (T)(out ? v : -v);
       }
       r[12 + j] = (T)(3.0 * c->h_cell_V[p] / c->h_face_area[fc]);
-      r[16 + j] = (T)c->h_face_area[fc];
+      area[4 * cn + j] = (T)c->h_face_area[fc];
       const int32_t l = c->h_face_l[fc], rr = c->h_face_r[fc];
       const int32_t o = (l == p) ? rr : l;
       ids[j] = fslot[fc];
       ids[4 + j] = o < 0 ? -1 : iperm[o];
     }
-    std::memcpy(r + 20, ids, sizeof ids);
+    std::memcpy(r + Rec<T>::IDS, ids, sizeof ids);
   }
   for (int q = 0; q < 3 * R.M; q++) w[q] = (T)R.dirs->h_w[q];
   R.last_cell = iperm[N - 1];
-  R.DS = sizeof(T) == 8 ? ((2 + R.G + 1) & ~1) : ((2 + R.G + 3) & ~3);
   R.GS = sizeof(T) == 8 ? ((R.G + 3) & ~3) : ((R.G + 7) & ~7);
   auto up = [&](void **dst, const void *src, size_t bytes) -> rrhd_status {
     if (cudaMalloc(dst, bytes) != cudaSuccess) return rrhd_fail(RRHD_ERR_OOM, "sweep allocation failed");
@@ -743,10 +735,10 @@ static rrhd_status rad_setup_t(rrhd_ctx *c) {
     return RRHD_OK;
   };
   rrhd_status s;
-  if ((s = up(&R.d_rec, rec.data(), sizeof(T) * rec.size())) || (s = up(&R.d_w, w.data(), sizeof(T) * w.size())))
+  if ((s = up(&R.d_rec, rec.data(), sizeof(T) * rec.size())) || (s = up(&R.d_w, w.data(), sizeof(T) * w.size())) ||
+      (s = up(&R.d_area, area.data(), sizeof(T) * area.size())))
     return s;
   if (cudaMalloc(&R.d_io, sizeof(SweepIO)) != cudaSuccess ||
-      cudaMalloc(&R.d_dyn, sizeof(T) * (size_t)R.DS * N) != cudaSuccess ||
       cudaMalloc(&R.d_fv, sizeof(T) * (size_t)c->F * R.DB * R.GS) != cudaSuccess)
     return rrhd_fail(RRHD_ERR_OOM, "sweep allocation failed");
   if ((s = build_plan<T>(c))) return s;
@@ -818,10 +810,10 @@ extern "C" rrhd_status rrhd_sweep(rrhd_ctx *c, const void *alpha, const void *be
   const int64_t N = c->N;
   if (R.prec == RRHD_RAD_FP64)
     k_dyn_from_arrays<double><<<grid_for(N, 256), 256, 0, c->stream>>>(
-        N, R.G, R.DS, c->d_perm, (const double *)alpha, (const double *)betta, (const double *)Q, (double *)R.d_dyn);
+        N, R.G, R.RW, c->d_perm, (const double *)alpha, (const double *)betta, (const double *)Q, (double *)R.d_rec);
   else
     k_dyn_from_arrays<float><<<grid_for(N, 256), 256, 0, c->stream>>>(
-        N, R.G, R.DS, c->d_perm, (const float *)alpha, (const float *)betta, (const float *)Q, (float *)R.d_dyn);
+        N, R.G, R.RW, c->d_perm, (const float *)alpha, (const float *)betta, (const float *)Q, (float *)R.d_rec);
   RRHD_CUDA(cudaGetLastError());
   SweepIO io{S, I, c->d_perm, 0};
   return launch_sweep(c, io);
@@ -914,11 +906,11 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
   const Emission em{o->emission.temp_coef, o->emission.sigma_sb, o->emission.pi, o->emission.rad_unit};
   // 2. opacities and emission from the new primitives, 3. sweep with the previous scattering integral
   if (fp64)
-    k_dyn_from_state<double><<<grid_for(N, 256), 256, 0, st>>>(N, R.G, R.DS, state, o->absorption, o->scattering,
-                                                                em, (double *)R.d_dyn);
+    k_dyn_from_state<double><<<grid_for(N, 256), 256, 0, st>>>(N, R.G, R.RW, state, o->absorption, o->scattering,
+                                                                em, (double *)R.d_rec);
   else
-    k_dyn_from_state<float><<<grid_for(N, 256), 256, 0, st>>>(N, R.G, R.DS, state, o->absorption, o->scattering, em,
-                                                               (float *)R.d_dyn);
+    k_dyn_from_state<float><<<grid_for(N, 256), 256, 0, st>>>(N, R.G, R.RW, state, o->absorption, o->scattering, em,
+                                                               (float *)R.d_rec);
   RRHD_CUDA(cudaGetLastError());
   SweepIO io{R.d_S, R.d_I, nullptr, 1};
   if ((s = launch_sweep(c, io))) return s;
