@@ -260,6 +260,49 @@ def scatter_component(dev, nhex=48, M=256, groups=1, kind=0, sigma=0.5, reps=5, 
     return out
 
 
+def scatter_scale_component(dev, cells=2_000_000, M=512, groups=16, reps=3, sample=65536):
+    """Config 2: 2M cells x 512 Fibonacci directions x 16 frequency groups in one launch
+    (rows = cell x group); I = 10^(-6 + 6g/15) lognormal(0, 1) (seeded), values over
+    ~12 decades.  Tensor-core forms timed on all 32M rows (I and S 64 GB each, FP32);
+    errors against the direct FP64 contraction on a seeded sample of rows."""
+    import torch
+    from radrhd_solver_b200 import _lib as L
+    from radrhd_solver_b200 import illum
+    from radrhd_solver_b200 import mesh as Mm
+    torch.cuda.empty_cache()
+    rows = cells * groups
+    d = Mm.fibonacci_directions(M)
+    dg = illum.DirectionGrid(d, dev)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    I32 = torch.empty(rows, M, dtype=torch.float32, device=f"cuda:{dev}")
+    L.check(L.lib.rrhd_fill_intensity_f32(I32.data_ptr(), rows, M, groups, 1, 1.0, None, 23, sp))
+    S32 = torch.empty_like(I32)
+    gen = torch.Generator(device="cpu").manual_seed(5)
+    idx = torch.randperm(rows, generator=gen)[:sample].sort().values.to(f"cuda:{dev}")
+    I64 = I32[idx].double()
+    S64 = torch.empty_like(I64)
+    L.check(L.lib.rrhd_scatter_fp64(dg.handle, I64.data_ptr(), S64.data_ptr(), sample, sp))
+    flop = 2.0 * rows * M * M
+    out = {"workload": f"{cells} cells x {groups} groups x {M} directions, one launch", "rows": rows,
+           "error_sample_rows": sample}
+    for form in ("bf16x3", "f16x3", "f16"):
+        tc = illum.ScatterTC(dg, form)
+
+        def run(tc=tc):
+            L.check(L.lib.rrhd_scatter_tc_run(tc._h, I32.data_ptr(), S32.data_ptr(), None, rows, sp))
+        ms = _time(run, reps, stream, warm=1)
+        tc.check()
+        rel = ((S32[idx].double() - S64).abs() / S64.abs()).flatten()
+        out["tc_" + form] = {"ms": ms, "row_dir_per_s": rows * M / (ms / 1e3), "tflops": flop / (ms / 1e3) / 1e12,
+                             "max_rel_err": float(rel.max()), "rms_rel_err": float(rel.pow(2).mean().sqrt())}
+        tc.close()
+    del I32, S32, I64, S64
+    dg.close()
+    torch.cuda.empty_cache()
+    return out
+
+
 def c2p_component(dev, n=8_000_000, epochs=8, reps=5):
     """Config 3: 8M states (rho, p/rho, W log-uniform; isotropic v; Gamma 4/3),
     network trained on the first 4M, plain vs learned-guess con2prim timed on the
@@ -320,7 +363,8 @@ def c2p_component(dev, n=8_000_000, epochs=8, reps=5):
 EM_JET = (1.0, 10.0, float(np.pi), 1.0)  # temp_coef, a_R, pi, kRadiation in code units: T = p / rho, B = a_R T^4 / pi
 
 
-def coupled_component(dev, m, W, steps=3, warm=1, M=256, G=4, train_epochs=2, forms=("plain", "chosen")):
+def coupled_component(dev, m, W, steps=3, warm=1, M=256, G=4, train_epochs=2, forms=("plain", "chosen"),
+                      batch=(128, 256)):
     """Config-4 coupled radiation-hydro jet step (radRHD_main.cpp:96-139) on the
     benchmark mesh: hydro step, opacities alpha = rho, betta = 0.5 rho, emission
     Q = a_R T^4 / pi / G per grey group, sweep of M directions x G groups,
@@ -347,7 +391,8 @@ def coupled_component(dev, m, W, steps=3, warm=1, M=256, G=4, train_epochs=2, fo
         g.set_state_prim(W)
         dg = illum.DirectionGrid(d, dev)
         t0 = time.perf_counter()
-        sw = illum.TransportSweep(g, dg, groups=G, precision="fp64" if form == "plain" else "fp32")
+        sw = illum.TransportSweep(g, dg, groups=G, precision="fp64" if form == "plain" else "fp32",
+                                  dirs_per_batch=batch[0] if form == "plain" else batch[1])
         t_plan = time.perf_counter() - t0
         if form == "chosen" and "plain_dump" in states:
             Wp, Up = states["plain_dump"]
@@ -378,7 +423,7 @@ def coupled_component(dev, m, W, steps=3, warm=1, M=256, G=4, train_epochs=2, fo
             states["plain_dump"] = (Wg, Ug)
         bpv = 8 if form == "plain" else 4
         sweep_alg = (2.0 * m.n_cells + 2.0 * m.n_faces) * M * G * bpv + m.n_cells * (20 * bpv + 32.0)
-        out[form] = {"ms_per_step": ms, "steps_per_s": 1e3 / ms, "cell_updates_per_s": m.n_cells / (ms / 1e3),
+        out[form] = {"dirs_per_batch": batch[0] if form == "plain" else batch[1], "ms_per_step": ms, "steps_per_s": 1e3 / ms, "cell_updates_per_s": m.n_cells / (ms / 1e3),
                      "cell_dir_group_per_s": m.n_cells * M * G / (ms / 1e3), "phase_ms_last_step": ph,
                      "sweep_levels": levels, "largest_level": biggest, "plan_build_s": t_plan,
                      "sweep_alg_gbs": sweep_alg / (ph["sweep"] / 1e3) / 1e9,
@@ -532,7 +577,8 @@ def run_ours(args):
             "step_stats": {"max_speed": st.max_speed, "n_fallback": st.n_fallback, "n_failed": st.n_failed}}
     g.close()
     if rank == 0 and not args.no_coupled:
-        line["coupled"] = coupled_component(dev, m, W, steps=args.coupled_steps)
+        line["coupled"] = coupled_component(dev, m, W, steps=args.coupled_steps,
+                                            batch=tuple(int(x) for x in args.coupled_batch.split(",")))
     if rank == 0 and not args.no_cpu:
         import oracle
         threads = cpu_threads()
@@ -548,6 +594,8 @@ def run_ours(args):
         sc = line["scatter"]
         if "fp64_fma" in sc:
             line.setdefault("chosen_vs_plain", {})["scatter_moments"] = sc["fp64_fma"]["ms"] / sc["tc_f16x3"]["ms"]
+    if rank == 0 and not args.no_scatter:
+        line["scatter_scale"] = scatter_scale_component(dev)
     if rank == 0 and "coupled" in line:
         line.setdefault("chosen_vs_plain", {})["coupled_step"] = line["coupled"]["chosen_vs_plain"]
     if rank == 0:
@@ -579,6 +627,11 @@ def main():
     ap.add_argument("--coupled-only", type=int, default=0, metavar="NHEX",
                     help="only time the coupled step on an NHEX^3 x 6 jet mesh (profiling runs)")
     ap.add_argument("--coupled-forms", default="plain,chosen", help="forms of --coupled-only")
+    ap.add_argument("--coupled-batch", default="128,256", help="directions per sweep batch (plain,chosen)")
+    ap.add_argument("--c2p-only", type=int, default=0, metavar="STATES",
+                    help="only time the con2prim component on STATES states (profiling runs)")
+    ap.add_argument("--scale-only", type=int, default=0, metavar="CELLS",
+                    help="only time the scattering-at-scale component on CELLS cells (profiling runs)")
     args = ap.parse_args()
     global NHEX
     NHEX = args.nhex
@@ -587,12 +640,22 @@ def main():
         torch.cuda.set_device(0)
         print(json.dumps(scatter_component(0, nhex=args.scatter_only, reps=args.steps)), flush=True)
         return
+    if args.c2p_only or args.scale_only:
+        import torch
+        torch.cuda.set_device(0)
+        if args.c2p_only:
+            print(json.dumps(c2p_component(0, n=args.c2p_only, reps=args.steps)), flush=True)
+        else:
+            print(json.dumps(scatter_scale_component(0, cells=args.scale_only, reps=args.steps,
+                                                     sample=min(65536, args.scale_only))), flush=True)
+        return
     if args.coupled_only:
         import torch
         torch.cuda.set_device(0)
         m, W = make_jet(args.coupled_only)
         print(json.dumps(coupled_component(0, m, W, steps=args.coupled_steps,
-                                           forms=tuple(args.coupled_forms.split(",")))), flush=True)
+                                           forms=tuple(args.coupled_forms.split(",")),
+                                           batch=tuple(int(x) for x in args.coupled_batch.split(",")))), flush=True)
         return
     if args.sweep_only:
         import torch
