@@ -751,7 +751,7 @@ extern "C" rrhd_status rrhd_rad_setup(rrhd_ctx *c, const rrhd_dirs *dirs, const 
   RRHD_CHECK_ARG(o->precision == RRHD_RAD_FP64 || o->precision == RRHD_RAD_FP32, "bad precision");
   RRHD_CHECK_ARG(dirs->device == c->device, "direction set lives on another device");
   int DB = o->dirs_per_batch;
-  RRHD_CHECK_ARG(DB == 0 || (DB > 0 && DB <= 64 && (DB & (DB - 1)) == 0), "dirs_per_batch: power of two <= 64");
+  RRHD_CHECK_ARG(DB == 0 || (DB > 0 && DB <= 256 && (DB & (DB - 1)) == 0), "dirs_per_batch: power of two <= 256");
   RRHD_CUDA(cudaSetDevice(c->device));
   RRHD_CUDA(cudaStreamSynchronize(c->stream));
   rrhd_rad_release(c);
