@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
 // parallel to it) hold the boundary value.  One thread per (cell, direction);
 // consecutive threads take consecutive directions of a cell, so face-value reads
 // and intensity writes are contiguous.
-template <class T>
+template <class T, int GT>
 __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= N * a.nbd) return;
@@ -343,10 +343,7 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
   bool have[4];
 #pragma unroll
   for (int j = 0; j < 4; j++) have[j] = cosf[j] > 0 || (cosf[j] < 0 && nbr[j] >= 0);
-  for (int gg = 0; gg < a.G; gg++) {
-    T fv[4];
-#pragma unroll
-    for (int j = 0; j < 4; j++) fv[j] = have[j] ? a.fv[((int64_t)fid[j] * a.DB + dl) * a.GS + gg] : a.bc;
+  auto cell_value = [&](const T *fv) {
     T curI = 0;
     if (!last) {
       T Ssum = 0;
@@ -361,7 +358,50 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
       for (int j = 0; j < 4; j++) curI += fv[j];
       curI /= (T)4;
     }
-    I[base + gg * gs] = curI;
+    return curI;
+  };
+  if constexpr (GT > 0) {
+    // all four face slots in flight at once, vector loads and a vector store
+    T f0[GT], f1[GT], f2[GT], f3[GT];
+    auto slot = [&](int j, T (&fj)[GT]) {
+      if (have[j]) {
+        ld_groups<T, GT>(a.fv + ((int64_t)fid[j] * a.DB + dl) * a.GS, fj);
+      } else {
+#pragma unroll
+        for (int q = 0; q < GT; q++) fj[q] = a.bc;
+      }
+    };
+    slot(0, f0);
+    slot(1, f1);
+    slot(2, f2);
+    slot(3, f3);
+    T out[GT];
+#pragma unroll
+    for (int q = 0; q < GT; q++) {
+      const T fv[4] = {f0[q], f1[q], f2[q], f3[q]};
+      out[q] = cell_value(fv);
+    }
+    if (io.layout) {
+      if constexpr (sizeof(T) == 8 && GT % 2 == 0) {
+#pragma unroll
+        for (int q = 0; q < GT / 2; q++) reinterpret_cast<double2 *>(I + base)[q] = make_double2(out[2 * q], out[2 * q + 1]);
+      } else if constexpr (sizeof(T) == 4 && GT == 4) {
+        *reinterpret_cast<float4 *>(I + base) = make_float4(out[0], out[1], out[2], out[3]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < GT; q++) I[base + q] = out[q];
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < GT; q++) I[base + q * gs] = out[q];
+    }
+  } else {
+    for (int gg = 0; gg < a.G; gg++) {
+      T fv[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) fv[j] = have[j] ? a.fv[((int64_t)fid[j] * a.DB + dl) * a.GS + gg] : a.bc;
+      I[base + gg * gs] = cell_value(fv);
+    }
   }
 }
 
@@ -662,7 +702,13 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
           default: k_sweep_level<T, 0><<<nb, kSweepThreads, 0, cs>>>(a); break;
         }
       }
-      k_recalc<T><<<grid_for(c->N * nbd, 256), 256, 0, cs>>>(a, c->N);
+      const unsigned nr = grid_for(c->N * nbd, 256);
+      switch (R.G) {
+        case 1: k_recalc<T, 1><<<nr, 256, 0, cs>>>(a, c->N); break;
+        case 2: k_recalc<T, 2><<<nr, 256, 0, cs>>>(a, c->N); break;
+        case 4: k_recalc<T, 4><<<nr, 256, 0, cs>>>(a, c->N); break;
+        default: k_recalc<T, 0><<<nr, 256, 0, cs>>>(a, c->N); break;
+      }
       base += c->N * nbd;
     }
     e = cudaStreamEndCapture(cs, &g);
