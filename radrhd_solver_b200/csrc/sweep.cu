@@ -194,28 +194,47 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
       E4[f] = e2 * e2;
     }
   }
-  // node selection: 3 bits per node (bit 2: no in-face; bit 3 of the pair: lam = 2/3)
-  uint64_t sel = 0;  // 4 bits per (out-face, node)
+  // node selection.  The restatement takes, for each node, the in-face with the smallest
+  // (t, face index); t = t4 for the face opposite the node's own vertex, t1 for the others.
+  // So only the two smallest in-faces by (t1, index) are needed: the node's candidate
+  // among the other faces is the best unless that is its own opposite face.
+  int b1 = -1, b2 = -1;
+  T tb1 = 0, tb2 = 0;
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    if (!(cosf[f] < 0)) continue;
+    if (b1 < 0 || t1[f] < tb1) {
+      b2 = b1;
+      tb2 = tb1;
+      b1 = f;
+      tb1 = t1[f];
+    } else if (b2 < 0 || t1[f] < tb2) {
+      b2 = f;
+      tb2 = t1[f];
+    }
+  }
+  // 4 bits per (out-face, node): face index, bit 2 lam = 2/3, bit 3 no in-face; out-faces
+  // compacted into slots (2 bits each in jo)
+  uint64_t sel = 0;
+  uint32_t jo = 0;
+  int nout = 0;
 #pragma unroll
   for (int j = 0; j < 4; j++) {
     if (!(cosf[j] > 0)) continue;
 #pragma unroll
     for (int q = 0; q < 3; q++) {
       const int vq = (j + 1 + q) & 3;
-      T tmin = 0;
-      int hmin = -1;
-#pragma unroll
-      for (int f = 0; f < 4; f++) {
-        if (!(cosf[f] < 0)) continue;
-        const T t = f == vq ? t4[f] : t1[f];
-        if (hmin < 0 || t < tmin) {
-          tmin = t;
-          hmin = f;
-        }
-      }
-      const uint32_t code = hmin < 0 ? 8u : (uint32_t)hmin | (hmin == vq ? 4u : 0u);
-      sel |= (uint64_t)code << (12 * j + 4 * q);
+      const int B = b1 != vq ? b1 : b2;
+      const T tB = b1 != vq ? tb1 : tb2;
+      uint32_t code;
+      if (cosf[vq] < 0 && (B < 0 || t4[vq] < tB || (t4[vq] == tB && vq < B)))
+        code = (uint32_t)vq | 4u;
+      else
+        code = B < 0 ? 8u : (uint32_t)B;
+      sel |= (uint64_t)code << (12 * nout + 4 * q);
     }
+    jo |= (uint32_t)j << (2 * nout);
+    nout++;
   }
   if constexpr (GT > 0) {
     // separate per-face arrays (not one [4][GT] array), selected by comparisons, so that
@@ -243,13 +262,15 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
     in_face(3, f3);
     const T E1_0 = E1[0], E1_1 = E1[1], E1_2 = E1[2], E1_3 = E1[3];
     const T E4_0 = E4[0], E4_1 = E4[1], E4_2 = E4[2], E4_3 = E4[3];
-    auto out_face = [&](int j) {
-      if (!(cosf[j] > 0)) return;
+    const int fid0 = fid[0], fid1 = fid[1], fid2 = fid[2], fid3 = fid[3];
+    // the (at most three) out-faces, one slot after another
+    for (int o = 0; o < nout; o++) {
+      const int j = (jo >> (2 * o)) & 3;
       T e[3];
       int h[3];
 #pragma unroll
       for (int n = 0; n < 3; n++) {
-        const uint32_t code = (uint32_t)(sel >> (12 * j + 4 * n)) & 15u;
+        const uint32_t code = (uint32_t)(sel >> (12 * o + 4 * n)) & 15u;
         h[n] = code & 8u ? -1 : (int)(code & 3u);
         const bool four = code & 4u;
         e[n] = h[n] == 0 ? (four ? E4_0 : E1_0)
@@ -269,12 +290,9 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
         Icur += (e[2] * (I0[2] - rhs[q]) + rhs[q]);
         out[q] = Icur * (T)0.3333333333333333;
       }
-      st_slot<T, GT>(a.fv + ((int64_t)fid[j] * a.DB + dl) * a.GS, out);
-    };
-    out_face(0);
-    out_face(1);
-    out_face(2);
-    out_face(3);
+      const int fj = j == 0 ? fid0 : j == 1 ? fid1 : j == 2 ? fid2 : fid3;
+      st_slot<T, GT>(a.fv + ((int64_t)fj * a.DB + dl) * a.GS, out);
+    }
   } else {
     for (int gg = 0; gg < a.G; gg++) {
       const T rhs = dy[2 + gg] + bk * Sv[base + gg * gs];
@@ -282,13 +300,12 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
 #pragma unroll
       for (int j = 0; j < 4; j++)
         fvals[j] = (cosf[j] < 0 && nbr[j] >= 0) ? a.fv[((int64_t)fid[j] * a.DB + dl) * a.GS + gg] : a.bc;
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        if (!(cosf[j] > 0)) continue;
+      for (int o = 0; o < nout; o++) {
+        const int j = (jo >> (2 * o)) & 3;
         T I0[3], e[3];
 #pragma unroll
         for (int n = 0; n < 3; n++) {
-          const uint32_t code = (uint32_t)(sel >> (12 * j + 4 * n)) & 15u;
+          const uint32_t code = (uint32_t)(sel >> (12 * o + 4 * n)) & 15u;
           const int h = code & 8u ? -1 : (int)(code & 3u);
           I0[n] = a.bc;
           e[n] = (T)1;
