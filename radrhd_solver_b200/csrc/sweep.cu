@@ -154,6 +154,12 @@ __device__ __forceinline__ void st_slot(T *p, const T (&v)[G]) {
 // and exp(-k 2 r_f / 3) = E1_f^4 (equal to a few ulp).
 template <class T, int GT>
 __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
+  // Levels after the first of a batch are launched with programmatic stream
+  // serialisation: the next level may start while this one drains, and everything up to
+  // the first face-value read (item, cell record, source record, S, geometry,
+  // exponentials) overlaps the previous level; griddepcontrol.wait then waits for the
+  // previous level to complete and its writes to be visible.
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= a.n) return;
   const uint32_t it = a.items[i];
@@ -248,6 +254,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
     }
 #pragma unroll
     for (int q = 0; q < GT; q++) rhs[q] = dy[2 + q] + bk * rhs[q];
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     auto in_face = [&](int j, T (&fj)[GT]) {
       if (cosf[j] < 0 && nbr[j] >= 0) {
         ld_groups<T, GT>(a.fv + ((int64_t)fid[j] * a.DB + dl) * a.GS, fj);
@@ -294,6 +301,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
       st_slot<T, GT>(a.fv + ((int64_t)fj * a.DB + dl) * a.GS, out);
     }
   } else {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     for (int gg = 0; gg < a.G; gg++) {
       const T rhs = dy[2 + gg] + bk * Sv[base + gg * gs];
       T fvals[4];
@@ -680,12 +688,28 @@ rrhd_status build_plan(rrhd_ctx *c) {
   return RRHD_OK;
 }
 
+template <class T, int GT>
+cudaError_t launch_level(const SweepArgs<T> &a, unsigned nb, cudaStream_t st, bool pdl) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nb);
+  cfg.blockDim = dim3(kSweepThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k_sweep_level<T, GT>, a);
+}
+
 template <class T>
 rrhd_status capture_sweep(rrhd_ctx *c) {
   RadState &R = c->rad;
   cudaStream_t cs = nullptr;
   RRHD_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
   cudaGraph_t g = nullptr;
+  cudaError_t launch_err = cudaSuccess;
   cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     SweepArgs<T> a;
@@ -712,12 +736,15 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
         a.items = R.d_plan + base + off[L];
         a.n = off[L + 1] - off[L];
         const unsigned nb = grid_for(a.n, kSweepThreads);
+        const bool pdl = L > 0;  // the first level of a batch follows a full dependency
+        cudaError_t le;
         switch (R.G) {
-          case 1: k_sweep_level<T, 1><<<nb, kSweepThreads, 0, cs>>>(a); break;
-          case 2: k_sweep_level<T, 2><<<nb, kSweepThreads, 0, cs>>>(a); break;
-          case 4: k_sweep_level<T, 4><<<nb, kSweepThreads, 0, cs>>>(a); break;
-          default: k_sweep_level<T, 0><<<nb, kSweepThreads, 0, cs>>>(a); break;
+          case 1: le = launch_level<T, 1>(a, nb, cs, pdl); break;
+          case 2: le = launch_level<T, 2>(a, nb, cs, pdl); break;
+          case 4: le = launch_level<T, 4>(a, nb, cs, pdl); break;
+          default: le = launch_level<T, 0>(a, nb, cs, pdl); break;
         }
+        if (le != cudaSuccess && launch_err == cudaSuccess) launch_err = le;
       }
       const unsigned nr = grid_for(c->N * nbd, 256);
       switch (R.G) {
@@ -730,6 +757,7 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
     }
     e = cudaStreamEndCapture(cs, &g);
   }
+  if (e == cudaSuccess) e = launch_err;
   if (e == cudaSuccess) e = cudaGraphInstantiate(&R.graph, g, 0);
   if (g) cudaGraphDestroy(g);
   cudaStreamDestroy(cs);
