@@ -22,7 +22,10 @@ rrhd_status scatter_fp64_cdg(const rrhd_dirs *d, const double *I, double *S, int
                              cudaStream_t st);
 rrhd_status moments_fp64_cdg(const rrhd_dirs *d, const double *I, double *E, double *F, double *T, int64_t cells,
                              int G, cudaStream_t st);
+// row_scales (may be NULL): the per-row power-of-two scales of the FP16 forms,
+// 2^(14 - floor(log2 max_d |I|)), when the caller has them already (the sweep's cell pass).
 rrhd_status scatter_tc_cdg(const rrhd_scatter_tc *t, const float *I, float *S, float *mom, int64_t cells, int G,
-                           cudaStream_t st);
+                           cudaStream_t st, const float *row_scales = nullptr);
+bool scatter_tc_scaled(const rrhd_scatter_tc *t);
 
 }  // namespace rrhd

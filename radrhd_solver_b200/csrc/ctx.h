@@ -55,6 +55,7 @@ struct RadState {
   // context numbering or -1), then the step's source record {k, betta/k, alpha Q_g/k}
   void *d_rec = nullptr;
   void *d_area = nullptr;  // [N][4] face areas
+  float *d_scale = nullptr;  // [N][G] row scales of the FP16 scattering, written by the cell pass
   uint32_t *d_plan = nullptr;               // all batches: items (cell << shift | d) in level order
   std::vector<std::vector<int64_t>> lvl;    // per batch: level offsets into d_plan
   int64_t levels = 0, max_level = 0;

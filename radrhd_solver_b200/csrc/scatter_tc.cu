@@ -680,7 +680,7 @@ extern "C" rrhd_status rrhd_scatter_tc_destroy(rrhd_scatter_tc *t) {
 // NG = 1: I, S are [rows][M]; NG = 2, 4: [rows / NG][M][NG] (row = cell * NG + group)
 template <int FORM, int NG>
 static rrhd_status launch_tc(const rrhd_scatter_tc *t, const float *I, float *S, float *mom, int64_t rows,
-                             cudaStream_t st) {
+                             const float *scales, cudaStream_t st) {
   constexpr int ng = NG;
   static bool attr = false;
   if (!attr) {
@@ -688,14 +688,14 @@ static rrhd_status launch_tc(const rrhd_scatter_tc *t, const float *I, float *S,
     attr = true;
   }
   constexpr bool SCALED = (FORM == FORM_F16X3 || FORM == FORM_F16);
-  if (SCALED) {
+  if (SCALED && !scales) {
     if (ng > 1)
       k_row_scale_cdg<<<(unsigned)((rows / ng + 7) / 8), 256, 0, st>>>(I, rows / ng, t->M, ng, t->d_scale);
     else
       k_row_scale<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(I, rows, t->M, t->d_scale);
     RRHD_CUDA(cudaGetLastError());
   }
-  TcParams P{I, S, mom, t->d_scale, rows, t->M, t->b_unscale, t->d_err};
+  TcParams P{I, S, mom, scales ? scales : t->d_scale, rows, t->M, t->b_unscale, t->d_err};
   CUtensorMap tm_a;
   {
     auto enc = get_encode();
@@ -718,8 +718,8 @@ static rrhd_status launch_tc(const rrhd_scatter_tc *t, const float *I, float *S,
 }
 
 static rrhd_status run_tc(const rrhd_scatter_tc *t, const float *I, float *S, float *mom, int64_t rows, int ng,
-                          cudaStream_t st) {
-  if ((t->form == FORM_F16X3 || t->form == FORM_F16) && t->scale_cap < rows) {
+                          const float *scales, cudaStream_t st) {
+  if ((t->form == FORM_F16X3 || t->form == FORM_F16) && !scales && t->scale_cap < rows) {
     rrhd_scatter_tc *tm = const_cast<rrhd_scatter_tc *>(t);
     RRHD_CUDA(cudaStreamSynchronize(st));
     cudaFree(tm->d_scale);
@@ -732,9 +732,9 @@ static rrhd_status run_tc(const rrhd_scatter_tc *t, const float *I, float *S, fl
                  "I, S and moments must be 16-byte aligned");
   switch (t->form * 3 + (ng == 4 ? 2 : ng == 2 ? 1 : 0)) {
 #define RRHD_TC_CASE(F)                                                        \
-  case 3 * F + 0: return launch_tc<F, 1>(t, I, S, mom, rows, st);           \
-  case 3 * F + 1: return launch_tc<F, 2>(t, I, S, mom, rows, st);           \
-  case 3 * F + 2: return launch_tc<F, 4>(t, I, S, mom, rows, st);
+  case 3 * F + 0: return launch_tc<F, 1>(t, I, S, mom, rows, scales, st);   \
+  case 3 * F + 1: return launch_tc<F, 2>(t, I, S, mom, rows, scales, st);   \
+  case 3 * F + 2: return launch_tc<F, 4>(t, I, S, mom, rows, scales, st);
     RRHD_TC_CASE(FORM_BF16X3)
     RRHD_TC_CASE(FORM_F16X3)
     RRHD_TC_CASE(FORM_F16)
@@ -745,19 +745,21 @@ static rrhd_status run_tc(const rrhd_scatter_tc *t, const float *I, float *S, fl
 }
 
 rrhd_status rrhd::scatter_tc_cdg(const rrhd_scatter_tc *t, const float *I, float *S, float *mom, int64_t cells,
-                                 int ng, cudaStream_t st) {
+                                 int ng, cudaStream_t st, const float *row_scales) {
   RRHD_CHECK_ARG(t && cells >= 0 && (ng == 1 || ng == 2 || ng == 4), "bad arguments");
   if (cells == 0) return RRHD_OK;
   RRHD_CHECK_ARG(I && S, "null I or S");
-  return run_tc(t, I, S, mom, cells * ng, ng, st);
+  return run_tc(t, I, S, mom, cells * ng, ng, row_scales, st);
 }
+
+bool rrhd::scatter_tc_scaled(const rrhd_scatter_tc *t) { return t->form == FORM_F16X3 || t->form == FORM_F16; }
 
 extern "C" rrhd_status rrhd_scatter_tc_run(const rrhd_scatter_tc *t, const float *I, float *S, float *mom,
                                            int64_t rows, void *stream) {
   RRHD_CHECK_ARG(t && rows >= 0, "bad arguments");
   if (rows == 0) return RRHD_OK;
   RRHD_CHECK_ARG(I && S, "null I or S");
-  return run_tc(t, I, S, mom, rows, 0, (cudaStream_t)stream);
+  return run_tc(t, I, S, mom, rows, 0, nullptr, (cudaStream_t)stream);
 }
 
 extern "C" rrhd_status rrhd_scatter_tc_run_cdg(const rrhd_scatter_tc *t, const float *I, float *S, float *mom,

@@ -94,6 +94,7 @@ struct SweepArgs {
   const T *rec;   // [N][RW]
   const T *area;  // [N][4] face areas (cell values)
   T *fv;         // [F][DB][GS] face values (GS >= G, full 32-byte sectors)
+  float *scale_out;  // cell pass: per-(cell, group) power-of-two scales for the FP16 scattering, or NULL
   T bc;
   int64_t last;
 };
@@ -420,6 +421,30 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
 #pragma unroll
       for (int q = 0; q < GT; q++) I[base + q * gs] = out[q];
     }
+    if constexpr (sizeof(T) == 4) {
+      if (a.scale_out) {
+        // one CTA is one cell (all its directions): the row scales of the FP16
+        // scattering, 2^(14 - floor(log2 max_d |I|)) per group, as the scattering's own
+        // pre-pass would compute them from the same values
+        __shared__ float s_max[256 / 32][GT];
+        float m[GT];
+#pragma unroll
+        for (int q = 0; q < GT; q++) {
+          m[q] = fabsf(out[q]);
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) m[q] = fmaxf(m[q], __shfl_xor_sync(0xffffffffu, m[q], o));
+        }
+        if ((threadIdx.x & 31) == 0)
+#pragma unroll
+          for (int q = 0; q < GT; q++) s_max[threadIdx.x >> 5][q] = m[q];
+        __syncthreads();
+        if (threadIdx.x < GT) {
+          float mg = 0.f;
+          for (int w = 0; w < (int)(blockDim.x >> 5); w++) mg = fmaxf(mg, s_max[w][threadIdx.x]);
+          a.scale_out[c * GT + threadIdx.x] = (mg > 0.f && isfinite(mg)) ? ldexpf(1.f, 14 - ilogbf(mg)) : 1.f;
+        }
+      }
+    }
   } else {
     for (int gg = 0; gg < a.G; gg++) {
       T fv[4];
@@ -723,6 +748,7 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
     a.rec = (const T *)R.d_rec;
     a.area = (const T *)R.d_area;
     a.fv = (T *)R.d_fv;
+    a.scale_out = R.d_scale;
     a.bc = (T)R.bc;
     a.last = R.last_cell;
     a.GS = R.GS;
@@ -770,7 +796,7 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
 void rrhd_rad_release(rrhd_ctx *c) {
   RadState &R = c->rad;
   if (R.graph) cudaGraphExecDestroy(R.graph);
-  void *ptrs[] = {R.d_w, R.d_rec, R.d_area, R.d_plan, R.d_io, R.d_fv, R.d_I, R.d_S, R.d_G4, R.d_mE, R.d_mF, R.d_mT,
+  void *ptrs[] = {R.d_w, R.d_rec, R.d_area, R.d_scale, R.d_plan, R.d_io, R.d_fv, R.d_I, R.d_S, R.d_G4, R.d_mE, R.d_mF, R.d_mT,
                   R.d_mom, R.d_cnt};
   for (void *p : ptrs) cudaFree(p);
   for (cudaEvent_t e : R.ev)
@@ -820,6 +846,11 @@ static rrhd_status rad_setup_t(rrhd_ctx *c) {
   for (int q = 0; q < 3 * R.M; q++) w[q] = (T)R.dirs->h_w[q];
   R.last_cell = iperm[N - 1];
   R.GS = sizeof(T) == 8 ? ((R.G + 3) & ~3) : ((R.G + 7) & ~7);
+  // the cell pass can hand the FP16 scattering its row scales when one CTA covers
+  // every direction of a cell: one batch of 256 directions, float, G in {1, 2, 4}
+  if (sizeof(T) == 4 && R.nbatch == 1 && R.M == 256 && (R.G == 1 || R.G == 2 || R.G == 4) &&
+      cudaMalloc(&R.d_scale, sizeof(float) * (size_t)N * R.G) != cudaSuccess)
+    return rrhd_fail(RRHD_ERR_OOM, "sweep allocation failed");
   auto up = [&](void **dst, const void *src, size_t bytes) -> rrhd_status {
     if (cudaMalloc(dst, bytes) != cudaSuccess) return rrhd_fail(RRHD_ERR_OOM, "sweep allocation failed");
     RRHD_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
@@ -1035,7 +1066,8 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
     if ((s = scatter_fp64_cdg(R.dirs, (const double *)R.d_I, (double *)R.d_S, N, R.G, false, st))) return s;
     if ((s = moments_fp64_cdg(R.dirs, (const double *)R.d_I, R.d_mE, R.d_mF, R.d_mT, N, R.G, st))) return s;
   } else {
-    if ((s = scatter_tc_cdg(R.tc, (const float *)R.d_I, (float *)R.d_S, R.d_mom, N, R.G, st))) return s;
+    const float *scales = (R.d_scale && scatter_tc_scaled(R.tc)) ? R.d_scale : nullptr;
+    if ((s = scatter_tc_cdg(R.tc, (const float *)R.d_I, (float *)R.d_S, R.d_mom, N, R.G, st, scales))) return s;
   }
   RRHD_CUDA(cudaEventRecord(R.ev[4], st));
   return hstat;

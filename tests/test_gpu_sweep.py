@@ -223,3 +223,27 @@ def test_coupled_chosen_form_tracks_plain():
     assert np.all(np.abs(Wc - Wp) <= 1e-10 * np.abs(Wp).max(0))
     assert dI <= 1e-4
     assert all(s[1].n_failed == 0 for s in sc)
+
+
+def test_coupled_chosen_row_scales_from_cell_pass():
+    """With one batch of 256 directions the sweep's cell pass hands the FP16 scattering
+    its row scales; the step is bit-identical to two batches of 128, where the
+    scattering computes them itself."""
+    m, W = jet(5)
+    W, U = oracle.port_p2c(W, 1, GAMMA_43)
+    d = fibonacci_directions(256)
+    out = []
+    for db in (256, 128):
+        g = rhllc.Grid(m, gamma=GAMMA_43)
+        g.set_boundary(-3, rhllc.BC_FIXED, JET_INFLOW)
+        g.set_state(W, U)
+        dg = illum.DirectionGrid(d)
+        sw = illum.TransportSweep(g, dg, groups=4, precision="fp32", dirs_per_batch=db)
+        step = rad_rhd.RadRHDStep(sw, em=rad_rhd.emission(*EM_JET), scatter="f16x3")
+        for _ in range(2):
+            step(0.3 * m.h_min)
+        Wg, Ug = g.get_state()
+        out.append((Ug, step.get("I"), step.get("S")))
+        g.close()
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
