@@ -111,6 +111,23 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(x: float, ws: int, device: str) -> float:
+    """The slowest rank's value (job time = max over ranks); every rank takes the
+    same collective step."""
+    if ws <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(units_per_rank: float, ws: int, steps: int, ms_max: float) -> float:
+    """Whole-job units per second: every replica processes units_per_rank per step."""
+    return ws * units_per_rank * steps / (ms_max / 1e3)
+
+
 def cpu_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -526,13 +543,9 @@ def run_ours(args):
     ms = e0.elapsed_time(e1)
     st = L.StepStats()
     L.check(L.lib.rrhd_hydro_step(g.handle, tau, ctypes.byref(st)))
-    ms_t = torch.tensor([ms], device=f"cuda:{dev}")
-    if ws > 1:
-        import torch.distributed as dist
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms = float(ms_t.item())
+    ms = max_over_ranks(ms, ws, f"cuda:{dev}")
     per_step = ms / args.steps
-    value = ws * m.n_cells * args.steps / (ms / 1e3)
+    value = job_throughput(m.n_cells, ws, args.steps, ms)
 
     # e2e through the host-buffer drop-in
     Wh = torch.empty((m.n_cells, 5), dtype=torch.float64).pin_memory()
@@ -546,11 +559,8 @@ def run_ours(args):
         L.check(L.lib.rrhd_hydro_step_host(g.handle, tau, Wh.data_ptr(), Uh.data_ptr(), 5, None))
     e1.record(stream)
     torch.cuda.synchronize()
-    ms_e = torch.tensor([e0.elapsed_time(e1)], device=f"cuda:{dev}")
-    if ws > 1:
-        import torch.distributed as dist
-        dist.all_reduce(ms_e, op=dist.ReduceOp.MAX)
-    e2e_value = ws * m.n_cells * e2e_steps / (float(ms_e.item()) / 1e3)
+    ms_e = max_over_ranks(e0.elapsed_time(e1), ws, f"cuda:{dev}")
+    e2e_value = job_throughput(m.n_cells, ws, e2e_steps, ms_e)
     io_bytes = 80 * m.n_cells
 
     # roofline of the fused step kernel (the only kernel in the step)
