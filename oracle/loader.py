@@ -100,6 +100,10 @@ def ref(variant: str) -> C.CDLL | None:
         "ref_eos": (C.c_int, []),
         "ref_get_illum": (D, [P, P, D, D]), "ref_get_rhs": (D, [D, D, D, D, P]),
         "ref_recalc_illum": (D, [I64, I64, P, P, P, I32, I32, P]),
+        "ref_write_solution": (C.c_int, [P, C.c_char_p]), "ref_write_geo": (C.c_int, [P, C.c_char_p, C.c_char_p]),
+        "ref_read_geo": (I64, [C.c_char_p, C.c_char_p, P, P, P, P, P, P, P, P, P]),
+        "ref_read_hllc_init": (I64, [C.c_char_p, P]), "ref_record_sizes": (C.c_int, [P]),
+        "ref_read_sphere_directions": (I64, [C.c_char_p, P, P, P]),
     }
     for n, (r, a) in sig.items():
         f = getattr(lib, n, None)
@@ -307,6 +311,17 @@ class HydroRef:
             return self.lib.ref_hydro_step_bc(self.h, tau, nthreads, _p(codes))
         return self.lib.ref_hydro_step(self.h, tau, nthreads)
 
+    def write_solution(self, directory):
+        """files_sys::bin::WriteSolution (lib/files_sys/src/writer_bin.cpp:56-114)
+        on this grid: density.bin, pressure.bin, velocity.bin under `directory`."""
+        d = os.path.join(directory, "")
+        os.makedirs(d, exist_ok=True)  # the reference's writer opens files only
+        return self.lib.ref_write_solution(self.h, d.encode())
+
+    def write_geo(self, faces_file, cells_file):
+        """files_sys::bin::WriteGridGeo of the face and cell records (writer_bin.h)."""
+        return self.lib.ref_write_geo(self.h, faces_file.encode(), cells_file.encode())
+
     def close(self):
         if self.h:
             self.lib.ref_hydro_destroy(self.h)
@@ -317,6 +332,54 @@ class HydroRef:
             self.close()
         except Exception:
             pass
+
+
+def ref_read_geo(faces_file, cells_file, variant="hydro_ideal_5_3"):
+    """files_sys::bin::ReadGridGeo of both geometry files
+    (lib/files_sys/include/reader_bin.h:113-135); returns a dict of the fields."""
+    lib = ref(variant)
+    nf = C.c_int64()
+    n = lib.ref_read_geo(faces_file.encode(), cells_file.encode(), C.byref(nf), *([None] * 8))
+    if n == 0:
+        raise OSError("ReadGridGeo failed")
+    F = nf.value
+    out = dict(face_id_l=np.zeros(F, np.int32), face_id_r=np.zeros(F, np.int32), face_n=np.zeros((F, 3)),
+               face_area=np.zeros(F), cell_faces=np.zeros((n, 4), np.int32), cell_sign=np.zeros(n, np.uint8),
+               cell_volume=np.zeros(n), cell_center=np.zeros((n, 3)))
+    lib.ref_read_geo(faces_file.encode(), cells_file.encode(), C.byref(nf), *(_p(out[k]) for k in
+                     ("face_id_l", "face_id_r", "face_n", "face_area", "cell_faces", "cell_sign", "cell_volume",
+                      "cell_center")))
+    return out
+
+
+def ref_read_hllc_init(path, variant="hydro_ideal_5_3"):
+    """files_sys::bin::ReadHllcInit (reader_bin.h:232-251); returns W [n,5]."""
+    lib = ref(variant)
+    n = lib.ref_read_hllc_init(path.encode(), None)
+    if n == 0:
+        raise OSError("ReadHllcInit failed")
+    W = np.zeros((n, 5))
+    lib.ref_read_hllc_init(path.encode(), _p(W))
+    return W
+
+
+def ref_read_sphere_directions(path, variant="hydro_ideal_5_3"):
+    """files_sys::txt::ReadSphereDirectionCartesian (reader_txt.cpp:6-37);
+    returns (dirs [M,3], areas [M], full_area)."""
+    lib = ref(variant)
+    M = lib.ref_read_sphere_directions(path.encode(), None, None, None)
+    if M < 0:
+        raise OSError("ReadSphereDirectionCartesian failed")
+    d, a, fa = np.zeros((M, 3)), np.zeros(M), C.c_double()
+    lib.ref_read_sphere_directions(path.encode(), _p(d), _p(a), C.byref(fa))
+    return d, a, fa.value
+
+
+def ref_record_sizes(variant="hydro_ideal_5_3"):
+    """sizeof(geo_face_t), sizeof(geo_cell_t), sizeof(flux_t) as compiled."""
+    out = np.zeros(3, np.int32)
+    ref(variant).ref_record_sizes(_p(out))
+    return tuple(int(x) for x in out)
 
 
 def ref_scatter(I, dirs, areas, full_area, nthreads=0):

@@ -26,6 +26,9 @@
 
 #if defined RRHD_SHIM_HYDRO
 #include "rhllc_calc.h"
+#include "reader_bin.h"
+#include "reader_txt.h"
+#include "writer_bin.h"
 #include "rhllc_flux_stab.h"
 #include "rhllc_flux.h"
 #include "rhllc_utils.h"
@@ -287,6 +290,76 @@ double ref_time_step(double cfl, double h_min, double max_speed) {
   rhllc::max_signal_speed = max_speed;
   std::vector<elem_t> none;
   return rhllc::GetTimeStep(cfg, none);
+}
+
+// The reference's own binary formats (lib/files_sys): the solution files of
+// files_sys::bin::WriteSolution (writer_bin.cpp:56-114), the geometry records of
+// WriteGridGeo / ReadGridGeo (writer_bin.h:95-117, reader_bin.h:113-135) and the hydro
+// initial state of ReadHllcInit (reader_bin.h:232-251).
+int ref_write_solution(void *p, const char *dir) {
+  return files_sys::bin::WriteSolution(std::string(dir), ((ref_hydro *)p)->grid);
+}
+int ref_write_geo(void *p, const char *faces_file, const char *cells_file) {
+  grid_t &g = ((ref_hydro *)p)->grid;
+  return files_sys::bin::WriteGridGeo(std::string(faces_file), g.faces) |
+         files_sys::bin::WriteGridGeo(std::string(cells_file), g.cells);
+}
+// reads both files into a fresh grid; returns the sizes (0 on failure) and copies the fields
+int64_t ref_read_geo(const char *faces_file, const char *cells_file, int64_t *n_faces, int32_t *face_id_l,
+                     int32_t *face_id_r, double *face_n, double *face_area, int32_t *cell_faces, uint8_t *cell_sign,
+                     double *cell_volume, double *cell_center) {
+  std::vector<face_t> faces;
+  std::vector<elem_t> cells;
+  if (files_sys::bin::ReadGridGeo(std::string(faces_file), faces) ||
+      files_sys::bin::ReadGridGeo(std::string(cells_file), cells))
+    return 0;
+  *n_faces = (int64_t)faces.size();
+  if (face_id_l) {
+    for (size_t f = 0; f < faces.size(); f++) {
+      face_id_l[f] = (int32_t)faces[f].geo.id_l;
+      face_id_r[f] = faces[f].geo.id_r;
+      for (int a = 0; a < 3; a++) face_n[3 * f + a] = faces[f].geo.n[a];
+      face_area[f] = faces[f].geo.S;
+    }
+    for (size_t c = 0; c < cells.size(); c++) {
+      for (int j = 0; j < 4; j++) cell_faces[4 * c + j] = cells[c].geo.id_faces[j];
+      cell_sign[c] = cells[c].geo.sign_n.bits;
+      cell_volume[c] = cells[c].geo.V;
+      for (int a = 0; a < 3; a++) cell_center[3 * c + a] = cells[c].geo.center[a];
+    }
+  }
+  return (int64_t)cells.size();
+}
+int64_t ref_read_hllc_init(const char *file, double *W) {
+  std::vector<elem_t> cells;
+  if (files_sys::bin::ReadHllcInit(std::string(file), cells)) return 0;
+  if (W)
+    for (size_t c = 0; c < cells.size(); c++) {
+      const flux_t &v = cells[c].phys_val;
+      W[5 * c] = v.d;
+      for (int a = 0; a < 3; a++) W[5 * c + 1 + a] = v.v[a];
+      W[5 * c + 4] = v.p;
+    }
+  return (int64_t)cells.size();
+}
+// files_sys::txt::ReadSphereDirectionCartesian (lib/files_sys/src/reader_txt.cpp:6-37):
+// returns the direction count (-1 on failure); dirs [M][3], areas [M], full_area.
+int64_t ref_read_sphere_directions(const char *file, double *dirs, double *areas, double *full_area) {
+  grid_directions_t gd;
+  if (files_sys::txt::ReadSphereDirectionCartesian(std::string(file), gd) != e_completion_success) return -1;
+  if (dirs)
+    for (int64_t i = 0; i < (int64_t)gd.size; i++) {
+      for (int a = 0; a < 3; a++) dirs[3 * i + a] = gd.directions[i].dir[a];
+      areas[i] = gd.directions[i].area;
+    }
+  if (full_area) *full_area = gd.full_area;
+  return (int64_t)gd.size;
+}
+int ref_record_sizes(int32_t *out) {
+  out[0] = (int32_t)sizeof(geo_face_t);
+  out[1] = (int32_t)sizeof(geo_cell_t);
+  out[2] = (int32_t)sizeof(flux_t);
+  return 0;
 }
 
 #endif  // RRHD_SHIM_HYDRO

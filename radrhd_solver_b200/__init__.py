@@ -3,7 +3,8 @@
 Native library: radrhd_solver_b200/librrhd.so (C ABI: include/rrhd.h).
 Modules mirror the reference's namespaces: `rhllc` (hydro step, con2prim),
 `illum` (scattering integral, moments), `rad_rhd` (radiation 4-force),
-`mesh` (synthetic meshes and direction sets).
+`mesh` (synthetic meshes and direction sets), `files_sys` (the reference's
+binary geometry, initial-state and solution files).
 
 Submodules load on first use, so `radrhd_solver_b200.build` runs on a tree
 where the library has not been built yet; every other submodule imports `_lib`,
@@ -11,10 +12,10 @@ which raises ImportError when librrhd.so is missing (there is no fallback).
 """
 import importlib
 
-__all__ = ["illum", "mesh", "rad_rhd", "rhllc"]
+__all__ = ["files_sys", "illum", "mesh", "rad_rhd", "rhllc"]
 
 
 def __getattr__(name):
-    if name in ("illum", "mesh", "rad_rhd", "rhllc", "coupled", "c2p_mlp", "scatter_tc", "sweep", "_lib"):
+    if name in ("illum", "mesh", "rad_rhd", "rhllc", "coupled", "c2p_mlp", "scatter_tc", "sweep", "files_sys", "_lib"):
         return importlib.import_module(f".{name}", __name__)
     raise AttributeError(name)

@@ -100,9 +100,14 @@ def fibonacci_directions(M: int) -> Directions:
 
 def read_sphere_directions(path: str) -> Directions:
     """Reads the reference's direction-sphere text format: N, then N lines of
-    `area x y z`, then full_area (lib/files_sys/src/reader_txt.cpp:6-24)."""
+    `area x y z`, then full_area (lib/files_sys/src/reader_txt.cpp:6-24).
+    A file with fewer values than announced is an error."""
     tok = open(path).read().split()
+    if not tok:
+        raise OSError(f"{path}: empty direction file")
     n = int(tok[0])
+    if n < 0 or len(tok) < 2 + 4 * n:
+        raise OSError(f"{path}: {n} directions announced, the file is shorter")
     vals = np.array([float(t) for t in tok[1:1 + 4 * n]]).reshape(n, 4)
     full = float(tok[1 + 4 * n])
     return Directions(np.ascontiguousarray(vals[:, 1:4]), np.ascontiguousarray(vals[:, 0]), full)

@@ -8,7 +8,8 @@ Every array in the .npz files is an input chosen here (seeded) or an output of
 the reference's own functions: GetConvValueStab / GetPhysValueStab /
 PhysPressureFix, GetFluxStab, Hllc3dStab, the scattering integral and the
 energy/stream/impulse moments, GetRadSource, GetIllum, GetRhsOpt and
-ReCalcIllumOpt.  The fixtures let the tests pin the oracle and the CUDA
+ReCalcIllumOpt.  tests/golden/files_sys/ holds files written by the reference's
+own files_sys::bin::WriteGridGeo and WriteSolution.  The fixtures let the tests pin the oracle and the CUDA
 library where the reference tree is absent.
 """
 from __future__ import annotations
@@ -151,6 +152,24 @@ def sweep_fixtures(out):
                               illum_cells_in=Ill0, illum_cells_out=Ill, recalc_norms=np.array(norms), emission=oracle.ref_rad_constants())
 
 
+def files_fixtures(out):
+    # boundary codes -1..-6 on the six box sides, plus an inflow disc (-3)
+    m = kuhn_box(2, 2, 2, jitter=0.15, seed=8, bc_codes=(-1, -2, -3, -4, -5, -6), inflow_radius=0.3,
+                 inflow_code=-7)
+    rng = np.random.default_rng(12)
+    W = np.stack([10 ** rng.uniform(-1, 1, m.n_cells), *rng.uniform(-.4, .4, (3, m.n_cells)),
+                  10 ** rng.uniform(-2, 0, m.n_cells)], 1)
+    W, U = oracle.ref_p2c(W, "hydro_ideal_5_3")
+    d = os.path.join(HERE, "files_sys")
+    os.makedirs(d, exist_ok=True)
+    h = oracle.HydroRef(m, "hydro_ideal_5_3")
+    h.set_state(W, U)
+    assert h.write_geo(os.path.join(d, "geo_faces.bin"), os.path.join(d, "geo_cells.bin")) == 0
+    assert h.write_solution(os.path.join(d, "Solve0")) == 0
+    h.close()
+    out["files_sys"] = mesh_arrays(m, "mesh_") | dict(W=W, U=U)
+
+
 def main():
     need = list(VARIANTS) + ["illum", "rad_ideal_4_3"]
     missing = [v for v in need if not oracle.have_ref(v)]
@@ -161,6 +180,7 @@ def main():
     step_fixtures(out)
     radiation_fixtures(out)
     sweep_fixtures(out)
+    files_fixtures(out)
     for name, arrays in out.items():
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **arrays)
         size = os.path.getsize(os.path.join(HERE, f"{name}.npz"))
