@@ -185,6 +185,7 @@ struct TcParams {
   int M;
   float b_unscale;
   int *err;
+  int b_copies;  // copies of the kernel matrix in global memory (resident kernel)
 };
 
 // Row scale for the scaled FP16 forms: 2^(14 - floor(log2(max_d |I[r][d]|))),
@@ -551,6 +552,470 @@ __global__ void __launch_bounds__(THREADS, 1)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Resident-tile kernel for M = 128 or 256 output directions.
+//
+// A CTA takes a tile of 128 rows and every output column.  The converter warps
+// split the tile's intensities once into hi/lo 16-bit K-major tiles that stay
+// in shared memory for the whole tile (M/64 chunks of 2 x 16 KiB); the MMA warp
+// then runs the output halves (128 directions each; the first carries the 16
+// moment columns in the same N = 144 product) over those chunks, so a row tile
+// is read and converted once whatever M is.  The intensities come straight
+// from global memory: 16-byte loads in which consecutive lanes read consecutive
+// addresses, one chunk prefetched in registers, then regrouped into rows with
+// lane shuffles (cell-direction-group layouts); the drain regroups the sums the
+// same way so that S leaves as 16-byte stores.  The kernel matrix streams
+// through a ring of 18 KiB stages, one 16-bit part per stage, and three TMEM
+// accumulators rotate between the MMA and the drain.  Per chunk and output half
+// the three products are issued cross terms first (hi x Bl, then lo x Bh) and
+// hi x Bh last into a fresh accumulator, so only the last four MMAs of a chunk
+// add to a sum of full size.
+//
+// Warp roles are whole warpgroups so that registers can move between them
+// (setmaxnreg): warpgroup 0 = TMA producer (warp 0), MMA issuer (warp 1) and two
+// idle warps, shrunk to R_REG_CTRL registers; warpgroups 1-2 = converters,
+// grown to R_REG_CONV; warpgroups 3-4 = accumulator drain, grown to R_REG_DRAIN.
+// The launcher checks the compiled register count against the sum first.
+constexpr int R_BST = 4;                     // kernel-matrix stages
+constexpr int R_KG = 1;                      // 64-direction chunks per accumulator group (2 measured slower,
+                                             // and its longer full-size sums less accurate)
+constexpr int R_BSTAGE = B_ROWS * BK * 2;    // 18 KiB: one 16-bit part, 144 rows x 64 directions
+constexpr int R_NACC = 3;                    // TMEM accumulators
+constexpr int R_ACC_STRIDE = 160;            // TMEM columns between accumulators (144 used)
+constexpr int R_GROUP = 2;                   // TMEM loads (x8) in flight per wait in the drain
+constexpr int R_THREADS = 640;               // 5 warpgroups
+constexpr int R_CONV0 = 4, R_DRAIN0 = 12;    // first converter / drain warp
+constexpr int R_REG_CTRL = 56, R_REG_CONV = 104, R_REG_DRAIN = 104;
+constexpr int R_COPIES = 1;                  // kernel-matrix copies in global memory (16 measured no faster)
+// registers the five warpgroups hold after the setmaxnreg split
+constexpr int R_REG_TOTAL = 128 * R_REG_CTRL + 256 * R_REG_CONV + 256 * R_REG_DRAIN;
+
+__host__ __device__ constexpr int r_smem_bytes(int nk) {
+  return 2 * nk * A_BYTES + R_BST * R_BSTAGE + 1024 /*align*/ + 256 /*barriers*/;
+}
+
+// Regroups the float4 a lane holds between quads (NG = 4) or pairs (NG = 2) of
+// lanes.  NG = 4 is a 4x4 transpose across the quad: lane p holds element
+// [p][0..3] and ends with [0..3][p] (groups of one direction -> directions of
+// one group, and back).  NG = 2: lane pairs hold {d g0, d g1, d+1 g0, d+1 g1};
+// the even lane ends with group 0, the odd with group 1 of directions 4m..4m+3.
+// NG = 1: rows are already direction-major.
+template <int NG>
+__device__ __forceinline__ void regroup(const float4 v, int lane, float (&x)[4]) {
+  if constexpr (NG == 1) {
+    x[0] = v.x;
+    x[1] = v.y;
+    x[2] = v.z;
+    x[3] = v.w;
+  } else if constexpr (NG == 2) {
+    const bool odd = lane & 1;
+    const float ra = __shfl_xor_sync(0xffffffffu, odd ? v.x : v.y, 1);
+    const float rb = __shfl_xor_sync(0xffffffffu, odd ? v.z : v.w, 1);
+    x[0] = odd ? ra : v.x;
+    x[1] = odd ? rb : v.z;
+    x[2] = odd ? v.y : ra;
+    x[3] = odd ? v.w : rb;
+  } else {
+    const bool b0 = lane & 1, b1 = lane & 2;
+    // stage 1, partner lane ^ 1: even lanes keep columns 0, 2; odd lanes keep 1, 3
+    const float ra = __shfl_xor_sync(0xffffffffu, b0 ? v.x : v.y, 1);
+    const float rb = __shfl_xor_sync(0xffffffffu, b0 ? v.z : v.w, 1);
+    const float y0 = b0 ? ra : v.x, y1 = b0 ? v.y : ra;
+    const float y2 = b0 ? rb : v.z, y3 = b0 ? v.w : rb;
+    // stage 2, partner lane ^ 2
+    const float sa = __shfl_xor_sync(0xffffffffu, b1 ? y0 : y2, 2);
+    const float sb = __shfl_xor_sync(0xffffffffu, b1 ? y1 : y3, 2);
+    x[0] = b1 ? sa : y0;
+    x[1] = b1 ? sb : y1;
+    x[2] = b1 ? y2 : sa;
+    x[3] = b1 ? y3 : sb;
+  }
+}
+
+// The inverse for the drain at NG = 2: the even lane holds group 0, the odd lane
+// group 1 of directions c..c+3; the even lane ends with {c g0, c g1, c+1 g0,
+// c+1 g1}, the odd one with directions c+2, c+3.
+__device__ __forceinline__ void ungroup2(const float (&v)[4], int lane, float (&x)[4]) {
+  const bool odd = lane & 1;
+  const float ra = __shfl_xor_sync(0xffffffffu, odd ? v[0] : v[2], 1);
+  const float rb = __shfl_xor_sync(0xffffffffu, odd ? v[1] : v[3], 1);
+  x[0] = odd ? ra : v[0];
+  x[1] = odd ? v[2] : ra;
+  x[2] = odd ? rb : v[1];
+  x[3] = odd ? v[3] : rb;
+}
+
+template <int FORM, int NG>
+__global__ void __launch_bounds__(R_THREADS, 1)
+    k_scatter_tc_res(const __grid_constant__ CUtensorMap tm_bh, const __grid_constant__ CUtensorMap tm_bl,
+                     const __grid_constant__ CUtensorMap tm_mh, const __grid_constant__ CUtensorMap tm_ml,
+                     const TcParams P) {
+  constexpr bool THREE = (FORM == FORM_BF16X3 || FORM == FORM_F16X3);
+  constexpr bool SCALED = (FORM == FORM_F16X3 || FORM == FORM_F16);
+  constexpr int FMT = (FORM == FORM_BF16X3 || FORM == FORM_BF16) ? 1 : 0;
+  constexpr int NPART = THREE ? 2 : 1;
+  constexpr int FPC = 16 * NG;   // float4 per cell and 64-direction chunk
+  constexpr int CPT = 128 / NG;  // cells per 128-row tile
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int nk = P.M / BK;  // 2 or 4 chunks
+  const int nS = NT;        // output directions per half
+  // the kernel-matrix copy this CTA reads (rows copy * (M + 16) .. of the replicated maps)
+  const int brow = (int)(blockIdx.x % (unsigned)P.b_copies) * (P.M + NMOM);
+  const int n_h = P.M / NT;
+  const bool mom = P.mom != nullptr;
+  uint8_t *a16 = smem;                         // [hi, lo][chunk][128 rows][128 B]
+  uint8_t *bst = smem + 2 * nk * A_BYTES;      // [R_BST][144 rows][128 B]
+  uint64_t *bars = reinterpret_cast<uint64_t *>(bst + R_BST * R_BSTAGE);
+  uint64_t *a_full = bars, *a_empty = bars + 4;
+  uint64_t *b_full = bars + 8, *b_empty = bars + 8 + R_BST;
+  uint64_t *acc_full = bars + 8 + 2 * R_BST, *acc_empty = acc_full + R_NACC;
+  uint64_t *mma_done = acc_empty + R_NACC;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mma_done + 1);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t n_rt = (P.rows + BM - 1) / BM;
+
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 4; k++) {
+      mbar_init(&a_full[k], CONV_WARPS);
+      mbar_init(&a_empty[k], 1);
+    }
+    for (int s = 0; s < R_BST; s++) {
+      mbar_init(&b_full[s], 1);
+      mbar_init(&b_empty[s], 1);
+    }
+    for (int b = 0; b < R_NACC; b++) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], ACC_WARPS);
+    }
+    mbar_init(mma_done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;\n" ::"r"(smem_u32(tmem_slot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  auto fail = [&]() {
+    *abort_flag = 1;
+    atomicOr(P.err, 1);
+  };
+
+  if (warp < R_CONV0) {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(R_REG_CTRL));
+    if (warp == 0 && lane == 0) {
+      // ---------------- kernel-matrix producer (TMA, one 16-bit part per stage)
+      int issued[R_BST] = {0};
+      int64_t s = 0;
+      bool ok = true;
+      // stage order per group: the R_KG chunks' lo parts, then their hi parts
+      for (int64_t rt = blockIdx.x; rt < n_rt && ok && !*abort_flag; rt += gridDim.x)
+        for (int h = 0; h < n_h && ok; h++)
+          for (int m = 0; m < nk / R_KG && ok; m++)
+            for (int pc = 0; pc < NPART * R_KG; pc++, s++) {
+              const int part = pc / R_KG, k = m * R_KG + pc % R_KG;
+              const int sb = (int)(s % R_BST);
+              if (s >= R_BST && !mbar_wait(&b_empty[sb], (uint32_t)((s / R_BST) - 1) & 1)) {
+                fail();
+                ok = false;
+                break;
+              }
+              if (*abort_flag) {
+                ok = false;
+                break;
+              }
+              const bool lo = THREE && part == 0;
+              const bool wm = (h == 0) && mom;
+              uint8_t *dst = bst + sb * R_BSTAGE;
+              mbar_arrive_expect_tx(&b_full[sb], (uint32_t)((nS + (wm ? NMOM : 0)) * BK * 2));
+              tma_load_2d(dst, lo ? &tm_bl : &tm_bh, k * BK, brow + h * nS, &b_full[sb]);
+              if (wm) tma_load_2d(dst + nS * 128, lo ? &tm_ml : &tm_mh, k * BK, brow + P.M, &b_full[sb]);
+              issued[sb]++;
+            }
+      // no copy may still be in flight when the CTA retires (bounded)
+      for (int sb = 0; sb < R_BST; sb++)
+        if (issued[sb] && !mbar_wait(&b_full[sb], (issued[sb] - 1) & 1)) fail();
+    } else if (warp == 1 && lane == 0) {
+      // ---------------- MMA issuer: group (tile, half, chunk) -> accumulator g % R_NACC, fresh each group
+      const uint64_t ddesc = umma_desc(0);
+      const uint32_t a16_u32 = smem_u32(a16), bst_u32 = smem_u32(bst);
+      int64_t s = 0, g = 0, ti = 0;
+      bool ok = true;
+      for (int64_t rt = blockIdx.x; rt < n_rt && ok && !*abort_flag; rt += gridDim.x, ti++)
+        for (int h = 0; h < n_h && ok; h++) {
+          const uint32_t idesc = umma_idesc(FMT, nS + ((h == 0 && mom) ? NMOM : 0));
+          for (int m = 0; m < nk / R_KG && ok; m++, g++) {
+            const int ab = (int)(g % R_NACC);
+            bool got = true;
+            if (h == 0)
+              for (int c = 0; c < R_KG; c++) got = got && mbar_wait(&a_full[m * R_KG + c], (uint32_t)(ti & 1));
+            if (!got || (g >= R_NACC && !mbar_wait(&acc_empty[ab], (uint32_t)((g / R_NACC) - 1) & 1))) {
+              fail();
+              ok = false;
+              break;
+            }
+            if (*abort_flag) {
+              ok = false;
+              break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t acc = tmem + ab * R_ACC_STRIDE;
+            // descriptors: constant fields | (address >> 4); the K step of 16 elements
+            // (32 bytes) adds 2 to the address field inside a 1 KiB-aligned tile
+            auto a_hi = [&](int c) { return ddesc | (uint64_t)((a16_u32 + (m * R_KG + c) * A_BYTES) >> 4); };
+            auto a_lo = [&](int c) { return ddesc | (uint64_t)((a16_u32 + (nk + m * R_KG + c) * A_BYTES) >> 4); };
+            auto b_at = [&](int64_t ss) { return ddesc | (uint64_t)((bst_u32 + (int)(ss % R_BST) * R_BSTAGE) >> 4); };
+            auto b_wait = [&](int64_t ss) {
+              if (!mbar_wait(&b_full[ss % R_BST], (uint32_t)(ss / R_BST) & 1)) {
+                fail();
+                ok = false;
+                return false;
+              }
+              asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+              return true;
+            };
+            const int64_t s0 = s;
+            if (THREE) {
+              // cross terms of every chunk of the group first (hi x Bl, lo x Bh), hi x Bh last
+              for (int c = 0; c < R_KG && ok; c++) {
+                if (!b_wait(s0 + c)) break;
+#pragma unroll
+                for (int kk = 0; kk < BK / 16; kk++)
+                  umma(acc, a_hi(c) + 2 * kk, b_at(s0 + c) + 2 * kk, idesc,
+                       (c > 0 || kk > 0) ? 1u : 0u);
+              }
+              if (!ok) break;
+              for (int c = 0; c < R_KG; c++) umma_commit(&b_empty[(s0 + c) % R_BST]);
+              for (int c = 0; c < R_KG && ok; c++) {
+                if (!b_wait(s0 + R_KG + c)) break;
+#pragma unroll
+                for (int kk = 0; kk < BK / 16; kk++)
+                  umma(acc, a_lo(c) + 2 * kk, b_at(s0 + R_KG + c) + 2 * kk, idesc, 1u);
+              }
+              if (!ok) break;
+              for (int c = 0; c < R_KG; c++)
+#pragma unroll
+                for (int kk = 0; kk < BK / 16; kk++)
+                  umma(acc, a_hi(c) + 2 * kk, b_at(s0 + R_KG + c) + 2 * kk, idesc, 1u);
+              for (int c = 0; c < R_KG; c++) umma_commit(&b_empty[(s0 + R_KG + c) % R_BST]);
+              s += 2 * R_KG;
+            } else {
+              for (int c = 0; c < R_KG && ok; c++) {
+                if (!b_wait(s0 + c)) break;
+#pragma unroll
+                for (int kk = 0; kk < BK / 16; kk++)
+                  umma(acc, a_hi(c) + 2 * kk, b_at(s0 + c) + 2 * kk, idesc,
+                       (c > 0 || kk > 0) ? 1u : 0u);
+                umma_commit(&b_empty[(s0 + c) % R_BST]);
+              }
+              if (!ok) break;
+              s += R_KG;
+            }
+            umma_commit(&acc_full[ab]);
+            if (h == n_h - 1)
+              for (int c = 0; c < R_KG; c++) umma_commit(&a_empty[m * R_KG + c]);
+          }
+        }
+      // every issued MMA has completed before TMEM is released (bounded)
+      if (s > 0) {
+        umma_commit(mma_done);
+        if (!mbar_wait(mma_done, 0)) fail();
+      }
+    }
+  } else if (warp < R_DRAIN0) {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(R_REG_CONV));
+    // ---------------- converters: chunk (tile, k) from global memory -> hi/lo tiles in smem
+    const int t = threadIdx.x - 32 * R_CONV0;
+    const int off = t % FPC;                  // float4 within a cell's chunk
+    const int c4 = off / NG;                  // direction quad of the row after regrouping
+    const int gsel = t & (NG - 1);            // group of the row after regrouping
+    const int64_t ncell = P.rows / NG;
+    const int64_t cstride = (int64_t)P.M * NG / 4;  // float4 per cell
+    const float4 *I4 = reinterpret_cast<const float4 *>(P.I);
+    const int64_t my_tiles = n_rt > blockIdx.x ? (n_rt - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const int64_t nchunks = my_tiles * nk;
+    auto cellrel = [&](int j) { return j * (256 / FPC) + t / FPC; };
+    // tiles start on even chunk numbers (nk is 2 or 4), so the scales of a tile
+    // always arrive with buffer A; row scales are powers of two, kept as their
+    // 8-bit biased exponents, four per word
+    float4 bufA[8], bufB[8];
+    uint32_t scA[2], sc[2];
+    auto scale_of = [&](const uint32_t (&e)[2], int j) {
+      return __uint_as_float(((e[j >> 2] >> (8 * (j & 3))) & 0xffu) << 23);
+    };
+    auto load = [&](int64_t gc, float4 (&buf)[8], bool with_scales) {
+      const int64_t rt = blockIdx.x + (gc / nk) * gridDim.x;
+      const int k = (int)(gc % nk);
+      const int64_t cell0 = rt * CPT;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const int64_t c = cell0 + cellrel(j);
+        buf[j] = c < ncell ? __ldcs(I4 + c * cstride + k * FPC + off) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      if (SCALED && with_scales && k == 0) {
+        scA[0] = scA[1] = 0u;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const int64_t r = (cell0 + cellrel(j)) * NG + gsel;
+          const float v = r < P.rows ? __ldg(P.scale + r) : 1.f;
+          scA[j >> 2] |= ((__float_as_uint(v) >> 23) & 0xffu) << (8 * (j & 3));
+        }
+      }
+    };
+    auto process = [&](int64_t gc, const float4 (&buf)[8]) -> bool {
+      const int64_t ti = gc / nk;
+      const int k = (int)(gc % nk);
+      if (SCALED && k == 0) {
+        sc[0] = scA[0];
+        sc[1] = scA[1];
+      }
+      // decisions stay warp-uniform: the regrouping below shuffles across lanes
+      const bool waited = ti == 0 || mbar_wait(&a_empty[k], (uint32_t)((ti - 1) & 1));
+      if (!__all_sync(0xffffffffu, waited)) {
+        fail();
+        return false;
+      }
+      if (__any_sync(0xffffffffu, *abort_flag != 0)) return false;
+      uint8_t *ah = a16 + k * A_BYTES, *al = a16 + (nk + k) * A_BYTES;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        float x[4];
+        regroup<NG>(buf[j], lane, x);
+        if (SCALED) {
+          const float f = scale_of(sc, j);
+#pragma unroll
+          for (int q = 0; q < 4; q++) x[q] *= f;
+        }
+        uint16_t hv[4], lv[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) Split<FORM>::run(x[q], hv[q], lv[q]);
+        const int row = cellrel(j) * NG + gsel;
+        const uint32_t o = row * 128 + ((((c4 >> 1) ^ (row & 7))) << 4) + ((c4 & 1) << 3);
+        *reinterpret_cast<uint2 *>(ah + o) =
+            make_uint2((uint32_t)hv[0] | ((uint32_t)hv[1] << 16), (uint32_t)hv[2] | ((uint32_t)hv[3] << 16));
+        if (THREE)
+          *reinterpret_cast<uint2 *>(al + o) =
+              make_uint2((uint32_t)lv[0] | ((uint32_t)lv[1] << 16), (uint32_t)lv[2] | ((uint32_t)lv[3] << 16));
+      }
+      // every lane's generic-proxy writes become visible to the MMA (async proxy)
+      // before the warp's one arrival
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&a_full[k]);
+      return true;
+    };
+    if (nchunks > 0) load(0, bufA, true);
+    for (int64_t gc = 0; gc < nchunks; gc += 2) {
+      if (gc + 1 < nchunks) load(gc + 1, bufB, false);
+      if (!process(gc, bufA)) break;
+      if (gc + 2 < nchunks) load(gc + 2, bufA, true);
+      if (gc + 1 < nchunks && !process(gc + 1, bufB)) break;
+    }
+  } else {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(R_REG_DRAIN));
+    // ---------------- accumulator warps: warp w reads TMEM lanes 32*(w%4)..+31 (one row
+    // per thread); the first four take the first half of the columns, the others the second
+    const int q = warp & 3, hf = (warp - R_DRAIN0) >> 2;
+    const int row = q * 32 + lane;
+    const int64_t ncell = P.rows / NG;
+    int64_t g = 0;
+    bool ok = true;
+    for (int64_t rt = blockIdx.x; rt < n_rt && ok && !*abort_flag; rt += gridDim.x) {
+      const int64_t gr = rt * BM + row;
+      const int64_t cell = gr / NG;  // the quad (pair) of lanes holding one cell's groups
+      // the row's unscale factor, loaded before the sums arrive
+      const float inv = (SCALED ? 1.f / (gr < P.rows ? __ldg(P.scale + gr) : 1.f) : 1.f) * P.b_unscale;
+      for (int h = 0; h < n_h && ok; h++) {
+        const bool with_mom = (h == 0) && mom;
+        const int half = (nS + (with_mom ? NMOM : 0)) >> 1;  // multiple of 8
+        const int c0 = hf * half;
+        float run[MAX_HALF];
+#pragma unroll
+        for (int j = 0; j < MAX_HALF; j++) run[j] = 0.f;
+        for (int m = 0; m < nk / R_KG; m++, g++) {
+          const int ab = (int)(g % R_NACC);
+          const bool got = mbar_wait(&acc_full[ab], (uint32_t)(g / R_NACC) & 1);
+          if (!__all_sync(0xffffffffu, got)) {
+            fail();
+            ok = false;
+            break;
+          }
+          if (__any_sync(0xffffffffu, *abort_flag != 0)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+          const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * R_ACC_STRIDE + c0);
+#pragma unroll
+          for (int j0 = 0; j0 < MAX_HALF / 8; j0 += R_GROUP) {
+            uint32_t r[R_GROUP][8];
+#pragma unroll
+            for (int jj = 0; jj < R_GROUP; jj++)
+              if ((j0 + jj) * 8 < half)
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                             : "=r"(r[jj][0]), "=r"(r[jj][1]), "=r"(r[jj][2]), "=r"(r[jj][3]), "=r"(r[jj][4]),
+                               "=r"(r[jj][5]), "=r"(r[jj][6]), "=r"(r[jj][7])
+                             : "r"(base + (j0 + jj) * 8));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+            for (int jj = 0; jj < R_GROUP; jj++)
+              if ((j0 + jj) * 8 < half)
+#pragma unroll
+                for (int i = 0; i < 8; i++)
+                  run[(j0 + jj) * 8 + i] = __fadd_rn(run[(j0 + jj) * 8 + i], __uint_as_float(r[jj][i]));
+          }
+          asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acc_empty[ab]);
+        }
+        if (!ok) break;
+        // every lane takes part in the regrouping shuffles; stores are guarded per cell.
+        // so: this lane's first output (direction h*nS + c0 + its quad / pair slot)
+        float *so = P.S + (NG == 4 ? (cell * P.M + h * nS + c0 + (lane & 3)) * 4
+                                   : NG == 2 ? (cell * P.M + h * nS + c0 + 2 * (lane & 1)) * 2
+                                             : gr * P.M + h * nS + c0);
+        const bool row_ok = NG > 1 ? cell < ncell : gr < P.rows;
+#pragma unroll
+        for (int j = 0; j < MAX_HALF / 4; j++) {
+          const int col = c0 + 4 * j;
+          if (4 * j < half) {
+            float v[4] = {run[4 * j] * inv, run[4 * j + 1] * inv, run[4 * j + 2] * inv, run[4 * j + 3] * inv};
+            if (col < nS) {
+              if constexpr (NG == 4) {
+                // lane (cell, g) holds group g of directions n..n+3 -> lane (cell, p): direction n+p, groups 0..3
+                float x[4];
+                regroup<4>(make_float4(v[0], v[1], v[2], v[3]), lane, x);
+                if (row_ok) __stcs(reinterpret_cast<float4 *>(so + 16 * j), make_float4(x[0], x[1], x[2], x[3]));
+              } else if constexpr (NG == 2) {
+                float x[4];
+                ungroup2(v, lane, x);
+                if (row_ok) __stcs(reinterpret_cast<float4 *>(so + 8 * j), make_float4(x[0], x[1], x[2], x[3]));
+              } else {
+                if (row_ok) __stcs(reinterpret_cast<float4 *>(so + 4 * j), make_float4(v[0], v[1], v[2], v[3]));
+              }
+            } else if (gr < P.rows) {
+              *reinterpret_cast<float4 *>(P.mom + gr * NMOM + (col - nS)) = make_float4(v[0], v[1], v[2], v[3]);
+            }
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(tmem));
+  }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -569,8 +1034,13 @@ struct rrhd_scatter_tc {
   int device = 0;
   int form = 0;
   int M = 0;
-  uint16_t *d_bh = nullptr, *d_bl = nullptr;  // [M + 16][M] 16-bit, row n = output column n
-  CUtensorMap tm_bh, tm_bl, tm_mh, tm_ml;
+  // [copies][M + 16][M] 16-bit, row n = output column n.  The resident kernel
+  // reads copy blockIdx % copies (R_COPIES, one by default: spreading the CTAs
+  // over 16 copies measured no faster).
+  uint16_t *d_bh = nullptr, *d_bl = nullptr;
+  int copies = 1;
+  CUtensorMap tm_bh, tm_bl, tm_mh, tm_ml;          // copy 0 (two-pass kernel)
+  CUtensorMap tr_bh, tr_bl, tr_mh, tr_ml;          // all copies (resident kernel)
   float b_unscale = 1.f;
   int *d_err = nullptr;
   float *d_scale = nullptr;  // row scales of the FP16 forms (grown on demand)
@@ -631,8 +1101,9 @@ extern "C" rrhd_status rrhd_scatter_tc_create(const rrhd_dirs *d, int32_t form, 
   t->M = M;
   t->b_unscale = (float)(1.0 / bscale);
   cudaDeviceGetAttribute(&t->num_sms, cudaDevAttrMultiProcessorCount, d->device);
+  t->copies = (M == 128 || M == 256) ? R_COPIES : 1;
   const size_t bytes = sizeof(uint16_t) * bh.size();
-  if (cudaMalloc(&t->d_bh, bytes) != cudaSuccess || cudaMalloc(&t->d_bl, bytes) != cudaSuccess ||
+  if (cudaMalloc(&t->d_bh, bytes * t->copies) != cudaSuccess || cudaMalloc(&t->d_bl, bytes * t->copies) != cudaSuccess ||
       cudaMalloc(&t->d_err, sizeof(int)) != cudaSuccess) {
     cudaFree(t->d_bh);
     cudaFree(t->d_bl);
@@ -640,8 +1111,10 @@ extern "C" rrhd_status rrhd_scatter_tc_create(const rrhd_dirs *d, int32_t form, 
     delete t;
     return rrhd_fail(RRHD_ERR_OOM, "tensor-core operand allocation failed");
   }
-  cudaMemcpy(t->d_bh, bh.data(), bytes, cudaMemcpyHostToDevice);
-  cudaMemcpy(t->d_bl, bl.data(), bytes, cudaMemcpyHostToDevice);
+  for (int c = 0; c < t->copies; c++) {
+    cudaMemcpy(t->d_bh + (size_t)c * bh.size(), bh.data(), bytes, cudaMemcpyHostToDevice);
+    cudaMemcpy(t->d_bl + (size_t)c * bl.size(), bl.data(), bytes, cudaMemcpyHostToDevice);
+  }
   cudaMemset(t->d_err, 0, sizeof(int));
   const CUtensorMapDataType dt = f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
   auto make = [&](CUtensorMap *m, uint16_t *base, int rows_total, int box_rows, int row0) -> bool {
@@ -655,7 +1128,9 @@ extern "C" rrhd_status rrhd_scatter_tc_create(const rrhd_dirs *d, int32_t form, 
   };
   const int box_n = M < NT ? M : NT;
   if (!make(&t->tm_bh, t->d_bh, M, box_n, 0) || !make(&t->tm_bl, t->d_bl, M, box_n, 0) ||
-      !make(&t->tm_mh, t->d_bh, NMOM, NMOM, M) || !make(&t->tm_ml, t->d_bl, NMOM, NMOM, M)) {
+      !make(&t->tm_mh, t->d_bh, NMOM, NMOM, M) || !make(&t->tm_ml, t->d_bl, NMOM, NMOM, M) ||
+      !make(&t->tr_bh, t->d_bh, t->copies * NB, box_n, 0) || !make(&t->tr_bl, t->d_bl, t->copies * NB, box_n, 0) ||
+      !make(&t->tr_mh, t->d_bh, t->copies * NB, NMOM, 0) || !make(&t->tr_ml, t->d_bl, t->copies * NB, NMOM, 0)) {
     cudaFree(t->d_bh);
     cudaFree(t->d_bl);
     cudaFree(t->d_err);
@@ -695,7 +1170,26 @@ static rrhd_status launch_tc(const rrhd_scatter_tc *t, const float *I, float *S,
       k_row_scale<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(I, rows, t->M, t->d_scale);
     RRHD_CUDA(cudaGetLastError());
   }
-  TcParams P{I, S, mom, scales ? scales : t->d_scale, rows, t->M, t->b_unscale, t->d_err};
+  TcParams P{I, S, mom, scales ? scales : t->d_scale, rows, t->M, t->b_unscale, t->d_err, t->copies};
+  // M = 128 or 256: one CTA per 128-row tile and all output columns, converted
+  // intensity resident.  Its warpgroups move registers between them (setmaxnreg);
+  // the kernel is used only if the registers it is launched with cover the split.
+  static int res_ok = -1;
+  if (res_ok < 0) {
+    cudaFuncAttributes fa;
+    res_ok = cudaFuncGetAttributes(&fa, k_scatter_tc_res<FORM, NG>) == cudaSuccess &&
+             fa.numRegs * R_THREADS >= R_REG_TOTAL &&
+             cudaFuncSetAttribute(k_scatter_tc_res<FORM, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  r_smem_bytes(4)) == cudaSuccess;
+    cudaGetLastError();
+  }
+  if (res_ok && (t->M == 128 || t->M == 256)) {
+    const unsigned grid = (unsigned)std::min<int64_t>((rows + BM - 1) / BM, t->num_sms);
+    k_scatter_tc_res<FORM, NG><<<grid, R_THREADS, r_smem_bytes(t->M / BK), st>>>(t->tr_bh, t->tr_bl, t->tr_mh,
+                                                                                t->tr_ml, P);
+    RRHD_CUDA(cudaGetLastError());
+    return RRHD_OK;
+  }
   CUtensorMap tm_a;
   {
     auto enc = get_encode();
