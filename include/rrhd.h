@@ -362,7 +362,10 @@ rrhd_status rrhd_sweep(rrhd_ctx *ctx, const void *alpha, const void *betta, cons
  * asynchronously at the start of each radiation iteration, before the sweep,
  * illum_multi_gpu_face_calc.cpp:59-66) added as U.E += tau G0, U.S += tau G,
  * then con2prim without fallback; finally the scattering integral and moments
- * of the new intensity for the next step. */
+ * of the new intensity for the next step.  The 4-force and the source con2prim
+ * share no data with the sweep and run on a second stream beside it; the call
+ * joins that stream before the scattering, so the context's stream orders
+ * everything that follows. */
 #define RRHD_SCATTER_FP64 (-1) /* rrhd_scatter_fp64_fma + rrhd_moments_fp64 (RRHD_RAD_FP64) */
 typedef struct {
   int32_t scatter;        /* RRHD_SCATTER_FP64, or an RRHD_TC_* form (RRHD_RAD_FP32)             */
@@ -377,8 +380,9 @@ typedef struct {
  * of the source con2prim; either one synchronises the stream. */
 rrhd_status rrhd_coupled_step(rrhd_ctx *ctx, double tau, const rrhd_coupled_opts *opts, rrhd_step_stats *hydro,
                               rrhd_c2p_stats *source);
-/* Device time (ms) of the phases of the last coupled step: hydro step; opacities
- * + sweep; 4-force + source con2prim; scattering + moments.  Synchronises. */
+/* Device time (ms) of the phases of the last coupled step: hydro step + opacities;
+ * sweep; 4-force + source con2prim (on a second stream, concurrent with the sweep,
+ * so it is not added to the step time); scattering + moments.  Synchronises. */
 rrhd_status rrhd_coupled_phase_ms(rrhd_ctx *ctx, float *ms4);
 /* Host copies (caller cell numbering, double) of the coupled step's radiation
  * arrays: RRHD_RAD_I / RRHD_RAD_S [N*G][M], RRHD_RAD_G4 [N][4] (4-force of the

@@ -63,7 +63,10 @@ struct RadState {
   SweepIO *d_io = nullptr;
   SweepIO h_io{};       // last pointers uploaded to d_io
   bool io_valid = false;
-  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // phase marks of the last coupled step
+  // phase marks of the last coupled step: 0 start, 1 hydro done, 2 sweep done, 3 source
+  // start and 4 source done (side stream), 5 join, 6 scattering done
+  cudaEvent_t ev[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  cudaStream_t side = nullptr;  // the coupled step's source term runs here, beside the sweep
   void *d_fv = nullptr;  // [F][DB][GS] face values
   // coupled step (context numbering, [N][M][G])
   void *d_I = nullptr, *d_S = nullptr;

@@ -801,6 +801,7 @@ void rrhd_rad_release(rrhd_ctx *c) {
   for (void *p : ptrs) cudaFree(p);
   for (cudaEvent_t e : R.ev)
     if (e) cudaEventDestroy(e);
+  if (R.side) cudaStreamDestroy(R.side);
   if (R.tc) rrhd_scatter_tc_destroy(R.tc);
   R = RadState();
 }
@@ -974,6 +975,7 @@ static rrhd_status alloc_coupled(rrhd_ctx *c) {
       cudaMalloc(&R.d_cnt, sizeof(unsigned long long) * 8) != cudaSuccess)
     return rrhd_fail(RRHD_ERR_OOM, "coupled-step allocation failed");
   for (cudaEvent_t &e : R.ev) RRHD_CUDA(cudaEventCreate(&e));
+  RRHD_CUDA(cudaStreamCreateWithFlags(&R.side, cudaStreamNonBlocking));
   RRHD_CUDA(cudaMemsetAsync(R.d_I, 0, big, c->stream));
   RRHD_CUDA(cudaMemsetAsync(R.d_S, 0, big, c->stream));
   RRHD_CUDA(cudaMemsetAsync(R.d_G4, 0, sizeof(double) * 4 * N, c->stream));
@@ -1017,6 +1019,8 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
   }
   cudaStream_t st = c->stream;
   const int64_t N = c->N;
+  // a previous step that returned early may have left its source term on the side stream
+  RRHD_CUDA(cudaStreamWaitEvent(st, R.ev[4], 0));
   RRHD_CUDA(cudaEventRecord(R.ev[0], st));
   // 1. hydro step (flux, update, con2prim with fallback)
   rrhd_step_stats hst;
@@ -1026,7 +1030,7 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
   RRHD_CUDA(cudaEventRecord(R.ev[1], st));
   double *state = c->d_state[c->cur];
   const Emission em{o->emission.temp_coef, o->emission.sigma_sb, o->emission.pi, o->emission.rad_unit};
-  // 2. opacities and emission from the new primitives, 3. sweep with the previous scattering integral
+  // 2. opacities and emission from the new primitives
   if (fp64)
     k_dyn_from_state<double><<<grid_for(N, 256), 256, 0, st>>>(N, R.G, R.RW, state, o->absorption, o->scattering,
                                                                 em, (double *)R.d_rec);
@@ -1034,33 +1038,43 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
     k_dyn_from_state<float><<<grid_for(N, 256), 256, 0, st>>>(N, R.G, R.RW, state, o->absorption, o->scattering, em,
                                                                (float *)R.d_rec);
   RRHD_CUDA(cudaGetLastError());
-  SweepIO io{R.d_S, R.d_I, nullptr, 1};
-  if ((s = launch_sweep(c, io))) return s;
-  RRHD_CUDA(cudaEventRecord(R.ev[2], st));
-  // 4. 4-force from the previous intensity's moments, source con2prim
-  k_source<<<grid_for(N, 128), 128, 0, st>>>(N, R.G, state, o->absorption, o->scattering, em, R.d_mE, R.d_mF, R.d_mT,
-                                              R.d_mom, R.d_G4);
+  // 4. 4-force from the previous intensity's moments and the source con2prim, on the side
+  // stream beside the sweep: they read the state after the opacities were taken from it and
+  // the previous step's moments, and write the state and G4, none of which the sweep touches.
+  RRHD_CUDA(cudaEventRecord(R.ev[3], st));
+  RRHD_CUDA(cudaStreamWaitEvent(R.side, R.ev[3], 0));
+  const cudaStream_t ss_st = R.side;
+  k_source<<<grid_for(N, 128), 128, 0, ss_st>>>(N, R.G, state, o->absorption, o->scattering, em, R.d_mE, R.d_mF,
+                                                 R.d_mT, R.d_mom, R.d_G4);
   RRHD_CUDA(cudaGetLastError());
   if (o->guess) {
     if ((s = mlp_c2p(o->guess, c->eos, c->gamma, state, state + 5, 10, R.d_G4, tau, nullptr, N, 0, k_stall, ss,
-                     nullptr, nullptr, st)))
+                     nullptr, nullptr, ss_st)))
       return s;
   } else {
-    RRHD_CUDA(cudaMemsetAsync(R.d_cnt, 0, sizeof(unsigned long long) * 8, st));
-    k_source_c2p<<<grid_for(N, 256), 256, 0, st>>>(N, eos_of(c), state, R.d_G4, tau, R.d_cnt);
+    RRHD_CUDA(cudaMemsetAsync(R.d_cnt, 0, sizeof(unsigned long long) * 8, ss_st));
+    k_source_c2p<<<grid_for(N, 256), 256, 0, ss_st>>>(N, eos_of(c), state, R.d_G4, tau, R.d_cnt);
     RRHD_CUDA(cudaGetLastError());
-    if (ss) {
-      unsigned long long h[8];
-      RRHD_CUDA(cudaMemcpyAsync(h, R.d_cnt, sizeof h, cudaMemcpyDeviceToHost, st));
-      RRHD_CUDA(cudaStreamSynchronize(st));
-      ss->n_ok = (int64_t)h[0];
-      ss->n_fallback = 0;
-      ss->n_failed = (int64_t)h[1];
-      ss->newton_iters = (int64_t)h[2];
-      ss->max_iters = (int32_t)h[3];
-    }
   }
-  RRHD_CUDA(cudaEventRecord(R.ev[3], st));
+  RRHD_CUDA(cudaEventRecord(R.ev[4], ss_st));
+  // 3. sweep with the previous scattering integral
+  SweepIO io{R.d_S, R.d_I, nullptr, 1};
+  if ((s = launch_sweep(c, io))) return s;
+  RRHD_CUDA(cudaEventRecord(R.ev[2], st));
+  // the scattering below overwrites the moments the source read, and the next step reads
+  // the state the source wrote: join the side stream
+  RRHD_CUDA(cudaStreamWaitEvent(st, R.ev[4], 0));
+  RRHD_CUDA(cudaEventRecord(R.ev[5], st));
+  if (!o->guess && ss) {
+    unsigned long long h[8];
+    RRHD_CUDA(cudaMemcpyAsync(h, R.d_cnt, sizeof h, cudaMemcpyDeviceToHost, st));
+    RRHD_CUDA(cudaStreamSynchronize(st));
+    ss->n_ok = (int64_t)h[0];
+    ss->n_fallback = 0;
+    ss->n_failed = (int64_t)h[1];
+    ss->newton_iters = (int64_t)h[2];
+    ss->max_iters = (int32_t)h[3];
+  }
   // 5. scattering integral and moments of the new intensity, for the next step
   if (fp64) {
     if ((s = scatter_fp64_cdg(R.dirs, (const double *)R.d_I, (double *)R.d_S, N, R.G, false, st))) return s;
@@ -1069,7 +1083,7 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
     const float *scales = (R.d_scale && scatter_tc_scaled(R.tc)) ? R.d_scale : nullptr;
     if ((s = scatter_tc_cdg(R.tc, (const float *)R.d_I, (float *)R.d_S, R.d_mom, N, R.G, st, scales))) return s;
   }
-  RRHD_CUDA(cudaEventRecord(R.ev[4], st));
+  RRHD_CUDA(cudaEventRecord(R.ev[6], st));
   return hstat;
 }
 
@@ -1078,8 +1092,12 @@ extern "C" rrhd_status rrhd_coupled_phase_ms(rrhd_ctx *c, float *ms) {
   RadState &R = c->rad;
   if (!R.ev[0]) return rrhd_fail(RRHD_ERR_STATE, "no coupled step has run");
   RRHD_CUDA(cudaSetDevice(c->device));
-  RRHD_CUDA(cudaEventSynchronize(R.ev[4]));
-  for (int k = 0; k < 4; k++) RRHD_CUDA(cudaEventElapsedTime(ms + k, R.ev[k], R.ev[k + 1]));
+  RRHD_CUDA(cudaEventSynchronize(R.ev[6]));
+  // hydro (with the opacities), sweep, source (side stream, beside the sweep), scattering
+  RRHD_CUDA(cudaEventElapsedTime(ms + 0, R.ev[0], R.ev[3]));
+  RRHD_CUDA(cudaEventElapsedTime(ms + 1, R.ev[3], R.ev[2]));
+  RRHD_CUDA(cudaEventElapsedTime(ms + 2, R.ev[3], R.ev[4]));
+  RRHD_CUDA(cudaEventElapsedTime(ms + 3, R.ev[5], R.ev[6]));
   return RRHD_OK;
 }
 
