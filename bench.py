@@ -259,9 +259,25 @@ def scatter_component(dev, nhex=48, M=256, groups=1, kind=0, sigma=0.5, reps=5, 
                                                 rows, sp))
             ms = _time(run, reps, stream)
             out[name] = {"ms": ms, "cell_dir_per_s": cd / (ms / 1e3), "tflops": flop / (ms / 1e3) / 1e12}
-        del I64, S64
+        # the same S and moments through the rank-7 Thomson identity (O(M) per row)
+        mom64 = torch.empty(rows, 16, dtype=torch.float64, device=I64.device)
+
+        def run_lr64():
+            L.check(L.lib.rrhd_scatter_lowrank(dg.handle, I64.data_ptr(), S64.data_ptr(), mom64.data_ptr(), rows, 1,
+                                               L.RRHD_RAD_FP64, sp))
+        ms = _time(run_lr64, reps, stream)
+        out["fp64_lowrank"] = {"ms": ms, "cell_dir_per_s": cd / (ms / 1e3),
+                               "gbs": (rows * M * 16 + rows * 128) / (ms / 1e3) / 1e9}
+        del I64, S64, mom64
     S32 = torch.empty_like(I32)
     mom = torch.empty(rows, 16, dtype=torch.float32, device=I32.device)
+
+    def run_lr32():
+        L.check(L.lib.rrhd_scatter_lowrank(dg.handle, I32.data_ptr(), S32.data_ptr(), mom.data_ptr(), rows, 1,
+                                           L.RRHD_RAD_FP32, sp))
+    ms = _time(run_lr32, reps, stream)
+    out["fp32_lowrank"] = {"ms": ms, "cell_dir_per_s": cd / (ms / 1e3),
+                           "gbs": (rows * M * 8 + rows * 64) / (ms / 1e3) / 1e9}
     for form in ("f16x3", "bf16x3", "f16"):
         tc = illum.ScatterTC(dg, form)
 
@@ -281,7 +297,8 @@ def scatter_scale_component(dev, cells=2_000_000, M=512, groups=16, reps=3, samp
     """Config 2: 2M cells x 512 Fibonacci directions x 16 frequency groups in one launch
     (rows = cell x group); I = 10^(-6 + 6g/15) lognormal(0, 1) (seeded), values over
     ~12 decades.  Tensor-core forms timed on all 32M rows (I and S 64 GB each, FP32);
-    errors against the direct FP64 contraction on a seeded sample of rows."""
+    errors against the direct FP64 contraction on a seeded sample of rows and against
+    the FP64 low-rank (rank-7 Thomson) values on every row."""
     import torch
     from radrhd_solver_b200 import _lib as L
     from radrhd_solver_b200 import illum
@@ -311,9 +328,18 @@ def scatter_scale_component(dev, cells=2_000_000, M=512, groups=16, reps=3, samp
         ms = _time(run, reps, stream, warm=1)
         tc.check()
         rel = ((S32[idx].double() - S64).abs() / S64.abs()).flatten()
+        mx_all, rms_all = illum.LowRankError(dg, I32, S32, stream=sp)
         out["tc_" + form] = {"ms": ms, "row_dir_per_s": rows * M / (ms / 1e3), "tflops": flop / (ms / 1e3) / 1e12,
-                             "max_rel_err": float(rel.max()), "rms_rel_err": float(rel.pow(2).mean().sqrt())}
+                             "max_rel_err": float(rel.max()), "rms_rel_err": float(rel.pow(2).mean().sqrt()),
+                             "all_rows_lowrank": {"max_rel_err": mx_all, "rms_rel_err": rms_all}}
         tc.close()
+    def run_lr():
+        L.check(L.lib.rrhd_scatter_lowrank(dg.handle, I32.data_ptr(), S32.data_ptr(), None, rows, 1,
+                                           L.RRHD_RAD_FP32, sp))
+    ms = _time(run_lr, reps, stream, warm=1)
+    rel = ((S32[idx].double() - S64).abs() / S64.abs()).flatten()
+    out["fp32_lowrank"] = {"ms": ms, "row_dir_per_s": rows * M / (ms / 1e3),
+                           "max_rel_err": float(rel.max()), "rms_rel_err": float(rel.pow(2).mean().sqrt())}
     del I32, S32, I64, S64
     dg.close()
     torch.cuda.empty_cache()
@@ -388,8 +414,10 @@ def coupled_component(dev, m, W, steps=3, warm=1, M=256, G=4, train_epochs=2, fo
     4-force + source con2prim, scattering integral + moments.  Plain form: FP64
     sweep, FP64 scattering (one FMA per term), reference con2prim guess.  Chosen
     form: FP32 sweep, tensor-core F16X3 scattering, learned con2prim guess
-    trained on the plain run's own states.  Both forms start from the same state;
-    the intensity arrays (N*G*M = 5.4e9 values) are far larger than L2."""
+    trained on the plain run's own states.  "plain_lowrank" / "chosen_lowrank": the
+    same with the scattering through the rank-7 Thomson identity (FP64 arithmetic).
+    All forms start from the same state; the intensity arrays (N*G*M = 5.4e9
+    values) are far larger than L2."""
     import torch
     from radrhd_solver_b200 import illum, rad_rhd, rhllc
     from radrhd_solver_b200 import mesh as Mm
@@ -402,16 +430,17 @@ def coupled_component(dev, m, W, steps=3, warm=1, M=256, G=4, train_epochs=2, fo
     states = {}
     net = None
     for form in forms:
+        fp64 = form.startswith("plain")
         torch.cuda.empty_cache()
         g = rhllc.Grid(m, eos=rhllc.EOS_IDEAL, gamma=GAMMA, device=dev)
         g.set_boundary(-3, rhllc.BC_FIXED, INFLOW)
         g.set_state_prim(W)
         dg = illum.DirectionGrid(d, dev)
         t0 = time.perf_counter()
-        sw = illum.TransportSweep(g, dg, groups=G, precision="fp64" if form == "plain" else "fp32",
-                                  dirs_per_batch=batch[0] if form == "plain" else batch[1])
+        sw = illum.TransportSweep(g, dg, groups=G, precision="fp64" if fp64 else "fp32",
+                                  dirs_per_batch=batch[0] if fp64 else batch[1])
         t_plan = time.perf_counter() - t0
-        if form == "chosen" and "plain_dump" in states:
+        if not fp64 and net is None and "plain_dump" in states:
             Wp, Up = states["plain_dump"]
             net = LearnedGuess(device=dev, seed=1)
             Ut = torch.tensor(Up, device=f"cuda:{dev}")
@@ -419,8 +448,8 @@ def coupled_component(dev, m, W, steps=3, warm=1, M=256, G=4, train_epochs=2, fo
             net.train(Ut, pt, epochs=train_epochs, batch=4096, lr=2e-3, seed=3)
             del Ut, pt
         step = rad_rhd.RadRHDStep(sw, absorption=1.0, scattering=0.5, em=rad_rhd.emission(*EM_JET),
-                                  scatter="fp64" if form == "plain" else "f16x3",
-                                  guess=None if form == "plain" else net)
+                                  scatter="lowrank" if form.endswith("_lowrank") else ("fp64" if fp64 else "f16x3"),
+                                  guess=None if fp64 else net)
         stream = torch.cuda.ExternalStream(g.stream)
         warm_stats = [step(tau, stats=True) for _ in range(warm)]
         torch.cuda.synchronize()
@@ -438,9 +467,9 @@ def coupled_component(dev, m, W, steps=3, warm=1, M=256, G=4, train_epochs=2, fo
         states[form] = Ug
         if form == "plain":
             states["plain_dump"] = (Wg, Ug)
-        bpv = 8 if form == "plain" else 4
+        bpv = 8 if fp64 else 4
         sweep_alg = (2.0 * m.n_cells + 2.0 * m.n_faces) * M * G * bpv + m.n_cells * (20 * bpv + 32.0)
-        out[form] = {"dirs_per_batch": batch[0] if form == "plain" else batch[1], "ms_per_step": ms, "steps_per_s": 1e3 / ms, "cell_updates_per_s": m.n_cells / (ms / 1e3),
+        out[form] = {"dirs_per_batch": batch[0] if fp64 else batch[1], "ms_per_step": ms, "steps_per_s": 1e3 / ms, "cell_updates_per_s": m.n_cells / (ms / 1e3),
                      "cell_dir_group_per_s": m.n_cells * M * G / (ms / 1e3), "phase_ms_last_step": ph,
                      "sweep_levels": levels, "largest_level": biggest, "plan_build_s": t_plan,
                      "sweep_alg_gbs": sweep_alg / (ph["sweep"] / 1e3) / 1e9,

@@ -299,6 +299,23 @@ rrhd_status rrhd_moments_fp64_cdg(const rrhd_dirs *d, const double *I, double *E
                                   int64_t cells, int32_t groups, void *stream);
 rrhd_status rrhd_scatter_tc_run_cdg(const rrhd_scatter_tc *t, const float *I, float *S, float *moments,
                                     int64_t cells, int32_t groups, void *stream);
+/* Scattering integral and moments through the rank-7 structure of the Thomson
+ * Gamma: 3/4 (1 + (w_d.w_k)^2) = 3/4 (1 + sum_ij w_d,i w_d,j w_k,i w_k,j), so
+ *   S[r][k] = 3/4 (E[r] + w_k^T T[r] w_k),  E = sum_d a_d I / A,  T = sum_d a_d w_d w_d^T I / A,
+ * the energy and impulse moments.  One pass over I, O(M) per row instead of O(M^2),
+ * FP64 arithmetic throughout; agrees with rrhd_scatter_fp64 to about 1e-15 relative.
+ * No counterpart in the reference, whose kernels sum the O(M^2) form
+ * (cuda_scattering.cu:82-105); valid for its phase function (scattering.h:32-35) only.
+ * I, S device [cells][M][groups] (groups 1 = the row layout [rows][M]), in FP64
+ * (precision RRHD_RAD_FP64) or FP32 (RRHD_RAD_FP32); moments NULL or [rows][16] in the
+ * same precision = {E, Fx, Fy, Fz, Txx, Txy, Txz, Tyy, Tyz, Tzz, 0...}. */
+rrhd_status rrhd_scatter_lowrank(const rrhd_dirs *d, const void *I, void *S, void *moments, int64_t cells,
+                                 int32_t groups, int32_t precision, void *stream);
+/* Max and rms relative error of an FP32 scattering integral S_test (same layout as
+ * rrhd_scatter_lowrank's FP32 case) against the FP64 low-rank values, over every
+ * row and direction.  Synchronises `stream`. */
+rrhd_status rrhd_scatter_lowrank_error(const rrhd_dirs *d, const float *I, const float *S_test, int64_t cells,
+                                       int32_t groups, double *max_rel, double *rms_rel, void *stream);
 /* Reads (and with clear != 0 resets) the error word of the tensor-core kernels:
  * RRHD_ERR_CUDA if a bounded pipeline wait timed out.  Synchronises `stream`. */
 rrhd_status rrhd_scatter_tc_check(const rrhd_scatter_tc *t, void *stream, int32_t clear);
@@ -366,9 +383,10 @@ rrhd_status rrhd_sweep(rrhd_ctx *ctx, const void *alpha, const void *betta, cons
  * share no data with the sweep and run on a second stream beside it; the call
  * joins that stream before the scattering, so the context's stream orders
  * everything that follows. */
-#define RRHD_SCATTER_FP64 (-1) /* rrhd_scatter_fp64_fma + rrhd_moments_fp64 (RRHD_RAD_FP64) */
+#define RRHD_SCATTER_FP64 (-1)    /* rrhd_scatter_fp64_fma + rrhd_moments_fp64 (RRHD_RAD_FP64) */
+#define RRHD_SCATTER_LOWRANK (-2) /* rrhd_scatter_lowrank, either sweep precision */
 typedef struct {
-  int32_t scatter;        /* RRHD_SCATTER_FP64, or an RRHD_TC_* form (RRHD_RAD_FP32)             */
+  int32_t scatter;        /* RRHD_SCATTER_FP64, RRHD_SCATTER_LOWRANK, or an RRHD_TC_* form (FP32)  */
   const rrhd_mlp *guess;  /* NULL: the reference's initial guess in the source con2prim; else the
                              learned guess (Newton for at most k_stall iterations from it)        */
   int32_t k_stall;        /* 0 = 12                                                             */

@@ -75,6 +75,7 @@ class Emission(C.Structure):
 RRHD_RAD_FP64 = 0
 RRHD_RAD_FP32 = 1
 RRHD_SCATTER_FP64 = -1
+RRHD_SCATTER_LOWRANK = -2
 RRHD_RAD_I = 0
 RRHD_RAD_S = 1
 RRHD_RAD_G4 = 2
@@ -148,6 +149,8 @@ _SIGS = {
     "rrhd_scatter_fp64_cdg": (I32, [P, P, P, I64, I32, I32, P]),
     "rrhd_moments_fp64_cdg": (I32, [P, P, P, P, P, I64, I32, P]),
     "rrhd_scatter_tc_run_cdg": (I32, [P, P, P, P, I64, I32, P]),
+    "rrhd_scatter_lowrank": (I32, [P, P, P, P, I64, I32, I32, P]),
+    "rrhd_scatter_lowrank_error": (I32, [P, P, P, I64, I32, P, P, P]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

@@ -32,6 +32,7 @@ SOURCES = {
     "hydro.cu": ["--fmad=false"],
     "radiation_fp64.cu": ["--fmad=false"],
     "scatter_tc.cu": [],
+    "scatter_lowrank.cu": [],
     "synth.cu": [],
     "c2p_mlp.cu": ["--fmad=false"],
     "sweep.cu": ["--fmad=false"],

@@ -27,5 +27,12 @@ rrhd_status moments_fp64_cdg(const rrhd_dirs *d, const double *I, double *E, dou
 rrhd_status scatter_tc_cdg(const rrhd_scatter_tc *t, const float *I, float *S, float *mom, int64_t cells, int G,
                            cudaStream_t st, const float *row_scales = nullptr);
 bool scatter_tc_scaled(const rrhd_scatter_tc *t);
+// Low-rank (Thomson) scattering and moments, cell-direction-group layout, G = 1, 2, 4:
+// FP64 with the moments as E [rows], F [rows][3], T [rows][3][3] (any may be NULL
+// together), FP32 with the moments as [rows][16] (mom may be NULL).
+rrhd_status scatter_lowrank_fp64(const rrhd_dirs *d, const double *I, double *S, double *mE, double *mF, double *mT,
+                                 int64_t cells, int G, cudaStream_t st);
+rrhd_status scatter_lowrank_fp32(const rrhd_dirs *d, const float *I, float *S, float *mom, int64_t cells, int G,
+                                 cudaStream_t st);
 
 }  // namespace rrhd

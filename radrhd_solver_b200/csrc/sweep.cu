@@ -1002,16 +1002,18 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
   RadState &R = c->rad;
   if (!R.ready) return rrhd_fail(RRHD_ERR_STATE, "rrhd_rad_setup has not run");
   const bool fp64 = R.prec == RRHD_RAD_FP64;
-  RRHD_CHECK_ARG(fp64 ? o->scatter == RRHD_SCATTER_FP64 : (o->scatter >= RRHD_TC_BF16X3 && o->scatter <= RRHD_TC_BF16),
+  const bool lowrank = o->scatter == RRHD_SCATTER_LOWRANK;
+  RRHD_CHECK_ARG(lowrank || (fp64 ? o->scatter == RRHD_SCATTER_FP64
+                                  : (o->scatter >= RRHD_TC_BF16X3 && o->scatter <= RRHD_TC_BF16)),
                  "scatter form does not match the sweep precision");
-  RRHD_CHECK_ARG(fp64 ? (64 % R.G == 0) : (R.G == 1 || R.G == 2 || R.G == 4),
-                 "coupled step groups: a divisor of 64 (FP64) or 1, 2, 4 (tensor cores)");
+  RRHD_CHECK_ARG((fp64 && !lowrank) ? (64 % R.G == 0) : (R.G == 1 || R.G == 2 || R.G == 4),
+                 "coupled step groups: a divisor of 64 (FP64 direct sum) or 1, 2, 4 (tensor cores, low rank)");
   const int k_stall = o->k_stall ? o->k_stall : 12;
   RRHD_CHECK_ARG(k_stall > 0 && k_stall <= 40, "k_stall must be in [1, 40]");
   RRHD_CUDA(cudaSetDevice(c->device));
   rrhd_status s;
   if (!R.d_I && (s = fp64 ? alloc_coupled<double>(c) : alloc_coupled<float>(c))) return s;
-  if (!fp64 && (!R.tc || R.tc_form != o->scatter)) {
+  if (!fp64 && !lowrank && (!R.tc || R.tc_form != o->scatter)) {
     if (R.tc) rrhd_scatter_tc_destroy(R.tc);
     R.tc = nullptr;
     if ((s = rrhd_scatter_tc_create(R.dirs, o->scatter, &R.tc))) return s;
@@ -1076,7 +1078,15 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
     ss->max_iters = (int32_t)h[3];
   }
   // 5. scattering integral and moments of the new intensity, for the next step
-  if (fp64) {
+  if (lowrank) {
+    if (fp64) {
+      if ((s = scatter_lowrank_fp64(R.dirs, (const double *)R.d_I, (double *)R.d_S, R.d_mE, R.d_mF, R.d_mT, N, R.G,
+                                    st)))
+        return s;
+    } else if ((s = scatter_lowrank_fp32(R.dirs, (const float *)R.d_I, (float *)R.d_S, R.d_mom, N, R.G, st))) {
+      return s;
+    }
+  } else if (fp64) {
     if ((s = scatter_fp64_cdg(R.dirs, (const double *)R.d_I, (double *)R.d_S, N, R.G, false, st))) return s;
     if ((s = moments_fp64_cdg(R.dirs, (const double *)R.d_I, R.d_mE, R.d_mF, R.d_mT, N, R.G, st))) return s;
   } else {

@@ -4,6 +4,7 @@
     dg = DirectionGrid(fibonacci_directions(256))          # InitDevice (directions)
     S = CalculateIntScattering(dg, I)                      # GetS_MPI_multi_device
     E, F, T = CalculateAllParam(dg, I)                     # MakeIllumParam
+    S, mom = ScatteringLowRank(dg, I)                      # both through the rank-7 Thomson identity
     sw = TransportSweep(grid, dg, groups=1)                # sweep plan (graph/ + make_trace/)
     CalculateIllum(sw, alpha, betta, Q, S, I)              # one sweep of separate_gpu::CalculateIllum
 
@@ -75,6 +76,34 @@ def CalculateAllParam(dg: DirectionGrid, I, stream=None):
 
 
 TC_FORMS = {"bf16x3": L.RRHD_TC_BF16X3, "f16x3": L.RRHD_TC_F16X3, "f16": L.RRHD_TC_F16, "bf16": L.RRHD_TC_BF16}
+
+
+def ScatteringLowRank(dg: DirectionGrid, I, S=None, moments: bool = True, groups: int = 1, stream=None):
+    """Scattering integral and moments through the rank-7 structure of the Thomson
+    phase function, S = 3/4 (E + w^T T w), FP64 arithmetic (no counterpart in the
+    reference, which sums the O(M^2) form).  I: CUDA float64 or float32 tensor
+    [rows, M] (groups = 1) or [cells, M, groups] (groups 2 or 4).  Returns S and the
+    [rows, 16] moments {E, F, Txx, Txy, Txz, Tyy, Tyz, Tzz, 0...} in I's dtype."""
+    import torch
+    assert I.is_cuda and I.is_contiguous() and I.dtype in (torch.float64, torch.float32)
+    if S is None:
+        S = torch.empty_like(I)
+    cells = I.shape[0]
+    rows = cells * groups
+    mom = torch.empty(rows, 16, dtype=I.dtype, device=I.device) if moments else None
+    prec = L.RRHD_RAD_FP64 if I.dtype == torch.float64 else L.RRHD_RAD_FP32
+    L.check(L.lib.rrhd_scatter_lowrank(dg.handle, I.data_ptr(), S.data_ptr(), mom.data_ptr() if moments else None,
+                                       cells, groups, prec, _stream(stream)), "rrhd_scatter_lowrank")
+    return S, mom
+
+
+def LowRankError(dg: DirectionGrid, I, S_test, groups: int = 1, stream=None):
+    """(max, rms) relative error of an FP32 scattering integral against the FP64
+    low-rank values, over every row and direction."""
+    mx, rms = C.c_double(), C.c_double()
+    L.check(L.lib.rrhd_scatter_lowrank_error(dg.handle, I.data_ptr(), S_test.data_ptr(), I.shape[0], groups,
+                                             C.byref(mx), C.byref(rms), _stream(stream)), "rrhd_scatter_lowrank_error")
+    return mx.value, rms.value
 
 
 class ScatterTC:

@@ -47,12 +47,13 @@ def C_ref(em):
 
 class RadRHDStep:
     """The coupled step of solvers/RadRHD/src/radRHD_main.cpp:96-139 on the Grid
-    of a TransportSweep.  scatter: "fp64" (plain form, needs an fp64 sweep) or a
-    tensor-core form "bf16x3" / "f16x3" / "f16" / "bf16" (fp32 sweep); guess: a
+    of a TransportSweep.  scatter: "fp64" (plain form, needs an fp64 sweep), "lowrank"
+    (the rank-7 Thomson identity, either sweep precision) or a tensor-core form
+    "bf16x3" / "f16x3" / "f16" / "bf16" (fp32 sweep); guess: a
     LearnedGuess for the source con2prim, or None for the reference guess."""
 
-    FORMS = {"fp64": L.RRHD_SCATTER_FP64, "bf16x3": L.RRHD_TC_BF16X3, "f16x3": L.RRHD_TC_F16X3,
-             "f16": L.RRHD_TC_F16, "bf16": L.RRHD_TC_BF16}
+    FORMS = {"fp64": L.RRHD_SCATTER_FP64, "lowrank": L.RRHD_SCATTER_LOWRANK, "bf16x3": L.RRHD_TC_BF16X3,
+             "f16x3": L.RRHD_TC_F16X3, "f16": L.RRHD_TC_F16, "bf16": L.RRHD_TC_BF16}
 
     def __init__(self, sweep, absorption: float = 1.0, scattering: float = 0.5, em=None, scatter: str = "fp64",
                  guess=None, k_stall: int = 0):
