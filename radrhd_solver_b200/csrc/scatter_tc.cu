@@ -347,22 +347,28 @@ __global__ void __launch_bounds__(THREADS, 1)
           const uint32_t ah = smem_u32(st), al = ah + A_BYTES;
           const uint32_t bh = al + A_BYTES, bl = bh + B_BYTES;
           const uint32_t acc_s = tmem + ab * ACC_STRIDE, acc_m = acc_s + nS;
+          // the split forms add the cross terms first (hi x Bl, lo x Bh) and hi x Bh last,
+          // so that only four MMAs add to an accumulator of full size
+          const uint32_t bm_h = bh + NT * 128, bm_l = bl + NT * 128;
+          if (THREE) {
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; kk++) {
+              const uint32_t o = kk * 32, acc = kk > 0 ? 1u : 0u;
+              umma(acc_s, umma_desc(ah + o), umma_desc(bl + o), idN, acc);
+              if (with_mom) umma(acc_m, umma_desc(ah + o), umma_desc(bm_l + o), idM, acc);
+            }
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; kk++) {
+              const uint32_t o = kk * 32;
+              umma(acc_s, umma_desc(al + o), umma_desc(bh + o), idN, 1u);
+              if (with_mom) umma(acc_m, umma_desc(al + o), umma_desc(bm_h + o), idM, 1u);
+            }
+          }
 #pragma unroll
           for (int kk = 0; kk < BK / 16; kk++) {
-            const uint32_t acc = kk > 0 ? 1u : 0u;
-            const uint32_t o = kk * 32;
+            const uint32_t o = kk * 32, acc = (THREE || kk > 0) ? 1u : 0u;
             umma(acc_s, umma_desc(ah + o), umma_desc(bh + o), idN, acc);
-            if (THREE) {
-              umma(acc_s, umma_desc(ah + o), umma_desc(bl + o), idN, 1u);
-              umma(acc_s, umma_desc(al + o), umma_desc(bh + o), idN, 1u);
-            }
-            if (with_mom) {
-              umma(acc_m, umma_desc(ah + o), umma_desc(bh + NT * 128 + o), idM, acc);
-              if (THREE) {
-                umma(acc_m, umma_desc(ah + o), umma_desc(bl + NT * 128 + o), idM, 1u);
-                umma(acc_m, umma_desc(al + o), umma_desc(bh + NT * 128 + o), idM, 1u);
-              }
-            }
+            if (with_mom) umma(acc_m, umma_desc(ah + o), umma_desc(bm_h + o), idM, acc);
           }
           umma_commit(&empty[s]);
           umma_commit(&acc_full[ab]);
