@@ -528,6 +528,53 @@ def sweep_component(dev, nhex=32, M=256, G=4, reps=3, precisions=("fp64", "fp32"
     return out
 
 
+def compton_component(dev, cells=1184, M=256, reps=3, cpu_cells=8):
+    """Frequency-coupled Compton scattering over the 100-bin spectrum
+    (rrhd_compton_full_spectrum) on seeded intensities [cells][M][100] (lognormal
+    times a smooth spectral shape) and velocities cycling through 0, 1e-6, 1e-5,
+    0.3, 0.9 and 0.99 c.  The unit is one term (cell, output direction, frequency,
+    incoming direction): cells x M x 100 x M per call.  The first cpu_cells cells
+    also run through the reference's own kernel source compiled for the host
+    (oracle/_ref, all host threads; the oracle port where that is absent), which
+    gives the CPU rate and the parity of the timed result on those cells."""
+    import torch
+    from radrhd_solver_b200 import illum
+    from radrhd_solver_b200 import mesh as Mm
+    d = Mm.fibonacci_directions(M)
+    dg = illum.DirectionGrid(d, dev)
+    gen = torch.Generator(device=f"cuda:{dev}").manual_seed(31)
+    f = torch.arange(100, device=f"cuda:{dev}", dtype=torch.float64)
+    shape = torch.exp(-((f - 60.0) / 25.0) ** 2) + 0.05
+    I = torch.exp(0.5 * torch.randn(cells, M, 100, generator=gen, device=f"cuda:{dev}", dtype=torch.float64)) * shape
+    u = torch.randn(cells, 3, generator=gen, device=f"cuda:{dev}", dtype=torch.float64)
+    speeds = torch.tensor([0.0, 1e-6, 1e-5, 0.3, 0.9, 0.99], device=f"cuda:{dev}", dtype=torch.float64)
+    vel = u / u.norm(dim=1, keepdim=True) * speeds[torch.arange(cells, device=f"cuda:{dev}") % 6][:, None]
+    S = torch.empty(cells, M, 100, dtype=torch.float64, device=f"cuda:{dev}")
+    stream = torch.cuda.current_stream(dev)
+    ms = _time(lambda: illum.FullSpectrumScattering(dg, I, vel, S=S), reps, stream, warm=1)
+    terms = float(cells) * M * 100 * M
+    out = {"workload": f"full-spectrum Compton scattering {cells} cells x {M} directions x 100 bins",
+           "ms": ms, "terms_per_s": terms / (ms / 1e3), "unit": "terms/s",
+           "l2": f"I {I.numel() * 8 / 1e6:.0f} MB > L2; the kernel is FP64-bound, not memory-bound"}
+    import oracle
+    threads = cpu_threads()
+    Ih, vh, Sh = I[:cpu_cells].cpu().numpy(), vel[:cpu_cells].cpu().numpy(), S[:cpu_cells].cpu().numpy()
+    t0 = time.perf_counter()
+    So = oracle.ref_compton(Ih, vh, d.dirs, d.areas, d.full_area, nthreads=threads)
+    kind = "reference"
+    if So is None:
+        So = oracle.port_compton(Ih, vh, d.dirs, d.areas, d.full_area, nthreads=threads)
+        kind = "port"
+    dt = time.perf_counter() - t0
+    nz = So != 0
+    out["max_rel_err_vs_cpu"] = float(np.max(np.abs(Sh[nz] - So[nz]) / np.abs(So[nz])))
+    out["cpu_baseline"] = {"value": cpu_cells * M * 100.0 * M / dt, "unit": "terms/s", "cores": threads,
+                           "kind": kind, "sample": f"{cpu_cells} cells of the same workload"}
+    out["vs_cpu"] = out["terms_per_s"] / out["cpu_baseline"]["value"]
+    dg.close()
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -635,6 +682,8 @@ def run_ours(args):
             line.setdefault("chosen_vs_plain", {})["scatter_moments"] = sc["fp64_fma"]["ms"] / sc["tc_f16x3"]["ms"]
     if rank == 0 and not args.no_scatter:
         line["scatter_scale"] = scatter_scale_component(dev)
+    if rank == 0 and not args.no_compton:
+        line["compton"] = compton_component(dev)
     if rank == 0 and "coupled" in line:
         line.setdefault("chosen_vs_plain", {})["coupled_step"] = line["coupled"]["chosen_vs_plain"]
     if rank == 0:
@@ -669,6 +718,10 @@ def main():
     ap.add_argument("--coupled-batch", default="128,256", help="directions per sweep batch (plain,chosen)")
     ap.add_argument("--c2p-only", type=int, default=0, metavar="STATES",
                     help="only time the con2prim component on STATES states (profiling runs)")
+    ap.add_argument("--no-compton", action="store_true", help="skip the full-spectrum Compton component")
+    ap.add_argument("--compton-only", type=int, default=0, metavar="CELLS",
+                    help="only time the full-spectrum Compton scattering on CELLS cells")
+    ap.add_argument("--compton-m", type=int, default=256, help="directions of --compton-only")
     ap.add_argument("--scale-only", type=int, default=0, metavar="CELLS",
                     help="only time the scattering-at-scale component on CELLS cells (profiling runs)")
     args = ap.parse_args()
@@ -678,6 +731,12 @@ def main():
         import torch
         torch.cuda.set_device(0)
         print(json.dumps(scatter_component(0, nhex=args.scatter_only, reps=args.steps)), flush=True)
+        return
+    if args.compton_only:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(compton_component(0, cells=args.compton_only, M=args.compton_m, reps=args.steps,
+                                           cpu_cells=2)), flush=True)
         return
     if args.c2p_only or args.scale_only:
         import torch

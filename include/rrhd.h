@@ -316,6 +316,23 @@ rrhd_status rrhd_scatter_lowrank(const rrhd_dirs *d, const void *I, void *S, voi
  * row and direction.  Synchronises `stream`. */
 rrhd_status rrhd_scatter_lowrank_error(const rrhd_dirs *d, const float *I, const float *S_test, int64_t cells,
                                        int32_t groups, double *max_rel, double *rms_rel, void *stream);
+/* Frequency-coupled Compton scattering integral over the 100-bin spectrum, replacing
+ * cuda::kernel::Get_full_spectrum_multi_device
+ * (cuda/src/short_characteristics/separate_gpu/spectrum/cuda_scat_full_spectrum.cu:61-118)
+ * as CalculateFullSpectrumIntScattering launches it
+ * (cuda/src/short_characteristics/separate_gpu/spectrum/cuda_interface_spectrum.cu:94-140):
+ *   S[i][k][f] = sum_d GammaC(w_{dir_disp+k}, w_d, frq_f, v_i) I[i][d][bin(frq1)] a_d / A
+ * with the Doppler and recoil frequency shift, the Klein-Nishina weight and the
+ * low/high cut-offs of that kernel (CGS constants of lib/global_consts.h:34-44).
+ * I device FP64 [cells][M][100] (I[i][d][99] is never read: the top bin is always cut);
+ * velocity device FP64 [cells][3] in units of c (velocity[shift_gpu + i] of the
+ * reference: pass the pointer to this chunk's first cell); S device FP64
+ * [cells][out_stride][100] (local_scattering_size = out_stride), output directions
+ * dir_disp .. dir_disp + dir_count - 1 (local_scattering_disp, end_dir).  I and S
+ * 16-byte aligned.  Asynchronous on `stream`. */
+rrhd_status rrhd_compton_full_spectrum(const rrhd_dirs *d, const double *I, const double *velocity, double *S,
+                                       int64_t cells, int32_t dir_disp, int32_t dir_count, int32_t out_stride,
+                                       void *stream);
 /* Reads (and with clear != 0 resets) the error word of the tensor-core kernels:
  * RRHD_ERR_CUDA if a bounded pipeline wait timed out.  Synchronises `stream`. */
 rrhd_status rrhd_scatter_tc_check(const rrhd_scatter_tc *t, void *stream, int32_t clear);

@@ -65,6 +65,8 @@ def port() -> C.CDLL:
             "orc_get_illum": (D, [P, P, D, D]), "orc_get_rhs": (D, [D, D, D, D, P]),
             "orc_recalc_illum": (D, [I64, P, P, P, I32, I32, P]),
             "orc_sweep": (I64, [P, I32, P, I32, P, P, P, P, D, P]),
+            "orc_compton_full_spectrum": (None, [I32, P, P, D, I64, P, P, I32, I32, I32, P, C.c_int]),
+            "orc_compton_frq": (D, [I32]), "orc_compton_frq_idx": (I32, [D]),
         }
         for n, (r, a) in sig.items():
             f = getattr(lib, n)
@@ -104,6 +106,9 @@ def ref(variant: str) -> C.CDLL | None:
         "ref_read_geo": (I64, [C.c_char_p, C.c_char_p, P, P, P, P, P, P, P, P, P]),
         "ref_read_hllc_init": (I64, [C.c_char_p, P]), "ref_record_sizes": (C.c_int, [P]),
         "ref_read_sphere_directions": (I64, [C.c_char_p, P, P, P]),
+        "ref_compton_full_spectrum": (C.c_int, [I32, P, P, D, I64, P, P, I32, I32, I32, P, C.c_int]),
+        "ref_compton_n_frq": (C.c_int, []), "ref_compton_get_frq": (D, [C.c_int]),
+        "ref_compton_get_frq_idx": (C.c_int, [D]), "ref_compton_gamma": (D, [D, D, P, D, D, P, P, P]),
     }
     for n, (r, a) in sig.items():
         f = getattr(lib, n, None)
@@ -487,3 +492,57 @@ def ref_rad_constants(variant="rad_ideal_4_3"):
     out = np.zeros(4)
     ref(variant).ref_rad_constants(_p(out))
     return out
+
+
+N_FRQ = 100  # N_Frq of the reference's full-spectrum kernel (cuda_scat_full_spectrum.cu:47)
+
+
+def _compton_args(I, vel, dirs, areas, dir_disp, dir_count, out_stride):
+    I = np.ascontiguousarray(I, dtype=np.float64)
+    vel = np.ascontiguousarray(vel, dtype=np.float64)
+    dirs = np.ascontiguousarray(dirs, dtype=np.float64)
+    areas = np.ascontiguousarray(areas, dtype=np.float64)
+    cells, M = I.shape[0], dirs.shape[0]
+    assert I.shape == (cells, M, N_FRQ) and vel.shape == (cells, 3)
+    dir_count = M - dir_disp if dir_count is None else dir_count
+    out_stride = dir_count if out_stride is None else out_stride
+    S = np.zeros((cells, out_stride, N_FRQ))
+    return I, vel, dirs, areas, cells, M, dir_count, out_stride, S
+
+
+def port_compton(I, vel, dirs, areas, full_area, dir_disp=0, dir_count=None, out_stride=None, nthreads=1):
+    """Full-spectrum Compton scattering S [cells][out_stride][100] by the C restatement."""
+    I, vel, dirs, areas, cells, M, dir_count, out_stride, S = _compton_args(I, vel, dirs, areas, dir_disp,
+                                                                            dir_count, out_stride)
+    port().orc_compton_full_spectrum(M, _p(dirs), _p(areas), full_area, cells, _p(I), _p(vel), dir_disp,
+                                     dir_count, out_stride, _p(S), nthreads)
+    return S
+
+
+def port_compton_frq(idx):
+    return port().orc_compton_frq(idx)
+
+
+def port_compton_frq_idx(frq):
+    return port().orc_compton_frq_idx(frq)
+
+
+def ref_compton(I, vel, dirs, areas, full_area, dir_disp=0, dir_count=None, out_stride=None, nthreads=0):
+    """The same through the reference's own device source compiled for the host."""
+    lib = ref("compton")
+    if lib is None:
+        return None
+    I, vel, dirs, areas, cells, M, dir_count, out_stride, S = _compton_args(I, vel, dirs, areas, dir_disp,
+                                                                            dir_count, out_stride)
+    rc = lib.ref_compton_full_spectrum(M, _p(dirs), _p(areas), full_area, cells, _p(I), _p(vel), dir_disp,
+                                       dir_count, out_stride, _p(S), nthreads)
+    assert rc == 0
+    return S
+
+
+def ref_compton_get_frq(idx):
+    return ref("compton").ref_compton_get_frq(idx)
+
+
+def ref_compton_get_frq_idx(frq):
+    return ref("compton").ref_compton_get_frq_idx(frq)

@@ -680,3 +680,104 @@ int64_t orc_sweep(const orc_sweep_mesh *m, int32_t M, const double *dirs, int32_
   free(queue);
   return missing;
 }
+
+/* ------------------------------------------------------------------ Compton
+ * Frequency-coupled Compton scattering over the full spectrum, restating
+ * cuda/src/short_characteristics/separate_gpu/spectrum/cuda_scat_full_spectrum.cu in the
+ * same operation order (the reference has it as device code only; its CGS constants are
+ * lib/global_consts.h:34-44, written here as the same products). */
+#define CMP_C_LIGHT (3 * 1e10)                                   /* kC_Light */
+#define CMP_C_LIGHT_INV (1.0 / (CMP_C_LIGHT))                    /* kC_LightInv */
+#define CMP_VELOCITY CMP_C_LIGHT                                 /* kVelocity, global_consts.h:74 */
+#define CMP_HMC ((6.62 * 1e-27) / (((9.109383701528 * 1e-28) * CMP_C_LIGHT) * CMP_C_LIGHT))
+#define CMP_COEF (((2 * 3.1415926535897932384626433832795) * (2.8179403 * 1e-13)) * (2.8179403 * 1e-13))
+static const double cmp_frq0 = 1e24; /* cuda_scat_full_spectrum.cu:48 */
+static const double cmp_betta = 350; /* :49 */
+
+/* :54-59 */
+double orc_compton_frq(int32_t idx) {
+  if (idx <= 0) return 0;
+  const double x = ORC_N_FRQ - idx;
+  return cmp_frq0 * exp((-x * x) / cmp_betta);
+}
+
+/* :50-53; (int)floor(...) converts like the device's cvt.rzi (NaN -> 0, saturating) */
+int32_t orc_compton_frq_idx(double frq) {
+  const double t = floor(sqrt(-cmp_betta * log(frq / cmp_frq0)) + 1);
+  int m;
+  if (t != t) m = 0;
+  else if (t >= 2147483647.0) m = 2147483647;
+  else if (t <= -2147483648.0) m = -2147483647 - 1;
+  else m = (int)t;
+  m = m < ORC_N_FRQ ? m : ORC_N_FRQ;
+  m = m > 0 ? m : 0;
+  return ORC_N_FRQ - m;
+}
+
+/* get_compton_frq, :8-14 and :16-20 */
+static inline double cmp_frq_doppler(double frq, double v, double cosf, double cosf1, double cosTh, double lorenz) {
+  const double eps = CMP_HMC * frq;
+  return frq * (1. - v * cosf) / (1. + eps / lorenz * (1 - cosTh) - v * cosf1);
+}
+static inline double cmp_frq_recoil(double frq, double cosTh) {
+  const double eps = CMP_HMC * frq;
+  return frq / (1. + eps * (1.0 - cosTh));
+}
+
+/* GammaC, :22-44 */
+static inline double cmp_gamma(double cosf, double v, const double *vel, double frq, double lorenz,
+                               const double *main_dir, const double *scat_dir, double *frq1) {
+  const double cosTh = dot3(main_dir, scat_dir);
+  if (v > (1. / CMP_VELOCITY)) {
+    const double cosf1 = dot3(vel, scat_dir) / v;
+    *frq1 = cmp_frq_doppler(frq, v, cosf, cosf1, cosTh, lorenz);
+  } else {
+    if (cosTh > 0.99999999) {
+      *frq1 = frq;
+      return 2.0 * CMP_COEF;
+    }
+    *frq1 = cmp_frq_recoil(frq, cosTh);
+  }
+  const double frq_frac = *frq1 / frq;
+  const double frq1_inv = 1. / frq_frac;
+  const double ds = CMP_COEF * frq_frac * frq_frac * (frq_frac + frq1_inv + cosTh * cosTh - 1.0);
+  return frq1_inv * ds;
+}
+
+/* Get_full_spectrum_multi_device, :61-118, for every (cell, direction, frequency).  The
+ * reference reads the intensity before the two cut-offs replace it by zero; reading it
+ * only when it is kept gives the same sum and stays inside the array. */
+void orc_compton_full_spectrum(int32_t M, const double *dirs, const double *areas, double full_area,
+                               int64_t cells, const double *I, const double *vel, int32_t dir_disp,
+                               int32_t dir_count, int32_t out_stride, double *S, int nthreads) {
+  const double low = 0.5 * (orc_compton_frq(0 + 1) + orc_compton_frq(0));
+  const double high = orc_compton_frq(ORC_N_FRQ - 1);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads > 0 ? nthreads : 1)
+  for (int64_t i = 0; i < cells; i++) {
+    const double *v3 = vel + 3 * i;
+    for (int32_t k = 0; k < dir_count; k++) {
+      const double *cur_dir = dirs + 3 * (int64_t)(dir_disp + k);
+      for (int f = 0; f < ORC_N_FRQ; f++) {
+        const double frq = 0.5 * (orc_compton_frq(f + 1) + orc_compton_frq(f));
+        const double v2 = dot3(v3, v3);
+        double lorenz = 1.0, v = 0.0, cosf = 0.0;
+        if (v2 > CMP_C_LIGHT_INV) {
+          lorenz = 1. / sqrt(1. - (v2));
+          v = sqrt(v2);
+          cosf = dot3(v3, cur_dir) / v;
+        }
+        double scatter = 0;
+        for (int32_t d = 0; d < M; d++) {
+          double frq1;
+          const double G = cmp_gamma(cosf, v, v3, frq, lorenz, cur_dir, dirs + 3 * (int64_t)d, &frq1);
+          double Iv = 0;
+          if (!(frq1 < low) && !(frq1 > high))
+            Iv = I[((int64_t)i * M + d) * ORC_N_FRQ + orc_compton_frq_idx(frq1)];
+          scatter += G * Iv * areas[d];
+        }
+        const double cfl = 1.0;
+        S[((int64_t)i * out_stride + k) * ORC_N_FRQ + f] = cfl * scatter / full_area;
+      }
+    }
+  }
+}

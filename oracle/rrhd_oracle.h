@@ -115,6 +115,20 @@ double orc_recalc_illum(int64_t N, const int32_t *cell_faces, const double *face
 int64_t orc_sweep(const orc_sweep_mesh *m, int32_t M, const double *dirs, int32_t G, const double *alpha,
                const double *betta, const double *Q, const double *S, double bc, double *I);
 
+/* Frequency-coupled Compton scattering over the 100-bin spectrum
+ * (cuda/src/short_characteristics/separate_gpu/spectrum/cuda_scat_full_spectrum.cu:8-118,
+ * one call per (cell, direction, frequency) of Get_full_spectrum_multi_device).
+ * I [cells][M][100], vel [cells][3] (units of c), dirs [M][3], areas [M];
+ * S [cells][out_stride][100], directions dir_disp .. dir_disp + dir_count - 1. */
+#define ORC_N_FRQ 100
+void orc_compton_full_spectrum(int32_t M, const double *dirs, const double *areas, double full_area,
+                               int64_t cells, const double *I, const double *vel, int32_t dir_disp,
+                               int32_t dir_count, int32_t out_stride, double *S, int nthreads);
+/* get_frq (cuda_scat_full_spectrum.cu:54-59) and get_frq_idx (:50-53), the latter with
+ * the device's saturating float-to-int conversion (NaN -> 0). */
+double orc_compton_frq(int32_t idx);
+int32_t orc_compton_frq_idx(double frq);
+
 #ifdef __cplusplus
 }
 #endif

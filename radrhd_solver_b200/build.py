@@ -36,6 +36,7 @@ SOURCES = {
     "synth.cu": [],
     "c2p_mlp.cu": ["--fmad=false"],
     "sweep.cu": ["--fmad=false"],
+    "compton.cu": [],
 }
 
 

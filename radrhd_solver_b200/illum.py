@@ -106,6 +106,30 @@ def LowRankError(dg: DirectionGrid, I, S_test, groups: int = 1, stream=None):
     return mx.value, rms.value
 
 
+N_FRQ = 100  # spectrum bins of the full-spectrum Compton scattering
+
+
+def FullSpectrumScattering(dg: DirectionGrid, I, velocity, S=None, dir_disp: int = 0, dir_count: int | None = None,
+                           out_stride: int | None = None, stream=None):
+    """Frequency-coupled Compton scattering integral over the 100-bin spectrum, the
+    reference's CalculateFullSpectrumIntScattering / Get_full_spectrum_multi_device
+    (cuda_interface_spectrum.cu:94-140, cuda_scat_full_spectrum.cu:61-118).
+    I: CUDA float64 [cells, M, 100]; velocity: CUDA float64 [cells, 3] in units of c.
+    Returns S [cells, out_stride, 100] for the output directions dir_disp ..
+    dir_disp + dir_count - 1 (all M by default)."""
+    import torch
+    assert I.is_cuda and I.is_contiguous() and I.dtype == torch.float64 and I.shape[1:] == (dg.size, N_FRQ)
+    assert velocity.is_contiguous() and velocity.dtype == torch.float64 and velocity.shape == (I.shape[0], 3)
+    dir_count = dg.size - dir_disp if dir_count is None else dir_count
+    out_stride = dir_count if out_stride is None else out_stride
+    if S is None:
+        S = torch.empty(I.shape[0], out_stride, N_FRQ, dtype=torch.float64, device=I.device)
+    L.check(L.lib.rrhd_compton_full_spectrum(dg.handle, I.data_ptr(), velocity.data_ptr(), S.data_ptr(), I.shape[0],
+                                             dir_disp, dir_count, out_stride, _stream(stream)),
+            "rrhd_compton_full_spectrum")
+    return S
+
+
 class ScatterTC:
     """Tensor-core (tcgen05) scattering integral + moments for one direction set
     and precision form ("bf16x3", "f16x3", "f16", "bf16"); FP32 in/out."""

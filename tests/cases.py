@@ -62,3 +62,21 @@ def intensity(N, M_, seed=3, centers=None, groups=1):
         r2 = (centers ** 2).sum(1)
         I *= np.repeat(np.exp(-r2 / 0.2), groups)[:, None]
     return I
+
+
+COMPTON_SPEEDS = (0.0, 1e-6, 1e-5, 0.3, 0.9, 0.99)
+
+
+def compton_case(cells, M_, seed=17, speeds=COMPTON_SPEEDS):
+    """Inputs of the full-spectrum Compton scattering: intensity [cells][M][100]
+    (lognormal(0, 0.5) times a smooth spectral shape) and velocities [cells][3] in
+    units of c whose magnitudes cycle through `speeds`: 0 and 1e-6 take the
+    recoil-only branch (v^2 below 1/c in CGS), 1e-5 and above the Doppler branch."""
+    rng = np.random.default_rng(seed)
+    f = np.arange(100)
+    shape = np.exp(-((f - 60.0) / 25.0) ** 2) + 0.05
+    I = np.exp(rng.normal(0.0, 0.5, (cells, M_, 100))) * shape
+    u = rng.normal(size=(cells, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    vel = u * np.array([speeds[i % len(speeds)] for i in range(cells)])[:, None]
+    return I, vel

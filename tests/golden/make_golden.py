@@ -170,17 +170,34 @@ def files_fixtures(out):
     out["files_sys"] = mesh_arrays(m, "mesh_") | dict(W=W, U=U)
 
 
+def compton_fixtures(out):
+    """Full-spectrum Compton scattering by the reference's own device source compiled
+    for the host (Get_full_spectrum_multi_device): all directions, and a slice of them
+    written into a wider output stride."""
+    from cases import compton_case
+    d = fibonacci_directions(16)
+    I, vel = compton_case(6, 16, seed=23)
+    S = oracle.ref_compton(I, vel, d.dirs, d.areas, d.full_area)
+    S_part = oracle.ref_compton(I, vel, d.dirs, d.areas, d.full_area, dir_disp=5, dir_count=7, out_stride=9)
+    frq = np.array([oracle.loader.ref_compton_get_frq(j) for j in range(101)])
+    out["compton"] = dict(dirs=d.dirs, areas=d.areas, full_area=np.float64(d.full_area), I=I, vel=vel, S=S,
+                          S_part=S_part, get_frq=frq)
+
+
+FIXTURES = {"hydro": hydro_fixtures, "step": step_fixtures, "radiation": radiation_fixtures,
+            "sweep": sweep_fixtures, "files": files_fixtures, "compton": compton_fixtures}
+
+
 def main():
-    need = list(VARIANTS) + ["illum", "rad_ideal_4_3"]
+    """`make_golden.py` regenerates every fixture; `make_golden.py compton ...` only the named ones."""
+    names = sys.argv[1:] or list(FIXTURES)
+    need = list(VARIANTS) + ["illum", "rad_ideal_4_3", "compton"]
     missing = [v for v in need if not oracle.have_ref(v)]
     if missing:
         sys.exit(f"reference variants not built ({', '.join(missing)}): run `make -C oracle ref` first")
     out = {}
-    hydro_fixtures(out)
-    step_fixtures(out)
-    radiation_fixtures(out)
-    sweep_fixtures(out)
-    files_fixtures(out)
+    for n in names:
+        FIXTURES[n](out)
     for name, arrays in out.items():
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **arrays)
         size = os.path.getsize(os.path.join(HERE, f"{name}.npz"))
