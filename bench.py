@@ -556,6 +556,14 @@ def compton_component(dev, cells=1184, M=256, reps=3, cpu_cells=8):
     out = {"workload": f"full-spectrum Compton scattering {cells} cells x {M} directions x 100 bins",
            "ms": ms, "terms_per_s": terms / (ms / 1e3), "unit": "terms/s",
            "l2": f"I {I.numel() * 8 / 1e6:.0f} MB > L2; the kernel is FP64-bound, not memory-bound"}
+    # single frequency (rrhd_compton_spectrum): the same intensities as 100 x cells rows at one frequency
+    I1 = I.permute(0, 2, 1).reshape(cells * 100, M).contiguous()
+    v1 = vel.repeat_interleave(100, dim=0).contiguous()
+    S1 = torch.empty_like(I1)
+    ms1 = _time(lambda: illum.SpectrumScattering(dg, I1, v1, 4.2e20, S=S1), reps, stream, warm=1)
+    out["single_frequency"] = {"workload": f"{cells * 100} cells x {M} directions at 4.2e20 Hz", "ms": ms1,
+                               "terms_per_s": float(cells) * 100 * M * M / (ms1 / 1e3)}
+    del I1, v1, S1
     import oracle
     threads = cpu_threads()
     Ih, vh, Sh = I[:cpu_cells].cpu().numpy(), vel[:cpu_cells].cpu().numpy(), S[:cpu_cells].cpu().numpy()

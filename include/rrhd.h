@@ -333,6 +333,17 @@ rrhd_status rrhd_scatter_lowrank_error(const rrhd_dirs *d, const float *I, const
 rrhd_status rrhd_compton_full_spectrum(const rrhd_dirs *d, const double *I, const double *velocity, double *S,
                                        int64_t cells, int32_t dir_disp, int32_t dir_count, int32_t out_stride,
                                        void *stream);
+/* Compton-shifted scattering integral at one frequency frq (Hz), replacing
+ * cuda::kernel::Get_spectrum_multi_device
+ * (cuda/src/short_characteristics/separate_gpu/spectrum/cuda_scat_spectrum.cu:41-83) as
+ * CalculateSpectrumIntScattering launches it (cuda_interface_spectrum.cu:46-92):
+ *   S[i][k] = 0.25 sum_d GammaC(w_{dir_disp+k}, w_d, frq, v_i) I[i][d] a_d / A
+ * (that kernel's weight has no forward special case; 0.25 is its cfl factor).
+ * I device FP64 [cells][M] at frq; velocity device FP64 [cells][3] in units of c;
+ * S device FP64 [cells][out_stride].  Asynchronous on `stream`. */
+rrhd_status rrhd_compton_spectrum(const rrhd_dirs *d, const double *I, const double *velocity, double *S,
+                                  int64_t cells, double frq, int32_t dir_disp, int32_t dir_count, int32_t out_stride,
+                                  void *stream);
 /* Reads (and with clear != 0 resets) the error word of the tensor-core kernels:
  * RRHD_ERR_CUDA if a bounded pipeline wait timed out.  Synchronises `stream`. */
 rrhd_status rrhd_scatter_tc_check(const rrhd_scatter_tc *t, void *stream, int32_t clear);

@@ -67,6 +67,7 @@ def port() -> C.CDLL:
             "orc_sweep": (I64, [P, I32, P, I32, P, P, P, P, D, P]),
             "orc_compton_full_spectrum": (None, [I32, P, P, D, I64, P, P, I32, I32, I32, P, C.c_int]),
             "orc_compton_frq": (D, [I32]), "orc_compton_frq_idx": (I32, [D]),
+            "orc_compton_spectrum": (None, [I32, P, P, D, I64, P, P, D, I32, I32, I32, P, C.c_int]),
         }
         for n, (r, a) in sig.items():
             f = getattr(lib, n)
@@ -109,6 +110,7 @@ def ref(variant: str) -> C.CDLL | None:
         "ref_compton_full_spectrum": (C.c_int, [I32, P, P, D, I64, P, P, I32, I32, I32, P, C.c_int]),
         "ref_compton_n_frq": (C.c_int, []), "ref_compton_get_frq": (D, [C.c_int]),
         "ref_compton_get_frq_idx": (C.c_int, [D]), "ref_compton_gamma": (D, [D, D, P, D, D, P, P, P]),
+        "ref_compton_spectrum": (C.c_int, [I32, P, P, D, I64, P, P, D, I32, I32, I32, P, C.c_int]),
     }
     for n, (r, a) in sig.items():
         f = getattr(lib, n, None)
@@ -546,3 +548,38 @@ def ref_compton_get_frq(idx):
 
 def ref_compton_get_frq_idx(frq):
     return ref("compton").ref_compton_get_frq_idx(frq)
+
+
+def _compton_one_args(I, vel, dirs, areas, dir_disp, dir_count, out_stride):
+    I = np.ascontiguousarray(I, dtype=np.float64)
+    vel = np.ascontiguousarray(vel, dtype=np.float64)
+    dirs = np.ascontiguousarray(dirs, dtype=np.float64)
+    areas = np.ascontiguousarray(areas, dtype=np.float64)
+    cells, M = I.shape[0], dirs.shape[0]
+    assert I.shape == (cells, M) and vel.shape == (cells, 3)
+    dir_count = M - dir_disp if dir_count is None else dir_count
+    out_stride = dir_count if out_stride is None else out_stride
+    return I, vel, dirs, areas, cells, M, dir_count, out_stride, np.zeros((cells, out_stride))
+
+
+def port_compton_spectrum(I, vel, dirs, areas, full_area, frq, dir_disp=0, dir_count=None, out_stride=None,
+                          nthreads=1):
+    """Single-frequency Compton scattering S [cells][out_stride] by the C restatement."""
+    I, vel, dirs, areas, cells, M, dir_count, out_stride, S = _compton_one_args(I, vel, dirs, areas, dir_disp,
+                                                                                dir_count, out_stride)
+    port().orc_compton_spectrum(M, _p(dirs), _p(areas), full_area, cells, _p(I), _p(vel), frq, dir_disp, dir_count,
+                                out_stride, _p(S), nthreads)
+    return S
+
+
+def ref_compton_spectrum(I, vel, dirs, areas, full_area, frq, dir_disp=0, dir_count=None, out_stride=None,
+                         nthreads=0):
+    """The same through the reference's own device source compiled for the host."""
+    lib = ref("compton")
+    if lib is None:
+        return None
+    I, vel, dirs, areas, cells, M, dir_count, out_stride, S = _compton_one_args(I, vel, dirs, areas, dir_disp,
+                                                                                dir_count, out_stride)
+    assert lib.ref_compton_spectrum(M, _p(dirs), _p(areas), full_area, cells, _p(I), _p(vel), frq, dir_disp,
+                                    dir_count, out_stride, _p(S), nthreads) == 0
+    return S

@@ -1,6 +1,8 @@
 // Test infrastructure, not product code: the checker, never the thing measured.
 //
-// Runs the reference's own frequency-coupled Compton scattering kernel on the CPU.
+// Runs the reference's own Compton scattering kernels on the CPU: the frequency-coupled
+// full-spectrum one, and (this file compiled a second time with RRHD_SHIM_ONE) the
+// single-frequency one of cuda_scat_spectrum.cu:41-83, Get_spectrum_multi_device.
 // The device source (cuda/src/short_characteristics/separate_gpu/spectrum/
 // cuda_scat_full_spectrum.cu:61-118, Get_full_spectrum_multi_device) is included from
 // its place in the reference tree and compiled by g++ with this file, with the host
@@ -14,7 +16,11 @@
 // shifted frequency lies above the spectrum (get_frq_idx returns N_Frq there; the
 // value read is then replaced by zero).  The intensity is therefore copied into a
 // buffer with a zero pad behind it, so that this read stays inside the allocation.
+#ifndef RRHD_SHIM_ONE
 #include "cuda_scat_full_spectrum.cu"
+#else
+#include "cuda_scat_spectrum.cu"
+#endif
 
 #include <omp.h>
 
@@ -22,6 +28,7 @@
 #include <cstring>
 #include <vector>
 
+#ifndef RRHD_SHIM_ONE
 thread_local uint3 threadIdx;
 thread_local uint3 blockIdx;
 thread_local dim3 blockDim;
@@ -94,3 +101,48 @@ extern "C" double ref_compton_gamma(double cosf, double v, const double *vel, do
   return GammaC(cosf, v, Vector3(vel[0], vel[1], vel[2]), frq, lorenz, Vector3(main_dir[0], main_dir[1], main_dir[2]),
                 Vector3(scat_dir[0], scat_dir[1], scat_dir[2]), *frq1);
 }
+
+#else  // RRHD_SHIM_ONE
+
+// S[i * out_stride + k], I[i * M + d] at the single frequency frq.
+extern "C" int ref_compton_spectrum(int32_t M, const double *dirs, const double *areas, double full_area,
+                                    int64_t cells, const double *I, const double *vel, double frq, int32_t dir_disp,
+                                    int32_t dir_count, int32_t out_stride, double *S, int nthreads) {
+  using namespace cuda::geo;
+  if (M <= 0 || cells < 0 || dir_count < 0 || dir_disp < 0 || dir_disp + dir_count > M || out_stride < dir_count)
+    return -1;
+  std::vector<direction_device_t> dd(M);
+  for (int d = 0; d < M; d++) {
+    dd[d].dir = Vector3(dirs[3 * d], dirs[3 * d + 1], dirs[3 * d + 2]);
+    dd[d].area = areas[d];
+  }
+  grid_directions_device_t gd;
+  gd.size = M;
+  gd.directions = dd.data();
+  gd.full_area = full_area;
+  std::vector<Vector3> v(cells);
+  for (int64_t i = 0; i < cells; i++) v[i] = Vector3(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
+  grid_device_t g;
+  g.size = cells;
+  g.loc_size_gpu = cells;
+  g.shift_gpu = 0;
+  g.loc_size_params = cells;
+  g.shift_params = 0;
+  g.local_scattering_size = out_stride;
+  g.local_scattering_disp = dir_disp;
+  g.illum = const_cast<double *>(I);
+  g.int_scattering = S;
+  g.velocity = v.data();
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+  for (int64_t i = 0; i < cells; i++) {
+    blockDim = dim3{1, 1, 1};
+    threadIdx = uint3{0, 0, 0};
+    for (int k = 0; k < dir_count; k++) {
+      blockIdx = uint3{(unsigned)i, (unsigned)k, 0};
+      cuda::kernel::Get_spectrum_multi_device(&gd, &g, frq, dir_count);
+    }
+  }
+  return 0;
+}
+#endif

@@ -781,3 +781,48 @@ void orc_compton_full_spectrum(int32_t M, const double *dirs, const double *area
     }
   }
 }
+
+/* GammaC of cuda_scat_spectrum.cu:22-39: the same weight as the full-spectrum kernel's
+ * without its forward-scattering special case. */
+static inline double cmp_gamma_one(double cosf, double v, const double *vel, double frq, double lorenz,
+                                   const double *main_dir, const double *scat_dir) {
+  const double cosTh = dot3(main_dir, scat_dir);
+  double frq1;
+  if (v > (1. / CMP_VELOCITY)) {
+    const double cosf1 = dot3(vel, scat_dir) / v;
+    frq1 = cmp_frq_doppler(frq, v, cosf, cosf1, cosTh, lorenz);
+  } else {
+    frq1 = cmp_frq_recoil(frq, cosTh);
+  }
+  const double frq_frac = frq1 / frq;
+  const double frq1_inv = 1. / frq_frac;
+  const double ds = CMP_COEF * frq_frac * frq_frac * (frq_frac + frq1_inv + cosTh * cosTh - 1.0);
+  return frq1_inv * ds;
+}
+
+/* Get_spectrum_multi_device, cuda_scat_spectrum.cu:41-83, for every (cell, direction). */
+void orc_compton_spectrum(int32_t M, const double *dirs, const double *areas, double full_area, int64_t cells,
+                          const double *I, const double *vel, double frq, int32_t dir_disp, int32_t dir_count,
+                          int32_t out_stride, double *S, int nthreads) {
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads > 0 ? nthreads : 1)
+  for (int64_t i = 0; i < cells; i++) {
+    const double *v3 = vel + 3 * i;
+    for (int32_t k = 0; k < dir_count; k++) {
+      const double *cur_dir = dirs + 3 * (int64_t)(dir_disp + k);
+      const double v2 = dot3(v3, v3);
+      double lorenz = 1.0, v = 0.0, cosf = 0.0;
+      if (v2 > CMP_C_LIGHT_INV) {
+        lorenz = 1. / sqrt(1. - (v2));
+        v = sqrt(v2);
+        cosf = dot3(v3, cur_dir) / v;
+      }
+      double scatter = 0;
+      for (int32_t d = 0; d < M; d++) {
+        const double Iv = I[(int64_t)i * M + d];
+        scatter += cmp_gamma_one(cosf, v, v3, frq, lorenz, cur_dir, dirs + 3 * (int64_t)d) * Iv * areas[d];
+      }
+      const double cfl = 0.25;
+      S[(int64_t)i * out_stride + k] = cfl * scatter / full_area;
+    }
+  }
+}

@@ -128,6 +128,13 @@ void orc_compton_full_spectrum(int32_t M, const double *dirs, const double *area
  * the device's saturating float-to-int conversion (NaN -> 0). */
 double orc_compton_frq(int32_t idx);
 int32_t orc_compton_frq_idx(double frq);
+/* Compton-shifted scattering integral at one frequency
+ * (cuda/src/short_characteristics/separate_gpu/spectrum/cuda_scat_spectrum.cu:41-83,
+ * Get_spectrum_multi_device; its GammaC :22-39 has no forward special case, cfl = 0.25).
+ * I [cells][M] at frequency frq; S [cells][out_stride]. */
+void orc_compton_spectrum(int32_t M, const double *dirs, const double *areas, double full_area, int64_t cells,
+                          const double *I, const double *vel, double frq, int32_t dir_disp, int32_t dir_count,
+                          int32_t out_stride, double *S, int nthreads);
 
 #ifdef __cplusplus
 }

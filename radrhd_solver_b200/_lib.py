@@ -152,6 +152,7 @@ _SIGS = {
     "rrhd_scatter_lowrank": (I32, [P, P, P, P, I64, I32, I32, P]),
     "rrhd_scatter_lowrank_error": (I32, [P, P, P, I64, I32, P, P, P]),
     "rrhd_compton_full_spectrum": (I32, [P, P, P, P, I64, I32, I32, I32, P]),
+    "rrhd_compton_spectrum": (I32, [P, P, P, P, I64, D, I32, I32, I32, P]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

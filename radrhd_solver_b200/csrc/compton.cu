@@ -245,6 +245,57 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
+// Compton-shifted scattering integral at one frequency (cuda_scat_spectrum.cu:41-83,
+// Get_spectrum_multi_device): S[i][k] = 0.25 sum_d GammaC(k, d, frq) I[i][d] a_d / A with
+// the same weight as above but no forward special case (its GammaC, :22-39) and no bins.
+// One block per cell at a time; the cell's directions, v cosf1 and 0.25 coef a_d I_d / A are
+// staged in shared memory and each thread sums one output direction over all of them.
+constexpr int kOneThreads = 256;
+constexpr double kOneCfl = 0.25;  // :79
+
+__global__ void __launch_bounds__(kOneThreads)
+    k_compton_one(const double *__restrict__ I, const double *__restrict__ vel, const double *__restrict__ w,
+                  const double *__restrict__ a, double scale, double eps, double *__restrict__ S, long long cells,
+                  int M, int dir_disp, int dir_count, int out_stride) {
+  extern __shared__ __align__(16) double sh1[];
+  double *sWx = sh1, *sWy = sWx + M, *sWz = sWy + M, *sVc1 = sWz + M, *sIa = sVc1 + M;
+  for (long long cell = blockIdx.x; cell < cells; cell += gridDim.x) {
+    const double vx = vel[3 * cell], vy = vel[3 * cell + 1], vz = vel[3 * cell + 2];
+    const double v2 = dot_rn(vx, vy, vz, vx, vy, vz);
+    const bool doppler = v2 > kCLightInv;  // :63-68
+    const double lorenz = doppler ? __ddiv_rn(1., __dsqrt_rn(__dadd_rn(1., -v2))) : 1.0;
+    const double v = doppler ? __dsqrt_rn(v2) : 0.0;
+    const double el = __ddiv_rn(eps, lorenz);
+    __syncthreads();  // the previous cell's readers are done with shared memory
+    for (int d = threadIdx.x; d < M; d += kOneThreads) {
+      const double x = w[3 * d], y = w[3 * d + 1], z = w[3 * d + 2];
+      sWx[d] = x;
+      sWy[d] = y;
+      sWz[d] = z;
+      sVc1[d] = doppler ? __dmul_rn(v, __ddiv_rn(dot_rn(vx, vy, vz, x, y, z), v)) : 0.0;
+      sIa[d] = scale * a[d] * I[cell * M + d];
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < dir_count; k += kOneThreads) {
+      const int kk = dir_disp + k;
+      const double kx = w[3 * kk], ky = w[3 * kk + 1], kz = w[3 * kk + 2];
+      const double A = doppler ? __dadd_rn(1., -__dmul_rn(v, __ddiv_rn(dot_rn(vx, vy, vz, kx, ky, kz), v))) : 1.0;
+      const double A2 = A * A;
+      double acc0 = 0.0, acc1 = 0.0;
+#pragma unroll 2
+      for (int d = 0; d < M; d++) {
+        const double cosTh = dot_rn(kx, ky, kz, sWx[d], sWy[d], sWz[d]);
+        const double C = __dadd_rn(1.0, -cosTh), c2m1 = fma(cosTh, cosTh, -1.0);
+        const double den = __dadd_rn(__dadd_rn(1.0, __dmul_rn(el, C)), -sVc1[d]);
+        const double y = rcp_nr(den);
+        const double t = fma(fma(y, fma(A2, y, A * c2m1), 1.0), sIa[d], (d & 1) ? acc1 : acc0);
+        if (d & 1) acc1 = t; else acc0 = t;
+      }
+      S[cell * out_stride + k] = acc0 + acc1;
+    }
+  }
+}
+
 }  // namespace
 
 extern "C" rrhd_status rrhd_compton_full_spectrum(const rrhd_dirs *d, const double *I, const double *velocity,
@@ -272,6 +323,37 @@ extern "C" rrhd_status rrhd_compton_full_spectrum(const rrhd_dirs *d, const doub
   k_compton_full<<<(unsigned)grid, kThreads, sm, (cudaStream_t)stream>>>(
       I, velocity, d->d_w, d->d_a, 1.0 / d->full_area, S, cells, d->M, dir_disp, dir_count, out_stride, dch,
       tables());
+  RRHD_CUDA(cudaGetLastError());
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_compton_spectrum(const rrhd_dirs *d, const double *I, const double *velocity, double *S,
+                                             int64_t cells, double frq, int32_t dir_disp, int32_t dir_count,
+                                             int32_t out_stride, void *stream) {
+  RRHD_CHECK_ARG(d && cells >= 0, "bad arguments");
+  RRHD_CHECK_ARG(frq > 0 && std::isfinite(frq), "frq must be positive and finite");
+  RRHD_CHECK_ARG(dir_disp >= 0 && dir_count >= 0 && (int64_t)dir_disp + dir_count <= d->M,
+                 "directions dir_disp .. dir_disp + dir_count - 1 must lie in 0 .. M - 1");
+  RRHD_CHECK_ARG(out_stride >= dir_count, "out_stride must be at least dir_count");
+  if (cells == 0 || dir_count == 0) return RRHD_OK;
+  RRHD_CHECK_ARG(I && velocity && S, "null I, velocity or S");
+  RRHD_CHECK_ARG(((uintptr_t)I % 8) == 0 && ((uintptr_t)S % 8) == 0 && ((uintptr_t)velocity % 8) == 0,
+                 "I, S and velocity must be 8-byte aligned");
+  RRHD_CUDA(cudaSetDevice(d->device));
+  int dev = 0, sms = 0, optin = 0, per_sm = 0;
+  RRHD_CUDA(cudaGetDevice(&dev));
+  RRHD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  RRHD_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const size_t sm = sizeof(double) * 5 * (size_t)d->M;
+  RRHD_CHECK_ARG(sm <= (size_t)optin, "too many directions for shared memory");
+  if (sm > 48 * 1024)
+    RRHD_CUDA(cudaFuncSetAttribute(k_compton_one, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  RRHD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_compton_one, kOneThreads, sm));
+  const long long grid = std::min<long long>(cells, (long long)sms * std::max(per_sm, 1));
+  // 0.25 coef / A (cfl, :79; the weight's 2 pi r_e^2, :35) folded into the staged intensity
+  const double scale = kOneCfl * kCoef / d->full_area;
+  k_compton_one<<<(unsigned)grid, kOneThreads, sm, (cudaStream_t)stream>>>(
+      I, velocity, d->d_w, d->d_a, scale, kHmc * frq, S, cells, d->M, dir_disp, dir_count, out_stride);
   RRHD_CUDA(cudaGetLastError());
   return RRHD_OK;
 }

@@ -130,6 +130,24 @@ def FullSpectrumScattering(dg: DirectionGrid, I, velocity, S=None, dir_disp: int
     return S
 
 
+def SpectrumScattering(dg: DirectionGrid, I, velocity, frq: float, S=None, dir_disp: int = 0,
+                       dir_count: int | None = None, out_stride: int | None = None, stream=None):
+    """Compton-shifted scattering integral at one frequency frq (Hz), the reference's
+    CalculateSpectrumIntScattering / Get_spectrum_multi_device (cuda_interface_spectrum.cu:46-92,
+    cuda_scat_spectrum.cu:41-83).  I: CUDA float64 [cells, M] at frq; velocity: CUDA
+    float64 [cells, 3] in units of c.  Returns S [cells, out_stride]."""
+    import torch
+    assert I.is_cuda and I.is_contiguous() and I.dtype == torch.float64 and I.shape[1] == dg.size
+    assert velocity.is_contiguous() and velocity.dtype == torch.float64 and velocity.shape == (I.shape[0], 3)
+    dir_count = dg.size - dir_disp if dir_count is None else dir_count
+    out_stride = dir_count if out_stride is None else out_stride
+    if S is None:
+        S = torch.empty(I.shape[0], out_stride, dtype=torch.float64, device=I.device)
+    L.check(L.lib.rrhd_compton_spectrum(dg.handle, I.data_ptr(), velocity.data_ptr(), S.data_ptr(), I.shape[0], frq,
+                                        dir_disp, dir_count, out_stride, _stream(stream)), "rrhd_compton_spectrum")
+    return S
+
+
 class ScatterTC:
     """Tensor-core (tcgen05) scattering integral + moments for one direction set
     and precision form ("bf16x3", "f16x3", "f16", "bf16"); FP32 in/out."""

@@ -180,8 +180,11 @@ def compton_fixtures(out):
     S = oracle.ref_compton(I, vel, d.dirs, d.areas, d.full_area)
     S_part = oracle.ref_compton(I, vel, d.dirs, d.areas, d.full_area, dir_disp=5, dir_count=7, out_stride=9)
     frq = np.array([oracle.loader.ref_compton_get_frq(j) for j in range(101)])
+    S_one = np.stack([oracle.ref_compton_spectrum(I[:, :, f], vel, d.dirs, d.areas, d.full_area, nu)
+                      for f, nu in ((3, 1e12), (50, 4.2e20), (97, 9e23))])
     out["compton"] = dict(dirs=d.dirs, areas=d.areas, full_area=np.float64(d.full_area), I=I, vel=vel, S=S,
-                          S_part=S_part, get_frq=frq)
+                          S_part=S_part, get_frq=frq, S_one=S_one, one_bins=np.array([3, 50, 97]),
+                          one_frq=np.array([1e12, 4.2e20, 9e23]))
 
 
 FIXTURES = {"hydro": hydro_fixtures, "step": step_fixtures, "radiation": radiation_fixtures,

@@ -2,6 +2,9 @@
 the oracle's restatement of Get_full_spectrum_multi_device and the golden fixture
 made by the reference's own kernel source.
 
+The single-frequency kernel (rrhd_compton_spectrum, Get_spectrum_multi_device) is
+checked the same way.
+
 Bar: every S[i][k][f] within 1e-12 relative of the oracle (all terms are positive,
 so the sum is well conditioned; measured differences are a few 1e-16, from the
 regrouped arithmetic and FMA).  A shifted frequency within rounding of a bin edge
@@ -81,6 +84,37 @@ def test_compton_direction_slice_and_stride():
     dg.close()
 
 
+@pytest.mark.parametrize("M,cells,frq", [(32, 37, 1e12), (256, 9, 4.2e20), (64, 13, 9e23), (1000, 3, 3e23)])
+def test_single_frequency_matches_oracle(M, cells, frq):
+    d = fibonacci_directions(M)
+    I3, vel = compton_case(cells, M, seed=M)
+    I = np.ascontiguousarray(I3[:, :, 40])
+    So = oracle.port_compton_spectrum(I, vel, d.dirs, d.areas, d.full_area, frq, nthreads=os.cpu_count() or 1)
+    dg = illum.DirectionGrid(d)
+    S = illum.SpectrumScattering(dg, torch.tensor(I, device="cuda"), torch.tensor(vel, device="cuda"), frq)
+    Sp = torch.full((cells, M + 3), 5.0, dtype=torch.float64, device="cuda")
+    illum.SpectrumScattering(dg, torch.tensor(I, device="cuda"), torch.tensor(vel, device="cuda"), frq, S=Sp,
+                             dir_disp=2, dir_count=M - 2, out_stride=M + 3)
+    torch.cuda.synchronize()
+    err = _rel(S.cpu().numpy(), So)
+    print(f"\nsingle frequency M={M} frq={frq:.1e}: max rel {err:.2e}")
+    assert err <= TOL
+    assert torch.equal(Sp[:, :M - 2], S[:, 2:]) and torch.all(Sp[:, M - 2:] == 5.0)
+    dg.close()
+
+
+def test_single_frequency_matches_reference_golden_fixture():
+    g = np.load(os.path.join(HERE, "golden", "compton.npz"))
+    d = fibonacci_directions(len(g["areas"]))
+    dg = illum.DirectionGrid(d)
+    vt = torch.tensor(g["vel"], device="cuda")
+    for S1, f, nu in zip(g["S_one"], g["one_bins"], g["one_frq"]):
+        S = illum.SpectrumScattering(dg, torch.tensor(np.ascontiguousarray(g["I"][:, :, f]), device="cuda"), vt,
+                                     float(nu))
+        assert _rel(S.cpu().numpy(), S1) <= TOL
+    dg.close()
+
+
 def test_compton_invalid_arguments():
     from radrhd_solver_b200 import _lib as L
     dg = illum.DirectionGrid(fibonacci_directions(16))
@@ -93,5 +127,8 @@ def test_compton_invalid_arguments():
     assert f(dg.handle, I.data_ptr(), v.data_ptr(), S.data_ptr(), 4, 0, 16, 15, s) == L.RRHD_ERR_INVALID
     assert f(dg.handle, I.data_ptr(), v.data_ptr(), S.data_ptr() + 8, 4, 0, 16, 16, s) == L.RRHD_ERR_INVALID
     assert f(dg.handle, I.data_ptr(), v.data_ptr(), S.data_ptr(), 0, 0, 16, 16, s) == L.RRHD_OK
+    g = L.lib.rrhd_compton_spectrum
+    assert g(dg.handle, I.data_ptr(), v.data_ptr(), S.data_ptr(), 4, 0.0, 0, 16, 16, s) == L.RRHD_ERR_INVALID
+    assert g(dg.handle, I.data_ptr(), v.data_ptr(), S.data_ptr(), 4, 1e20, 3, 14, 16, s) == L.RRHD_ERR_INVALID
     torch.cuda.synchronize()
     dg.close()

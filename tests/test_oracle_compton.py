@@ -36,6 +36,24 @@ def test_port_matches_golden_fixture_bit_for_bit():
                              dir_count=7, out_stride=9)
     assert np.array_equal(Sp, g["S_part"])
     assert np.array_equal(np.array([oracle.port_compton_frq(j) for j in range(101)]), g["get_frq"])
+    for S1, f, nu in zip(g["S_one"], g["one_bins"], g["one_frq"]):
+        S1p = oracle.port_compton_spectrum(g["I"][:, :, f], g["vel"], g["dirs"], g["areas"], float(g["full_area"]), nu)
+        assert np.array_equal(S1p, S1)
+
+
+@pytest.mark.skipif(not oracle.have_ref("compton"), reason="reference Compton kernel not built (make -C oracle ref)")
+@pytest.mark.parametrize("frq", [1e9, 1e12, 3e20, 9e23, 5e24])
+def test_single_frequency_port_matches_reference_kernel_bit_for_bit(frq):
+    M = 24
+    d = fibonacci_directions(M)
+    I3, vel = compton_case(12, M, seed=6)
+    I = I3[:, :, 30]
+    Sr = oracle.ref_compton_spectrum(I, vel, d.dirs, d.areas, d.full_area, frq)
+    Sp = oracle.port_compton_spectrum(I, vel, d.dirs, d.areas, d.full_area, frq, nthreads=2)
+    assert np.array_equal(Sp, Sr)
+    Sr = oracle.ref_compton_spectrum(I, vel, d.dirs, d.areas, d.full_area, frq, dir_disp=4, dir_count=9, out_stride=11)
+    Sp = oracle.port_compton_spectrum(I, vel, d.dirs, d.areas, d.full_area, frq, dir_disp=4, dir_count=9, out_stride=11)
+    assert np.array_equal(Sp, Sr)
 
 
 @pytest.mark.skipif(not oracle.have_ref("compton"), reason="reference Compton kernel not built (make -C oracle ref)")
@@ -85,6 +103,18 @@ def test_low_frequency_rest_frame_limit_is_thomson():
     St = oracle.port_scatter(Id, d.dirs, d.areas, d.full_area)
     for f in range(1, 5):
         assert np.allclose(S[:, :, f], 4.0 / 3.0 * COEF * St, rtol=1e-6, atol=0)
+
+
+def test_single_frequency_low_limit_is_quarter_thomson():
+    """At rest and low frequency (no shift) the single-frequency kernel is
+    0.25 coef sum_d (1 + cos^2) I_d a_d / A = 1/3 coef S_Thomson (cfl = 0.25)."""
+    M = 24
+    d = fibonacci_directions(M)
+    rng = np.random.default_rng(9)
+    I = np.exp(rng.normal(0, 0.5, (3, M)))
+    S = oracle.port_compton_spectrum(I, np.zeros((3, 3)), d.dirs, d.areas, d.full_area, 1e9)
+    St = oracle.port_scatter(I, d.dirs, d.areas, d.full_area)
+    assert np.allclose(S, COEF / 3.0 * St, rtol=1e-9, atol=0)
 
 
 def test_direction_slice_equals_columns_of_full_result():
