@@ -583,6 +583,43 @@ def compton_component(dev, cells=1184, M=256, reps=3, cpu_cells=8):
     return out
 
 
+def ray_component(dev, n_box=48, n_sphere=64, frame=11, reps=3, cpu_rays=1500):
+    """Image-plane ray tracing (rrhd_ray_trace): one frame of 600 x 300 rays against the
+    triangulated boundary of a box around the scene plus a sphere around the accretor
+    (tests/cases.py ray_surface); the unit is one ray-triangle test.  The reference's own
+    kernel sources compiled for the host time a sample of the rays."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from cases import ray_surface
+    from radrhd_solver_b200 import ray_tracing as RT
+    ids, abc = ray_surface(n_box, n_sphere)
+    rt = RT.RayTracer(RT.face_cells(ids, abc), dev)
+    rays_h = RT.MakeRays(frame)
+    rays = torch.tensor(rays_h, device=f"cuda:{dev}")
+    codes = torch.empty(len(rays_h), dtype=torch.int32, device=f"cuda:{dev}")
+    stream = torch.cuda.current_stream(dev)
+    out = {"workload": f"ray tracing {len(rays_h)} rays x {len(ids)} triangles", "unit": "tests/s"}
+    tests = float(len(rays_h)) * len(ids)
+    for mode, name in ((RT.SURFACE, "surface"), (RT.ROCHE, "roche"), (RT.INNER, "inner")):
+        ms = _time(lambda: rt.trace(rays, mode, codes), reps, stream, warm=1)
+        out[name] = {"ms": ms, "tests_per_s": tests / (ms / 1e3)}
+    import oracle
+    sample = rays_h[:: len(rays_h) // cpu_rays][:cpu_rays]
+    t0 = time.perf_counter()
+    got = oracle.ref_ray(RT.SURFACE, sample, ids, abc, nthreads=cpu_threads())
+    kind = "reference"
+    if got is None:
+        got = oracle.port_ray_trace(RT.SURFACE, sample, ids, abc, nthreads=cpu_threads())
+        kind = "port"
+    dt = time.perf_counter() - t0
+    gpu = rt.trace(rays, RT.SURFACE, codes).cpu().numpy()[:: len(rays_h) // cpu_rays][:cpu_rays]
+    out["codes_equal_to_cpu"] = bool(np.array_equal(gpu, got))
+    out["cpu_baseline"] = {"value": len(sample) * float(len(ids)) / dt, "unit": "tests/s", "cores": cpu_threads(),
+                           "kind": kind, "sample": f"{len(sample)} rays of the frame, surface mode"}
+    rt.close()
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -692,6 +729,8 @@ def run_ours(args):
         line["scatter_scale"] = scatter_scale_component(dev)
     if rank == 0 and not args.no_compton:
         line["compton"] = compton_component(dev)
+    if rank == 0 and not args.no_ray:
+        line["ray_tracing"] = ray_component(dev)
     if rank == 0 and "coupled" in line:
         line.setdefault("chosen_vs_plain", {})["coupled_step"] = line["coupled"]["chosen_vs_plain"]
     if rank == 0:
@@ -727,6 +766,8 @@ def main():
     ap.add_argument("--c2p-only", type=int, default=0, metavar="STATES",
                     help="only time the con2prim component on STATES states (profiling runs)")
     ap.add_argument("--no-compton", action="store_true", help="skip the full-spectrum Compton component")
+    ap.add_argument("--no-ray", action="store_true", help="skip the image-plane ray-tracing component")
+    ap.add_argument("--ray-only", action="store_true", help="only time the image-plane ray tracing")
     ap.add_argument("--compton-only", type=int, default=0, metavar="CELLS",
                     help="only time the full-spectrum Compton scattering on CELLS cells")
     ap.add_argument("--compton-m", type=int, default=256, help="directions of --compton-only")
@@ -739,6 +780,11 @@ def main():
         import torch
         torch.cuda.set_device(0)
         print(json.dumps(scatter_component(0, nhex=args.scatter_only, reps=args.steps)), flush=True)
+        return
+    if args.ray_only:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(ray_component(0, reps=args.steps)), flush=True)
         return
     if args.compton_only:
         import torch

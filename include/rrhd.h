@@ -344,6 +344,43 @@ rrhd_status rrhd_compton_full_spectrum(const rrhd_dirs *d, const double *I, cons
 rrhd_status rrhd_compton_spectrum(const rrhd_dirs *d, const double *I, const double *velocity, double *S,
                                   int64_t cells, double frq, int32_t dir_disp, int32_t dir_count, int32_t out_stride,
                                   void *stream);
+/* ---- Image-plane ray tracing (solvers/ray_tracing, cuda/src/ray_tracing) ----------
+ * A surface of triangles resident on the device, replacing cuda::ray_tracing::interface::
+ * InitDevice / ClearDevice (cuda/src/ray_tracing/cuda_ray_interface.cu:83-99).  face_cells:
+ * n FaceCell records as the reference stores them (lib/geometry/include/geo_types.h:77-83:
+ * int32 face_id, 4 bytes padding, double A[3], B[3], C[3]; 80 bytes), host or device. */
+typedef struct rrhd_ray_surface rrhd_ray_surface;
+rrhd_status rrhd_ray_surface_create(const void *face_cells, int64_t n, int32_t device, rrhd_ray_surface **out);
+rrhd_status rrhd_ray_surface_destroy(rrhd_ray_surface *s);
+/* First intersection of each ray, replacing StartTracing / TracingGrid / FindInnerIntersection
+ * (cuda_ray_interface.cu:17-80) and their kernels (cuda/src/ray_tracing/cuda_ray_calc.cu):
+ *   mode RRHD_RAY_SURFACE (RayTracing), RRHD_RAY_ROCHE (RayTracing_Phl1445: the donor's Roche
+ *   lobe, cuda_ray_geo_intersect.cu:22-86, then nearer triangles), RRHD_RAY_INNER
+ *   (InnerRayTracing: accretor sphere / disk, :110-169, else the triangles), RRHD_RAY_GRID
+ *   (RayTracingGrid).  rays device [M] Ray_t records {orig[3], direction[3]} (48 bytes);
+ *   codes device [M]: the triangle's face_id, or RRHD_RAY_NONE / _DISK / _SPHERE / _ROCHE
+ *   (e_ray_intersect_code, ray_tracing_const.h).  Asynchronous on `stream`. */
+#define RRHD_RAY_SURFACE 0
+#define RRHD_RAY_ROCHE 1
+#define RRHD_RAY_INNER 2
+#define RRHD_RAY_GRID 3
+#define RRHD_RAY_NONE (-1)
+#define RRHD_RAY_DISK (-2)
+#define RRHD_RAY_SPHERE (-3)
+#define RRHD_RAY_LOBE (-4)
+rrhd_status rrhd_ray_trace(const rrhd_ray_surface *s, const double *rays, int64_t M, int32_t mode, int32_t *codes,
+                           void *stream);
+/* The image-plane rays of frame `frame` (ray_tracing::MakeRays, solvers/ray_tracing/src/
+ * ray_tracing_build_plane.cpp, constants of ray_tracing_const.h): host [600 * 300][6],
+ * ray i * 300 + j for pixel (i, j).  Host code. */
+rrhd_status rrhd_ray_make_rays(int32_t frame, double *rays);
+/* One frame of MakeIllumAndCurve / MakeEnergyAndCurve (ray_tracing_calc_illum.cpp): image[i]
+ * = value by code (0 none, 1e-5 Roche lobe, 5 disk, 10 sphere, else value[code / cell_size]),
+ * *curve = sum of image[i] * pixel_factor (pixel area for the illumination curve, 1 for the
+ * energy curve), in a fixed order.  *bad is OR-ed with 1 for a negative code the reference
+ * would stop on (DIE_IF).  All pointers device; asynchronous on `stream`. */
+rrhd_status rrhd_ray_image(const int32_t *codes, int64_t M, const double *value, int32_t cell_size,
+                           double pixel_factor, double *image, double *curve, int32_t *bad, void *stream);
 /* Reads (and with clear != 0 resets) the error word of the tensor-core kernels:
  * RRHD_ERR_CUDA if a bounded pipeline wait timed out.  Synchronises `stream`. */
 rrhd_status rrhd_scatter_tc_check(const rrhd_scatter_tc *t, void *stream, int32_t clear);

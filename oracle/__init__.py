@@ -12,5 +12,6 @@ from .loader import (HydroRef, build_port, have_ref, port, port_c2p, port_flux, 
                      ref_variant_for, port_get_illum, port_get_rhs, port_recalc_illum, port_sweep, ref_get_illum,
                      ref_get_rhs, ref_recalc_illum, ref_rad_constants, sweep_neighbours, port_compton,
                      port_compton_frq, port_compton_frq_idx, ref_compton, N_FRQ,
-                     port_compton_spectrum, ref_compton_spectrum)
+                     port_compton_spectrum, ref_compton_spectrum, port_ray_trace, port_ray_make_rays,
+                     ref_ray, ref_ray_make_rays, RAY_PIXELS)
 from . import loader  # noqa: F401

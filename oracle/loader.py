@@ -68,6 +68,8 @@ def port() -> C.CDLL:
             "orc_compton_full_spectrum": (None, [I32, P, P, D, I64, P, P, I32, I32, I32, P, C.c_int]),
             "orc_compton_frq": (D, [I32]), "orc_compton_frq_idx": (I32, [D]),
             "orc_compton_spectrum": (None, [I32, P, P, D, I64, P, P, D, I32, I32, I32, P, C.c_int]),
+            "orc_ray_triangle": (D, [P, P]), "orc_ray_roche": (I32, [P, P]), "orc_ray_sphere_disk": (I32, [P]),
+            "orc_ray_trace": (None, [I32, P, I64, P, P, I64, P, C.c_int]), "orc_ray_make_rays": (None, [I32, P]),
         }
         for n, (r, a) in sig.items():
             f = getattr(lib, n)
@@ -111,6 +113,8 @@ def ref(variant: str) -> C.CDLL | None:
         "ref_compton_n_frq": (C.c_int, []), "ref_compton_get_frq": (D, [C.c_int]),
         "ref_compton_get_frq_idx": (C.c_int, [D]), "ref_compton_gamma": (D, [D, D, P, D, D, P, P, P]),
         "ref_compton_spectrum": (C.c_int, [I32, P, P, D, I64, P, P, D, I32, I32, I32, P, C.c_int]),
+        "ref_ray_trace": (C.c_int, [I32, P, I32, P, P, I32, P, C.c_int]), "ref_ray_triangle": (D, [P, P]),
+        "ref_ray_roche": (C.c_int, [P, P]), "ref_ray_make_rays": (C.c_int, [C.c_int, P]),
     }
     for n, (r, a) in sig.items():
         f = getattr(lib, n, None)
@@ -583,3 +587,71 @@ def ref_compton_spectrum(I, vel, dirs, areas, full_area, frq, dir_disp=0, dir_co
     assert lib.ref_compton_spectrum(M, _p(dirs), _p(areas), full_area, cells, _p(I), _p(vel), frq, dir_disp,
                                     dir_count, out_stride, _p(S), nthreads) == 0
     return S
+
+
+RAY_PIXELS = (600, 300)  # image plane of solvers/ray_tracing/include/ray_tracing_const.h
+
+
+def _ray_args(rays, ids, abc):
+    rays = np.ascontiguousarray(rays, dtype=np.float64).reshape(-1, 6)
+    ids = np.ascontiguousarray(ids, dtype=np.int32)
+    abc = np.ascontiguousarray(abc, dtype=np.float64).reshape(-1, 9)
+    assert len(ids) == len(abc)
+    return rays, ids, abc
+
+
+def port_ray_trace(mode, rays, ids, abc, nthreads=1):
+    """Intersection code per ray (mode 0 RayTracing, 1 RayTracing_Phl1445, 2 InnerRayTracing,
+    3 RayTracingGrid) by the C restatement."""
+    rays, ids, abc = _ray_args(rays, ids, abc)
+    out = np.empty(len(rays), dtype=np.int32)
+    port().orc_ray_trace(mode, _p(rays), len(rays), _p(ids), _p(abc), len(ids), _p(out), nthreads)
+    return out
+
+
+def port_ray_make_rays(frame):
+    rays = np.empty((RAY_PIXELS[0] * RAY_PIXELS[1], 6))
+    port().orc_ray_make_rays(frame, _p(rays))
+    return rays
+
+
+def port_ray_triangle(ray, abc):
+    ray, abc = np.ascontiguousarray(ray, dtype=np.float64), np.ascontiguousarray(abc, dtype=np.float64)
+    return port().orc_ray_triangle(_p(ray), _p(abc))
+
+
+def port_ray_roche(ray):
+    ray = np.ascontiguousarray(ray, dtype=np.float64)
+    d = C.c_double()
+    code = port().orc_ray_roche(_p(ray), C.byref(d))
+    return code, d.value
+
+
+def ref_ray(mode, rays, ids, abc, nthreads=0):
+    """The same through the reference's own device source compiled for the host."""
+    lib = ref("ray")
+    if lib is None:
+        return None
+    rays, ids, abc = _ray_args(rays, ids, abc)
+    out = np.empty(len(rays), dtype=np.int32)
+    assert lib.ref_ray_trace(mode, _p(rays), len(rays), _p(ids), _p(abc), len(ids), _p(out), nthreads) == 0
+    return out
+
+
+def ref_ray_make_rays(frame):
+    lib = ref("ray")
+    rays = np.empty((RAY_PIXELS[0] * RAY_PIXELS[1], 6))
+    assert lib.ref_ray_make_rays(frame, _p(rays)) == len(rays)
+    return rays
+
+
+def ref_ray_triangle(ray, abc):
+    ray, abc = np.ascontiguousarray(ray, dtype=np.float64), np.ascontiguousarray(abc, dtype=np.float64)
+    return ref("ray").ref_ray_triangle(_p(ray), _p(abc))
+
+
+def ref_ray_roche(ray):
+    ray = np.ascontiguousarray(ray, dtype=np.float64)
+    d = C.c_double()
+    code = ref("ray").ref_ray_roche(_p(ray), C.byref(d))
+    return code, d.value

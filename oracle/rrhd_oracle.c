@@ -826,3 +826,207 @@ void orc_compton_spectrum(int32_t M, const double *dirs, const double *areas, do
     }
   }
 }
+
+/* ------------------------------------------------------------------ ray tracing
+ * Restates cuda/src/ray_tracing/cuda_ray_calc.cu and cuda_ray_geo_intersect.cu, and the
+ * image-plane construction of solvers/ray_tracing/src/ray_tracing_build_plane.cpp,
+ * in the reference's operation order (Eigen's cross product component by component
+ * as (a1 b2 - a2 b1, a2 b0 - a0 b2, a0 b1 - a1 b0)). */
+static inline void cross3(const double *a, const double *b, double *r) {
+  r[0] = a[1] * b[2] - a[2] * b[1];
+  r[1] = a[2] * b[0] - a[0] * b[2];
+  r[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* RayIntersectsTriangle, cuda_ray_calc.cu:10-44 */
+double orc_ray_triangle(const double *ray, const double *abc) {
+  const double eps = 1e-10;
+  const double *o = ray, *dir = ray + 3, *A = abc, *B = abc + 3, *C = abc + 6;
+  double e1[3], e2[3], h[3], s[3], q[3];
+  for (int k = 0; k < 3; k++) {
+    e1[k] = B[k] - A[k];
+    e2[k] = C[k] - A[k];
+  }
+  cross3(dir, e2, h);
+  const double det = dot3(e1, h);
+  if (det > -eps && det < eps) return -1;
+  const double inv_det = 1.0 / det;
+  for (int k = 0; k < 3; k++) s[k] = o[k] - A[k];
+  const double u = inv_det * dot3(s, h);
+  if (u < 0.0 || u > 1.0) return -1;
+  cross3(s, e1, q);
+  const double v = inv_det * dot3(dir, q);
+  if (v < 0.0 || u + v > 1.0) return -1;
+  const double dist = inv_det * dot3(e2, q);
+  if (dist > 0.0) return dist;
+  return -1;
+}
+
+/* Rosh, cuda_ray_geo_intersect.cu:22-42 */
+static double ray_rosh(const double *ray, double t) {
+  const double max_potential = -1.82547, m = 0.8795180722891566;
+  const double *S = ray, *a = ray + 3;
+  const double x1 = S[0] + a[0] * t;
+  const double x2 = (S[1] + a[1] * t) * (S[1] + a[1] * t);
+  const double x3 = (S[2] + a[2] * t) * (S[2] + a[2] * t);
+  return -max_potential - ((x1 - m) * (x1 - m) + x2 + x3) * 0.5 - m / sqrt((x1 - 1) * (x1 - 1) + x2 + x3) -
+         (1 - m) / sqrt(x1 * x1 + x2 + x3);
+}
+
+/* FindRoshRoots (:44-64) and GetIntersectionWithRosh (:66-86).  The reference stores the
+ * roots in an array of 6 without a bound; more than 6 sign changes would overrun it.  Here
+ * the count goes on, only the first 6 are stored (the result needs roots[1] and a count of
+ * 4 or 6), and the bubble sort of the already ascending roots is the identity. */
+int32_t orc_ray_roche(const double *ray, double *dist) {
+  const int n = 1001;
+  const double a = -3, b = 3;
+  const double step = (b - a) / (n - 1);
+  double roots[6];
+  int size = 0;
+  double fi_1 = ray_rosh(ray, a + 0 * step);
+  for (int i = 1; i < n; ++i) {
+    const double fi_2 = ray_rosh(ray, a + (i)*step);
+    if (fi_1 * fi_2 < 0) {
+      if (size < 6) roots[size] = ((2 * a + (2. * i - 1) * step) / 2.);
+      size++;
+    }
+    fi_1 = fi_2;
+  }
+  if (size == 6 || size == 4) {
+    const double x0 = ray[0] + ray[3] * roots[1];
+    if (x0 < 0.3) {
+      *dist = roots[1];
+      return ORC_RAY_ROCHE;
+    }
+  }
+  *dist = -1;
+  return ORC_RAY_NONE;
+}
+
+/* IntersectionWithPlane (:88-101) and GetIntersectionWithSphereOfDisk (:110-169); the
+ * reference returns "sphere" as soon as the ray meets the accretor sphere (the code after
+ * that return never runs). */
+int32_t orc_ray_sphere_disk(const double *ray) {
+  const double A[3] = {1, 0, 0}, B[3] = {0, 0.9928768384869221, 0.11914522061843064}, C[3] = {2, 0, 0};
+  const double *o = ray, *n = ray + 3;
+  const double pa = A[1] * (B[2] - C[2]) + B[1] * (C[2] - A[2]) + C[1] * (A[2] - B[2]);
+  const double pb = A[0] * (C[2] - B[2]) + B[0] * (A[2] - C[2]) + C[0] * (B[2] - A[2]);
+  const double pc = A[0] * (B[1] - C[1]) + B[0] * (C[1] - A[1]) + C[0] * (A[1] - B[1]);
+  const double pd = A[0] * (C[1] * B[2] - B[1] * C[2]) + B[0] * (A[1] * C[2] - C[1] * A[2]) +
+                    C[0] * (B[1] * A[2] - A[1] * B[2]);
+  const double t = -(pa * o[0] + pb * o[1] + pc * o[2] + pd) / (pa * n[0] + pb * n[1] + pc * n[2]);
+  double res[3];
+  for (int k = 0; k < 3; k++) res[k] = n[k] * t + o[k];
+  const double vec_1[3] = {1, 0, 0}, vec_2[3] = {0, -0.992877, -0.119145};
+  double loc0 = 0, loc1 = 0;
+  for (int k = 0; k < 3; k++) {
+    loc0 += (res[k]) * vec_1[k];
+    loc1 += (res[k]) * vec_2[k];
+  }
+  const double loc_x = loc0 - 1, loc_y = loc1 - 0;
+  const double loc_sq = loc_x * loc_x + loc_y * loc_y;
+  const double An = dot3(n, n);
+  const double oc[3] = {o[0] - 1, o[1] - 0, o[2] - 0};
+  const double proj = dot3(oc, n);
+  const double r_s = 0.01, r_in = 0.01, r_ex = 0.06;
+  const double radical = 4. * (proj * proj - An * (1 - 2 * o[0] + dot3(o, o) - r_s * r_s));
+  if (radical >= 0) return ORC_RAY_SPHERE;
+  if (loc_sq < r_ex * r_ex && (loc_sq > r_in * r_in)) return ORC_RAY_DISK;
+  return ORC_RAY_NONE;
+}
+
+/* RayTracing (:46-73), RayTracing_Phl1445 (:75-114), InnerRayTracing (:116-152),
+ * RayTracingGrid (:154-177): the nearest triangle hit (strictly closer than the best so
+ * far, so the first in index order among equal distances), after the Roche lobe (mode 1)
+ * or instead of the triangles when the accretor sphere or disk is met (mode 2). */
+void orc_ray_trace(int32_t mode, const double *rays, int64_t M, const int32_t *ids, const double *abc, int64_t N,
+                   int32_t *out, int nthreads) {
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads > 0 ? nthreads : 1)
+  for (int64_t r = 0; r < M; r++) {
+    const double *ray = rays + 6 * r;
+    int32_t loc_id = ORC_RAY_NONE;
+    double loc_dist = 1e10;
+    if (mode == 1) {
+      double rd;
+      if (orc_ray_roche(ray, &rd) != ORC_RAY_NONE) {
+        loc_dist = rd;
+        loc_id = ORC_RAY_ROCHE;
+      }
+    } else if (mode == 2) {
+      const int32_t code = orc_ray_sphere_disk(ray);
+      if (code != ORC_RAY_NONE) {
+        out[r] = code;
+        continue;
+      }
+    }
+    for (int64_t i = 0; i < N; i++) {
+      const double d = orc_ray_triangle(ray, abc + 9 * i);
+      if (d > 0 && d < loc_dist) {
+        loc_id = ids[i];
+        loc_dist = d;
+      }
+    }
+    out[r] = loc_id;
+  }
+}
+
+/* Eigen normalize: v / sqrt((x^2 + y^2) + z^2) component by component */
+static void normalize3(double *v) {
+  const double z = dot3(v, v);
+  if (z > 0) {
+    const double s = sqrt(z);
+    for (int k = 0; k < 3; k++) v[k] = v[k] / s;
+  }
+}
+
+/* intersection::SetBasis (lib/geometry/src/intersections.cpp:3-40), row-major basis */
+static void ray_set_basis(const double *nrm, double *basis) {
+  double v1[3], v2[3];
+  if (fabs(nrm[1]) < 1e-20) {
+    v1[0] = 0;
+    v1[1] = 1;
+    v1[2] = 0;
+  } else {
+    v1[0] = 1;
+    v1[2] = 0;
+    v1[1] = -(nrm[0] * v1[0] + nrm[2] * v1[2]) / nrm[1];
+  }
+  if (nrm[1] < 0)
+    for (int k = 0; k < 3; k++) v1[k] = -v1[k];
+  cross3(nrm, v1, v2);
+  normalize3(v1);
+  normalize3(v2);
+  for (int k = 0; k < 3; k++) {
+    basis[k] = v2[k];
+    basis[3 + k] = v1[k];
+    basis[6 + k] = nrm[k];
+  }
+}
+
+/* MakeRays(num_frame, rays) and MakeRays(center_ray, rays), ray_tracing_build_plane.cpp;
+ * constants of solvers/ray_tracing/include/ray_tracing_const.h (GRB_TASK plane 1.2 x 0.6,
+ * 600 x 300 pixels, 120 frames, height 0.1 above the centre of mass (0.879518, 0, 0)). */
+void orc_ray_make_rays(int32_t frame, double *rays) {
+  const double PIv = 3.1415926535897932384626433832795, com[3] = {0.879518, 0, 0};
+  const int nw = 600, nh = 300, nframes = 120;
+  const double width = 1.2, height = 0.6, above = 0.1;
+  const double start_angle = 2 * PIv / nframes * frame;
+  const double start[3] = {cos(start_angle) + com[0], sin(start_angle) + com[1], above + com[2]};
+  double dir[3] = {com[0] - start[0], com[1] - start[1], com[2] - start[2]};
+  normalize3(dir);
+  double basis[9];
+  ray_set_basis(dir, basis);
+  const double ap[3] = {-(width / 2), -(height / 2), 0};
+  const double step_x = width / nw, step_y = height / nh;
+  for (int i = 0; i < nw; ++i)
+    for (int j = 0; j < nh; ++j) {
+      const double o2[3] = {ap[0] + i * step_x, ap[1] + j * step_y, 0};
+      double o3[3];
+      matTvec(basis, o2, o3);
+      double *r = rays + 6 * ((int64_t)i * nh + j);
+      for (int k = 0; k < 3; k++) {
+        r[k] = o3[k] + start[k];
+        r[3 + k] = dir[k];
+      }
+    }
+}

@@ -135,6 +135,23 @@ int32_t orc_compton_frq_idx(double frq);
 void orc_compton_spectrum(int32_t M, const double *dirs, const double *areas, double full_area, int64_t cells,
                           const double *I, const double *vel, double frq, int32_t dir_disp, int32_t dir_count,
                           int32_t out_stride, double *S, int nthreads);
+/* Ray tracing of the image plane (cuda/src/ray_tracing/cuda_ray_calc.cu,
+ * cuda_ray_geo_intersect.cu).  ray [6] = {orig, dir}; abc [9] = {A, B, C}.
+ * Codes: -1 none, -2 disk, -3 sphere, -4 Roche lobe, else the triangle's id. */
+#define ORC_RAY_NONE (-1)
+#define ORC_RAY_DISK (-2)
+#define ORC_RAY_SPHERE (-3)
+#define ORC_RAY_ROCHE (-4)
+double orc_ray_triangle(const double *ray, const double *abc);
+int32_t orc_ray_roche(const double *ray, double *dist);
+int32_t orc_ray_sphere_disk(const double *ray);
+/* mode 0 RayTracing, 1 RayTracing_Phl1445, 2 InnerRayTracing, 3 RayTracingGrid; rays [M][6],
+ * ids [N], abc [N][9]; out [M]. */
+void orc_ray_trace(int32_t mode, const double *rays, int64_t M, const int32_t *ids, const double *abc, int64_t N,
+                   int32_t *out, int nthreads);
+/* ray_tracing::MakeRays(frame) (solvers/ray_tracing/src/ray_tracing_build_plane.cpp):
+ * rays [600 * 300][6], ray i * 300 + j for pixel (i, j). */
+void orc_ray_make_rays(int32_t frame, double *rays);
 
 #ifdef __cplusplus
 }

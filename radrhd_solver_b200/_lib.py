@@ -153,6 +153,11 @@ _SIGS = {
     "rrhd_scatter_lowrank_error": (I32, [P, P, P, I64, I32, P, P, P]),
     "rrhd_compton_full_spectrum": (I32, [P, P, P, P, I64, I32, I32, I32, P]),
     "rrhd_compton_spectrum": (I32, [P, P, P, P, I64, D, I32, I32, I32, P]),
+    "rrhd_ray_surface_create": (I32, [P, I64, I32, P]),
+    "rrhd_ray_surface_destroy": (I32, [P]),
+    "rrhd_ray_trace": (I32, [P, P, I64, I32, P, P]),
+    "rrhd_ray_make_rays": (I32, [I32, P]),
+    "rrhd_ray_image": (I32, [P, I64, P, I32, D, P, P, P, P]),
 }
 
 for _name, (_res, _args) in _SIGS.items():

@@ -37,6 +37,7 @@ SOURCES = {
     "c2p_mlp.cu": ["--fmad=false"],
     "sweep.cu": ["--fmad=false"],
     "compton.cu": [],
+    "raytrace.cu": ["--fmad=false"],
 }
 
 

@@ -80,3 +80,45 @@ def compton_case(cells, M_, seed=17, speeds=COMPTON_SPEEDS):
     u /= np.linalg.norm(u, axis=1, keepdims=True)
     vel = u * np.array([speeds[i % len(speeds)] for i in range(cells)])[:, None]
     return I, vel
+
+
+def ray_surface(n_box=12, n_sphere=16, seed=21):
+    """Triangle surface for the image-plane ray tracing: the boundary of the box
+    [0.43, 1.33] x [-0.35, 0.35] x [-0.25, 0.25] around the centre of mass (n_box x n_box
+    quads per side, two triangles each, shared edges as in a mesh boundary) and a
+    latitude-longitude sphere of radius 0.08 around the accretor (1, 0, 0) with jittered
+    vertices.  Returns unique shuffled ids [n] and vertices [n][9]."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.array([0.43, -0.35, -0.25]), np.array([1.33, 0.35, 0.25])
+    tris = []
+    g = np.linspace(0.0, 1.0, n_box + 1)
+    for ax in range(3):
+        u, v = [a for a in range(3) if a != ax]
+        for side in (0, 1):
+            for i in range(n_box):
+                for j in range(n_box):
+                    q = []
+                    for di, dj in ((0, 0), (1, 0), (1, 1), (0, 1)):
+                        p = np.empty(3)
+                        p[ax] = lo[ax] if side == 0 else hi[ax]
+                        p[u] = lo[u] + (hi[u] - lo[u]) * g[i + di]
+                        p[v] = lo[v] + (hi[v] - lo[v]) * g[j + dj]
+                        q.append(p)
+                    tris.append(np.concatenate([q[0], q[1], q[2]]))
+                    tris.append(np.concatenate([q[0], q[2], q[3]]))
+    c, r = np.array([1.0, 0.0, 0.0]), 0.08
+    th = np.linspace(0, np.pi, n_sphere + 1)
+    ph = np.linspace(0, 2 * np.pi, 2 * n_sphere + 1)
+    P = np.empty((n_sphere + 1, 2 * n_sphere + 1, 3))
+    for a in range(n_sphere + 1):
+        for b in range(2 * n_sphere + 1):
+            rr = r * (1 + (0.05 * rng.uniform(-1, 1) if 0 < a < n_sphere else 0))
+            P[a, b] = c + rr * np.array([np.sin(th[a]) * np.cos(ph[b % (2 * n_sphere)]),
+                                         np.sin(th[a]) * np.sin(ph[b % (2 * n_sphere)]), np.cos(th[a])])
+    for a in range(n_sphere):
+        for b in range(2 * n_sphere):
+            tris.append(np.concatenate([P[a, b], P[a + 1, b], P[a + 1, b + 1]]))
+            tris.append(np.concatenate([P[a, b], P[a + 1, b + 1], P[a, b + 1]]))
+    abc = np.array(tris)
+    ids = rng.permutation(4 * len(abc))[:len(abc)].astype(np.int32)
+    return ids, abc

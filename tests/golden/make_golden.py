@@ -187,14 +187,27 @@ def compton_fixtures(out):
                           one_frq=np.array([1e12, 4.2e20, 9e23]))
 
 
+def ray_fixtures(out):
+    """Image-plane rays of three frames (a sample of pixels) by the reference's MakeRays and
+    their intersection codes in the four tracing modes by its own kernels."""
+    from cases import ray_surface
+    ids, abc = ray_surface(6, 8)
+    frames = np.array([3, 40, 88])
+    sample = np.arange(0, 600 * 300, 173)
+    rays = np.stack([oracle.ref_ray_make_rays(int(f))[sample] for f in frames])
+    codes = np.stack([oracle.ref_ray(m, rays.reshape(-1, 6), ids, abc) for m in range(4)])
+    out["ray"] = dict(ids=ids, abc=abc, frames=frames, sample=sample, rays=rays, codes=codes)
+
+
 FIXTURES = {"hydro": hydro_fixtures, "step": step_fixtures, "radiation": radiation_fixtures,
-            "sweep": sweep_fixtures, "files": files_fixtures, "compton": compton_fixtures}
+            "sweep": sweep_fixtures, "files": files_fixtures, "compton": compton_fixtures,
+            "ray": ray_fixtures}
 
 
 def main():
     """`make_golden.py` regenerates every fixture; `make_golden.py compton ...` only the named ones."""
     names = sys.argv[1:] or list(FIXTURES)
-    need = list(VARIANTS) + ["illum", "rad_ideal_4_3", "compton"]
+    need = list(VARIANTS) + ["illum", "rad_ideal_4_3", "compton", "ray"]
     missing = [v for v in need if not oracle.have_ref(v)]
     if missing:
         sys.exit(f"reference variants not built ({', '.join(missing)}): run `make -C oracle ref` first")
