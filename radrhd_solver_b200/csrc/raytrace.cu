@@ -16,9 +16,9 @@
 //
 // Layout: the surface lives on the device as [n][9] doubles {A, B - A, C - A} plus the
 // triangles' ids; rays as the reference's Ray_t records {orig[3], direction[3]}.  A block
-// of 256 rays streams the triangles through shared memory in tiles of 256 (one coalesced
-// 72-byte record per thread), every thread testing its ray against each staged triangle
-// (broadcast reads).  Work is rays x triangles FP64 tests, most rejected after the
+// of 256 rays streams the triangles through shared memory in tiles of 256 (a thread
+// stages one triangle), every thread testing its ray against each staged triangle
+// (broadcast reads).  Work is rays x triangles FP64 tests, most rejected by the
 // barycentric u test.
 #include <cuda_runtime.h>
 
@@ -138,12 +138,24 @@ __device__ int sphere_disk(const double *o, const double *n) {
 // mode 0 RayTracing / 3 RayTracingGrid: nearest triangle; 1 RayTracing_Phl1445: the
 // Roche lobe first, triangles only if nearer; 2 InnerRayTracing: accretor sphere or disk,
 // else the nearest triangle.
+//
+// Two savings that leave every decision the reference's:
+//  * a block whose rays share one direction (every ray of an image plane does) stages
+//    h = dir x (C - A) and det = (B - A) . h once per triangle with the tile instead of once
+//    per ray and triangle (the same operations on the same operands, so the same bits);
+//  * u = fl(fl(1 / det) (s . h)) is first settled without the division where it is
+//    certain: u < 0 exactly when s . h is non-zero with the sign opposite to det, and
+//    u > 1 certainly when |s . h| > |det| (1 + 2^-48) (two roundings move it by less than
+//    2^-52); only the remaining tests divide, and then exactly as the reference does.
+constexpr int kRec = 16;  // doubles per staged triangle: A, B - A, C - A, h, det, padding
 __global__ void __launch_bounds__(kRayThreads)
     k_ray_trace(const double *__restrict__ rays, int64_t M, const double *__restrict__ tri,
                 const int32_t *__restrict__ ids, int64_t n, int mode, int32_t *__restrict__ out) {
-  __shared__ double st[kTile * 9];
+  __shared__ __align__(16) double st[kTile * kRec];
   __shared__ int32_t sid[kTile];
-  const int64_t r = blockIdx.x * (int64_t)kRayThreads + threadIdx.x;
+  __shared__ double dir0[3];
+  const int64_t r0 = blockIdx.x * (int64_t)kRayThreads;
+  const int64_t r = r0 + threadIdx.x;
   const bool live = r < M;
   double o[3] = {0, 0, 0}, dir[3] = {0, 0, 1};
   if (live)
@@ -151,6 +163,12 @@ __global__ void __launch_bounds__(kRayThreads)
       o[k] = rays[6 * r + k];
       dir[k] = rays[6 * r + 3 + k];
     }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; k++) dir0[k] = dir[k];
+  __syncthreads();
+  const bool uni = __syncthreads_and(!live || (__double_as_longlong(dir[0]) == __double_as_longlong(dir0[0]) &&
+                                               __double_as_longlong(dir[1]) == __double_as_longlong(dir0[1]) &&
+                                               __double_as_longlong(dir[2]) == __double_as_longlong(dir0[2])));
   int32_t best_id = kNone;
   double best = 1e10;
   bool done = !live;
@@ -167,22 +185,41 @@ __global__ void __launch_bounds__(kRayThreads)
       done = true;
     }
   }
+  constexpr double kHi = 1.0 + 3.552713678800501e-15;  // 1 + 2^-48
   for (int64_t t0 = 0; t0 < n; t0 += kTile) {
     const int nt = n - t0 < kTile ? (int)(n - t0) : kTile;
     __syncthreads();
-    for (int e = threadIdx.x; e < nt * 9; e += kRayThreads) st[e] = tri[9 * t0 + e];
-    if (threadIdx.x < nt) sid[threadIdx.x] = ids[t0 + threadIdx.x];
+    if (threadIdx.x < nt) {
+      const double *g = tri + 9 * (t0 + threadIdx.x);
+      double *T = st + kRec * threadIdx.x;
+      for (int k = 0; k < 9; k++) T[k] = g[k];
+      if (uni) {
+        double h[3];
+        cross3(dir0, T + 6, h);
+        T[9] = h[0], T[10] = h[1], T[11] = h[2];
+        T[12] = dot3(T + 3, h);
+      }
+      sid[threadIdx.x] = ids[t0 + threadIdx.x];
+    }
     __syncthreads();
     if (done) continue;
     for (int j = 0; j < nt; j++) {
-      const double *A = st + 9 * j, *e1 = A + 3, *e2 = A + 6;
-      double h[3];
-      cross3(dir, e2, h);
-      const double det = dot3(e1, h);
+      const double *A = st + kRec * j, *e1 = A + 3, *e2 = A + 6;
+      double h[3], det;
+      if (uni) {
+        h[0] = A[9], h[1] = A[10], h[2] = A[11];
+        det = A[12];
+      } else {
+        cross3(dir, e2, h);
+        det = dot3(e1, h);
+      }
       if (det > -kEps && det < kEps) continue;
-      const double inv_det = 1.0 / det;
       const double s[3] = {o[0] - A[0], o[1] - A[1], o[2] - A[2]};
-      const double u = inv_det * dot3(s, h);
+      const double un = dot3(s, h);
+      if (un != 0.0 && ((un < 0.0) != (det < 0.0))) continue;  // u < 0
+      if (fabs(un) > fabs(det) * kHi) continue;                // u > 1
+      const double inv_det = 1.0 / det;
+      const double u = inv_det * un;
       if (u < 0.0 || u > 1.0) continue;
       double q[3];
       cross3(s, e1, q);
