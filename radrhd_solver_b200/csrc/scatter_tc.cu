@@ -141,40 +141,33 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar) {
                : "memory");
 }
 
+// Four values to packed hi (and lo) 16-bit parts: hi = round-to-nearest 16-bit value, lo =
+// the rounded remainder (the three-product forms), two values per conversion instruction.
 template <int FORM>
-struct Split;
-template <>
-struct Split<FORM_BF16X3> {
-  __device__ static void run(float x, uint16_t &h, uint16_t &l) {
-    const __nv_bfloat16 a = __float2bfloat16_rn(x);
-    const __nv_bfloat16 b = __float2bfloat16_rn(x - __bfloat162float(a));
-    h = __bfloat16_as_ushort(a);
-    l = __bfloat16_as_ushort(b);
+__device__ __forceinline__ void split4(const float (&x)[4], uint2 &hi, uint2 &lo) {
+  if constexpr (FORM == FORM_F16X3 || FORM == FORM_F16) {
+    const __half2 a = __floats2half2_rn(x[0], x[1]), b = __floats2half2_rn(x[2], x[3]);
+    hi = make_uint2(*reinterpret_cast<const uint32_t *>(&a), *reinterpret_cast<const uint32_t *>(&b));
+    if constexpr (FORM == FORM_F16X3) {
+      const float2 fa = __half22float2(a), fb = __half22float2(b);
+      const __half2 c = __floats2half2_rn(x[0] - fa.x, x[1] - fa.y), d = __floats2half2_rn(x[2] - fb.x, x[3] - fb.y);
+      lo = make_uint2(*reinterpret_cast<const uint32_t *>(&c), *reinterpret_cast<const uint32_t *>(&d));
+    } else {
+      lo = make_uint2(0u, 0u);
+    }
+  } else {
+    const __nv_bfloat162 a = __floats2bfloat162_rn(x[0], x[1]), b = __floats2bfloat162_rn(x[2], x[3]);
+    hi = make_uint2(*reinterpret_cast<const uint32_t *>(&a), *reinterpret_cast<const uint32_t *>(&b));
+    if constexpr (FORM == FORM_BF16X3) {
+      const float2 fa = __bfloat1622float2(a), fb = __bfloat1622float2(b);
+      const __nv_bfloat162 c = __floats2bfloat162_rn(x[0] - fa.x, x[1] - fa.y),
+                           d = __floats2bfloat162_rn(x[2] - fb.x, x[3] - fb.y);
+      lo = make_uint2(*reinterpret_cast<const uint32_t *>(&c), *reinterpret_cast<const uint32_t *>(&d));
+    } else {
+      lo = make_uint2(0u, 0u);
+    }
   }
-};
-template <>
-struct Split<FORM_BF16> {
-  __device__ static void run(float x, uint16_t &h, uint16_t &l) {
-    h = __bfloat16_as_ushort(__float2bfloat16_rn(x));
-    l = 0;
-  }
-};
-template <>
-struct Split<FORM_F16X3> {
-  __device__ static void run(float x, uint16_t &h, uint16_t &l) {
-    const __half a = __float2half_rn(x);
-    const __half b = __float2half_rn(x - __half2float(a));
-    h = __half_as_ushort(a);
-    l = __half_as_ushort(b);
-  }
-};
-template <>
-struct Split<FORM_F16> {
-  __device__ static void run(float x, uint16_t &h, uint16_t &l) {
-    h = __half_as_ushort(__float2half_rn(x));
-    l = 0;
-  }
-};
+}
 
 struct TcParams {
   const float *I;
@@ -434,15 +427,11 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
             for (int q = 0; q < 4; q++) x[q] *= sc;
           }
-          uint16_t h[4], l[4];
-#pragma unroll
-          for (int q = 0; q < 4; q++) Split<FORM>::run(x[q], h[q], l[q]);
+          uint2 hv, lv;
+          split4<FORM>(x, hv, lv);
           const uint32_t off = row * 128 + ((((c4 >> 1) ^ (row & 7))) << 4) + ((c4 & 1) << 3);
-          *reinterpret_cast<uint2 *>(ah + off) =
-              make_uint2((uint32_t)h[0] | ((uint32_t)h[1] << 16), (uint32_t)h[2] | ((uint32_t)h[3] << 16));
-          if (THREE)
-            *reinterpret_cast<uint2 *>(al + off) =
-                make_uint2((uint32_t)l[0] | ((uint32_t)l[1] << 16), (uint32_t)l[2] | ((uint32_t)l[3] << 16));
+          *reinterpret_cast<uint2 *>(ah + off) = hv;
+          if (THREE) *reinterpret_cast<uint2 *>(al + off) = lv;
         };
         if constexpr (NG == 4) {
           // staged tile [32 cells][64 directions][4 groups]: unit (cell, c4) = float4s 4u..4u+3, one per direction
@@ -899,16 +888,12 @@ __global__ void __launch_bounds__(R_THREADS, 1)
 #pragma unroll
           for (int q = 0; q < 4; q++) x[q] *= f;
         }
-        uint16_t hv[4], lv[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) Split<FORM>::run(x[q], hv[q], lv[q]);
+        uint2 hv, lv;
+        split4<FORM>(x, hv, lv);
         const int row = cellrel(j) * NG + gsel;
         const uint32_t o = row * 128 + ((((c4 >> 1) ^ (row & 7))) << 4) + ((c4 & 1) << 3);
-        *reinterpret_cast<uint2 *>(ah + o) =
-            make_uint2((uint32_t)hv[0] | ((uint32_t)hv[1] << 16), (uint32_t)hv[2] | ((uint32_t)hv[3] << 16));
-        if (THREE)
-          *reinterpret_cast<uint2 *>(al + o) =
-              make_uint2((uint32_t)lv[0] | ((uint32_t)lv[1] << 16), (uint32_t)lv[2] | ((uint32_t)lv[3] << 16));
+        *reinterpret_cast<uint2 *>(ah + o) = hv;
+        if (THREE) *reinterpret_cast<uint2 *>(al + o) = lv;
       }
       // every lane's generic-proxy writes become visible to the MMA (async proxy)
       // before the warp's one arrival
