@@ -34,6 +34,14 @@ struct rrhd_ray_surface {
   int64_t n = 0;
   double *tri = nullptr;  // [n][9] {A, E1 = B - A, E2 = C - A}
   int32_t *ids = nullptr;
+  // image-plane bins (one trace call at a time per surface)
+  int32_t *bins = nullptr;    // [NB + 1] counts, then offsets
+  int32_t *cursor = nullptr;  // [NB]
+  int32_t *entries = nullptr; // [kMaxBins * n] triangle indices by bin
+  int32_t *glist = nullptr;   // [n] triangles every ray tests
+  long long *ctrl = nullptr;  // [8]: uniform flag, global count, ray box keys (x0, x1, y0, y1)
+  double *ray2d = nullptr;    // [cap][2]
+  int64_t ray_cap = 0;
 };
 
 namespace {
@@ -150,7 +158,9 @@ __device__ int sphere_disk(const double *o, const double *n) {
 constexpr int kRec = 16;  // doubles per staged triangle: A, B - A, C - A, h, det, padding
 __global__ void __launch_bounds__(kRayThreads)
     k_ray_trace(const double *__restrict__ rays, int64_t M, const double *__restrict__ tri,
-                const int32_t *__restrict__ ids, int64_t n, int mode, int32_t *__restrict__ out) {
+                const int32_t *__restrict__ ids, int64_t n, int mode, int32_t *__restrict__ out,
+                const long long *__restrict__ binned) {
+  if (binned && binned[0] != 0) return;  // every ray shares one direction: the image-plane bins answered
   __shared__ __align__(16) double st[kTile * kRec];
   __shared__ int32_t sid[kTile];
   __shared__ double dir0[3];
@@ -235,6 +245,244 @@ __global__ void __launch_bounds__(kRayThreads)
   if (live) out[r] = best_id;
 }
 
+// ---------------------------------------------------------------- image-plane bins
+// When every ray of a call has the same direction (an image plane), each ray tests only the
+// triangles whose projection onto the plane normal to that direction can contain the ray's
+// projected origin, instead of all of them; the test itself is unchanged, so the answer is
+// the brute-force one.  Soundness: a triangle the reference accepts for a ray contains the
+// ray's projected origin up to the rounding of its u, v (a few 1e-16 relative, amplified by
+// at most 1e6 for triangles neither sliver-shaped nor seen edge-on), and its projected box is
+// widened by 1e-7 of the scene size; slivers (sin of the corner angle < 1e-3), triangles seen
+// within 1e-3 of edge-on and triangles covering more than kMaxBins bins go to a list every ray
+// tests; triangles with |det| < 1e-10 never hit (the reference rejects them as parallel).  The
+// nearest hit is the smallest (distance, input index), which is what the reference's strictly-
+// closer loop in input order returns, so the bins need no order.
+constexpr int kGX = 256, kGY = 128, kNB = kGX * kGY;
+constexpr int kMaxBins = 128;
+constexpr double kMargin = 1e-7;
+
+__device__ __forceinline__ long long dkey(double x) {  // order-preserving double -> int64
+  const long long b = __double_as_longlong(x);
+  return b >= 0 ? b : b ^ 0x7fffffffffffffffll;
+}
+__device__ __forceinline__ double dval(long long k) {
+  return __longlong_as_double(k >= 0 ? k : k ^ 0x7fffffffffffffffll);
+}
+
+// orthonormal u, v spanning the plane normal to d
+__device__ void plane_basis(const double *d, double *u, double *v) {
+  const double ax = fabs(d[0]), ay = fabs(d[1]), az = fabs(d[2]);
+  const double e[3] = {(ax <= ay && ax <= az) ? 1.0 : 0.0, (!(ax <= ay && ax <= az) && ay <= az) ? 1.0 : 0.0,
+                       (!(ax <= ay && ax <= az) && !(ay <= az)) ? 1.0 : 0.0};
+  cross3(d, e, u);
+  const double nu = sqrt(dot3(u, u));
+  for (int k = 0; k < 3; k++) u[k] /= nu;
+  cross3(d, u, v);
+  const double nv = sqrt(dot3(v, v));
+  for (int k = 0; k < 3; k++) v[k] /= nv;
+}
+
+struct Box {
+  double x0, x1, y0, y1, ix, iy, margin;
+};
+__device__ Box ray_box(const long long *ctrl) {
+  Box b;
+  b.x0 = dval(ctrl[2]), b.x1 = dval(ctrl[3]), b.y0 = dval(ctrl[4]), b.y1 = dval(ctrl[5]);
+  b.ix = b.x1 > b.x0 ? kGX / (b.x1 - b.x0) : 0.0;
+  b.iy = b.y1 > b.y0 ? kGY / (b.y1 - b.y0) : 0.0;
+  b.margin = kMargin * (1.0 + fmax(fmax(fabs(b.x0), fabs(b.x1)), fmax(fabs(b.y0), fabs(b.y1))));
+  return b;
+}
+__device__ __forceinline__ int bin_x(const Box &b, double x) {
+  const double f = floor((x - b.x0) * b.ix);
+  return f < 0 ? 0 : f > kGX - 1 ? kGX - 1 : (int)f;
+}
+__device__ __forceinline__ int bin_y(const Box &b, double y) {
+  const double f = floor((y - b.y0) * b.iy);
+  return f < 0 ? 0 : f > kGY - 1 ? kGY - 1 : (int)f;
+}
+
+__global__ void k_bins_reset(int32_t *bins, long long *ctrl) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i <= kNB) bins[i] = 0;
+  if (i == 0) {
+    ctrl[0] = 1;  // uniform until a ray says otherwise
+    ctrl[1] = 0;
+    ctrl[2] = ctrl[4] = 0x7fffffffffffffffll;
+    ctrl[3] = ctrl[5] = -0x7fffffffffffffffll - 1;
+  }
+}
+
+// projected ray origins, their box, and whether all directions equal ray 0's
+__global__ void __launch_bounds__(256) k_rays_project(const double *__restrict__ rays, int64_t M, double *ray2d,
+                                                      long long *ctrl) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const double d0[3] = {rays[3], rays[4], rays[5]};
+  double u[3], v[3];
+  plane_basis(d0, u, v);
+  long long kx0 = 0x7fffffffffffffffll, ky0 = kx0, kx1 = -kx0 - 1, ky1 = kx1;
+  bool same = true;
+  if (r < M) {
+    const double *ry = rays + 6 * r;
+    same = __double_as_longlong(ry[3]) == __double_as_longlong(d0[0]) &&
+           __double_as_longlong(ry[4]) == __double_as_longlong(d0[1]) &&
+           __double_as_longlong(ry[5]) == __double_as_longlong(d0[2]);
+    const double x = dot3(ry, u), y = dot3(ry, v);
+    ray2d[2 * r] = x;
+    ray2d[2 * r + 1] = y;
+    kx0 = kx1 = dkey(x);
+    ky0 = ky1 = dkey(y);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    kx0 = min(kx0, __shfl_xor_sync(0xffffffffu, kx0, o));
+    kx1 = max(kx1, __shfl_xor_sync(0xffffffffu, kx1, o));
+    ky0 = min(ky0, __shfl_xor_sync(0xffffffffu, ky0, o));
+    ky1 = max(ky1, __shfl_xor_sync(0xffffffffu, ky1, o));
+  }
+  const bool all_same = __all_sync(0xffffffffu, same);
+  if ((threadIdx.x & 31) == 0) {
+    if (!all_same) atomicExch((unsigned long long *)&ctrl[0], 0ull);
+    atomicMin(&ctrl[2], kx0);
+    atomicMax(&ctrl[3], kx1);
+    atomicMin(&ctrl[4], ky0);
+    atomicMax(&ctrl[5], ky1);
+  }
+}
+
+// classification of triangle t for direction d0: -1 skip, 0 every-ray list, 1 binned (range out)
+__device__ int classify(const double *T, const double *d0, const double *u, const double *v, const Box &b,
+                        int *bx0, int *bx1, int *by0, int *by1) {
+  const double *e1 = T + 3, *e2 = T + 6;
+  double h[3];
+  cross3(d0, e2, h);
+  const double det = dot3(e1, h);
+  if (det > -kEps && det < kEps) return -1;  // rejected as parallel by the reference, whatever the ray
+  double n[3];
+  cross3(e1, e2, n);
+  const double nn = dot3(n, n), l1 = dot3(e1, e1), l2 = dot3(e2, e2), dd = dot3(d0, d0);
+  const double nd = dot3(n, d0);
+  if (!(nn >= 1e-6 * l1 * l2) || !(nd * nd >= 1e-6 * nn * dd)) return 0;
+  double xs[3], ys[3];
+  for (int k = 0; k < 3; k++) {
+    const double p[3] = {T[0] + (k == 1 ? e1[0] : k == 2 ? e2[0] : 0.0), T[1] + (k == 1 ? e1[1] : k == 2 ? e2[1] : 0.0),
+                         T[2] + (k == 1 ? e1[2] : k == 2 ? e2[2] : 0.0)};
+    xs[k] = dot3(p, u);
+    ys[k] = dot3(p, v);
+  }
+  const double m = b.margin + kMargin * fmax(fmax(fabs(xs[0]), fabs(ys[0])), fmax(fabs(T[0]), fabs(T[1])));
+  const double xmin = fmin(fmin(xs[0], xs[1]), xs[2]) - m, xmax = fmax(fmax(xs[0], xs[1]), xs[2]) + m;
+  const double ymin = fmin(fmin(ys[0], ys[1]), ys[2]) - m, ymax = fmax(fmax(ys[0], ys[1]), ys[2]) + m;
+  if (xmax < b.x0 || xmin > b.x1 || ymax < b.y0 || ymin > b.y1) return -1;  // no ray projects there
+  *bx0 = bin_x(b, xmin), *bx1 = bin_x(b, xmax), *by0 = bin_y(b, ymin), *by1 = bin_y(b, ymax);
+  return (*bx1 - *bx0 + 1) * (*by1 - *by0 + 1) > kMaxBins ? 0 : 1;
+}
+
+template <bool FILL>
+__global__ void __launch_bounds__(256) k_tri_bin(const double *__restrict__ rays, const double *__restrict__ tri,
+                                                 int64_t n, int32_t *bins, int32_t *cursor, int32_t *entries,
+                                                 int32_t *glist, long long *ctrl) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n || ctrl[0] == 0) return;
+  const double d0[3] = {rays[3], rays[4], rays[5]};
+  double u[3], v[3];
+  plane_basis(d0, u, v);
+  const Box b = ray_box(ctrl);
+  int bx0, bx1, by0, by1;
+  const int c = classify(tri + 9 * t, d0, u, v, b, &bx0, &bx1, &by0, &by1);
+  if (c < 0) return;
+  if (c == 0) {
+    if (!FILL) glist[atomicAdd((unsigned long long *)&ctrl[1], 1ull)] = (int32_t)t;
+    return;
+  }
+  for (int y = by0; y <= by1; y++)
+    for (int x = bx0; x <= bx1; x++) {
+      const int k = y * kGX + x;
+      if (FILL)
+        entries[atomicAdd(&cursor[k], 1)] = (int32_t)t;
+      else
+        atomicAdd(&bins[k], 1);
+    }
+}
+
+// exclusive scan of the kNB counts into offsets (bins[kNB] = total), cursor = offsets
+__global__ void __launch_bounds__(1024) k_bins_scan(int32_t *bins, int32_t *cursor) {
+  constexpr int per = kNB / 1024;
+  __shared__ int32_t part[1024];
+  const int base = threadIdx.x * per;
+  int32_t s = 0;
+  for (int i = 0; i < per; i++) s += bins[base + i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const int32_t add = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += add;
+    __syncthreads();
+  }
+  int32_t run = part[threadIdx.x] - s;
+  for (int i = 0; i < per; i++) {
+    const int32_t c = bins[base + i];
+    bins[base + i] = run;
+    cursor[base + i] = run;
+    run += c;
+  }
+  if (threadIdx.x == 1023) bins[kNB] = run;
+}
+
+// one thread per ray: its bin's triangles and the every-ray list, smallest (distance, index)
+__global__ void __launch_bounds__(256)
+    k_ray_trace_binned(const double *__restrict__ rays, int64_t M, const double *__restrict__ ray2d,
+                       const double *__restrict__ tri, const int32_t *__restrict__ ids, const int32_t *bins,
+                       const int32_t *entries, const int32_t *glist, const long long *ctrl, int mode,
+                       int32_t *__restrict__ out) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= M || ctrl[0] == 0) return;
+  const double o[3] = {rays[6 * r], rays[6 * r + 1], rays[6 * r + 2]};
+  const double dir[3] = {rays[6 * r + 3], rays[6 * r + 4], rays[6 * r + 5]};
+  int32_t code = kNone;
+  double best = 1e10;
+  int64_t best_t = -1;
+  if (mode == 1) {
+    double rd;
+    if (roche(o, dir, &rd) != kNone) {
+      best = rd;
+      code = kRoche;
+    }
+  } else if (mode == 2) {
+    const int c = sphere_disk(o, dir);
+    if (c != kNone) {
+      out[r] = c;
+      return;
+    }
+  }
+  auto test = [&](int64_t t) {
+    const double *A = tri + 9 * t, *e1 = A + 3, *e2 = A + 6;
+    double h[3];
+    cross3(dir, e2, h);
+    const double det = dot3(e1, h);
+    if (det > -kEps && det < kEps) return;
+    const double inv_det = 1.0 / det;
+    const double s[3] = {o[0] - A[0], o[1] - A[1], o[2] - A[2]};
+    const double u = inv_det * dot3(s, h);
+    if (u < 0.0 || u > 1.0) return;
+    double q[3];
+    cross3(s, e1, q);
+    const double v = inv_det * dot3(dir, q);
+    if (v < 0.0 || u + v > 1.0) return;
+    const double d = inv_det * dot3(e2, q);
+    if (d > 0.0 && (d < best || (d == best && best_t >= 0 && t < best_t))) {
+      best = d;
+      best_t = t;
+    }
+  };
+  const Box b = ray_box(ctrl);
+  const int k = bin_y(b, ray2d[2 * r + 1]) * kGX + bin_x(b, ray2d[2 * r]);
+  for (int e = bins[k]; e < bins[k + 1]; e++) test(entries[e]);
+  const int ng = (int)ctrl[1];
+  for (int e = 0; e < ng; e++) test(glist[e]);
+  out[r] = best_t >= 0 ? ids[best_t] : code;
+}
+
 // MakeIllumAndCurve / MakeEnergyAndCurve (ray_tracing_calc_illum.cpp): pixel value by
 // intersection code, curve = sum of value * pixel_factor.  One block: each thread sums a
 // strided slice, then a fixed-order tree, so the curve is deterministic.
@@ -310,6 +558,12 @@ extern "C" rrhd_status rrhd_ray_surface_destroy(rrhd_ray_surface *s) {
   cudaSetDevice(s->device);
   cudaFree(s->tri);
   cudaFree(s->ids);
+  cudaFree(s->bins);
+  cudaFree(s->cursor);
+  cudaFree(s->entries);
+  cudaFree(s->glist);
+  cudaFree(s->ctrl);
+  cudaFree(s->ray2d);
   delete s;
   return RRHD_OK;
 }
@@ -321,8 +575,38 @@ extern "C" rrhd_status rrhd_ray_trace(const rrhd_ray_surface *s, const double *r
   if (M == 0) return RRHD_OK;
   RRHD_CHECK_ARG(rays && codes, "null rays or codes");
   RRHD_CUDA(cudaSetDevice(s->device));
-  k_ray_trace<<<(unsigned)((M + kRayThreads - 1) / kRayThreads), kRayThreads, 0, (cudaStream_t)stream>>>(
-      rays, M, s->tri, s->ids, s->n, mode, codes);
+  rrhd_ray_surface *sm = const_cast<rrhd_ray_surface *>(s);
+  if (!sm->bins) {
+    RRHD_CUDA(cudaMalloc(&sm->bins, sizeof(int32_t) * (kNB + 1)));
+    RRHD_CUDA(cudaMalloc(&sm->cursor, sizeof(int32_t) * kNB));
+    RRHD_CUDA(cudaMalloc(&sm->ctrl, sizeof(long long) * 8));
+    if (s->n > 0) {
+      RRHD_CUDA(cudaMalloc(&sm->entries, sizeof(int32_t) * kMaxBins * (size_t)s->n));
+      RRHD_CUDA(cudaMalloc(&sm->glist, sizeof(int32_t) * (size_t)s->n));
+    }
+  }
+  if (sm->ray_cap < M) {
+    RRHD_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    cudaFree(sm->ray2d);
+    sm->ray2d = nullptr;
+    sm->ray_cap = 0;
+    RRHD_CUDA(cudaMalloc(&sm->ray2d, sizeof(double) * 2 * (size_t)M));
+    sm->ray_cap = M;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const unsigned rb = (unsigned)((M + 255) / 256), tb = (unsigned)((s->n + 255) / 256);
+  k_bins_reset<<<(kNB + 1 + 255) / 256, 256, 0, st>>>(sm->bins, sm->ctrl);
+  k_rays_project<<<rb, 256, 0, st>>>(rays, M, sm->ray2d, sm->ctrl);
+  if (s->n > 0) {
+    k_tri_bin<false><<<tb, 256, 0, st>>>(rays, s->tri, s->n, sm->bins, sm->cursor, sm->entries, sm->glist, sm->ctrl);
+    k_bins_scan<<<1, 1024, 0, st>>>(sm->bins, sm->cursor);
+    k_tri_bin<true><<<tb, 256, 0, st>>>(rays, s->tri, s->n, sm->bins, sm->cursor, sm->entries, sm->glist, sm->ctrl);
+  }
+  k_ray_trace_binned<<<rb, 256, 0, st>>>(rays, M, sm->ray2d, s->tri, s->ids, sm->bins, sm->entries, sm->glist,
+                                         sm->ctrl, mode, codes);
+  // rays of several directions: every ray against every triangle
+  k_ray_trace<<<(unsigned)((M + kRayThreads - 1) / kRayThreads), kRayThreads, 0, st>>>(rays, M, s->tri, s->ids, s->n,
+                                                                                        mode, codes, sm->ctrl);
   RRHD_CUDA(cudaGetLastError());
   return RRHD_OK;
 }
