@@ -404,27 +404,52 @@ __global__ void __launch_bounds__(256) k_tri_bin(const double *__restrict__ rays
     }
 }
 
-// exclusive scan of the kNB counts into offsets (bins[kNB] = total), cursor = offsets
+// exclusive scan of the kNB counts into offsets (bins[kNB] = total), cursor = offsets: a thread
+// owns 32 consecutive bins (vector loads, all in flight), warp shuffles scan the thread sums
 __global__ void __launch_bounds__(1024) k_bins_scan(int32_t *bins, int32_t *cursor) {
   constexpr int per = kNB / 1024;
-  __shared__ int32_t part[1024];
-  const int base = threadIdx.x * per;
-  int32_t s = 0;
-  for (int i = 0; i < per; i++) s += bins[base + i];
-  part[threadIdx.x] = s;
-  __syncthreads();
-  for (int o = 1; o < 1024; o <<= 1) {
-    const int32_t add = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
-    __syncthreads();
-    part[threadIdx.x] += add;
-    __syncthreads();
+  static_assert(per % 4 == 0, "bins per thread must be whole int4s");
+  __shared__ int32_t wsum[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int4 *b4 = reinterpret_cast<int4 *>(bins + per * threadIdx.x);
+  int4 *c4 = reinterpret_cast<int4 *>(cursor + per * threadIdx.x);
+  int32_t v[per];
+#pragma unroll
+  for (int i = 0; i < per / 4; i++) {
+    const int4 x = b4[i];
+    v[4 * i] = x.x, v[4 * i + 1] = x.y, v[4 * i + 2] = x.z, v[4 * i + 3] = x.w;
   }
-  int32_t run = part[threadIdx.x] - s;
-  for (int i = 0; i < per; i++) {
-    const int32_t c = bins[base + i];
-    bins[base + i] = run;
-    cursor[base + i] = run;
-    run += c;
+  int32_t sum = 0;
+#pragma unroll
+  for (int i = 0; i < per; i++) sum += v[i];
+  int32_t incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int32_t w = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t t = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += t;
+    }
+    wsum[lane] = w;
+  }
+  __syncthreads();
+  int32_t run = incl - sum + (warp > 0 ? wsum[warp - 1] : 0);
+#pragma unroll
+  for (int i = 0; i < per / 4; i++) {
+    int4 x;
+    x.x = run, run += v[4 * i];
+    x.y = run, run += v[4 * i + 1];
+    x.z = run, run += v[4 * i + 2];
+    x.w = run, run += v[4 * i + 3];
+    b4[i] = x;
+    c4[i] = x;
   }
   if (threadIdx.x == 1023) bins[kNB] = run;
 }
@@ -477,9 +502,16 @@ __global__ void __launch_bounds__(256)
   };
   const Box b = ray_box(ctrl);
   const int k = bin_y(b, ray2d[2 * r + 1]) * kGX + bin_x(b, ray2d[2 * r]);
-  for (int e = bins[k]; e < bins[k + 1]; e++) test(entries[e]);
+  const int e0 = bins[k], e1 = bins[k + 1];
+  int e = e0;
+  for (; e + 1 < e1; e += 2) {  // two candidates' loads in flight at once
+    const int t0 = entries[e], t1 = entries[e + 1];
+    test(t0);
+    test(t1);
+  }
+  if (e < e1) test(entries[e]);
   const int ng = (int)ctrl[1];
-  for (int e = 0; e < ng; e++) test(glist[e]);
+  for (int g = 0; g < ng; g++) test(glist[g]);
   out[r] = best_t >= 0 ? ids[best_t] : code;
 }
 
