@@ -1,0 +1,54 @@
+"""The drop-in adapter (adapter/rhllc_3d_stab_b200.cpp) inside the reference's own build.
+
+oracle/_ref/librrhd_ref_adapter_hydro_5_3.so is the reference's hydro sources (ideal gas,
+Gamma = 5/3) with the adapter linked in place of solvers/rhllc/src/rhllc_3d_stab.cpp, on the
+B200 library -- what a maintainer's build becomes.  Two grid_t objects, one per build, are
+stepped through the reference's own entry point rhllc::Hllc3dStab(tau, grid): cell states,
+face fluxes left in grid.faces[].f and rhllc::max_signal_speed must agree bit for bit."""
+import numpy as np
+import pytest
+
+import oracle
+from cases import GAMMA_53, shock_tube
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not (oracle.have_ref("adapter_hydro_5_3") and oracle.have_ref("hydro_ideal_5_3")),
+                                 reason="reference builds not present (make -C oracle ref)")]
+
+
+def test_adapter_hllc3dstab_matches_reference_build():
+    m, W = shock_tube(24, 4, 4)
+    W, U = oracle.port_p2c(W, 1, GAMMA_53)
+    ref = oracle.HydroRef(m, "hydro_ideal_5_3")
+    ada = oracle.HydroRef(m, "adapter_hydro_5_3")
+    ref.set_state(W, U)
+    ada.set_state(W, U)
+    tau = 0.3 * 0.25 / 24
+    for step in range(12):
+        s_ref = ref.step(tau, nthreads=4)
+        s_ada = ada.step(tau)
+        assert s_ada == s_ref, f"max signal speed differs at step {step}"
+    Wr, Ur = ref.get_state()
+    Wa, Ua = ada.get_state()
+    assert np.array_equal(Ua, Ur) and np.array_equal(Wa, Wr)
+    assert np.array_equal(ada.face_flux(), ref.face_flux())
+    assert np.abs(Ur - U).max() > 0  # the state moved
+    ref.close()
+    ada.close()
+
+
+def test_adapter_rebuilds_for_a_new_grid():
+    """A second grid (other size) through the same process: the adapter notices and
+    rebuilds its device copy."""
+    for n in (12, 16):
+        m, W = shock_tube(n, 2, 2)
+        W, U = oracle.port_p2c(W, 1, GAMMA_53)
+        ref = oracle.HydroRef(m, "hydro_ideal_5_3")
+        ada = oracle.HydroRef(m, "adapter_hydro_5_3")
+        ref.set_state(W, U)
+        ada.set_state(W, U)
+        for _ in range(3):
+            assert ada.step(1e-3) == ref.step(1e-3, nthreads=2)
+        assert all(np.array_equal(a, b) for a, b in zip(ada.get_state(), ref.get_state()))
+        ref.close()
+        ada.close()
