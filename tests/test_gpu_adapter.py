@@ -52,3 +52,42 @@ def test_adapter_rebuilds_for_a_new_grid():
         assert all(np.array_equal(a, b) for a, b in zip(ada.get_state(), ref.get_state()))
         ref.close()
         ada.close()
+
+
+def test_radiation_adapter_through_the_reference_interface():
+    """adapter/cuda_interface_sep_b200.cpp under the reference's headers and types:
+    separate_device::InitDevice on a grid_t / grid_directions_t, then
+    CalculateIntScatteringAsync as the illum drivers call it.  grid.scattering and the
+    energy / stream / impulse moments equal the oracle's restatement of the reference
+    kernels bit for bit, for all directions and for a slice of them."""
+    import ctypes as C
+    import os
+
+    from cases import intensity
+    from radrhd_solver_b200.mesh import fibonacci_directions
+    path = os.path.join(oracle.loader.REF_DIR, "librrhd_ref_adapter_rad.so")
+    if not os.path.exists(path):
+        pytest.skip("radiation adapter build not present (make -C oracle ref)")
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    lib.radad_create.restype = P
+    lib.radad_create.argtypes = [C.c_int64, C.c_int32, P, P, C.c_double]
+    lib.radad_scatter.restype = C.c_int
+    lib.radad_scatter.argtypes = [P, P, C.c_int32, C.c_int32, P, P, P, P]
+    lib.radad_destroy.argtypes = [P]
+    N, M = 700, 64
+    d = fibonacci_directions(M)
+    I = np.ascontiguousarray(intensity(N, M, seed=14))
+    h = lib.radad_create(N, M, d.dirs.ctypes.data, d.areas.ctypes.data, d.full_area)
+    assert h
+    So = oracle.port_scatter(I, d.dirs, d.areas, d.full_area)
+    Eo, Fo, To = oracle.port_moments(I, d.dirs, d.areas, d.full_area)
+    for start, end in ((0, M), (10, 30)):
+        S = np.zeros((N, end - start))
+        E, F, T = np.zeros(N), np.zeros((N, 3)), np.zeros((N, 9))
+        assert lib.radad_scatter(h, I.ctypes.data, start, end, S.ctypes.data, E.ctypes.data, F.ctypes.data,
+                                 T.ctypes.data) == 0
+        assert np.array_equal(S, So[:, start:end])
+        assert np.array_equal(E, Eo) and np.array_equal(F, Fo)
+        assert np.array_equal(T.reshape(N, 3, 3), To.reshape(N, 3, 3))
+    lib.radad_destroy(h)
