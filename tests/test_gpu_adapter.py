@@ -91,3 +91,29 @@ def test_radiation_adapter_through_the_reference_interface():
         assert np.array_equal(E, Eo) and np.array_equal(F, Fo)
         assert np.array_equal(T.reshape(N, 3, 3), To.reshape(N, 3, 3))
     lib.radad_destroy(h)
+
+
+def test_ray_tracing_adapter_through_the_reference_interface():
+    """adapter/cuda_ray_interface_b200.cpp under the reference's headers and types: the
+    FaceCell / Ray_t vectors of RunRayTracing through InitDevice and the four tracing calls;
+    every intersection code equals the reference kernels' (compiled for the host), including
+    the reference's call-to-kernel mapping (StartTracing = the Roche-lobe kernel)."""
+    import ctypes as C
+    import os
+
+    from cases import ray_surface
+    path = os.path.join(oracle.loader.REF_DIR, "librrhd_ref_adapter_ray.so")
+    if not os.path.exists(path) or not oracle.have_ref("ray"):
+        pytest.skip("ray adapter or reference ray build not present (make -C oracle ref)")
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    lib.rayad_run.restype = C.c_int
+    lib.rayad_run.argtypes = [P, P, C.c_int64, P, C.c_int64, C.c_int, P]
+    ids, abc = ray_surface(8, 10)
+    ids, abc = np.ascontiguousarray(ids), np.ascontiguousarray(abc)
+    rays = np.ascontiguousarray(oracle.port_ray_make_rays(19)[::7])
+    for call, mode in ((0, 1), (1, 0), (2, 2), (3, 3)):
+        out = np.empty(len(rays), dtype=np.int32)
+        assert lib.rayad_run(ids.ctypes.data, abc.ctypes.data, len(ids), rays.ctypes.data, len(rays), call,
+                             out.ctypes.data) == 0
+        assert np.array_equal(out, oracle.ref_ray(mode, rays, ids, abc))
