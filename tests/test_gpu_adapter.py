@@ -117,3 +117,49 @@ def test_ray_tracing_adapter_through_the_reference_interface():
         assert lib.rayad_run(ids.ctypes.data, abc.ctypes.data, len(ids), rays.ctypes.data, len(rays), call,
                              out.ctypes.data) == 0
         assert np.array_equal(out, oracle.ref_ray(mode, rays, ids, abc))
+
+
+def test_spectrum_adapter_through_the_reference_interface():
+    """The SPECTRUM build of adapter/cuda_interface_sep_b200.cpp: SendVelocity and
+    CalculateFullSpectrumIntScattering / CalculateSpectrumIntScattering as the spectrum
+    module calls them (grid_t with size_frq = 100, frq_grid, cur_frq_id).  The scattering
+    equals the reference's own Compton kernels compiled for the host to within 1e-12."""
+    import ctypes as C
+    import os
+
+    from cases import compton_case
+    from radrhd_solver_b200.mesh import fibonacci_directions
+    path = os.path.join(oracle.loader.REF_DIR, "librrhd_ref_adapter_rad_spectrum.so")
+    if not os.path.exists(path) or not oracle.have_ref("compton"):
+        pytest.skip("spectrum adapter or reference Compton build not present (make -C oracle ref)")
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    lib.radad_create.restype = P
+    lib.radad_create.argtypes = [C.c_int64, C.c_int32, P, P, C.c_double]
+    lib.radad_full_spectrum.restype = C.c_int
+    lib.radad_full_spectrum.argtypes = [P, P, P, C.c_int32, C.c_int32, P]
+    lib.radad_spectrum.restype = C.c_int
+    lib.radad_spectrum.argtypes = [P, P, P, C.c_double, C.c_double, C.c_int32, C.c_int32, P]
+    lib.radad_destroy.argtypes = [P]
+    N, M = 9, 32
+    d = fibonacci_directions(M)
+    I, vel = compton_case(N, M, seed=41)
+    I, vel = np.ascontiguousarray(I), np.ascontiguousarray(vel)
+    h = lib.radad_create(N, M, d.dirs.ctypes.data, d.areas.ctypes.data, d.full_area)
+    assert h
+
+    def rel(a, b):
+        assert np.array_equal(a == 0, b == 0)
+        nz = b != 0
+        return np.max(np.abs(a[nz] - b[nz]) / np.abs(b[nz]))
+
+    for start, end in ((0, M), (4, 20)):
+        S = np.zeros((N, end - start, 100))
+        assert lib.radad_full_spectrum(h, I.ctypes.data, vel.ctypes.data, start, end, S.ctypes.data) == 0
+        want = oracle.ref_compton(I, vel, d.dirs, d.areas, d.full_area, dir_disp=start, dir_count=end - start)
+        assert rel(S, want) <= 1e-12
+    I1 = np.ascontiguousarray(I[:, :, 55])
+    S1 = np.zeros((N, M))
+    assert lib.radad_spectrum(h, I1.ctypes.data, vel.ctypes.data, 3e20, 5e20, 0, M, S1.ctypes.data) == 0
+    assert rel(S1, oracle.ref_compton_spectrum(I1, vel, d.dirs, d.areas, d.full_area, 0.5 * (3e20 + 5e20))) <= 1e-12
+    lib.radad_destroy(h)
