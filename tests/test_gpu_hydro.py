@@ -258,3 +258,41 @@ def test_host_dropin_matches_device_path():
     L.check(L.lib.rrhd_set_state(g.handle, L.ptr(rec), L.ptr(rec[:, 5:]), 17, L.RRHD_HOST))
     Wg, Ug = g.get_state()
     assert np.array_equal(Wg, W) and np.array_equal(Ug, U) and Wv.shape == W.shape
+
+
+def test_config0_shock_tube_200_steps_matches_reference():
+    """The plain form's parity case as specified: the relativistic shock tube on
+    [0,1] x [0,0.05]^2, 200 x 10 x 10 hexes split into 6 Kuhn tets (120,000 cells, interior
+    vertices jittered by +-0.15 h), ideal gas Gamma = 5/3, CFL 0.3, transmissive boundaries,
+    200 steps with tau = CFL h_min / (previous step's max signal speed).  Every conserved and
+    primitive field of every cell equals the reference's own compiled Hllc3dStab (the oracle
+    restatement where that build is absent) after every 20th step and at the end."""
+    import os
+    m, W = shock_tube(200, 10, 10)
+    assert m.n_cells == 120000
+    W, U = oracle.port_p2c(W, 1, GAMMA_53)
+    use_ref = oracle.have_ref("hydro_ideal_5_3")
+    ref = oracle.HydroRef(m, "hydro_ideal_5_3") if use_ref else None
+    if use_ref:
+        ref.set_state(W, U)
+    g = _grid(m, GAMMA_53)
+    g.set_state(W, U)
+    tau = 0.3 * m.h_min / 1.0
+    threads = os.cpu_count() or 1
+    for k in range(200):
+        st = rhllc.Hllc3dStab(tau, g)
+        if use_ref:
+            vmax = ref.step(tau, nthreads=threads)
+        else:
+            U, W, _, _, vmax = oracle.port_hydro_step(m, U, W, tau, 1, GAMMA_53, nthreads=threads)
+        assert st.max_speed == vmax, f"step {k}: max signal speed differs"
+        if k % 20 == 19:
+            Wo, Uo = ref.get_state() if use_ref else (W, U)
+            Wg, Ug = g.get_state()
+            assert np.array_equal(Ug, Uo), f"step {k}: U differs, max {np.abs(Ug - Uo).max()}"
+            assert np.array_equal(Wg, Wo), f"step {k}: W differs"
+        tau = 0.3 * m.h_min / vmax
+    assert st.n_failed == 0
+    g.close()
+    if use_ref:
+        ref.close()
