@@ -270,10 +270,12 @@ rrhd_status rrhd_moments_fp64(const rrhd_dirs *d, const double *I, double *E, do
 /* Scattering integral and moments on the tensor cores (tcgen05), FP32 in/out.
  * The same contraction as rrhd_scatter_fp64 plus the moments as 16 extra
  * output columns, with the kernel matrix split into 16-bit parts once at
- * creation.  Forms (error against FP64 measured by the tests):
- *   RRHD_TC_BF16X3 : bf16 hi/lo split of I and K, three products
- *   RRHD_TC_F16X3  : per-row power-of-two scaled fp16 hi/lo split, three products
- *   RRHD_TC_F16    : per-row scaled fp16, one product
+ * creation.  Forms (maximum relative error against FP64 measured by the tests on the
+ * 256- and 512-direction cases, intensities over 12 decades):
+ *   RRHD_TC_BF16X3 : bf16 hi/lo split of I and K, three products        (about 1e-5)
+ *   RRHD_TC_F16X3  : per-row power-of-two scaled fp16 hi/lo split, three
+ *                    products                                           (below 1e-6)
+ *   RRHD_TC_F16    : per-row scaled fp16, one product                   (about 5e-4)
  *   RRHD_TC_BF16   : bf16, one product
  * M must be 64, 128, 192, 256 or a multiple of 256 (<= 1024).  Stands behind
  * CalculateIntScatteringAsync + CalculateAllParamAsync (cuda_multi_interface.h:69, :81). */

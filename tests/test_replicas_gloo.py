@@ -1,5 +1,5 @@
 """The multi-GPU path of bench.py is replicas only (the sweep, the hydro step and the
-scattering of the north-star workloads run on one GPU; no data-path collective):
+scattering of the benchmark workloads run on one GPU; no data-path collective):
 each rank times its own replica and the job time is the maximum over ranks.  This
 checks that host logic with two gloo ranks on CPU."""
 import os
