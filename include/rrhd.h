@@ -360,7 +360,7 @@ rrhd_status rrhd_ray_surface_destroy(rrhd_ray_surface *s);
  *   lobe, cuda_ray_geo_intersect.cu:22-86, then nearer triangles), RRHD_RAY_INNER
  *   (InnerRayTracing: accretor sphere / disk, :110-169, else the triangles), RRHD_RAY_GRID
  *   (RayTracingGrid).  rays device [M] Ray_t records {orig[3], direction[3]} (48 bytes);
- *   codes device [M]: the triangle's face_id, or RRHD_RAY_NONE / _DISK / _SPHERE / _ROCHE
+ *   codes device [M]: the triangle's face_id, or RRHD_RAY_NONE / _DISK / _SPHERE / _LOBE
  *   (e_ray_intersect_code, ray_tracing_const.h).  Asynchronous on `stream`.  Rays sharing one
  *   direction (an image plane) are answered through image-plane bins kept with the surface, so
  *   calls on one surface must not overlap on the GPU; the first call, and a call with more rays
