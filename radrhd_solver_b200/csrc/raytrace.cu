@@ -259,6 +259,7 @@ __global__ void __launch_bounds__(kRayThreads)
 // closer loop in input order returns, so the bins need no order.
 constexpr int kGX = 256, kGY = 128, kNB = kGX * kGY;
 constexpr int kMaxBins = 128;
+constexpr int64_t kMaxBinnedTriangles = 0x7fffffff / kMaxBins;  // bin offsets stay within int32
 constexpr double kMargin = 1e-7;
 
 __device__ __forceinline__ long long dkey(double x) {  // order-preserving double -> int64
@@ -607,6 +608,14 @@ extern "C" rrhd_status rrhd_ray_trace(const rrhd_ray_surface *s, const double *r
   if (M == 0) return RRHD_OK;
   RRHD_CHECK_ARG(rays && codes, "null rays or codes");
   RRHD_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (s->n > kMaxBinnedTriangles) {
+    // bin offsets are 32-bit: a surface this large takes the every-triangle kernel
+    k_ray_trace<<<(unsigned)((M + kRayThreads - 1) / kRayThreads), kRayThreads, 0, st>>>(rays, M, s->tri, s->ids,
+                                                                                          s->n, mode, codes, nullptr);
+    RRHD_CUDA(cudaGetLastError());
+    return RRHD_OK;
+  }
   rrhd_ray_surface *sm = const_cast<rrhd_ray_surface *>(s);
   if (!sm->bins) {
     RRHD_CUDA(cudaMalloc(&sm->bins, sizeof(int32_t) * (kNB + 1)));
@@ -625,7 +634,6 @@ extern "C" rrhd_status rrhd_ray_trace(const rrhd_ray_surface *s, const double *r
     RRHD_CUDA(cudaMalloc(&sm->ray2d, sizeof(double) * 2 * (size_t)M));
     sm->ray_cap = M;
   }
-  cudaStream_t st = (cudaStream_t)stream;
   const unsigned rb = (unsigned)((M + 255) / 256), tb = (unsigned)((s->n + 255) / 256);
   k_bins_reset<<<(kNB + 1 + 255) / 256, 256, 0, st>>>(sm->bins, sm->ctrl);
   k_rays_project<<<rb, 256, 0, st>>>(rays, M, sm->ray2d, sm->ctrl);
