@@ -151,6 +151,53 @@ rrhd_status rrhd_get_face_flux(rrhd_ctx *ctx, double *F);
 /* Per-cell status bytes of the last step (bits above), caller's numbering. */
 rrhd_status rrhd_get_cell_status(rrhd_ctx *ctx, uint8_t *status);
 
+/* ------------------------------------------------ hydro step split over ranks */
+
+/* Cell order of a context built on `mesh` with rrhd_opts.renumber = `renumber`:
+ * order[k] = caller id of the context's k-th cell (Morton order of the cell centres, or
+ * the input order when renumber < 0).  Host only; needs no device. */
+rrhd_status rrhd_cell_order(const rrhd_mesh_desc *mesh, int32_t renumber, int32_t *order);
+
+/* Split of the hydro step over `world` ranks, each holding the whole mesh: rank q updates
+ * the CTA blocks [nb q/world, nb (q+1)/world) of the context order (nb blocks of
+ * `cells_per_block` cells; 0 = 256) and exchanges with the other ranks the states of the
+ * face neighbours of its cells that they update.  Host only; needs no device.
+ *   cell_range[2]   this rank's cells [begin, end) in context order;
+ *   send_counts, recv_counts [world]: cells sent to / received from each rank;
+ *   send_ids, recv_ids: context-order cell ids grouped by peer in rank order, ascending
+ *                   within a peer (NULL for a counts-only call).
+ * rank q's recv_ids from rank p equal rank p's send_ids to rank q.  Stands behind
+ * rhllc_mpi::InitMpiConfig (solvers/rhllc/src/rhllc_3d_mpi.cpp:86-369), whose partition
+ * is a caller-grouped METIS map; here it is Morton-ordered CTA blocks. */
+rrhd_status rrhd_part_plan(const rrhd_mesh_desc *mesh, const int32_t *order, int32_t cells_per_block,
+                           int32_t world, int32_t rank, int64_t *cell_range, int64_t *send_counts,
+                           int64_t *recv_counts, int32_t *send_ids, int32_t *recv_ids);
+
+/* Restricts the context's hydro step to rank `rank`'s blocks of rrhd_part_plan and keeps
+ * its exchange lists on the device; world = 1 restores the whole-mesh step.  Cells outside
+ * the rank's range are not written by the step.  A rank's step follows the reference's
+ * rhllc_mpi::Hllc3dStab (rhllc_3d_mpi.cpp:371-486):
+ *   rrhd_hydro_pack_halo -> exchange of the send / recv buffers between ranks ->
+ *   rrhd_hydro_unpack_halo -> rrhd_hydro_step -> max-reduction over ranks of the double
+ *   at rrhd_hydro_max_speed_ptr (the next step's tau <= 0 reads it).
+ * The coupled step and rrhd_hydro_step_host refuse a split context. */
+rrhd_status rrhd_hydro_set_part(rrhd_ctx *ctx, int32_t world, int32_t rank);
+/* cell_range[2], send_counts / recv_counts [world] of the split, and the caller ids of the
+ * rank's cells [cell_range[1] - cell_range[0]].  Any pointer may be NULL. */
+rrhd_status rrhd_hydro_part_info(rrhd_ctx *ctx, int64_t *cell_range, int64_t *send_counts,
+                                 int64_t *recv_counts, int32_t *cells);
+/* Gathers the current states (U(5), W(5): 10 doubles a cell) of the cells to send into
+ * send_buf [sum send_counts][10] (device), in send_ids order, on the context's stream.
+ * Stands behind the send side of StartExchangeBoundaryCells (rhllc_3d_mpi.cpp:69-80). */
+rrhd_status rrhd_hydro_pack_halo(rrhd_ctx *ctx, double *send_buf);
+/* Scatters recv_buf [sum recv_counts][10] (device) into the current states of the
+ * received cells, on the context's stream (SyncExchangeBoundaryCells, :81-85). */
+rrhd_status rrhd_hydro_unpack_halo(rrhd_ctx *ctx, const double *recv_buf);
+/* Device address of the last step's max signal speed (one double; the address alternates
+ * between steps, so query it after every step).  rhllc::max_signal_speed, which
+ * rhllc_mpi::Hllc3dStab reduces with MPI_MAX over ranks (:461-485). */
+rrhd_status rrhd_hydro_max_speed_ptr(rrhd_ctx *ctx, double **max_speed);
+
 /* ------------------------------------------------------------ batch kernels */
 
 /* con2prim for n states, device pointers, on `stream` (a cudaStream_t, may be

@@ -106,6 +106,13 @@ _SIGS = {
     "rrhd_keep_face_flux": (I32, [P, I32]),
     "rrhd_get_face_flux": (I32, [P, P]),
     "rrhd_get_cell_status": (I32, [P, P]),
+    "rrhd_cell_order": (I32, [P, I32, P]),
+    "rrhd_part_plan": (I32, [P, P, I32, I32, I32, P, P, P, P, P]),
+    "rrhd_hydro_set_part": (I32, [P, I32, I32]),
+    "rrhd_hydro_part_info": (I32, [P, P, P, P, P]),
+    "rrhd_hydro_pack_halo": (I32, [P, P]),
+    "rrhd_hydro_unpack_halo": (I32, [P, P]),
+    "rrhd_hydro_max_speed_ptr": (I32, [P, P]),
     "rrhd_con2prim_batch": (I32, [I32, D, P, P, P, I64, I32, P]),
     "rrhd_prim2con_batch": (I32, [I32, D, P, P, I64, P]),
     "rrhd_con2prim_batch_stats": (I32, [I32, D, P, P, P, I64, I32, P, P]),

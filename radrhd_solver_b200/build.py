@@ -29,6 +29,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path
 # source -> extra flags
 SOURCES = {
     "mesh.cpp": [],
+    "partition.cpp": [],
     "hydro.cu": ["--fmad=false"],
     "radiation_fp64.cu": ["--fmad=false"],
     "scatter_tc.cu": [],

@@ -116,6 +116,15 @@ struct rrhd_ctx {
 
   rrhd::StepScalars *d_scal = nullptr;  // [2]
   int scal_cur = 0;
+
+  // split of the hydro step over ranks (rrhd_hydro_set_part): this context updates the
+  // CTA blocks [part_b0, part_b1); the cells it sends / receives, grouped by peer rank
+  int part_world = 1, part_rank = 0;
+  int part_b0 = 0, part_b1 = 0;
+  int64_t part_c0 = 0, part_c1 = 0;
+  int64_t n_send = 0, n_recv = 0;
+  std::vector<int64_t> send_counts, recv_counts;
+  int32_t *d_send_ids = nullptr, *d_recv_ids = nullptr;
   double cfl = 0.3, h_min = 0.0;
 
   bool keep_face_flux = false;

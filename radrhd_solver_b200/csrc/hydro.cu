@@ -38,6 +38,7 @@ struct StepParams {
   Eos eos;
   int N;
   int cpb;
+  int b0;  // first CTA block of this launch (the rank's range under a split)
   const int32_t *__restrict__ off;
   const int32_t *__restrict__ halo_off;
   const int32_t *__restrict__ halo_ids;
@@ -167,7 +168,7 @@ __global__ void __launch_bounds__(kStepThreads, RRHD_STEP_MIN_BLOCKS) k_hydro_st
   __shared__ unsigned long long s_cnt[2];
   __shared__ unsigned short s_fail[kMaxCellsPerBlock];
   __shared__ int s_nfail;
-  const int b = blockIdx.x;
+  const int b = P.b0 + blockIdx.x;
   const int c0 = b * P.cpb;
   const int nc = min(P.cpb, P.N - c0);
   const int e0 = P.off[b], e1 = P.off[b + 1];
@@ -279,7 +280,7 @@ __global__ void __launch_bounds__(kStepThreads, RRHD_STEP_MIN_BLOCKS) k_hydro_st
               (unsigned long long)__double_as_longlong(m));
     if (s_cnt[0]) atomicAdd(&P.out->n_fallback, s_cnt[0]);
     if (s_cnt[1]) atomicAdd(&P.out->n_failed, s_cnt[1]);
-    if (b == 0) P.out->tau = tau;
+    if (blockIdx.x == 0) P.out->tau = tau;
   }
 }
 
@@ -465,16 +466,6 @@ Eos make_eos(int eos, double gamma) {
   return e;
 }
 
-uint64_t spread3(uint64_t x) {
-  x &= 0x1fffff;
-  x = (x | x << 32) & 0x1f00000000ffffull;
-  x = (x | x << 16) & 0x1f0000ff0000ffull;
-  x = (x | x << 8) & 0x100f00f00f00f00full;
-  x = (x | x << 4) & 0x10c30c30c30c30c3ull;
-  x = (x | x << 2) & 0x1249249249249249ull;
-  return x;
-}
-
 template <class T>
 rrhd_status upload(T **dst, const std::vector<T> &src) {
   RRHD_CUDA(cudaMalloc((void **)dst, sizeof(T) * std::max<size_t>(src.size(), 1)));
@@ -488,7 +479,8 @@ void free_ctx(rrhd_ctx *c) {
   rrhd_rad_release(c);
   void *ptrs[] = {c->d_perm, c->d_iperm, c->d_bface_off, c->d_bface_lr, c->d_bface_nS, c->d_halo_off, c->d_halo_ids,
                   c->d_bface_gid, c->d_cell_slot, c->d_cell_sign, c->d_cell_V, c->d_state[0],
-                  c->d_state[1], c->d_status, c->d_scal, c->d_face_flux, c->d_scratch_io};
+                  c->d_state[1], c->d_status, c->d_scal, c->d_face_flux, c->d_scratch_io,
+                  c->d_send_ids, c->d_recv_ids};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -533,36 +525,17 @@ extern "C" rrhd_status rrhd_create(const rrhd_mesh_desc *m, const rrhd_opts *opt
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     return fail(rrhd_fail(RRHD_ERR_CUDA, "stream creation failed"));
 
-  // renumbering: Morton order of cell centres
+  // renumbering: Morton order of cell centres (rrhd_cell_order)
   std::vector<int32_t> perm(N), iperm(N);
-  std::iota(perm.begin(), perm.end(), 0);
-  const bool renumber = !(opts && opts->renumber < 0);
-  if (renumber) {
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    for (int64_t i = 0; i < N; i++)
-      for (int a = 0; a < 3; a++) {
-        lo[a] = std::min(lo[a], m->cell_center[3 * i + a]);
-        hi[a] = std::max(hi[a], m->cell_center[3 * i + a]);
-      }
-    std::vector<uint64_t> key(N);
-    for (int64_t i = 0; i < N; i++) {
-      uint64_t code = 0;
-      for (int a = 0; a < 3; a++) {
-        const double ext = hi[a] - lo[a];
-        const double t = ext > 0 ? (m->cell_center[3 * i + a] - lo[a]) / ext : 0.0;
-        const uint64_t q = (uint64_t)std::min(2097151.0, std::max(0.0, t * 2097151.0));
-        code |= spread3(q) << a;
-      }
-      key[i] = code;
-    }
-    std::stable_sort(perm.begin(), perm.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
-  }
+  if ((st = rrhd_cell_order(m, opts ? opts->renumber : 0, perm.data()))) return fail(st);
   for (int64_t i = 0; i < N; i++) iperm[perm[i]] = (int32_t)i;
 
   // per-CTA face lists
   const int cpb = c->cpb;
   const int nb = (int)((N + cpb - 1) / cpb);
   c->nblocks = nb;
+  c->part_b1 = nb;
+  c->part_c1 = N;
   std::vector<int32_t> off(nb + 1, 0);
   std::vector<int2> lr;
   std::vector<double4> nS;
@@ -784,6 +757,7 @@ extern "C" rrhd_status rrhd_hydro_step(rrhd_ctx *c, double tau, rrhd_step_stats 
   P.eos = make_eos(c->eos, c->gamma);
   P.N = (int)c->N;
   P.cpb = c->cpb;
+  P.b0 = c->part_b0;
   P.off = c->d_bface_off;
   P.halo_off = c->d_halo_off;
   P.halo_ids = c->d_halo_ids;
@@ -805,7 +779,7 @@ extern "C" rrhd_status rrhd_hydro_step(rrhd_ctx *c, double tau, rrhd_step_stats 
   P.cfl_hmin = c->cfl * c->h_min;
   P.bc = c->bc;
   RRHD_CUDA(cudaMemsetAsync(P.out, 0, sizeof(StepScalars), c->stream));
-  k_hydro_step<<<c->nblocks, kStepThreads, c->step_smem, c->stream>>>(P);
+  k_hydro_step<<<c->part_b1 - c->part_b0, kStepThreads, c->step_smem, c->stream>>>(P);
   RRHD_CUDA(cudaGetLastError());
   c->cur ^= 1;
   c->scal_cur ^= 1;
@@ -831,8 +805,110 @@ extern "C" rrhd_status rrhd_get_step_info(rrhd_ctx *c, double *tau_used, double 
   return RRHD_OK;
 }
 
+namespace {
+
+__global__ void k_pack_states(const int32_t *__restrict__ ids, int64_t n, const double2 *__restrict__ state,
+                              double2 *__restrict__ buf) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= 5 * n) return;
+  const int64_t k = i / 5;
+  buf[i] = state[5 * (int64_t)ids[k] + (i - 5 * k)];
+}
+
+__global__ void k_unpack_states(const int32_t *__restrict__ ids, int64_t n, const double2 *__restrict__ buf,
+                                double2 *__restrict__ state) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= 5 * n) return;
+  const int64_t k = i / 5;
+  state[5 * (int64_t)ids[k] + (i - 5 * k)] = buf[i];
+}
+
+}  // namespace
+
+extern "C" rrhd_status rrhd_hydro_set_part(rrhd_ctx *c, int32_t world, int32_t rank) {
+  RRHD_CHECK_ARG(c, "null context");
+  RRHD_CUDA(cudaSetDevice(c->device));
+  rrhd_mesh_desc m{};
+  m.n_cells = c->N;
+  m.n_faces = c->F;
+  m.face_id_l = c->h_face_l.data();
+  m.face_id_r = c->h_face_r.data();
+  int64_t range[2];
+  std::vector<int64_t> sc(std::max(world, 1)), rc(std::max(world, 1));
+  rrhd_status st = rrhd_part_plan(&m, c->h_perm.data(), c->cpb, world, rank, range, sc.data(), rc.data(),
+                                  nullptr, nullptr);
+  if (st) return st;
+  const int64_t ns = std::accumulate(sc.begin(), sc.end(), int64_t(0));
+  const int64_t nr = std::accumulate(rc.begin(), rc.end(), int64_t(0));
+  std::vector<int32_t> sid(std::max<int64_t>(ns, 1)), rid(std::max<int64_t>(nr, 1));
+  if ((st = rrhd_part_plan(&m, c->h_perm.data(), c->cpb, world, rank, range, sc.data(), rc.data(), sid.data(),
+                           rid.data())))
+    return st;
+  RRHD_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->d_send_ids) cudaFree(c->d_send_ids);
+  if (c->d_recv_ids) cudaFree(c->d_recv_ids);
+  c->d_send_ids = c->d_recv_ids = nullptr;
+  if ((st = upload(&c->d_send_ids, sid)) || (st = upload(&c->d_recv_ids, rid))) return st;
+  c->part_world = world;
+  c->part_rank = rank;
+  c->part_b0 = (int)(c->nblocks * (int64_t)rank / world);
+  c->part_b1 = (int)(c->nblocks * (int64_t)(rank + 1) / world);
+  c->part_c0 = range[0];
+  c->part_c1 = range[1];
+  c->n_send = ns;
+  c->n_recv = nr;
+  c->send_counts = sc;
+  c->recv_counts = rc;
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_hydro_part_info(rrhd_ctx *c, int64_t *cell_range, int64_t *send_counts,
+                                            int64_t *recv_counts, int32_t *cells) {
+  RRHD_CHECK_ARG(c, "null context");
+  if (cell_range) cell_range[0] = c->part_c0, cell_range[1] = c->part_c1;
+  for (int q = 0; q < c->part_world; q++) {
+    if (send_counts) send_counts[q] = c->part_world > 1 ? c->send_counts[q] : 0;
+    if (recv_counts) recv_counts[q] = c->part_world > 1 ? c->recv_counts[q] : 0;
+  }
+  if (cells)
+    for (int64_t k = c->part_c0; k < c->part_c1; k++) cells[k - c->part_c0] = c->h_perm[k];
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_hydro_pack_halo(rrhd_ctx *c, double *send_buf) {
+  RRHD_CHECK_ARG(c, "null context");
+  if (c->n_send == 0) return RRHD_OK;
+  RRHD_CHECK_ARG(send_buf, "null send buffer");
+  RRHD_CUDA(cudaSetDevice(c->device));
+  k_pack_states<<<grid1d(5 * c->n_send, 256), 256, 0, c->stream>>>(
+      c->d_send_ids, c->n_send, reinterpret_cast<const double2 *>(c->d_state[c->cur]),
+      reinterpret_cast<double2 *>(send_buf));
+  RRHD_CUDA(cudaGetLastError());
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_hydro_unpack_halo(rrhd_ctx *c, const double *recv_buf) {
+  RRHD_CHECK_ARG(c, "null context");
+  if (c->n_recv == 0) return RRHD_OK;
+  RRHD_CHECK_ARG(recv_buf, "null receive buffer");
+  RRHD_CUDA(cudaSetDevice(c->device));
+  k_unpack_states<<<grid1d(5 * c->n_recv, 256), 256, 0, c->stream>>>(
+      c->d_recv_ids, c->n_recv, reinterpret_cast<const double2 *>(recv_buf),
+      reinterpret_cast<double2 *>(c->d_state[c->cur]));
+  RRHD_CUDA(cudaGetLastError());
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_hydro_max_speed_ptr(rrhd_ctx *c, double **max_speed) {
+  RRHD_CHECK_ARG(c && max_speed, "null argument");
+  *max_speed = &c->d_scal[c->scal_cur ^ 1].max_speed;
+  return RRHD_OK;
+}
+
 extern "C" rrhd_status rrhd_hydro_step_host(rrhd_ctx *c, double tau, double *W, double *U, int64_t stride,
                                            rrhd_step_stats *stats) {
+  RRHD_CHECK_ARG(c, "null context");
+  RRHD_CHECK_ARG(c->part_world == 1, "host-buffer step of a split context: use rrhd_hydro_step");
   rrhd_status st = rrhd_set_state(c, W, U, stride, RRHD_HOST);
   if (st) return st;
   rrhd_status step = rrhd_hydro_step(c, tau, stats);

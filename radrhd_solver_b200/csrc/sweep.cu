@@ -999,6 +999,7 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
                                          rrhd_c2p_stats *ss) {
   RRHD_CHECK_ARG(c && o, "null argument");
   RRHD_CHECK_ARG(tau > 0, "tau must be > 0");
+  RRHD_CHECK_ARG(c->part_world == 1, "the coupled step runs on a whole mesh (no rrhd_hydro_set_part split)");
   RadState &R = c->rad;
   if (!R.ready) return rrhd_fail(RRHD_ERR_STATE, "rrhd_rad_setup has not run");
   const bool fp64 = R.prec == RRHD_RAD_FP64;

@@ -37,6 +37,7 @@ class Grid:
         self.eos = eos
         self.gamma = gamma
         self.size = mesh.n_cells
+        self.device = device
         o = L.Opts(eos, gamma, device, cells_per_block, 0 if renumber else -1)
         h = C.c_void_p()
         L.check(L.lib.rrhd_create(C.byref(mesh.desc()), C.byref(o), C.byref(h)), "rrhd_create")

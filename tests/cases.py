@@ -64,6 +64,19 @@ def intensity(N, M_, seed=3, centers=None, groups=1):
     return I
 
 
+def split_case(nx=40, ny=8, nz=8, seed=4):
+    """Shock tube with perturbed density, pressure and velocity in every cell (so that
+    every face carries flux), for the hydro step split over ranks."""
+    m, W = shock_tube(nx, ny, nz)
+    rng = np.random.default_rng(seed)
+    W[:, 0] *= 1 + 0.2 * rng.uniform(-1, 1, m.n_cells)
+    W[:, 4] *= 1 + 0.2 * rng.uniform(-1, 1, m.n_cells)
+    W[:, 1:4] = 0.3 * rng.uniform(-1, 1, (m.n_cells, 3))
+    return m, W
+
+
+SPLIT_POISON = np.array([2.0, 0.0, 0.0, 0.0, 0.5])  # state of the cells a rank neither owns nor receives
+
 COMPTON_SPEEDS = (0.0, 1e-6, 1e-5, 0.3, 0.9, 0.99)
 
 
