@@ -89,6 +89,12 @@ class Directions:
     def size(self) -> int:
         return int(self.areas.shape[0])
 
+    def subset(self, first: int, count: int) -> "Directions":
+        """Directions first .. first + count - 1 (one rank's share of a direction split),
+        with the full sphere's area."""
+        return Directions(np.ascontiguousarray(self.dirs[first:first + count]),
+                          np.ascontiguousarray(self.areas[first:first + count]), self.full_area)
+
 
 def fibonacci_directions(M: int) -> Directions:
     d = np.zeros((M, 3))
