@@ -180,7 +180,8 @@ rrhd_status rrhd_part_plan(const rrhd_mesh_desc *mesh, const int32_t *order, int
  *   rrhd_hydro_pack_halo -> exchange of the send / recv buffers between ranks ->
  *   rrhd_hydro_unpack_halo -> rrhd_hydro_step -> max-reduction over ranks of the double
  *   at rrhd_hydro_max_speed_ptr (the next step's tau <= 0 reads it).
- * The coupled step and rrhd_hydro_step_host refuse a split context. */
+ * Kept face fluxes (rrhd_keep_face_flux) are written for the faces whose id_l cell the rank
+ * updates.  The coupled step and rrhd_hydro_step_host refuse a split context. */
 rrhd_status rrhd_hydro_set_part(rrhd_ctx *ctx, int32_t world, int32_t rank);
 /* cell_range[2], send_counts / recv_counts [world] of the split, and the caller ids of the
  * rank's cells [cell_range[1] - cell_range[0]].  Any pointer may be NULL. */

@@ -119,3 +119,11 @@ def test_plan_edges():
         RM.part_plan(m, order, 2, 2)
     ident = RM.cell_order(m, renumber=False)
     assert np.array_equal(ident, np.arange(m.n_cells))
+    bad = order.copy()
+    bad[1] = bad[0]  # not a permutation
+    with pytest.raises(L.RrhdError):
+        RM.part_plan(m, bad, 2, 0)
+    # identity order: rank 0 of 2 owns the first half of the caller's cells
+    p0 = RM.part_plan(m, ident, 2, 0)
+    assert p0.cell_range == (0, 256 * (nb // 2))
+    assert np.all(p0.send_ids < p0.cell_range[1]) and np.all(p0.recv_ids >= p0.cell_range[1])
