@@ -88,3 +88,17 @@ def test_get_send_disp():
         for n in range(0, 40):
             c, d = GetSend(np_, n), GetDisp(np_, n)
             assert sum(c) == n and d == [sum(c[:i]) for i in range(np_)] and max(c) - min(c) <= 1
+
+
+def test_direction_subset():
+    """A rank's share of the direction set keeps the directions' order, their areas and the
+    whole sphere's area (the scattering weights a_d / full_area stay the same)."""
+    sys.path[:0] = [ROOT]
+    from radrhd_solver_b200.illum_mpi import GetDisp, GetSend
+    from radrhd_solver_b200.mesh import fibonacci_directions
+    d = fibonacci_directions(26)
+    parts = [d.subset(o, c) for o, c in zip(GetDisp(3, 26), GetSend(3, 26))]
+    assert [p.size for p in parts] == [9, 9, 8]
+    assert np.array_equal(np.concatenate([p.dirs for p in parts]), d.dirs)
+    assert np.array_equal(np.concatenate([p.areas for p in parts]), d.areas)
+    assert all(p.full_area == d.full_area and p.dirs.flags.c_contiguous for p in parts)
