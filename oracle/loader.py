@@ -65,6 +65,7 @@ def port() -> C.CDLL:
             "orc_get_illum": (D, [P, P, D, D]), "orc_get_rhs": (D, [D, D, D, D, P]),
             "orc_recalc_illum": (D, [I64, P, P, P, I32, I32, P]),
             "orc_sweep": (I64, [P, I32, P, I32, P, P, P, P, D, P]),
+            "orc_trace_nodes": (None, [P, I32, P, P, P]),
             "orc_compton_full_spectrum": (None, [I32, P, P, D, I64, P, P, I32, I32, I32, P, C.c_int]),
             "orc_compton_frq": (D, [I32]), "orc_compton_frq_idx": (I32, [D]),
             "orc_compton_spectrum": (None, [I32, P, P, D, I64, P, P, D, I32, I32, I32, P, C.c_int]),
@@ -450,6 +451,78 @@ def sweep_neighbours(mesh):
     nl, nr = l[cf], r[cf]
     nb = np.where(nl == own, nr, nl)
     return np.where(nb < 0, -1, nb).astype(np.int32)
+
+
+def _sweep_mesh(mesh):
+    keep = [np.ascontiguousarray(mesh.cell_volume, np.float64),
+            np.ascontiguousarray(mesh.cell_faces, np.int32), sweep_neighbours(mesh),
+            np.ascontiguousarray(mesh.cell_sign, np.uint8), np.ascontiguousarray(mesh.face_n, np.float64),
+            np.ascontiguousarray(mesh.face_area, np.float64)]
+    return OrcSweepMesh(mesh.n_cells, mesh.n_faces, *(_p(a) for a in keep)), keep
+
+
+def port_trace_nodes(mesh, dirs):
+    """orc_trace_nodes: the sweep's node geometry, in_face and s [M][N][4][3] (in the
+    mesh's local faces; node q of face j has weight 2/3 at vertex (j + 1 + q) & 3)."""
+    dirs = np.ascontiguousarray(dirs, np.float64)
+    M, N = len(dirs), mesh.n_cells
+    sm, keep = _sweep_mesh(mesh)
+    hf = np.zeros((M, N, 4, 3), np.int32)
+    s = np.zeros((M, N, 4, 3))
+    port().orc_trace_nodes(C.byref(sm), M, _p(dirs), _p(hf), _p(s))
+    return hf, s
+
+
+_TRACE = None
+
+
+def ref_trace():
+    """The reference's make_trace / graph preprocessing compiled from its sources
+    (oracle/_ref/librrhd_ref_trace.so), or None where it was not built."""
+    global _TRACE
+    if _TRACE is None:
+        path = os.path.join(REF_DIR, "librrhd_ref_trace.so")
+        if not os.path.exists(path):
+            return None
+        lib = C.CDLL(path)
+        lib.ref_trace_nodes.restype = I64
+        lib.ref_trace_nodes.argtypes = [I64, P, P, I32, P, P, P, P, P]
+        lib.ref_graph_levels.restype = I32
+        lib.ref_graph_levels.argtypes = [I64, P, P, I32, P, P]
+        _TRACE = lib
+    return _TRACE
+
+
+def ref_trace_nodes(points, normals, dirs):
+    """trace::GetInterpolationNodes + trace::GetLocNodes per direction (make_trace/src/
+    trace_main.cpp) on cells given by their points in VTK order [N][4][3] and the outward
+    normals of VTK's faces [N][4][3].  Returns (in-face bits [M][N], in_face [M][N][4][3],
+    s [M][N][4][3], nodes [N][4][3][3], faces the reference would stop on)."""
+    lib = ref_trace()
+    pts = np.ascontiguousarray(points, np.float64)
+    nrm = np.ascontiguousarray(normals, np.float64)
+    dirs = np.ascontiguousarray(dirs, np.float64)
+    M, N = len(dirs), len(pts)
+    st = np.zeros((M, N), np.int32)
+    hf = np.zeros((M, N, 4, 3), np.int32)
+    s = np.zeros((M, N, 4, 3))
+    nodes = np.zeros((N, 4, 3, 3))
+    missed = lib.ref_trace_nodes(N, _p(pts), _p(nrm), M, _p(dirs), _p(st), _p(hf), _p(s), _p(nodes))
+    return st, hf, s, nodes, missed
+
+
+def ref_graph_levels(neighbours, normals, dirs):
+    """The front index of every cell per direction in graph::RunGraphModule's sweep order
+    (graph/src/graph_by_direction.cpp); neighbours [N][4] = neighbour cell * 4 + its
+    local face, < 0 on the boundary.  Returns (levels [M][N], incomplete directions)."""
+    lib = ref_trace()
+    nb = np.ascontiguousarray(neighbours, np.int32)
+    nrm = np.ascontiguousarray(normals, np.float64)
+    dirs = np.ascontiguousarray(dirs, np.float64)
+    M, N = len(dirs), len(nb)
+    lv = np.zeros((M, N), np.int32)
+    bad = lib.ref_graph_levels(N, _p(nb), _p(nrm), M, _p(dirs), _p(lv))
+    return lv, bad
 
 
 def port_sweep(mesh, dirs, alpha, betta, Q, S, bc=0.0, I=None):

@@ -613,6 +613,35 @@ static void cell_normal(const orc_sweep_mesh *m, int64_t c, int j, double *n) {
   }
 }
 
+/* The short-characteristic geometry orc_sweep uses, for every (direction d, cell c,
+ * local face j, node q): the in-face h and the distance s of trace_face where face j is
+ * an out-face (cos_j > 0), -1 and 0 elsewhere; in_face and s are [M][N][4][3]. */
+void orc_trace_nodes(const orc_sweep_mesh *m, int32_t M, const double *dirs, int32_t *in_face, double *s) {
+  const int64_t N = m->n_cells;
+  for (int32_t dd = 0; dd < M; dd++) {
+    const double *w = dirs + 3 * dd;
+    for (int64_t c = 0; c < N; c++) {
+      double n[4][3], H[4], cosf[4];
+      for (int j = 0; j < 4; j++) {
+        cell_normal(m, c, j, n[j]);
+        H[j] = 3.0 * m->cell_volume[c] / m->face_area[m->cell_faces[4 * c + j]];
+        cosf[j] = dot3(n[j], w);
+      }
+      for (int j = 0; j < 4; j++) {
+        int32_t *hf = in_face + (((int64_t)dd * N + c) * 4 + j) * 3;
+        double *sd = s + (((int64_t)dd * N + c) * 4 + j) * 3;
+        int h[3] = {-1, -1, -1};
+        double sdist[3] = {0, 0, 0};
+        if (cosf[j] > 0) trace_face(H, cosf, j, h, sdist);
+        for (int q = 0; q < 3; q++) {
+          hf[q] = h[q];
+          sd[q] = sdist[q];
+        }
+      }
+    }
+  }
+}
+
 int64_t orc_sweep(const orc_sweep_mesh *m, int32_t M, const double *dirs, int32_t G, const double *alpha,
                   const double *betta, const double *Q, const double *S, double bc, double *I) {
   const int64_t N = m->n_cells, F = m->n_faces;

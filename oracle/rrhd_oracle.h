@@ -112,6 +112,7 @@ double orc_recalc_illum(int64_t N, const int32_t *cell_faces, const double *face
 /* One sweep of all M directions and G groups: S [N*G][M] (rows cell*G+g) in,
  * I [N*G][M] out.  alpha, betta [N]; Q [N][G] emission per group.  Returns the
  * number of (cell, direction) pairs a dependency cycle left unswept (0 normally). */
+void orc_trace_nodes(const orc_sweep_mesh *m, int32_t M, const double *dirs, int32_t *in_face, double *s);
 int64_t orc_sweep(const orc_sweep_mesh *m, int32_t M, const double *dirs, int32_t G, const double *alpha,
                const double *betta, const double *Q, const double *S, double bc, double *I);
 
