@@ -10,8 +10,16 @@
 //   * every call uploads cells[].conv_val / phys_val, runs the fused RHLLC flux + update +
 //     con2prim step on the GPU, and downloads them back (rrhd_hydro_step_host: the state
 //     records are read and written in place, with elem_t's size as the stride);
-//   * rhllc::max_signal_speed is set from the step, and the face fluxes are written back into
-//     grid.faces[].f (KeepFaceFlux(false) skips that download);
+//   * in resident mode (SetResident(true)) the state stays on the device between calls:
+//     the first call after SetResident or SyncToDevice uploads it, later calls only step,
+//     and SyncToHost(grid) writes it back into grid.cells -- RunRhllcModule reads
+//     grid.cells only in WriteSolution (rhllc::GetTimeStep reads max_signal_speed alone,
+//     solvers/rhllc/src/rhllc_utils.cpp:15-23), so one SyncToHost before each
+//     WriteSolution keeps its output identical while the per-step copies disappear;
+//   * rhllc::max_signal_speed is set from the step; the face fluxes are written back into
+//     grid.faces[].f only after KeepFaceFlux(true) (no reference caller reads faces[].f
+//     outside Hllc3dStab, rhllc_main.cpp:42-57, so the 40 bytes per face of that download
+//     are skipped by default);
 //   * a cell where con2prim and PhysPressureFix both fail stops the program, as the
 //     reference's DIE_IF does.
 // The results are the reference's bit for bit (the library's FP64 step is compiled without
@@ -24,6 +32,7 @@
 #include "rhllc_calc.h"
 #include "rhllc_utils.h"
 
+#include "rhllc_3d_stab_b200.h"
 #include "rrhd.h"
 
 #include <cstddef>
@@ -41,7 +50,9 @@ struct Bc {
 static rrhd_ctx *g_ctx = nullptr;
 static const elem_t *g_cells = nullptr;
 static size_t g_n = 0, g_f = 0;
-static bool g_face_flux = true;
+static bool g_face_flux = false;
+static bool g_resident = false;
+static bool g_dev_valid = false;  // resident mode: the device holds the latest state
 static std::vector<Bc> g_bc;
 static std::vector<double> g_flux;
 
@@ -60,19 +71,53 @@ void SetBoundary(int code, int kind, const double *W) {
   if (g_ctx && rrhd_set_boundary(g_ctx, code, kind, W) != RRHD_OK) fail("rrhd_set_boundary");
 }
 
-/// Whether grid.faces[].f is refreshed after each step (on by default, as in the reference).
+/// Whether grid.faces[].f is refreshed after each step (off by default; the reference's
+/// step writes them, but none of its callers reads them).
 void KeepFaceFlux(bool on) {
   g_face_flux = on;
   if (g_ctx && rrhd_keep_face_flux(g_ctx, on ? 1 : 0) != RRHD_OK) fail("rrhd_keep_face_flux");
 }
 
-/// Frees the device copy (the next call rebuilds it).
+/// Frees the device copy (the next call rebuilds it).  In resident mode, call
+/// SyncToHost first: the device state is lost.
 void Release() {
   if (g_ctx) rrhd_destroy(g_ctx);
   g_ctx = nullptr;
   g_cells = nullptr;
   g_n = g_f = 0;
+  g_dev_valid = false;
 }
+
+static void state_ptrs(grid_t &grid, double **W, double **U, int64_t *stride) {
+  static_assert(sizeof(flux_t) == 5 * sizeof(double), "flux_t must be 5 contiguous doubles");
+  static_assert(sizeof(elem_t) % sizeof(double) == 0, "elem_t must be a whole number of doubles");
+  elem_t &c0 = grid.cells[0];
+  *W = reinterpret_cast<double *>(&c0.phys_val);
+  *U = reinterpret_cast<double *>(&c0.conv_val);
+  *stride = sizeof(elem_t) / sizeof(double);
+}
+
+/// Resident mode on or off.  On: the state is uploaded by the next call and then stays
+/// on the device; grid.cells is refreshed only by SyncToHost.  Off (the default): every
+/// call copies the state both ways.
+void SetResident(bool on) {
+  g_resident = on;
+  g_dev_valid = false;
+}
+
+/// Resident mode: writes the device state into grid.cells (before WriteSolution or any
+/// other read of the cells on the host).  No effect outside resident mode.
+void SyncToHost(grid_t &grid) {
+  if (!g_resident || !g_ctx || !g_dev_valid || g_cells != grid.cells.data()) return;
+  double *W, *U;
+  int64_t stride;
+  state_ptrs(grid, &W, &U, &stride);
+  if (rrhd_get_state(g_ctx, W, U, stride, RRHD_HOST) != RRHD_OK) fail("rrhd_get_state");
+}
+
+/// Resident mode: the host has changed grid.cells (e.g. a source term applied on the
+/// host); the next call uploads them again.
+void SyncToDevice(grid_t &) { g_dev_valid = false; }
 
 static void init(const grid_t &grid) {
   Release();
@@ -106,6 +151,7 @@ static void init(const grid_t &grid) {
   g_cells = grid.cells.data();
   g_n = N;
   g_f = F;
+  g_dev_valid = false;
 }
 
 }  // namespace rhllc_b200
@@ -113,14 +159,20 @@ static void init(const grid_t &grid) {
 void rhllc::Hllc3dStab(const Type tau, grid_t &grid) {
   using namespace rhllc_b200;
   if (!g_ctx || g_cells != grid.cells.data() || g_n != grid.cells.size() || g_f != grid.faces.size()) init(grid);
-  static_assert(sizeof(flux_t) == 5 * sizeof(double), "flux_t must be 5 contiguous doubles");
-  static_assert(sizeof(elem_t) % sizeof(double) == 0, "elem_t must be a whole number of doubles");
-  const int64_t stride = sizeof(elem_t) / sizeof(double);
-  elem_t &c0 = grid.cells[0];
+  double *W, *U;
+  int64_t stride;
+  state_ptrs(grid, &W, &U, &stride);
   rrhd_step_stats st;
-  const rrhd_status s =
-      rrhd_hydro_step_host(g_ctx, tau, reinterpret_cast<double *>(&c0.phys_val), reinterpret_cast<double *>(&c0.conv_val),
-                           stride, &st);
+  rrhd_status s;
+  if (g_resident) {
+    if (!g_dev_valid) {
+      if (rrhd_set_state(g_ctx, W, U, stride, RRHD_HOST) != RRHD_OK) fail("rrhd_set_state");
+      g_dev_valid = true;
+    }
+    s = rrhd_hydro_step(g_ctx, tau, &st);
+  } else {
+    s = rrhd_hydro_step_host(g_ctx, tau, W, U, stride, &st);
+  }
   if (s == RRHD_ERR_C2P) fail("con2prim and PhysPressureFix failed in some cell");
   if (s != RRHD_OK) fail("rrhd_hydro_step_host");
   rhllc::max_signal_speed = st.max_speed;

@@ -32,6 +32,9 @@
 #include "rhllc_flux_stab.h"
 #include "rhllc_flux.h"
 #include "rhllc_utils.h"
+#if defined RRHD_ADAPTER_HYDRO
+#include "rhllc_3d_stab_b200.h"
+#endif
 #endif
 #if defined RRHD_SHIM_ILLUM
 #include "illum_integrate.h"
@@ -361,6 +364,14 @@ int ref_record_sizes(int32_t *out) {
   out[2] = (int32_t)sizeof(flux_t);
   return 0;
 }
+
+#if defined RRHD_ADAPTER_HYDRO
+// The drop-in adapter's own controls (adapter/rhllc_3d_stab_b200.h), for the build that
+// links the adapter in place of rhllc_3d_stab.cpp.
+void ref_adapter_keep_face_flux(int on) { rhllc_b200::KeepFaceFlux(on != 0); }
+void ref_adapter_set_resident(int on) { rhllc_b200::SetResident(on != 0); }
+void ref_adapter_sync_to_host(void *p) { rhllc_b200::SyncToHost(((ref_hydro *)p)->grid); }
+#endif
 
 #endif  // RRHD_SHIM_HYDRO
 

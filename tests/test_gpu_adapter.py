@@ -5,6 +5,8 @@ Gamma = 5/3) with the adapter linked in place of solvers/rhllc/src/rhllc_3d_stab
 B200 library -- what a maintainer's build becomes.  Two grid_t objects, one per build, are
 stepped through the reference's own entry point rhllc::Hllc3dStab(tau, grid): cell states,
 face fluxes left in grid.faces[].f and rhllc::max_signal_speed must agree bit for bit."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -16,13 +18,25 @@ pytestmark = [pytest.mark.gpu,
                                  reason="reference builds not present (make -C oracle ref)")]
 
 
+def _adapter_controls():
+    lib = oracle.ref("adapter_hydro_5_3")
+    lib.ref_adapter_keep_face_flux.argtypes = [ctypes.c_int]
+    lib.ref_adapter_set_resident.argtypes = [ctypes.c_int]
+    lib.ref_adapter_sync_to_host.argtypes = [ctypes.c_void_p]
+    return lib
+
+
 def test_adapter_hllc3dstab_matches_reference_build():
+    """Default mode: the state goes both ways every call; with KeepFaceFlux(true) the
+    face fluxes are written back into grid.faces[].f as the reference's step leaves them."""
+    lib = _adapter_controls()
     m, W = shock_tube(24, 4, 4)
     W, U = oracle.port_p2c(W, 1, GAMMA_53)
     ref = oracle.HydroRef(m, "hydro_ideal_5_3")
     ada = oracle.HydroRef(m, "adapter_hydro_5_3")
     ref.set_state(W, U)
     ada.set_state(W, U)
+    lib.ref_adapter_keep_face_flux(1)
     tau = 0.3 * 0.25 / 24
     for step in range(12):
         s_ref = ref.step(tau, nthreads=4)
@@ -33,6 +47,42 @@ def test_adapter_hllc3dstab_matches_reference_build():
     assert np.array_equal(Ua, Ur) and np.array_equal(Wa, Wr)
     assert np.array_equal(ada.face_flux(), ref.face_flux())
     assert np.abs(Ur - U).max() > 0  # the state moved
+    lib.ref_adapter_keep_face_flux(0)
+    ref.close()
+    ada.close()
+
+
+def test_adapter_resident_mode_matches_reference_build():
+    """Resident mode: the state is uploaded by the first call and stays on the device;
+    grid.cells keeps the initial state until SyncToHost, which then gives the
+    reference build's state bit for bit.  Face fluxes are not downloaded by default."""
+    lib = _adapter_controls()
+    m, W = shock_tube(24, 4, 4)
+    W, U = oracle.port_p2c(W, 1, GAMMA_53)
+    ref = oracle.HydroRef(m, "hydro_ideal_5_3")
+    ada = oracle.HydroRef(m, "adapter_hydro_5_3")
+    ref.set_state(W, U)
+    ada.set_state(W, U)
+    F0 = ada.face_flux()
+    lib.ref_adapter_set_resident(1)
+    try:
+        tau = 0.3 * 0.25 / 24
+        for step in range(10):
+            assert ada.step(tau) == ref.step(tau, nthreads=4), f"max signal speed differs at step {step}"
+        Wa0, Ua0 = ada.get_state()
+        assert np.array_equal(Ua0, U) and np.array_equal(Wa0, W)  # host copy untouched while resident
+        assert np.array_equal(ada.face_flux(), F0)
+        lib.ref_adapter_sync_to_host(ada.h)
+        Wr, Ur = ref.get_state()
+        Wa, Ua = ada.get_state()
+        assert np.array_equal(Ua, Ur) and np.array_equal(Wa, Wr)
+        # stepping on after a sync continues from the device state
+        for _ in range(3):
+            assert ada.step(tau) == ref.step(tau, nthreads=4)
+        lib.ref_adapter_sync_to_host(ada.h)
+        assert all(np.array_equal(a, b) for a, b in zip(ada.get_state(), ref.get_state()))
+    finally:
+        lib.ref_adapter_set_resident(0)
     ref.close()
     ada.close()
 
