@@ -39,6 +39,7 @@ NHEX = 96
 GAMMA = 4.0 / 3.0
 CFL = 0.3
 INFLOW = [0.01, 0.0, 0.0, float(np.sqrt(1.0 - 1.0 / 49.0)), 1e-3]
+DATA = "synthetic (seeded Kuhn mesh, jet initial state)"
 
 
 def peaks():
@@ -48,15 +49,34 @@ def peaks():
         return None
 
 
-def make_jet(n=None, seed=2024):
+JET_MESH = dict(lo=(-1, -1, -1), hi=(1, 1, 1), jitter=0.15, inflow_radius=0.1, inflow_code=-3)
+
+
+def make_jet(n=None, seed=2024, independent=False):
+    """The jet mesh and its ambient primitive state.  independent=True builds the
+    mesh with the oracle's numpy generator (bit-identical to the library's, pinned
+    by tests/test_oracle_kuhn.py), so that the CPU reference arm never loads the
+    CUDA library."""
     n = n or NHEX
-    from radrhd_solver_b200 import mesh as M
-    m = M.kuhn_box(n, n, n, lo=(-1, -1, -1), hi=(1, 1, 1), jitter=0.15, seed=seed, inflow_radius=0.1,
-                   inflow_code=-3)
+    if independent:
+        from oracle import kuhn as K
+        m = K.kuhn_box(n, n, n, seed=seed, **JET_MESH)
+    else:
+        from radrhd_solver_b200 import mesh as M
+        m = M.kuhn_box(n, n, n, seed=seed, **JET_MESH)
     W = np.zeros((m.n_cells, 5))
     W[:, 0] = 1.0
     W[:, 4] = 1e-3
     return m, W
+
+
+def bench_config(m, ws):
+    """The workload description both arms print (identical keys and values)."""
+    return {"workload": f"coupled-jet mesh {NHEX}^3x6 tets: RHLLC flux + update + con2prim step",
+            "cells": m.n_cells, "faces": m.n_faces, "gamma": GAMMA, "tau": CFL * m.h_min,
+            "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+            "l2": f"state 2 x {80 * m.n_cells / 1e6:.0f} MB, L2 126 MB: "
+                  + ("larger than L2, no flush" if 80 * m.n_cells > 126e6 else "fits in L2 (a small case)")}
 
 
 class Clocks:
@@ -138,7 +158,7 @@ def cpu_threads():
 def reference_steps(m, W, U, steps, threads, bc_u):
     """Times `steps` reference hydro steps on the host; returns seconds per step and kind."""
     import oracle
-    variant = "hydro_ideal_4_3_fast"
+    variant = REF_VARIANT
     if oracle.have_ref(variant):
         h = oracle.HydroRef(m, variant)
         h.set_bc(-3, 1, np.array(INFLOW), bc_u)
@@ -160,31 +180,41 @@ def reference_steps(m, W, U, steps, threads, bc_u):
     return (time.perf_counter() - t0) / steps, "port"
 
 
+REF_VARIANT = "hydro_ideal_4_3_fast"
+
+
 def inflow_conservative():
-    """Conservative inflow state (rhllc::GetConvValue) for the CPU legs."""
+    """Conservative inflow state (rhllc::GetConvValue, solvers/rhllc/src/rhllc_flux.cpp:7-16)
+    for the CPU legs: the reference's own function where it was built, else the oracle's."""
     import oracle
     u = np.zeros(5)
+    w = np.array(INFLOW)
+    lib = oracle.ref(REF_VARIANT)
+    if lib is not None:
+        lib.ref_p2c_plain(w.ctypes.data, u.ctypes.data, 1)
+        return u
     e = oracle.loader.OrcEos(1, GAMMA)
-    oracle.port().orc_p2c_plain(ctypes.byref(e), np.array(INFLOW).ctypes.data, u.ctypes.data)
+    oracle.port().orc_p2c_plain(ctypes.byref(e), w.ctypes.data, u.ctypes.data)
     return u
 
 
 def run_reference(args):
+    """The reference's CPU hydro step (rhllc::Hllc3dStab from its own sources) on the
+    same mesh, state and time step as the GPU arm; this process never loads the CUDA
+    library (mesh from the oracle's generator, states from the reference's prim->cons)."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    import oracle
-    m, W = make_jet()
-    W, U = oracle.port_p2c(W, 1, GAMMA) if m.n_cells < 100000 else _p2c_fast(W)
+    m, W = make_jet(independent=True)
+    W, U = _p2c_fast(W)
     threads = cpu_threads()
     bc_u = inflow_conservative()
     dt, kind = reference_steps(m, W, U, max(1, args.steps), threads, bc_u)
     v = m.n_cells / dt
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"coupled-jet mesh {NHEX}^3x6 tets, RHLLC hydro step", "cells": m.n_cells,
-                       "faces": m.n_faces},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
+            "config": bench_config(m, args.gpus),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
                              "sample": f"{args.steps} full steps of the {m.n_cells}-cell mesh"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -192,10 +222,14 @@ def run_reference(args):
 
 
 def _p2c_fast(W):
-    """prim->cons for the uniform bench state through the library's batch kernel
-    would need a GPU; the ambient state is uniform, so compute it once."""
+    """prim->cons (GetConvValueStab) of the uniform ambient state, computed once by
+    the reference's own function where it was built (else the oracle's) and
+    repeated over the mesh."""
     import oracle
-    Wu, Uu = oracle.port_p2c(W[:1], 1, GAMMA)
+    if oracle.have_ref(REF_VARIANT):
+        Wu, Uu = oracle.ref_p2c(W[:1], REF_VARIANT)
+    else:
+        Wu, Uu = oracle.port_p2c(W[:1], 1, GAMMA)
     return np.repeat(Wu, len(W), 0), np.repeat(Uu, len(W), 0)
 
 
@@ -406,14 +440,15 @@ def c2p_component(dev, n=8_000_000, epochs=8, reps=5):
 EM_JET = (1.0, 10.0, float(np.pi), 1.0)  # temp_coef, a_R, pi, kRadiation in code units: T = p / rho, B = a_R T^4 / pi
 
 
-def coupled_component(dev, m, W, steps=3, warm=1, M=256, G=4, train_epochs=2, forms=("plain", "chosen"),
+def coupled_component(dev, m, W, steps=100, warm=1, M=256, G=4, train_epochs=2, forms=("plain", "chosen"),
                       batch=(128, 256)):
     """Config-4 coupled radiation-hydro jet step (radRHD_main.cpp:96-139) on the
     benchmark mesh: hydro step, opacities alpha = rho, betta = 0.5 rho, emission
     Q = a_R T^4 / pi / G per grey group, sweep of M directions x G groups,
     4-force + source con2prim, scattering integral + moments.  Plain form: FP64
     sweep, FP64 scattering (one FMA per term), reference con2prim guess.  Chosen
-    form: FP32 sweep, tensor-core F16X3 scattering, learned con2prim guess
+    form: mixed-precision sweep (FP64 arithmetic and face values, FP32 intensity
+    and scattering integral), tensor-core F16X3 scattering, learned con2prim guess
     trained on the plain run's own states.  "plain_lowrank" / "chosen_lowrank": the
     same with the scattering through the rank-7 Thomson identity (FP64 arithmetic).
     All forms start from the same state; the intensity arrays (N*G*M = 5.4e9
@@ -437,7 +472,7 @@ def coupled_component(dev, m, W, steps=3, warm=1, M=256, G=4, train_epochs=2, fo
         g.set_state_prim(W)
         dg = illum.DirectionGrid(d, dev)
         t0 = time.perf_counter()
-        sw = illum.TransportSweep(g, dg, groups=G, precision="fp64" if fp64 else "fp32",
+        sw = illum.TransportSweep(g, dg, groups=G, precision="fp64" if fp64 else "mixed",
                                   dirs_per_batch=batch[0] if fp64 else batch[1])
         t_plan = time.perf_counter() - t0
         if not fp64 and net is None and "plain_dump" in states:
@@ -455,9 +490,12 @@ def coupled_component(dev, m, W, steps=3, warm=1, M=256, G=4, train_epochs=2, fo
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(steps - 1):
-            step(tau)
-        hs, ss = step(tau, stats=True)  # the last step reads its statistics back
+        fails = [0, 0, 0]  # hydro cells failed after the fallback, hydro fallbacks, source con2prim failures
+        for _ in range(steps):
+            hs, ss = step(tau, stats=True)  # reads the step's counters back (one sync per step)
+            fails[0] += hs.n_failed
+            fails[1] += hs.n_fallback
+            fails[2] += ss.n_failed
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / steps
@@ -467,14 +505,15 @@ def coupled_component(dev, m, W, steps=3, warm=1, M=256, G=4, train_epochs=2, fo
         states[form] = Ug
         if form == "plain":
             states["plain_dump"] = (Wg, Ug)
-        bpv = 8 if fp64 else 4
-        sweep_alg = (2.0 * m.n_cells + 2.0 * m.n_faces) * M * G * bpv + m.n_cells * (20 * bpv + 32.0)
+        bio = 8 if fp64 else 4  # bytes per intensity / scattering value; face values are double
+        sweep_alg = (2.0 * m.n_cells * bio + 2.0 * m.n_faces * 8) * M * G + m.n_cells * (20 * 8 + 32.0)
         out[form] = {"dirs_per_batch": batch[0] if fp64 else batch[1], "ms_per_step": ms, "steps_per_s": 1e3 / ms, "cell_updates_per_s": m.n_cells / (ms / 1e3),
                      "cell_dir_group_per_s": m.n_cells * M * G / (ms / 1e3), "phase_ms_last_step": ph,
                      "sweep_levels": levels, "largest_level": biggest, "plan_build_s": t_plan,
                      "sweep_alg_gbs": sweep_alg / (ph["sweep"] / 1e3) / 1e9,
-                     "source_c2p": {"newton_iters_per_state": ss.newton_iters / m.n_cells, "failed": ss.n_failed},
-                     "hydro": {"n_fallback": hs.n_fallback, "n_failed": hs.n_failed},
+                     "source_c2p": {"newton_iters_per_state_last_step": ss.newton_iters / m.n_cells,
+                                    "failed_all_steps": fails[2]},
+                     "hydro": {"n_fallback_all_steps": fails[1], "n_failed_all_steps": fails[0]},
                      "warmup_failures": [[h.n_failed, s_.n_failed] for h, s_ in warm_stats]}
         g.close()
         dg.close()
@@ -483,7 +522,11 @@ def coupled_component(dev, m, W, steps=3, warm=1, M=256, G=4, train_epochs=2, fo
         net.close()
     if "plain" in states and "chosen" in states:
         up, uc = states["plain"], states["chosen"]
-        out["state_max_rel_diff"] = float(np.max(np.abs(uc - up) / np.maximum(np.abs(up).max(0), 1e-300)))
+        # per cell: D and E relative to themselves, the momentum relative to the cell's E
+        E = np.abs(up[:, 4])
+        du = max(float(np.max(np.abs(uc[:, [0, 4]] - up[:, [0, 4]]) / np.abs(up[:, [0, 4]]))),
+                 float(np.max(np.abs(uc[:, 1:4] - up[:, 1:4]) / E[:, None])))
+        out["state_max_rel_diff_per_cell"] = du
         out["chosen_vs_plain"] = out["plain"]["ms_per_step"] / out["chosen"]["ms_per_step"]
     return out
 
@@ -686,6 +729,26 @@ def run_ours(args):
     e2e_value = job_throughput(m.n_cells, ws, e2e_steps, ms_e)
     io_bytes = 80 * m.n_cells
 
+    # e2e in the drop-in's resident mode: the host state uploaded once, every step reading
+    # back its step scalars (max signal speed) as rhllc::Hllc3dStab must, the state written
+    # back to the host buffers every SAVE steps (the save cadence of WriteSolution)
+    SAVE = 10
+    res_steps = max(SAVE, (args.steps // SAVE) * SAVE)
+    stt = L.StepStats()
+    barrier()
+    e0.record(stream)
+    L.check(L.lib.rrhd_set_state(g.handle, Wh.data_ptr(), Uh.data_ptr(), 5, L.RRHD_HOST))
+    for k in range(res_steps):
+        L.check(L.lib.rrhd_hydro_step(g.handle, tau, ctypes.byref(stt)))
+        if (k + 1) % SAVE == 0:
+            L.check(L.lib.rrhd_get_state(g.handle, Wh.data_ptr(), Uh.data_ptr(), 5, L.RRHD_HOST))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_r = max_over_ranks(e0.elapsed_time(e1), ws, f"cuda:{dev}")
+    e2e_res = {"value": job_throughput(m.n_cells, ws, res_steps, ms_r), "unit": UNIT,
+               "h2d_bytes_per_step": io_bytes / res_steps, "d2h_bytes_per_step": io_bytes / SAVE + 32,
+               "save_every_steps": SAVE, "steps": res_steps}
+
     # roofline of the fused step kernel (the only kernel in the step)
     alg_bytes = 185.0 * m.n_cells + 40.0 * m.n_faces
     achieved = alg_bytes / (per_step / 1e3) / 1e9
@@ -695,16 +758,14 @@ def run_ours(args):
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Kuhn mesh, jet initial state)",
-            "config": {"workload": f"coupled-jet mesh {NHEX}^3x6 tets: RHLLC flux + update + con2prim step",
-                       "cells": m.n_cells, "faces": m.n_faces, "gamma": GAMMA, "tau": tau,
-                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-                       "l2": "state 2 x 425 MB > L2 (126 MB): no flush"},
+            "vs_baseline": None, "dtype": "f64", "data": DATA,
+            "config": bench_config(m, ws),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": "measured" if pk else "fallback",
                          "algorithmic_bytes_per_cell_update": alg_bytes / m.n_cells},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
+            "e2e_resident": e2e_res,
             "gpu_launches": args.steps,
             "clocks": clk.summary(),
             "step_stats": {"max_speed": st.max_speed, "n_fallback": st.n_fallback, "n_failed": st.n_failed}}
@@ -755,7 +816,7 @@ def main():
     ap.add_argument("--no-scatter", action="store_true", help="skip the scattering component")
     ap.add_argument("--no-c2p", action="store_true", help="skip the con2prim (learned guess) component")
     ap.add_argument("--no-coupled", action="store_true", help="skip the coupled radiation-hydro step component")
-    ap.add_argument("--coupled-steps", type=int, default=3, help="timed coupled steps per form")
+    ap.add_argument("--coupled-steps", type=int, default=100, help="timed coupled steps per form")
     ap.add_argument("--scatter-only", type=int, default=0, metavar="NHEX",
                     help="only time the scattering component on an NHEX^3 x 6 mesh (profiling runs)")
     ap.add_argument("--sweep-only", type=int, default=0, metavar="NHEX",

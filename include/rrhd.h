@@ -217,8 +217,11 @@ typedef struct {
 } rrhd_c2p_stats;
 
 /* rrhd_con2prim_batch plus the totals above, reduced per CTA into a device
- * scratch buffer (one per device, allocated on first use) and then summed in a
- * fixed order.  Synchronises `stream` when stats is not NULL.  Same reference
+ * scratch buffer and then summed in a fixed order.  The scratch is one buffer
+ * per (device, stream), allocated on first use and grown (after synchronising
+ * that stream) when a batch needs more: calls on one stream are ordered, calls
+ * on different streams or host threads use separate buffers and may overlap.
+ * Synchronises `stream` when stats is not NULL.  Same reference
  * functions as rrhd_con2prim_batch (rhllc::GetPhysValueStab / PhysPressureFix);
  * the iteration counts are those of the loop at rhllc_flux_stab.cpp:153-183. */
 rrhd_status rrhd_con2prim_batch_stats(int32_t eos, double gamma, double *U, double *W,
@@ -232,9 +235,10 @@ rrhd_status rrhd_con2prim_batch_stats(int32_t eos, double gamma, double *U, doub
  * synchronisation.  The per-CTA partial totals live in a fixed file-scope
  * device array of 320 KiB, held by every GPU that loads the library until the
  * process exits, so n is limited to 16,777,216 states (RRHD_ERR_LIMIT beyond).
- * The first call on a device looks up that array's device address (make it
- * before any stream capture).  Every call shares the array: calls that overlap
- * on the GPU race and must be serialised by the caller. */
+ * The first call on a device (and the first after the device was reset) looks
+ * up that array's device address (make it before any stream capture).  Every
+ * call shares the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
 rrhd_status rrhd_con2prim_batch_stats_noalloc(int32_t eos, double gamma, double *U, double *W,
                                               uint8_t *status, int64_t n, int32_t fallback,
                                               rrhd_c2p_stats *stats, void *stream);
@@ -466,11 +470,16 @@ rrhd_status rrhd_rad_source(const rrhd_emission *em, const double *W, const doub
  * graph/ and make_trace/ tools) is built on the device at setup as levels of
  * cells whose upwind neighbours are all done; one level is one kernel launch,
  * all launches of a sweep are one CUDA graph. */
-#define RRHD_RAD_FP64 0 /* sweep arithmetic and storage in double */
-#define RRHD_RAD_FP32 1 /* in float (input of the tensor-core scattering) */
+#define RRHD_RAD_FP64 0  /* sweep arithmetic and storage in double */
+#define RRHD_RAD_FP32 1  /* in float (input of the tensor-core scattering) */
+#define RRHD_RAD_MIXED 2 /* arithmetic, face values and opacities in double; the scattering
+                            integral S read and the intensity I written in float (the
+                            tensor-core scattering's input and output): the intensity is
+                            the double sweep's rounded once, where the float sweep's
+                            rounding accumulates along each characteristic */
 typedef struct {
   int32_t groups;         /* frequency groups G >= 1 (grey copies, rows cell * G + g)           */
-  int32_t precision;      /* RRHD_RAD_FP64 or RRHD_RAD_FP32                                     */
+  int32_t precision;      /* RRHD_RAD_FP64, RRHD_RAD_FP32 or RRHD_RAD_MIXED                     */
   int32_t dirs_per_batch; /* directions swept together (face values [F][dirs_per_batch][groups] are
                              kept for them): power of two <= 256; 0 = min(64, M)                */
   double boundary_value;  /* intensity entering through boundary faces (illum::BoundaryConditions
@@ -482,10 +491,16 @@ typedef struct {
 rrhd_status rrhd_rad_setup(rrhd_ctx *ctx, const rrhd_dirs *dirs, const rrhd_rad_opts *opts);
 /* Levels summed over direction batches and the largest level (items). */
 rrhd_status rrhd_rad_plan_info(const rrhd_ctx *ctx, int64_t *levels, int64_t *max_level_items);
+/* The plan as the reference's sweep order would number it: levels [M][N] (caller cell
+ * numbering) the level of direction d's batch in which cell c is swept for d -- the
+ * depth of c in the upwind graph of d, which is the index of the front graph::
+ * RunGraphModule puts c in (graph/src/graph_by_direction.cpp).  Synchronises. */
+rrhd_status rrhd_rad_plan_levels(const rrhd_ctx *ctx, int32_t *levels);
 /* One sweep of all directions and groups on ctx's stream.  Device pointers of the
- * setup's precision (double or float), caller cell numbering: alpha, betta [N]
- * absorption and scattering coefficients, Q [N][G] emission B / kRadiation per
- * group, S [N*G][M] scattering integral in, I [N*G][M] intensity out. */
+ * setup's precision (double or float; RRHD_RAD_MIXED: alpha, betta, Q double, S and
+ * I float), caller cell numbering: alpha, betta [N] absorption and scattering
+ * coefficients, Q [N][G] emission B / kRadiation per group, S [N*G][M] scattering
+ * integral in, I [N*G][M] intensity out. */
 rrhd_status rrhd_sweep(rrhd_ctx *ctx, const void *alpha, const void *betta, const void *Q, const void *S, void *I);
 
 /* ------------------------------------------------------------ coupled step
@@ -522,11 +537,15 @@ rrhd_status rrhd_coupled_step(rrhd_ctx *ctx, double tau, const rrhd_coupled_opts
 rrhd_status rrhd_coupled_phase_ms(rrhd_ctx *ctx, float *ms4);
 /* Host copies (caller cell numbering, double) of the coupled step's radiation
  * arrays: RRHD_RAD_I / RRHD_RAD_S [N*G][M], RRHD_RAD_G4 [N][4] (4-force of the
- * last step); rrhd_rad_set writes I or S (e.g. the scattering integral of a
- * previous run). */
+ * last step), RRHD_RAD_MOM [N*G][10] (energy, stream and impulse moments of the
+ * last scattering per row cell * G + g: E, F0..2, T00, T01, T02, T11, T12, T22,
+ * as cuda_sep::MakeEnergy/MakeStream/MakeImpuls give them,
+ * cuda/src/short_characteristics/separate_gpu/cuda_illum_sep_param.cu:9-69);
+ * rrhd_rad_set writes I or S (e.g. the scattering integral of a previous run). */
 #define RRHD_RAD_I 0
 #define RRHD_RAD_S 1
 #define RRHD_RAD_G4 2
+#define RRHD_RAD_MOM 3
 rrhd_status rrhd_rad_get(rrhd_ctx *ctx, int32_t what, double *out);
 rrhd_status rrhd_rad_set(rrhd_ctx *ctx, int32_t what, const double *in);
 

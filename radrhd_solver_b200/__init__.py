@@ -12,10 +12,10 @@ which raises ImportError when librrhd.so is missing (there is no fallback).
 """
 import importlib
 
-__all__ = ["files_sys", "illum", "mesh", "rad_rhd", "rhllc"]
+__all__ = ["c2p_mlp", "files_sys", "illum", "illum_mpi", "mesh", "rad_rhd", "ray_tracing", "rhllc", "rhllc_mpi"]
 
 
 def __getattr__(name):
-    if name in ("illum", "mesh", "rad_rhd", "rhllc", "coupled", "c2p_mlp", "scatter_tc", "sweep", "files_sys", "_lib"):
+    if name in __all__ or name == "_lib":
         return importlib.import_module(f".{name}", __name__)
     raise AttributeError(name)

@@ -74,11 +74,13 @@ class Emission(C.Structure):
 
 RRHD_RAD_FP64 = 0
 RRHD_RAD_FP32 = 1
+RRHD_RAD_MIXED = 2
 RRHD_SCATTER_FP64 = -1
 RRHD_SCATTER_LOWRANK = -2
 RRHD_RAD_I = 0
 RRHD_RAD_S = 1
 RRHD_RAD_G4 = 2
+RRHD_RAD_MOM = 3
 
 
 class RadOpts(C.Structure):
@@ -148,6 +150,7 @@ _SIGS = {
     "rrhd_con2prim_batch_mlp": (I32, [P, I32, D, P, P, P, I64, I32, I32, P, P, P, P]),
     "rrhd_rad_setup": (I32, [P, P, P]),
     "rrhd_rad_plan_info": (I32, [P, P, P]),
+    "rrhd_rad_plan_levels": (I32, [P, P]),
     "rrhd_sweep": (I32, [P, P, P, P, P, P]),
     "rrhd_coupled_step": (I32, [P, D, P, P, P]),
     "rrhd_rad_get": (I32, [P, I32, P]),

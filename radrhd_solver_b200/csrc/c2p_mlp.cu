@@ -49,16 +49,21 @@ struct Norm {
   float mu[3], sig[3], mu_t, sig_t;
 };
 
+// tau and Q are formed in FP64 (both are differences that cancel: Q carries the thermal
+// energy of cold fast flows); the ratios and logarithms only feed a BF16 network and are
+// taken in FP32 with the fast hardware approximations, so that the features cost a few
+// FP32 instructions rather than three FP64 logarithms and divisions.
 __device__ __forceinline__ bool features(const double *U, float *f, double &tau) {
   const double D = U[0], E = U[4];
   tau = E - D;
   const double m2 = (U[1] * U[1] + U[2] * U[2]) + U[3] * U[3];
-  const double S = sqrt(m2);
   const double Q = E - sqrt(m2 + D * D);
   if (!(D > 0.0) || !(tau > 0.0) || !(Q > 0.0)) return false;
-  f[0] = (float)log(Q / tau);
-  f[1] = (float)log(fmax(S / tau, 1e-30));
-  f[2] = (float)log(tau / D);
+  const float tf = (float)tau;
+  const float S = sqrtf((float)m2);
+  f[0] = __logf(__fdividef((float)Q, tf));
+  f[1] = __logf(fmaxf(__fdividef(S, tf), 1e-30f));
+  f[2] = __logf(__fdividef(tf, (float)D));
   return isfinite(f[0]) && isfinite(f[1]) && isfinite(f[2]);
 }
 
@@ -284,7 +289,10 @@ __device__ __forceinline__ float mlp_warp(const float *xs, const float *sW1, con
 // States i live at U + stride*i and W + stride*i (stride 5 for separate arrays,
 // 10 for a solver state [n][10] = U, W).  With G4 != NULL the radiation source
 // is added first, U.E += tau G0 and U.S += tau G[1..3] (radRHD_main.cpp:117-126).
-__global__ void __launch_bounds__(IT) k_c2p_mlp(Eos eos, double *U, double *W, int64_t stride, const double *G4,
+#ifndef RRHD_MLP_MIN_BLOCKS
+#define RRHD_MLP_MIN_BLOCKS 1  // CTAs per SM the register budget of k_c2p_mlp is sized for
+#endif
+__global__ void __launch_bounds__(IT, RRHD_MLP_MIN_BLOCKS) k_c2p_mlp(Eos eos, double *U, double *W, int64_t stride, const double *G4,
                                                 double tau_src, uint8_t *status, int64_t n, int fallback,
                                                 int k_stall, const float *__restrict__ theta,
                                                 const uint32_t *__restrict__ frag, Norm nm, MlpPartial *scratch,
@@ -331,7 +339,7 @@ __global__ void __launch_bounds__(IT) k_c2p_mlp(Eos eos, double *U, double *W, i
     int it1 = 0, it2 = 0, code = 1;
     bool u_dirty = G4 != nullptr;
     if (feat) {
-      const double p0 = tau * exp((double)(y * nm.sig_t + nm.mu_t));
+      const double p0 = tau * (double)__expf(y * nm.sig_t + nm.mu_t);
       if (guess_out) guess_out[i] = p0;
       code = c2p_from(eos, u, wv, p0, true, &it1, k_stall);
     }

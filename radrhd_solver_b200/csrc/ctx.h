@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <climits>
+
 #include <vector>
 
 #include "rrhd.h"
@@ -23,6 +25,24 @@ struct BcTable {
   double W[8][5];
   double U[8][5];
 };
+
+// One entry of a CTA's face list (40 bytes): the face's unit normal and area and
+// its two sides as CTA-local state slots (r < 0: boundary code).
+struct FaceRec {
+  double n0, n1, n2, area;
+  int32_t l, r;
+};
+// Marks the padding entry that rounds a CTA's face list up to an even count.
+constexpr int32_t kFacePad = INT32_MIN;
+
+// Per-cell record of the step (16 bytes): the CTA-local slots of the cell's four
+// faces in id_faces order, each with the cell's sign_n bit of that face in bit
+// 15, and the cell volume.
+struct CellRec {
+  uint16_t s[4];
+  double V;
+};
+static_assert(sizeof(FaceRec) == 40 && sizeof(CellRec) == 16, "step record layout");
 
 }  // namespace rrhd
 
@@ -98,16 +118,13 @@ struct rrhd_ctx {
 
   // per-CTA face lists
   int32_t *d_bface_off = nullptr;  // [nblocks+1]
-  int2 *d_bface_lr = nullptr;      // [E] (l, r) as CTA-local state slots; r < 0: boundary code
+  rrhd::FaceRec *d_bface_rec = nullptr;  // [E] face records, every CTA's list padded to an even count
   int32_t *d_halo_off = nullptr;   // [nblocks+1]
   int32_t *d_halo_ids = nullptr;   // neighbour cells (new numbering) staged after the CTA's own
-  double4 *d_bface_nS = nullptr;   // [E] (n0, n1, n2, area)
   int32_t *d_bface_gid = nullptr;  // [E] caller face id on the owner CTA, else -1
 
   // per cell (new numbering)
-  ushort4 *d_cell_slot = nullptr;  // local face slots
-  uint8_t *d_cell_sign = nullptr;
-  double *d_cell_V = nullptr;
+  rrhd::CellRec *d_cell_rec = nullptr;
 
   // state [N][10] = U(5), W(5); two buffers, `cur` holds the current one
   double *d_state[2] = {nullptr, nullptr};

@@ -6,14 +6,18 @@
 //          two buffers (read one, write the other) so that no CTA overwrites a
 //          neighbour state another CTA still reads.
 //   per CTA (cells_per_block consecutive cells) a list of every face touching
-//   one of its cells: (l, r) as CTA-local state slots (int2), (n, area)
-//   double4, owner flag; and a halo list of the neighbour cells owned by other
-//   CTAs.  A face between two CTAs sits in both lists and is computed by both,
-//   bit-identically.  Per cell: 4 local face slots (ushort4), sign bits, volume.
+//   one of its cells as 40-byte records {n0, n1, n2, area, l, r} (l, r the
+//   CTA-local state slots, r < 0 a boundary code), padded to an even count so
+//   that every CTA's list starts on a 16-byte boundary; and a halo list of the
+//   neighbour cells owned by other CTAs.  A face between two CTAs sits in both
+//   lists and is computed by both, bit-identically.  Per cell a 16-byte record
+//   {4 local face slots with the cell's sign bit in bit 15, volume}.
 // One kernel does the whole step:
-//   phase 0  cp.async stages the CTA's own states (one contiguous range) and
-//            its halo states into shared memory, all requests in flight at once;
-//   phase 1  face fluxes from the staged states into shared memory;
+//   phase 0  cp.async stages the CTA's own states (one contiguous range), its
+//            halo states, its face records and its cell records into shared
+//            memory, all requests in flight at once;
+//   phase 1  face fluxes from the staged states; each thread overwrites the
+//            face record it has read with that face's flux;
 //   phase 2  each cell sums its 4 faces in the reference's order (id_faces
 //            j = 0..3 with sign_n), updates U, runs con2prim with the
 //            PhysPressureFix fallback and writes U, W and a status byte.
@@ -22,9 +26,12 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <numeric>
 #include <vector>
+
+#include <cuda.h>
 
 #include "ctx.h"
 #include "hydro_phys.cuh"
@@ -43,12 +50,9 @@ struct StepParams {
   const int32_t *__restrict__ halo_off;
   const int32_t *__restrict__ halo_ids;
   int max_halo;
-  const int2 *__restrict__ lr;
-  const double4 *__restrict__ nS;
+  const FaceRec *__restrict__ face;
   const int32_t *__restrict__ gid;
-  const ushort4 *__restrict__ slot;
-  const uint8_t *__restrict__ sign;
-  const double *__restrict__ V;
+  const CellRec *__restrict__ cell;
   const double *__restrict__ sin;
   double *__restrict__ sout;
   uint8_t *__restrict__ status;
@@ -61,21 +65,6 @@ struct StepParams {
   BcTable bc;
 };
 
-__device__ __forceinline__ void load_state(const double *s, int c, double *U, double *W) {
-  const double2 *p = reinterpret_cast<const double2 *>(s + 10 * (size_t)c);
-  const double2 a = __ldg(p), b = __ldg(p + 1), d = __ldg(p + 2), e = __ldg(p + 3), f = __ldg(p + 4);
-  U[0] = a.x;
-  U[1] = a.y;
-  U[2] = b.x;
-  U[3] = b.y;
-  U[4] = d.x;
-  W[0] = d.y;
-  W[1] = e.x;
-  W[2] = e.y;
-  W[3] = f.x;
-  W[4] = f.y;
-}
-
 __device__ __forceinline__ void store_state(double *s, int c, const double *U, const double *W) {
   double2 *p = reinterpret_cast<double2 *>(s + 10 * (size_t)c);
   p[0] = make_double2(U[0], U[1]);
@@ -86,9 +75,9 @@ __device__ __forceinline__ void store_state(double *s, int c, const double *U, c
 }
 
 // rhllc::BoundConditions (solvers/rhllc/src/rhllc_utils.cpp:45-133) from the table.
-__device__ __forceinline__ void boundary(const BcTable &bc, int code, const double4 &g,
-                                         const double *UL, const double *WL, double *UR,
-                                         double *WR) {
+// R is the face's rotation (GetRotationMatrix of its normal).  UR/WR may alias UL/WL.
+__device__ __forceinline__ void boundary(const BcTable &bc, int code, const Rot &R, const double *UL,
+                                         const double *WL, double *UR, double *WR) {
   const int k = -code - 1;
   const int kind = (k < 8) ? bc.kind[k] : 0;
   if (kind == RRHD_BC_FIXED) {
@@ -105,33 +94,21 @@ __device__ __forceinline__ void boundary(const BcTable &bc, int code, const doub
     WR[i] = WL[i];
   }
   if (kind == RRHD_BC_REFLECT) {
-    Rot R, Rt;
-    rotation(g.x, g.y, g.z, R);
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-      for (int j = 0; j < 3; j++) Rt.t[3 * i + j] = R.t[3 * j + i];
+    // v -> T^T diag(-1, 1, 1) T v, with T^T formed as a matrix (Matrix3 * Vector3 order)
     double r[3];
     matvec(R, UR + 1, r);
-    UR[1] = -r[0];
-    UR[2] = r[1];
-    UR[3] = r[2];
+    r[0] = -r[0];
+    matvec_transposed(R, r, UR + 1);
     matvec(R, WR + 1, r);
-    WR[1] = -r[0];
-    WR[2] = r[1];
-    WR[3] = r[2];
-    matvec(Rt, UR + 1, r);
-    UR[1] = r[0];
-    UR[2] = r[1];
-    UR[3] = r[2];
-    matvec(Rt, WR + 1, r);
-    WR[1] = r[0];
-    WR[2] = r[1];
-    WR[3] = r[2];
+    r[0] = -r[0];
+    matvec_transposed(R, r, WR + 1);
   }
 }
 
-constexpr int kStepThreads = 256;
+#ifndef RRHD_STEP_THREADS
+#define RRHD_STEP_THREADS 256  // threads per CTA of the step kernel
+#endif
+constexpr int kStepThreads = RRHD_STEP_THREADS;
 constexpr int kMaxCellsPerBlock = 1024;  // local cell index fits 12 bits
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
@@ -160,25 +137,31 @@ __device__ __forceinline__ void load_state_smem(const double *s, int slot, doubl
 #ifndef RRHD_STEP_MIN_BLOCKS
 #define RRHD_STEP_MIN_BLOCKS 3  // CTAs per SM the register budget is sized for
 #endif
+// kFaceFlux: also write every face's flux to P.face_flux (caller numbering), for
+// rrhd_keep_face_flux; a separate instantiation keeps the common one lean.
+template <bool kFaceFlux>
 __global__ void __launch_bounds__(kStepThreads, RRHD_STEP_MIN_BLOCKS) k_hydro_step(const StepParams P) {
   extern __shared__ double2 smem_raw[];
-  double *sstate = reinterpret_cast<double *>(smem_raw);  // [cpb + max_halo][10]
-  double *sflux = sstate + 10 * (P.cpb + P.max_halo);     // [entries][5]
+  double *sstate = reinterpret_cast<double *>(smem_raw);      // [cpb + max_halo][10]
+  double *sface = sstate + 10 * (P.cpb + P.max_halo);         // [entries][5]: record, then flux
+  const int b = P.b0 + blockIdx.x;
+  const int e0 = P.off[b], e1 = P.off[b + 1];
+  CellRec *scell = reinterpret_cast<CellRec *>(sface + 5 * (e1 - e0));  // [cpb]
   __shared__ double s_red[kStepThreads / 32];
   __shared__ unsigned long long s_cnt[2];
   __shared__ unsigned short s_fail[kMaxCellsPerBlock];
   __shared__ int s_nfail;
-  const int b = P.b0 + blockIdx.x;
   const int c0 = b * P.cpb;
   const int nc = min(P.cpb, P.N - c0);
-  const int e0 = P.off[b], e1 = P.off[b + 1];
   const int h0 = P.halo_off[b], h1 = P.halo_off[b + 1];
   double tau = P.tau;
   if (P.device_tau) tau = P.cfl_hmin / P.prev->max_speed;
   if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0;
   if (threadIdx.x == 0) s_nfail = 0;
 
-  // phase 0: stage own (contiguous) and halo states, 16 bytes per request
+  // phase 0: stage own (contiguous) and halo states, the face records and the
+  // cell records, 16 bytes per request.  Each CTA's face list starts on a
+  // 16-byte boundary and holds an even number of 40-byte records.
   {
     const char *g = reinterpret_cast<const char *>(P.sin);
     char *sm = reinterpret_cast<char *>(sstate);
@@ -188,28 +171,43 @@ __global__ void __launch_bounds__(kStepThreads, RRHD_STEP_MIN_BLOCKS) k_hydro_st
       const int h = q / 5, k = q - 5 * h;
       cp_async16(sm + 80 * (P.cpb + h) + 16 * k, g + 80 * (size_t)P.halo_ids[h0 + h] + 16 * k);
     }
+    const char *gf = reinterpret_cast<const char *>(P.face + e0);
+    char *sf = reinterpret_cast<char *>(sface);
+    for (int q = threadIdx.x; q < (e1 - e0) * 40 / 16; q += kStepThreads) cp_async16(sf + 16 * q, gf + 16 * q);
+    const char *gc = reinterpret_cast<const char *>(P.cell + c0);
+    char *sc = reinterpret_cast<char *>(scell);
+    for (int q = threadIdx.x; q < nc; q += kStepThreads) cp_async16(sc + 16 * q, gc + 16 * q);
     cp_async_wait_all();
   }
   __syncthreads();
 
-  // phase 1: every face touching this CTA's cells
+  // phase 1: every face touching this CTA's cells; the flux replaces the record
   double vmax = 0.0;
-  for (int e = e0 + threadIdx.x; e < e1; e += kStepThreads) {
-    const int2 lr = P.lr[e];
-    const double4 g = P.nS[e];
-    double UL[5], WL[5], UR[5], WR[5], Fl[5];
-    load_state_smem(sstate, lr.x, UL, WL);
+  for (int e = threadIdx.x; e < e1 - e0; e += kStepThreads) {
+    double *rec = sface + 5 * e;
+    const double n0 = rec[0], n1 = rec[1], n2 = rec[2], area = rec[3];
+    const int2 lr = *reinterpret_cast<const int2 *>(rec + 4);
+    if (lr.y == kFacePad) continue;
+    Rot R;
+    rotation(n0, n1, n2, R);
+    double U[5], W[5], Fl[5];
+    load_state_smem(sstate, lr.x, U, W);
+    const FaceSide sl = face_side(P.eos, R, U, W);
     if (lr.y >= 0)
-      load_state_smem(sstate, lr.y, UR, WR);
+      load_state_smem(sstate, lr.y, U, W);
     else
-      boundary(P.bc, lr.y, g, UL, WL, UR, WR);
-    const double s = hllc_flux(P.eos, UL, UR, WL, WR, g.x, g.y, g.z, g.w, Fl);
-    vmax = smax(vmax, s);
-    double *dst = sflux + 5 * (e - e0);
+      boundary(P.bc, lr.y, R, U, W, U, W);  // ghost state from the left one, in place
+    const FaceSide sr = face_side(P.eos, R, U, W);
+    const FaceStar fs = face_star(sl, sr);
+    vmax = smax(vmax, fs.vmax);
+    // the selected side's conservative state again (registers are the scarce resource)
+    load_state_smem(sstate, (fs.right && lr.y >= 0) ? lr.y : lr.x, U, W);
+    if (fs.right && lr.y < 0) boundary(P.bc, lr.y, R, U, W, U, W);
+    face_flux(R, U, fs.right ? sr : sl, fs, area, Fl);
 #pragma unroll
-    for (int i = 0; i < 5; i++) dst[i] = Fl[i];
-    if (P.face_flux) {
-      const int gf = P.gid[e];
+    for (int i = 0; i < 5; i++) rec[i] = Fl[i];
+    if (kFaceFlux) {
+      const int gf = P.gid[e0 + e];
       if (gf >= 0) {
 #pragma unroll
         for (int i = 0; i < 5; i++) P.face_flux[5 * (size_t)gf + i] = Fl[i];
@@ -223,14 +221,12 @@ __global__ void __launch_bounds__(kStepThreads, RRHD_STEP_MIN_BLOCKS) k_hydro_st
   unsigned n_fb = 0, n_fail = 0;
   for (int cl = threadIdx.x; cl < nc; cl += kStepThreads) {
     const int c = c0 + cl;
-    const ushort4 sl = P.slot[c];
-    const unsigned sg = P.sign[c];
-    const unsigned short sls[4] = {sl.x, sl.y, sl.z, sl.w};
+    const CellRec cr = scell[cl];
     double sum[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-      const double *f = sflux + 5 * sls[j];
-      if ((sg >> j) & 1u) {
+      const double *f = sface + 5 * (cr.s[j] & 0x7fff);
+      if (cr.s[j] & 0x8000) {
 #pragma unroll
         for (int i = 0; i < 5; i++) sum[i] += f[i];
       } else {
@@ -238,7 +234,7 @@ __global__ void __launch_bounds__(kStepThreads, RRHD_STEP_MIN_BLOCKS) k_hydro_st
         for (int i = 0; i < 5; i++) sum[i] -= f[i];
       }
     }
-    const double sc = (tau / P.V[c]);
+    const double sc = (tau / cr.V);
     double U[5], W[5];
     load_state_smem(sstate, cl, U, W);
 #pragma unroll
@@ -356,7 +352,10 @@ struct C2pPartial {
   unsigned long long ok, fallback, failed, iters, max_iters;
 };
 
-__global__ void __launch_bounds__(kC2pThreads) k_c2p_stats(Eos eos, double *U, double *W, uint8_t *status,
+#ifndef RRHD_C2P_MIN_BLOCKS
+#define RRHD_C2P_MIN_BLOCKS 1  // CTAs per SM the register budget of k_c2p_stats is sized for
+#endif
+__global__ void __launch_bounds__(kC2pThreads, RRHD_C2P_MIN_BLOCKS) k_c2p_stats(Eos eos, double *U, double *W, uint8_t *status,
                                                           int64_t n, int fallback, C2pPartial *scratch) {
   unsigned long long ok = 0, fb = 0, failed = 0, iters = 0, mx = 0;
   const int64_t base = (int64_t)blockIdx.x * kC2pPerBlock;
@@ -477,8 +476,8 @@ void free_ctx(rrhd_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
   rrhd_rad_release(c);
-  void *ptrs[] = {c->d_perm, c->d_iperm, c->d_bface_off, c->d_bface_lr, c->d_bface_nS, c->d_halo_off, c->d_halo_ids,
-                  c->d_bface_gid, c->d_cell_slot, c->d_cell_sign, c->d_cell_V, c->d_state[0],
+  void *ptrs[] = {c->d_perm, c->d_iperm, c->d_bface_off, c->d_bface_rec, c->d_halo_off, c->d_halo_ids,
+                  c->d_bface_gid, c->d_cell_rec, c->d_state[0],
                   c->d_state[1], c->d_status, c->d_scal, c->d_face_flux, c->d_scratch_io,
                   c->d_send_ids, c->d_recv_ids};
   for (void *p : ptrs)
@@ -537,15 +536,11 @@ extern "C" rrhd_status rrhd_create(const rrhd_mesh_desc *m, const rrhd_opts *opt
   c->part_b1 = nb;
   c->part_c1 = N;
   std::vector<int32_t> off(nb + 1, 0);
-  std::vector<int2> lr;
-  std::vector<double4> nS;
+  std::vector<FaceRec> frec;
   std::vector<int32_t> gid;
-  lr.reserve((size_t)(F * 1.3));
-  nS.reserve((size_t)(F * 1.3));
+  frec.reserve((size_t)(F * 1.3));
   gid.reserve((size_t)(F * 1.3));
-  std::vector<ushort4> slot(N);
-  std::vector<uint8_t> sign(N);
-  std::vector<double> vol(N);
+  std::vector<CellRec> crec(N);
   std::vector<int32_t> stamp(F, -1), local(F, 0);
   std::vector<int32_t> hstamp(N, -1), hlocal(N, 0);
   std::vector<int32_t> hoff(nb + 1, 0), hids;
@@ -576,18 +571,23 @@ extern "C" rrhd_status rrhd_create(const rrhd_mesh_desc *m, const rrhd_opts *opt
           const int32_t r = m->face_id_r[f] >= 0 ? iperm[m->face_id_r[f]] : m->face_id_r[f];
           const int32_t ls = slot_of(l);
           const int32_t rs = r >= 0 ? slot_of(r) : r;
-          lr.push_back(make_int2(ls, rs));
-          nS.push_back(make_double4(m->face_n[3 * f], m->face_n[3 * f + 1], m->face_n[3 * f + 2],
-                                    m->face_area[f]));
+          frec.push_back(FaceRec{m->face_n[3 * f], m->face_n[3 * f + 1], m->face_n[3 * f + 2], m->face_area[f],
+                                 ls, rs});
           gid.push_back((l / cpb == b) ? f : -1);
         }
         s4[j] = (unsigned short)local[f];
       }
-      slot[cn] = make_ushort4(s4[0], s4[1], s4[2], s4[3]);
-      sign[cn] = m->cell_sign[co];
-      vol[cn] = m->cell_volume[co];
+      CellRec &cr = crec[cn];
+      for (int j = 0; j < 4; j++)
+        cr.s[j] = (uint16_t)(s4[j] | (((m->cell_sign[co] >> j) & 1u) << 15));
+      cr.V = m->cell_volume[co];
     }
-    if (ne > 65535) return fail(rrhd_fail(RRHD_ERR_LIMIT, "CTA face list too long"));
+    if (ne & 1) {  // pad to an even count: every CTA's list then starts on a 16-byte boundary
+      frec.push_back(FaceRec{0.0, 0.0, 0.0, 0.0, 0, kFacePad});
+      gid.push_back(-1);
+      ne++;
+    }
+    if (ne > 32767) return fail(rrhd_fail(RRHD_ERR_LIMIT, "CTA face list too long"));
     max_e = std::max(max_e, ne);
     max_h = std::max(max_h, nh);
     off[b + 1] = off[b] + ne;
@@ -605,10 +605,8 @@ extern "C" rrhd_status rrhd_create(const rrhd_mesh_desc *m, const rrhd_opts *opt
   c->n_entries = off[nb];
   c->h_perm = perm;
   if ((st = upload(&c->d_perm, perm)) || (st = upload(&c->d_iperm, iperm)) ||
-      (st = upload(&c->d_bface_off, off)) || (st = upload(&c->d_bface_lr, lr)) ||
-      (st = upload(&c->d_bface_nS, nS)) || (st = upload(&c->d_bface_gid, gid)) ||
-      (st = upload(&c->d_cell_slot, slot)) || (st = upload(&c->d_cell_sign, sign)) ||
-      (st = upload(&c->d_cell_V, vol)) || (st = upload(&c->d_halo_off, hoff)) ||
+      (st = upload(&c->d_bface_off, off)) || (st = upload(&c->d_bface_rec, frec)) ||
+      (st = upload(&c->d_bface_gid, gid)) || (st = upload(&c->d_cell_rec, crec)) || (st = upload(&c->d_halo_off, hoff)) ||
       (st = upload(&c->d_halo_ids, hids)))
     return fail(st);
   const size_t ssz = sizeof(double) * 10 * N;
@@ -623,12 +621,13 @@ extern "C" rrhd_status rrhd_create(const rrhd_mesh_desc *m, const rrhd_opts *opt
   cudaMemcpy(c->d_scal, init, sizeof init, cudaMemcpyHostToDevice);
   c->scal_cur = 0;
   for (int k = 0; k < 8; k++) c->bc.kind[k] = RRHD_BC_TRANSMISSIVE;
-  // staged states (own + halo) and the CTA's face fluxes
-  const size_t smem = sizeof(double) * (10 * (size_t)(cpb + max_h) + 5 * (size_t)max_e);
+  // staged states (own + halo), the CTA's face records (then fluxes) and cell records
+  const size_t smem = sizeof(double) * (10 * (size_t)(cpb + max_h) + 5 * (size_t)max_e) + sizeof(CellRec) * cpb;
   c->step_smem = smem;
   if (smem > 227 * 1024)
     return fail(rrhd_fail(RRHD_ERR_LIMIT, "step needs %zu B of shared memory per CTA; lower cells_per_block", smem));
-  if (cudaFuncSetAttribute(k_hydro_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+  if (cudaFuncSetAttribute(k_hydro_step<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaFuncSetAttribute(k_hydro_step<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return fail(rrhd_fail(RRHD_ERR_LIMIT, "cannot reserve %zu B of shared memory", smem));
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(rrhd_fail(RRHD_ERR_CUDA, "%s", cudaGetErrorString(cudaGetLastError())));
   *out = c;
@@ -762,12 +761,9 @@ extern "C" rrhd_status rrhd_hydro_step(rrhd_ctx *c, double tau, rrhd_step_stats 
   P.halo_off = c->d_halo_off;
   P.halo_ids = c->d_halo_ids;
   P.max_halo = c->max_halo;
-  P.lr = c->d_bface_lr;
-  P.nS = c->d_bface_nS;
+  P.face = c->d_bface_rec;
   P.gid = c->d_bface_gid;
-  P.slot = c->d_cell_slot;
-  P.sign = c->d_cell_sign;
-  P.V = c->d_cell_V;
+  P.cell = c->d_cell_rec;
   P.sin = c->d_state[c->cur];
   P.sout = c->d_state[c->cur ^ 1];
   P.status = c->d_status;
@@ -779,7 +775,10 @@ extern "C" rrhd_status rrhd_hydro_step(rrhd_ctx *c, double tau, rrhd_step_stats 
   P.cfl_hmin = c->cfl * c->h_min;
   P.bc = c->bc;
   RRHD_CUDA(cudaMemsetAsync(P.out, 0, sizeof(StepScalars), c->stream));
-  k_hydro_step<<<c->part_b1 - c->part_b0, kStepThreads, c->step_smem, c->stream>>>(P);
+  if (P.face_flux)
+    k_hydro_step<true><<<c->part_b1 - c->part_b0, kStepThreads, c->step_smem, c->stream>>>(P);
+  else
+    k_hydro_step<false><<<c->part_b1 - c->part_b0, kStepThreads, c->step_smem, c->stream>>>(P);
   RRHD_CUDA(cudaGetLastError());
   c->cur ^= 1;
   c->scal_cur ^= 1;
@@ -845,10 +844,17 @@ extern "C" rrhd_status rrhd_hydro_set_part(rrhd_ctx *c, int32_t world, int32_t r
                            rid.data())))
     return st;
   RRHD_CUDA(cudaStreamSynchronize(c->stream));
+  // upload the new id lists first: on failure the context keeps its previous split
+  int32_t *d_sid = nullptr, *d_rid = nullptr;
+  if ((st = upload(&d_sid, sid)) || (st = upload(&d_rid, rid))) {
+    if (d_sid) cudaFree(d_sid);
+    if (d_rid) cudaFree(d_rid);
+    return st;
+  }
   if (c->d_send_ids) cudaFree(c->d_send_ids);
   if (c->d_recv_ids) cudaFree(c->d_recv_ids);
-  c->d_send_ids = c->d_recv_ids = nullptr;
-  if ((st = upload(&c->d_send_ids, sid)) || (st = upload(&c->d_recv_ids, rid))) return st;
+  c->d_send_ids = d_sid;
+  c->d_recv_ids = d_rid;
   c->part_world = world;
   c->part_rank = rank;
   c->part_b0 = (int)(c->nblocks * (int64_t)rank / world);
@@ -961,15 +967,31 @@ extern "C" rrhd_status rrhd_prim2con_batch(int32_t eos, double gamma, double *W,
   return RRHD_OK;
 }
 
-// Scratch of rrhd_con2prim_batch_stats: one buffer per device, allocated on
-// first use and grown when a larger batch needs more partial records.
+// Scratch of rrhd_con2prim_batch_stats: one buffer per (device, stream),
+// allocated on first use and grown when a larger batch needs more partial
+// records.  Calls on one stream run one after another on the GPU, so they can
+// share a buffer; calls on different streams get different buffers and may
+// overlap.  The registry lock is held from the lookup until the kernels and the
+// read-back of the totals are enqueued, so a call that grows a stream's buffer
+// (after synchronising that stream) can never free memory that another thread
+// has looked up but not yet used.
 namespace {
+struct ScratchKey {
+  int dev;
+  cudaStream_t stream;
+  bool operator<(const ScratchKey &o) const { return dev != o.dev ? dev < o.dev : stream < o.stream; }
+};
+struct ScratchBuf {
+  C2pPartial *ptr = nullptr;
+  int64_t cap = 0;
+};
 std::mutex g_c2p_scratch_mu;
-C2pPartial *g_c2p_scratch[64] = {nullptr};
-int64_t g_c2p_scratch_cap[64] = {0};
+std::map<ScratchKey, ScratchBuf> g_c2p_scratch;
 
-rrhd_status c2p_stats_launch(Eos eos, double *U, double *W, uint8_t *status, int64_t n, int32_t fallback,
-                             C2pPartial *scratch, rrhd_c2p_stats *stats, cudaStream_t stream) {
+// Enqueues the batch and the reduction (and, with stats, the read-back of the
+// totals into *total) on `stream`; the caller synchronises before reading it.
+rrhd_status c2p_stats_enqueue(Eos eos, double *U, double *W, uint8_t *status, int64_t n, int32_t fallback,
+                              C2pPartial *scratch, C2pPartial *total, cudaStream_t stream) {
   const int64_t nb = (n + kC2pPerBlock - 1) / kC2pPerBlock;
   if (nb > 0) {
     k_c2p_stats<<<(unsigned)nb, kC2pThreads, 0, stream>>>(eos, U, W, status, n, fallback, scratch);
@@ -977,16 +999,18 @@ rrhd_status c2p_stats_launch(Eos eos, double *U, double *W, uint8_t *status, int
   }
   k_c2p_stats_reduce<<<1, 256, 0, stream>>>(scratch, (int)nb);
   RRHD_CUDA(cudaGetLastError());
-  if (stats) {
-    C2pPartial t;
-    RRHD_CUDA(cudaMemcpyAsync(&t, scratch + nb, sizeof t, cudaMemcpyDeviceToHost, stream));
-    RRHD_CUDA(cudaStreamSynchronize(stream));
-    stats->n_ok = (int64_t)t.ok;
-    stats->n_fallback = (int64_t)t.fallback;
-    stats->n_failed = (int64_t)t.failed;
-    stats->newton_iters = (int64_t)t.iters;
-    stats->max_iters = (int32_t)t.max_iters;
-  }
+  if (total) RRHD_CUDA(cudaMemcpyAsync(total, scratch + nb, sizeof *total, cudaMemcpyDeviceToHost, stream));
+  return RRHD_OK;
+}
+
+rrhd_status c2p_stats_finish(const C2pPartial *total, rrhd_c2p_stats *stats, cudaStream_t stream) {
+  if (!stats) return RRHD_OK;
+  RRHD_CUDA(cudaStreamSynchronize(stream));
+  stats->n_ok = (int64_t)total->ok;
+  stats->n_fallback = (int64_t)total->fallback;
+  stats->n_failed = (int64_t)total->failed;
+  stats->newton_iters = (int64_t)total->iters;
+  stats->max_iters = (int32_t)total->max_iters;
   return RRHD_OK;
 }
 }  // namespace
@@ -998,25 +1022,29 @@ extern "C" rrhd_status rrhd_con2prim_batch_stats(int32_t eos, double gamma, doub
   RRHD_CHECK_ARG(eos == RRHD_EOS_IDEAL || eos == RRHD_EOS_TAUB, "bad eos");
   int dev = 0;
   RRHD_CUDA(cudaGetDevice(&dev));
-  RRHD_CHECK_ARG(dev >= 0 && dev < 64, "device ordinal out of range");
+  const cudaStream_t s = (cudaStream_t)stream;
   const int64_t need = (n + kC2pPerBlock - 1) / kC2pPerBlock + 1;
-  C2pPartial *scratch = nullptr;
+  C2pPartial total{};
   {
     std::lock_guard<std::mutex> lk(g_c2p_scratch_mu);
-    if (g_c2p_scratch_cap[dev] < need) {
-      if (g_c2p_scratch[dev]) {
-        RRHD_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
-        cudaFree(g_c2p_scratch[dev]);
-        g_c2p_scratch[dev] = nullptr;
-        g_c2p_scratch_cap[dev] = 0;
+    ScratchBuf &buf = g_c2p_scratch[ScratchKey{dev, s}];
+    if (buf.cap < need) {
+      if (buf.ptr) {
+        // every earlier user of this buffer enqueued its work on `stream`
+        RRHD_CUDA(cudaStreamSynchronize(s));
+        cudaFree(buf.ptr);
+        buf.ptr = nullptr;
+        buf.cap = 0;
       }
       const int64_t cap = std::max<int64_t>(need, 1024);
-      RRHD_CUDA(cudaMalloc(&g_c2p_scratch[dev], sizeof(C2pPartial) * cap));
-      g_c2p_scratch_cap[dev] = cap;
+      RRHD_CUDA(cudaMalloc(&buf.ptr, sizeof(C2pPartial) * cap));
+      buf.cap = cap;
     }
-    scratch = g_c2p_scratch[dev];
+    const rrhd_status st =
+        c2p_stats_enqueue(make_eos(eos, gamma), U, W, status, n, fallback, buf.ptr, stats ? &total : nullptr, s);
+    if (st) return st;
   }
-  return c2p_stats_launch(make_eos(eos, gamma), U, W, status, n, fallback, scratch, stats, (cudaStream_t)stream);
+  return c2p_stats_finish(&total, stats, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -1031,8 +1059,10 @@ extern "C" rrhd_status rrhd_con2prim_batch_stats(int32_t eos, double gamma, doub
 //
 // Host code cannot use the array's name as a device address (it is a host-side
 // stand-in), so the first call on each device looks the address up with
-// cudaGetSymbolAddress while that device is current and caches it; make that
-// first call before any stream capture.  All calls share the array and it keeps
+// cudaGetSymbolAddress while that device is current and caches it together with
+// the device's current context (a reset device gets a new context, and the
+// address is looked up again); make that first call before any stream capture.
+// All calls share the array and it keeps
 // the last call's contents: every call rewrites all the records it reads (one
 // per CTA, then the total), so nothing has to be cleared, but calls that
 // overlap on the GPU (concurrent streams) race on it and must be serialised.
@@ -1042,7 +1072,11 @@ static __device__ __align__(256) C2pPartial g_c2p_noalloc_scratch[kNoallocMaxBlo
 
 namespace {
 std::mutex g_noalloc_mu;
+// device address of the array per device ordinal, with the primary context it
+// was looked up in: a reset device (cudaDeviceReset) gets a new context and the
+// module is loaded again, so the address is looked up again.
 C2pPartial *g_noalloc_addr[64] = {nullptr};
+CUcontext g_noalloc_ctx[64] = {nullptr};
 }  // namespace
 
 extern "C" rrhd_status rrhd_con2prim_batch_stats_noalloc(int32_t eos, double gamma, double *U, double *W,
@@ -1056,15 +1090,33 @@ extern "C" rrhd_status rrhd_con2prim_batch_stats_noalloc(int32_t eos, double gam
   int dev = 0;
   RRHD_CUDA(cudaGetDevice(&dev));
   RRHD_CHECK_ARG(dev >= 0 && dev < 64, "device ordinal out of range");
-  C2pPartial *scratch = nullptr;
+  RRHD_CUDA(cudaSetDevice(dev));  // initialises the device's primary context and makes it current
+  // the driver's cuCtxGetCurrent through the runtime, so that the library has no
+  // link-time dependency on the driver library
+  static CUresult (*ctx_get_current)(CUcontext *) = nullptr;
+  if (!ctx_get_current) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      ctx_get_current = reinterpret_cast<CUresult (*)(CUcontext *)>(p);
+  }
+  CUcontext ctx = nullptr;
+  if (!ctx_get_current || ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx)
+    return rrhd_fail(RRHD_ERR_CUDA, "rrhd_con2prim_batch_stats_noalloc: no current CUDA context");
+  const cudaStream_t s = (cudaStream_t)stream;
+  C2pPartial total{};
   {
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
+    if (!g_noalloc_addr[dev] || g_noalloc_ctx[dev] != ctx) {
       void *addr = nullptr;
       RRHD_CUDA(cudaGetSymbolAddress(&addr, g_c2p_noalloc_scratch));
       g_noalloc_addr[dev] = reinterpret_cast<C2pPartial *>(addr);
+      g_noalloc_ctx[dev] = ctx;
     }
-    scratch = g_noalloc_addr[dev];
+    const rrhd_status st = c2p_stats_enqueue(make_eos(eos, gamma), U, W, status, n, fallback, g_noalloc_addr[dev],
+                                             stats ? &total : nullptr, s);
+    if (st) return st;
   }
-  return c2p_stats_launch(make_eos(eos, gamma), U, W, status, n, fallback, scratch, stats, (cudaStream_t)stream);
+  return c2p_stats_finish(&total, stats, s);
 }

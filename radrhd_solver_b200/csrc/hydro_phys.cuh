@@ -63,6 +63,13 @@ __device__ __forceinline__ void matvec(const Rot &R, const double *v, double *r)
   r[1] = (T[3] * v[0] + T[4] * v[1]) + T[5] * v[2];
   r[2] = T[6] * v[0] + (T[7] * v[1] + T[8] * v[2]);
 }
+// T.transpose() materialised as a Matrix3 and then times v (the Matrix3 * Vector3 order above).
+__device__ __forceinline__ void matvec_transposed(const Rot &R, const double *v, double *r) {
+  const double *T = R.t;
+  r[0] = (T[0] * v[0] + T[3] * v[1]) + T[6] * v[2];
+  r[1] = (T[1] * v[0] + T[4] * v[1]) + T[7] * v[2];
+  r[2] = T[2] * v[0] + (T[5] * v[1] + T[8] * v[2]);
+}
 __device__ __forceinline__ void matTvec(const Rot &R, const double *v, double *r) {
   const double *T = R.t;
   r[0] = (T[0] * v[0] + T[3] * v[1]) + T[6] * v[2];
@@ -261,84 +268,107 @@ __device__ __forceinline__ double sound_speed2(const Eos &e, double d, double p)
   return theta / (3.0 * h) * (5.0 * h - 8.0 * theta) / (h - theta);
 }
 
-// GetFluxStab, rhllc_flux_stab.cpp:240-431.  Fout = area * flux in the global
-// frame; returns max(lambda_L, lambda_R).
-__device__ __forceinline__ double hllc_flux(const Eos &e, const double *UL0, const double *UR0,
-                                            const double *WL0, const double *WR0, double n0,
-                                            double n1, double n2, double area, double *Fout) {
-  Rot R;
-  rotation(n0, n1, n2, R);
-  double UL[5], UR[5], Vel_L[3], Vel_R[3];
-  UL[0] = UL0[0];
-  UL[4] = UL0[4];
-  matvec(R, UL0 + 1, UL + 1);
-  UR[0] = UR0[0];
-  UR[4] = UR0[4];
-  matvec(R, UR0 + 1, UR + 1);
-  matvec(R, WL0 + 1, Vel_L);
-  matvec(R, WR0 + 1, Vel_R);
-  const double d_L = WL0[0], d_R = WR0[0];
-  const double p_L = WL0[4], p_R = WR0[4];
-  const double VV_L = dot3(Vel_L[0], Vel_L[1], Vel_L[2], Vel_L[0], Vel_L[1], Vel_L[2]);
-  const double VV_R = dot3(Vel_R[0], Vel_R[1], Vel_R[2], Vel_R[0], Vel_R[1], Vel_R[2]);
-  const double cs_L2 = sound_speed2(e, d_L, p_L);
-  const double cs_R2 = sound_speed2(e, d_R, p_R);
-  double cmax_L, cmax_R, cmin_L, cmin_R;
-  signal_speed(cs_L2, Vel_L[0], VV_L, cmin_L, cmax_L);
-  signal_speed(cs_R2, Vel_R[0], VV_R, cmin_R, cmax_R);
-  const double lambda_L = smin(cmin_L, cmin_R);
-  const double lambda_R = smax(cmax_L, cmax_R);
+// GetFluxStab, rhllc_flux_stab.cpp:240-431, split in three parts so that a thread
+// holds few values at a time (the step kernel is latency-bound and runs more warps
+// when each needs fewer registers).  Every value is formed by the reference's
+// operations in the reference's order, so the flux is the reference's bit for bit:
+//   face_side    one side's rotated normal velocity and momentum, energy, pressure,
+//                sound speed and signal speeds (:257-318);
+//   face_star    the wave speeds lambda_L/R, the branch, and in the HLLC branch the
+//                contact speed us and pressure ps (:319-394);
+//   face_flux    the flux of the side the branch selects, from that side's state
+//                reloaded in the global frame, rotated back and times the area
+//                (:331-346, :395-431).
+struct FaceSide {
+  double cmin, cmax;  // signal speeds (GetSignalSpeed, :231-238)
+  double m1;          // momentum along the normal: row 0 of T * U.v
+  double E;           // U.p (total energy)
+  double vn;          // velocity along the normal: row 0 of T * W.v
+  double p;           // W.p
+};
 
-  double F[5];
+__device__ __forceinline__ FaceSide face_side(const Eos &e, const Rot &R, const double *U, const double *W) {
+  double vel[3];
+  matvec(R, W + 1, vel);
+  FaceSide s;
+  s.m1 = (R.t[0] * U[1] + R.t[1] * U[2]) + R.t[2] * U[3];
+  s.E = U[4];
+  s.vn = vel[0];
+  s.p = W[4];
+  const double VV = dot3(vel[0], vel[1], vel[2], vel[0], vel[1], vel[2]);
+  const double cs2 = sound_speed2(e, W[0], W[4]);
+  signal_speed(cs2, vel[0], VV, s.cmin, s.cmax);
+  return s;
+}
+
+// Which side's flux the face takes and the star-state parameters.
+struct FaceStar {
+  double vmax;  // max(lambda_L, lambda_R), the value GetFluxStab returns
+  double lam;   // the selected side's wave speed (HLLC branch)
+  double us, ps;
+  bool right;   // the flux is built from the right state
+  bool star;    // HLLC branch (star state), else the upwind flux of one side
+};
+
+__device__ __forceinline__ FaceStar face_star(const FaceSide &L, const FaceSide &R) {
+  const double lambda_L = smin(L.cmin, R.cmin);
+  const double lambda_R = smax(L.cmax, R.cmax);
+  FaceStar f;
+  f.vmax = smax(lambda_L, lambda_R);
+  f.lam = 0.0;
+  f.us = 0.0;
+  f.ps = 0.0;
+  f.star = false;
   if (lambda_L >= 0.0) {
-    F[0] = UL[0] * Vel_L[0];
-    F[1] = UL[1] * Vel_L[0];
-    F[2] = UL[2] * Vel_L[0];
-    F[3] = UL[3] * Vel_L[0];
-    F[4] = UL[1];
-    F[1] += p_L;
+    f.right = false;
   } else if (lambda_R <= 0.0) {
-    F[0] = UR[0] * Vel_R[0];
-    F[1] = UR[1] * Vel_R[0];
-    F[2] = UR[2] * Vel_R[0];
-    F[3] = UR[3] * Vel_R[0];
-    F[4] = UR[1];
-    F[1] += p_R;
+    f.right = true;
   } else {
-    const double F_L[5] = {UL[0] * Vel_L[0], UL[1] * Vel_L[0], UL[2] * Vel_L[0], UL[3] * Vel_L[0], UL[1]};
-    const double F_R[5] = {UR[0] * Vel_R[0], UR[1] * Vel_R[0], UR[2] * Vel_R[0], UR[3] * Vel_R[0], UR[1]};
-    const double AL = lambda_L * UL[4] - F_L[4];
-    const double AR = lambda_R * UR[4] - F_R[4];
-    const double BL = lambda_L * UL[1] - F_L[1] - p_L;
-    const double BR = lambda_R * UR[1] - F_R[1] - p_R;
+    // F_L = {D vn, m vn, m1}: F_L.p = m1, F_L.v[0] = m1 vn
+    const double AL = lambda_L * L.E - L.m1;
+    const double AR = lambda_R * R.E - R.m1;
+    const double BL = lambda_L * L.m1 - L.m1 * L.vn - L.p;
+    const double BR = lambda_R * R.m1 - R.m1 * R.vn - R.p;
     const double a = AR * lambda_L - AL * lambda_R;
     const double b = AL + BL * lambda_R - AR - BR * lambda_L;
     const double c = BR - BL;
     const double scrh = -0.5 * (b + (b < 0.0 ? -1.0 : 1.0) * sqrt(b * b - 4.0 * a * c));
-    const double us = c / scrh;
-    const double ps = (AL * us - BL) / (1.0 - us * lambda_L);
-    // star state on the side of the contact (us >= 0: left)
-    const bool left = us >= 0.0;
-    const double lam = left ? lambda_L : lambda_R;
-    const double *Us = left ? UL : UR;
-    const double vn = left ? Vel_L[0] : Vel_R[0];
-    const double *Fs = left ? F_L : F_R;
-    const double pS = left ? p_L : p_R;
+    f.us = c / scrh;
+    f.ps = (AL * f.us - BL) / (1.0 - f.us * lambda_L);
+    f.star = true;
+    f.right = !(f.us >= 0.0);
+    f.lam = f.right ? lambda_R : lambda_L;
+  }
+  return f;
+}
+
+// Fout = area * flux in the global frame, from the selected side's conservative
+// state U (global frame) and its FaceSide values.
+__device__ __forceinline__ void face_flux(const Rot &R, const double *U, const FaceSide &s, const FaceStar &f,
+                                          double area, double *Fout) {
+  double Ur[5];
+  Ur[0] = U[0];
+  Ur[4] = U[4];
+  matvec(R, U + 1, Ur + 1);
+  const double vn = s.vn;
+  double F[5] = {Ur[0] * vn, Ur[1] * vn, Ur[2] * vn, Ur[3] * vn, Ur[1]};
+  if (f.star) {
+    const double lam = f.lam, us = f.us;
     double st[5];
     const double dif = 1.0 / (lam - us);
-    st[0] = Us[0] * (lam - vn) * dif;
-    st[1] = (lam * (Us[4] + ps) - Us[1]) * us * dif;
-    st[2] = Us[2] * (lam - vn) * dif;
-    st[3] = Us[3] * (lam - vn) * dif;
-    st[4] = Us[4] + (st[1] - Us[1]) / lam;
+    st[0] = Ur[0] * (lam - vn) * dif;
+    st[1] = (lam * (Ur[4] + f.ps) - Ur[1]) * us * dif;
+    st[2] = Ur[2] * (lam - vn) * dif;
+    st[3] = Ur[3] * (lam - vn) * dif;
+    st[4] = Ur[4] + (st[1] - Ur[1]) / lam;
 #pragma unroll
-    for (int i = 0; i < 5; i++) st[i] -= Us[i];
+    for (int i = 0; i < 5; i++) st[i] -= Ur[i];
 #pragma unroll
     for (int i = 0; i < 5; i++) st[i] *= lam;
 #pragma unroll
-    for (int i = 0; i < 5; i++) F[i] = Fs[i] + st[i];
-    F[1] += pS;
+    for (int i = 0; i < 5; i++) F[i] = F[i] + st[i];
   }
+  F[1] += s.p;
   Fout[0] = F[0] * area;
   Fout[4] = F[4] * area;
   double Fv[3];
@@ -346,7 +376,6 @@ __device__ __forceinline__ double hllc_flux(const Eos &e, const double *UL0, con
   Fout[1] = Fv[0] * area;
   Fout[2] = Fv[1] * area;
   Fout[3] = Fv[2] * area;
-  return smax(lambda_L, lambda_R);
 }
 
 }  // namespace rrhd

@@ -153,7 +153,7 @@ __device__ __forceinline__ void st_slot(T *p, const T (&v)[G]) {
 // node's own vertex, 1/6 otherwise), compared exactly as in the restatement.
 // The attenuations need only one exponential per in-face: E1_f = exp(-k r_f / 6)
 // and exp(-k 2 r_f / 3) = E1_f^4 (equal to a few ulp).
-template <class T, int GT>
+template <class T, class TI, int GT>
 __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
   // Levels after the first of a batch are launched with programmatic stream
   // serialisation: the next level may start while this one drains, and everything up to
@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
   const T *dy = rc + Rec<T>::DYN;
   const T k = dy[0], bk = dy[1];
   const SweepIO io = *a.io;
-  const T *Sv = (const T *)io.S;
+  const TI *Sv = (const TI *)io.S;
   // S element (group gg) of this cell and direction: base + gg * gs
   int64_t base, gs;
   if (io.layout) {
@@ -247,14 +247,15 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
     // separate per-face arrays (not one [4][GT] array), selected by comparisons, so that
     // no selection turns into an indexed local-memory access
     T rhs[GT], f0[GT], f1[GT], f2[GT], f3[GT];
+    TI sv[GT];
     if (io.layout) {
-      ld_groups<T, GT>(Sv + base, rhs);
+      ld_groups<TI, GT>(Sv + base, sv);
     } else {
 #pragma unroll
-      for (int q = 0; q < GT; q++) rhs[q] = Sv[base + q * gs];
+      for (int q = 0; q < GT; q++) sv[q] = Sv[base + q * gs];
     }
 #pragma unroll
-    for (int q = 0; q < GT; q++) rhs[q] = dy[2 + q] + bk * rhs[q];
+    for (int q = 0; q < GT; q++) rhs[q] = dy[2 + q] + bk * (T)sv[q];
     asm volatile("griddepcontrol.wait;" ::: "memory");
     auto in_face = [&](int j, T (&fj)[GT]) {
       if (cosf[j] < 0 && nbr[j] >= 0) {
@@ -304,7 +305,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
   } else {
     asm volatile("griddepcontrol.wait;" ::: "memory");
     for (int gg = 0; gg < a.G; gg++) {
-      const T rhs = dy[2 + gg] + bk * Sv[base + gg * gs];
+      const T rhs = dy[2 + gg] + bk * (T)Sv[base + gg * gs];
       T fvals[4];
 #pragma unroll
       for (int j = 0; j < 4; j++)
@@ -340,7 +341,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
 // parallel to it) hold the boundary value.  One thread per (cell, direction);
 // consecutive threads take consecutive directions of a cell, so face-value reads
 // and intensity writes are contiguous.
-template <class T, int GT>
+template <class T, class TI, int GT>
 __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= N * a.nbd) return;
@@ -356,7 +357,7 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
 #pragma unroll
   for (int j = 0; j < 4; j++) A[j] = __ldg(a.area + 4 * c + j);
   const SweepIO io = *a.io;
-  T *I = (T *)io.I;
+  TI *I = (TI *)io.I;
   int64_t base, gs;
   if (io.layout) {
     base = (c * a.M + d) * a.G;
@@ -401,17 +402,17 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
     slot(1, f1);
     slot(2, f2);
     slot(3, f3);
-    T out[GT];
+    TI out[GT];  // the cell values as stored (rounded to float in the mixed form)
 #pragma unroll
     for (int q = 0; q < GT; q++) {
       const T fv[4] = {f0[q], f1[q], f2[q], f3[q]};
-      out[q] = cell_value(fv);
+      out[q] = (TI)cell_value(fv);
     }
     if (io.layout) {
-      if constexpr (sizeof(T) == 8 && GT % 2 == 0) {
+      if constexpr (sizeof(TI) == 8 && GT % 2 == 0) {
 #pragma unroll
         for (int q = 0; q < GT / 2; q++) reinterpret_cast<double2 *>(I + base)[q] = make_double2(out[2 * q], out[2 * q + 1]);
-      } else if constexpr (sizeof(T) == 4 && GT == 4) {
+      } else if constexpr (sizeof(TI) == 4 && GT == 4) {
         *reinterpret_cast<float4 *>(I + base) = make_float4(out[0], out[1], out[2], out[3]);
       } else {
 #pragma unroll
@@ -421,7 +422,7 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
 #pragma unroll
       for (int q = 0; q < GT; q++) I[base + q * gs] = out[q];
     }
-    if constexpr (sizeof(T) == 4) {
+    if constexpr (sizeof(TI) == 4) {
       if (a.scale_out) {
         // one CTA is one cell (all its directions): the row scales of the FP16
         // scattering, 2^(14 - floor(log2 max_d |I|)) per group, as the scattering's own
@@ -450,7 +451,7 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
       T fv[4];
 #pragma unroll
       for (int j = 0; j < 4; j++) fv[j] = have[j] ? a.fv[((int64_t)fid[j] * a.DB + dl) * a.GS + gg] : a.bc;
-      I[base + gg * gs] = cell_value(fv);
+      I[base + gg * gs] = (TI)cell_value(fv);
     }
   }
 }
@@ -713,7 +714,7 @@ rrhd_status build_plan(rrhd_ctx *c) {
   return RRHD_OK;
 }
 
-template <class T, int GT>
+template <class T, class TI, int GT>
 cudaError_t launch_level(const SweepArgs<T> &a, unsigned nb, cudaStream_t st, bool pdl) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nb);
@@ -725,10 +726,10 @@ cudaError_t launch_level(const SweepArgs<T> &a, unsigned nb, cudaStream_t st, bo
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = pdl ? 1 : 0;
-  return cudaLaunchKernelEx(&cfg, k_sweep_level<T, GT>, a);
+  return cudaLaunchKernelEx(&cfg, k_sweep_level<T, TI, GT>, a);
 }
 
-template <class T>
+template <class T, class TI>
 rrhd_status capture_sweep(rrhd_ctx *c) {
   RadState &R = c->rad;
   cudaStream_t cs = nullptr;
@@ -765,19 +766,19 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
         const bool pdl = L > 0;  // the first level of a batch follows a full dependency
         cudaError_t le;
         switch (R.G) {
-          case 1: le = launch_level<T, 1>(a, nb, cs, pdl); break;
-          case 2: le = launch_level<T, 2>(a, nb, cs, pdl); break;
-          case 4: le = launch_level<T, 4>(a, nb, cs, pdl); break;
-          default: le = launch_level<T, 0>(a, nb, cs, pdl); break;
+          case 1: le = launch_level<T, TI, 1>(a, nb, cs, pdl); break;
+          case 2: le = launch_level<T, TI, 2>(a, nb, cs, pdl); break;
+          case 4: le = launch_level<T, TI, 4>(a, nb, cs, pdl); break;
+          default: le = launch_level<T, TI, 0>(a, nb, cs, pdl); break;
         }
         if (le != cudaSuccess && launch_err == cudaSuccess) launch_err = le;
       }
       const unsigned nr = grid_for(c->N * nbd, 256);
       switch (R.G) {
-        case 1: k_recalc<T, 1><<<nr, 256, 0, cs>>>(a, c->N); break;
-        case 2: k_recalc<T, 2><<<nr, 256, 0, cs>>>(a, c->N); break;
-        case 4: k_recalc<T, 4><<<nr, 256, 0, cs>>>(a, c->N); break;
-        default: k_recalc<T, 0><<<nr, 256, 0, cs>>>(a, c->N); break;
+        case 1: k_recalc<T, TI, 1><<<nr, 256, 0, cs>>>(a, c->N); break;
+        case 2: k_recalc<T, TI, 2><<<nr, 256, 0, cs>>>(a, c->N); break;
+        case 4: k_recalc<T, TI, 4><<<nr, 256, 0, cs>>>(a, c->N); break;
+        default: k_recalc<T, TI, 0><<<nr, 256, 0, cs>>>(a, c->N); break;
       }
       base += c->N * nbd;
     }
@@ -806,7 +807,9 @@ void rrhd_rad_release(rrhd_ctx *c) {
   R = RadState();
 }
 
-template <class T>
+// T: arithmetic and storage of the records and face values; TI: the intensity and
+// scattering-integral arrays the sweep reads and writes.
+template <class T, class TI>
 static rrhd_status rad_setup_t(rrhd_ctx *c) {
   RadState &R = c->rad;
   const int64_t N = c->N;
@@ -849,7 +852,7 @@ static rrhd_status rad_setup_t(rrhd_ctx *c) {
   R.GS = sizeof(T) == 8 ? ((R.G + 3) & ~3) : ((R.G + 7) & ~7);
   // the cell pass can hand the FP16 scattering its row scales when one CTA covers
   // every direction of a cell: one batch of 256 directions, float, G in {1, 2, 4}
-  if (sizeof(T) == 4 && R.nbatch == 1 && R.M == 256 && (R.G == 1 || R.G == 2 || R.G == 4) &&
+  if (sizeof(TI) == 4 && R.nbatch == 1 && R.M == 256 && (R.G == 1 || R.G == 2 || R.G == 4) &&
       cudaMalloc(&R.d_scale, sizeof(float) * (size_t)N * R.G) != cudaSuccess)
     return rrhd_fail(RRHD_ERR_OOM, "sweep allocation failed");
   auto up = [&](void **dst, const void *src, size_t bytes) -> rrhd_status {
@@ -865,13 +868,14 @@ static rrhd_status rad_setup_t(rrhd_ctx *c) {
       cudaMalloc(&R.d_fv, sizeof(T) * (size_t)c->F * R.DB * R.GS) != cudaSuccess)
     return rrhd_fail(RRHD_ERR_OOM, "sweep allocation failed");
   if ((s = build_plan<T>(c))) return s;
-  return capture_sweep<T>(c);
+  return capture_sweep<T, TI>(c);
 }
 
 extern "C" rrhd_status rrhd_rad_setup(rrhd_ctx *c, const rrhd_dirs *dirs, const rrhd_rad_opts *o) {
   RRHD_CHECK_ARG(c && dirs && o, "null argument");
   RRHD_CHECK_ARG(o->groups >= 1 && o->groups <= 64, "groups must be in [1, 64]");
-  RRHD_CHECK_ARG(o->precision == RRHD_RAD_FP64 || o->precision == RRHD_RAD_FP32, "bad precision");
+  RRHD_CHECK_ARG(o->precision == RRHD_RAD_FP64 || o->precision == RRHD_RAD_FP32 || o->precision == RRHD_RAD_MIXED,
+                 "bad precision");
   RRHD_CHECK_ARG(dirs->device == c->device, "direction set lives on another device");
   int DB = o->dirs_per_batch;
   RRHD_CHECK_ARG(DB == 0 || (DB > 0 && DB <= 256 && (DB & (DB - 1)) == 0), "dirs_per_batch: power of two <= 256");
@@ -894,7 +898,9 @@ extern "C" rrhd_status rrhd_rad_setup(rrhd_ctx *c, const rrhd_dirs *dirs, const 
   R.nbatch = (R.M + DB - 1) / DB;
   R.prec = o->precision;
   R.bc = o->boundary_value;
-  const rrhd_status s = R.prec == RRHD_RAD_FP64 ? rad_setup_t<double>(c) : rad_setup_t<float>(c);
+  const rrhd_status s = R.prec == RRHD_RAD_FP64   ? rad_setup_t<double, double>(c)
+                        : R.prec == RRHD_RAD_MIXED ? rad_setup_t<double, float>(c)
+                                                   : rad_setup_t<float, float>(c);
   if (s) {
     rrhd_rad_release(c);
     return s;
@@ -908,6 +914,33 @@ extern "C" rrhd_status rrhd_rad_plan_info(const rrhd_ctx *c, int64_t *levels, in
   if (!c->rad.ready) return rrhd_fail(RRHD_ERR_STATE, "rrhd_rad_setup has not run");
   if (levels) *levels = c->rad.levels;
   if (max_level_items) *max_level_items = c->rad.max_level;
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_rad_plan_levels(const rrhd_ctx *c, int32_t *levels) {
+  RRHD_CHECK_ARG(c && levels, "null argument");
+  const RadState &R = c->rad;
+  if (!R.ready) return rrhd_fail(RRHD_ERR_STATE, "rrhd_rad_setup has not run");
+  RRHD_CUDA(cudaSetDevice(c->device));
+  const int64_t N = c->N, total = N * (int64_t)R.M;
+  std::vector<uint32_t> plan((size_t)total);
+  RRHD_CUDA(cudaStreamSynchronize(c->stream));
+  RRHD_CUDA(cudaMemcpy(plan.data(), R.d_plan, sizeof(uint32_t) * total, cudaMemcpyDeviceToHost));
+  for (int64_t i = 0; i < total; i++) levels[i] = -1;
+  int64_t base = 0;
+  for (int b = 0; b < R.nbatch; b++) {
+    const int d0 = b * R.DB;
+    const int nbd = std::min(R.DB, R.M - d0);
+    const std::vector<int64_t> &off = R.lvl[b];
+    for (size_t L = 0; L + 1 < off.size(); L++)
+      for (int64_t k = off[L]; k < off[L + 1]; k++) {
+        const uint32_t it = plan[(size_t)(base + k)];
+        const int64_t cc = it >> R.shift;
+        const int d = d0 + (int)(it & (uint32_t)(R.DB - 1));
+        levels[(int64_t)d * N + c->h_perm[cc]] = (int32_t)L;
+      }
+    base += N * nbd;
+  }
   return RRHD_OK;
 }
 
@@ -931,7 +964,7 @@ extern "C" rrhd_status rrhd_sweep(rrhd_ctx *c, const void *alpha, const void *be
   if (!R.ready) return rrhd_fail(RRHD_ERR_STATE, "rrhd_rad_setup has not run");
   RRHD_CUDA(cudaSetDevice(c->device));
   const int64_t N = c->N;
-  if (R.prec == RRHD_RAD_FP64)
+  if (R.prec != RRHD_RAD_FP32)
     k_dyn_from_arrays<double><<<grid_for(N, 256), 256, 0, c->stream>>>(
         N, R.G, R.RW, c->d_perm, (const double *)alpha, (const double *)betta, (const double *)Q, (double *)R.d_rec);
   else
@@ -954,6 +987,25 @@ __global__ void k_cdg_to_rows(int64_t N, int M, int G, const int32_t *perm, cons
   dst[((int64_t)perm[c] * G + g) * M + d] = (double)src[i];
 }
 
+// Moments of the last scattering per row (cell * G + g), caller order, as
+// {E, F0, F1, F2, T00, T01, T02, T11, T12, T22}: from the FP64 arrays (E [rows],
+// F [rows][3], T [rows][9] column-major) or the FP32 [rows][16] columns.
+__global__ void k_mom_to_rows(int64_t N, int G, const int32_t *perm, const double *mE, const double *mF,
+                              const double *mT, const float *mom, double *dst) {
+  const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= N * G) return;
+  const int64_t c = r / G, g = r - c * G;
+  double *o = dst + ((int64_t)perm[c] * G + g) * 10;
+  if (mom) {
+    for (int k = 0; k < 10; k++) o[k] = (double)mom[16 * r + k];
+    return;
+  }
+  o[0] = mE[r];
+  for (int k = 0; k < 3; k++) o[1 + k] = mF[3 * r + k];
+  const int ij[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+  for (int k = 0; k < 6; k++) o[4 + k] = mT[9 * r + 3 * ij[k][1] + ij[k][0]];
+}
+
 template <class T>
 __global__ void k_rows_to_cdg(int64_t N, int M, int G, const int32_t *perm, const double *src, T *dst) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -965,6 +1017,7 @@ __global__ void k_rows_to_cdg(int64_t N, int M, int G, const int32_t *perm, cons
 }
 }  // namespace
 
+// T: the element type of the intensity and scattering-integral arrays.
 template <class T>
 static rrhd_status alloc_coupled(rrhd_ctx *c) {
   RadState &R = c->rad;
@@ -1002,7 +1055,8 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
   RRHD_CHECK_ARG(c->part_world == 1, "the coupled step runs on a whole mesh (no rrhd_hydro_set_part split)");
   RadState &R = c->rad;
   if (!R.ready) return rrhd_fail(RRHD_ERR_STATE, "rrhd_rad_setup has not run");
-  const bool fp64 = R.prec == RRHD_RAD_FP64;
+  const bool fp64 = R.prec == RRHD_RAD_FP64;         // intensity and scattering integral in double
+  const bool rec64 = R.prec != RRHD_RAD_FP32;        // sweep arithmetic and records in double
   const bool lowrank = o->scatter == RRHD_SCATTER_LOWRANK;
   RRHD_CHECK_ARG(lowrank || (fp64 ? o->scatter == RRHD_SCATTER_FP64
                                   : (o->scatter >= RRHD_TC_BF16X3 && o->scatter <= RRHD_TC_BF16)),
@@ -1034,7 +1088,7 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
   double *state = c->d_state[c->cur];
   const Emission em{o->emission.temp_coef, o->emission.sigma_sb, o->emission.pi, o->emission.rad_unit};
   // 2. opacities and emission from the new primitives
-  if (fp64)
+  if (rec64)
     k_dyn_from_state<double><<<grid_for(N, 256), 256, 0, st>>>(N, R.G, R.RW, state, o->absorption, o->scattering,
                                                                 em, (double *)R.d_rec);
   else
@@ -1115,14 +1169,18 @@ extern "C" rrhd_status rrhd_coupled_phase_ms(rrhd_ctx *c, float *ms) {
 extern "C" rrhd_status rrhd_rad_get(rrhd_ctx *c, int32_t what, double *out) {
   RRHD_CHECK_ARG(c && out, "null argument");
   RadState &R = c->rad;
-  RRHD_CHECK_ARG(what == RRHD_RAD_I || what == RRHD_RAD_S || what == RRHD_RAD_G4, "bad array id");
+  RRHD_CHECK_ARG(what == RRHD_RAD_I || what == RRHD_RAD_S || what == RRHD_RAD_G4 || what == RRHD_RAD_MOM,
+                 "bad array id");
   if (!R.ready || !R.d_I) return rrhd_fail(RRHD_ERR_STATE, "no coupled step has run");
   RRHD_CUDA(cudaSetDevice(c->device));
   const int64_t N = c->N;
-  const int64_t width = what == RRHD_RAD_G4 ? 4 : (int64_t)R.G * R.M;
+  const int64_t width = what == RRHD_RAD_G4 ? 4 : what == RRHD_RAD_MOM ? 10 * (int64_t)R.G : (int64_t)R.G * R.M;
   double *tmp = nullptr;
   RRHD_CUDA(cudaMalloc(&tmp, sizeof(double) * N * width));
-  if (what == RRHD_RAD_G4)
+  if (what == RRHD_RAD_MOM)
+    k_mom_to_rows<<<grid_for(N * R.G, 256), 256, 0, c->stream>>>(N, R.G, c->d_perm, R.d_mom ? nullptr : R.d_mE,
+                                                                  R.d_mF, R.d_mT, R.d_mom, tmp);
+  else if (what == RRHD_RAD_G4)
     k_rows_to_host_order<double><<<grid_for(N * width, 256), 256, 0, c->stream>>>(N, width, c->d_perm, R.d_G4, tmp);
   else if (R.prec == RRHD_RAD_FP64)
     k_cdg_to_rows<double><<<grid_for(N * width, 256), 256, 0, c->stream>>>(

@@ -198,14 +198,23 @@ class TransportSweep:
     """Device sweep plan for a hydro Grid's mesh and a DirectionGrid: the
     upwind order the reference reads from its offline graph/ and make_trace/
     outputs (sorted_graph, vec_x0), built on the GPU as levels.  precision:
-    "fp64" or "fp32" (storage and arithmetic of alpha, betta, Q, S, I)."""
+    "fp64" or "fp32" (storage and arithmetic of alpha, betta, Q, S, I), or "mixed"
+    (double arithmetic and face values, alpha, betta, Q double, S and I float)."""
 
     def __init__(self, grid, dg: DirectionGrid, groups: int = 1, precision: str = "fp64", dirs_per_batch: int = 0,
                  boundary_value: float = 0.0):
-        prec = {"fp64": L.RRHD_RAD_FP64, "fp32": L.RRHD_RAD_FP32}[precision]
+        prec = {"fp64": L.RRHD_RAD_FP64, "fp32": L.RRHD_RAD_FP32, "mixed": L.RRHD_RAD_MIXED}[precision]
         o = L.RadOpts(groups, prec, dirs_per_batch, boundary_value)
         L.check(L.lib.rrhd_rad_setup(grid.handle, dg.handle, C.byref(o)), "rrhd_rad_setup")
         self.grid, self.dg, self.groups, self.precision = grid, dg, groups, precision
+
+    def plan_levels(self):
+        """[M, N] (caller numbering): the level in which each (cell, direction) is swept,
+        the front index the reference's graph::RunGraphModule gives it."""
+        import numpy as np
+        out = np.zeros((self.dg.size, self.grid.size), np.int32)
+        L.check(L.lib.rrhd_rad_plan_levels(self.grid.handle, L.ptr(out)), "rrhd_rad_plan_levels")
+        return out
 
     def plan_info(self):
         lv, mx = C.c_int64(), C.c_int64()
@@ -216,13 +225,16 @@ class TransportSweep:
 def CalculateIllum(sw: TransportSweep, alpha, betta, Q, S, I=None):
     """One sweep of all directions and groups (the direction loop of
     solvers/illum/src/mpi/multi_gpu/illum_multi_gpu_face_calc.cpp:91-190) on the
-    grid's stream.  CUDA tensors in the sweep precision, caller cell numbering:
-    alpha, betta [N], Q [N, G], S [N*G, M]; returns I [N*G, M]."""
+    grid's stream.  CUDA tensors in the sweep precision (mixed: alpha, betta, Q
+    double, S and I float), caller cell numbering: alpha, betta [N], Q [N, G],
+    S [N*G, M]; returns I [N*G, M]."""
     import torch
     if I is None:
         I = torch.empty_like(S)
-    for t in (alpha, betta, Q, S, I):
-        assert t.is_contiguous() and t.dtype == (torch.float64 if sw.precision == "fp64" else torch.float32)
+    f64 = torch.float64 if sw.precision in ("fp64", "mixed") else torch.float32
+    io = torch.float64 if sw.precision == "fp64" else torch.float32
+    for t, dt in ((alpha, f64), (betta, f64), (Q, f64), (S, io), (I, io)):
+        assert t.is_contiguous() and t.dtype == dt
     L.check(L.lib.rrhd_sweep(sw.grid.handle, L.ptr(alpha), L.ptr(betta), L.ptr(Q), L.ptr(S), L.ptr(I)),
             "CalculateIllum")
     return I

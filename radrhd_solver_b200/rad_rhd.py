@@ -85,12 +85,14 @@ class RadRHDStep:
         L.check(L.lib.rrhd_coupled_phase_ms(self.grid.handle, ms), "rrhd_coupled_phase_ms")
         return dict(zip(("hydro", "sweep", "source_c2p", "scatter_moments"), list(ms)))
 
-    _KEYS = {"I": L.RRHD_RAD_I, "S": L.RRHD_RAD_S, "G4": L.RRHD_RAD_G4}
+    _KEYS = {"I": L.RRHD_RAD_I, "S": L.RRHD_RAD_S, "G4": L.RRHD_RAD_G4, "MOM": L.RRHD_RAD_MOM}
 
     def get(self, what: str):
-        """Host copy, caller numbering: "I" / "S" [N*G, M], "G4" [N, 4]."""
+        """Host copy, caller numbering: "I" / "S" [N*G, M], "G4" [N, 4], "MOM" [N*G, 10]
+        (E, F0..2, T00, T01, T02, T11, T12, T22 of the last scattering)."""
         n = self.grid.size
-        shape = (n, 4) if what == "G4" else (n * self.sweep.groups, self.sweep.dg.size)
+        shape = {"G4": (n, 4), "MOM": (n * self.sweep.groups, 10)}.get(what, (n * self.sweep.groups,
+                                                                              self.sweep.dg.size))
         out = np.zeros(shape)
         L.check(L.lib.rrhd_rad_get(self.grid.handle, self._KEYS[what], L.ptr(out)), "rrhd_rad_get")
         return out

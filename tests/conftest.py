@@ -7,6 +7,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
+# The reference source tree (read-only; present only where the oracle is built):
+# the same setting as oracle/Makefile's REF and __graft_entry__.REFERENCE.
+REFERENCE = os.environ.get("RRHD_REFERENCE", "/root/reference")
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")

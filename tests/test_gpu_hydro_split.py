@@ -5,8 +5,9 @@ The ranks are emulated in one process on one GPU: one context per rank, launched
 after another from the host (no kernel waits on another), with device-to-device copies
 standing in for the all-to-all between ranks and a max over the ranks' speeds written back
 through rrhd_hydro_max_speed_ptr.  Every cell a rank does not own starts from a poison
-state.  Bar: each rank's cells, the time steps and the max signal speed equal the
-whole-mesh step bit for bit over five device-time-stepped steps.
+state.  Bar: each rank's cells, the time steps and the max signal speed equal the oracle's
+(the reference's arithmetic on the CPU, oracle.port_hydro_step) and the whole-mesh step bit
+for bit over five device-time-stepped steps.
 
 The torch.distributed path (rhllc_mpi) runs with a one-rank NCCL group in a child
 process: it must equal the whole-mesh step too.
@@ -93,10 +94,17 @@ def test_split_step_bitexact_emulated(world):
         torch.cuda.synchronize()
     tau_w, speed_w = whole.step_info()
     Ww, Uw = whole.get_state()
+    # the oracle (the reference's arithmetic on the CPU) over the same device-time-stepped steps
+    Uo, Wo, speed_o = U0, W0, 1.0
+    for _ in range(STEPS):
+        tau_o = (CFL * H_MIN) / speed_o
+        Uo, Wo, _, _, speed_o = oracle.port_hydro_step(m, Uo, Wo, tau_o, 1, GAMMA_53)
+    assert tau_w == tau_o and speed_w == speed_o
     for k in ranks:
         tau, speed = k["g"].step_info()  # reads the max written through the aliased address
-        assert tau == tau_w and speed == speed_w
+        assert tau == tau_o and speed == speed_o
         W, U = k["g"].get_state()
+        assert np.array_equal(W[k["own"]], Wo[k["own"]]) and np.array_equal(U[k["own"]], Uo[k["own"]])
         assert np.array_equal(W[k["own"]], Ww[k["own"]]) and np.array_equal(U[k["own"]], Uw[k["own"]])
     owned = np.concatenate([k["own"] for k in ranks])
     assert np.array_equal(np.sort(owned), np.arange(N))

@@ -16,9 +16,10 @@ from radrhd_solver_b200.mesh import fibonacci_directions
 
 pytestmark = pytest.mark.gpu
 
-# max / rms relative error bounds per form (measured on B200: f16x3 7.0e-7 / 3.3e-7,
-# bf16x3 1.9e-6 / 3.8e-7, f16 1.0e-4 / 2.0e-5, bf16 8.1e-4 / 1.8e-4 at M=256)
-BOUND = {"f16x3": (1.2e-6, 5e-7), "bf16x3": (4e-6, 8e-7), "f16": (3e-4, 6e-5), "bf16": (2e-3, 5e-4)}
+# max / rms relative error bounds per form (measured on B200: f16x3 3.5e-7 / 1.6e-7,
+# bf16x3 1.9e-6 / 3.8e-7, f16 1.0e-4 / 2.0e-5, bf16 8.1e-4 / 1.8e-4 at M=256).  F16X3
+# is the form held to the 1e-6 relative bar on the scattering integral.
+BOUND = {"f16x3": (1e-6, 5e-7), "bf16x3": (4e-6, 8e-7), "f16": (3e-4, 6e-5), "bf16": (2e-3, 5e-4)}
 
 
 def _errors(S, Mom, So, Eo, Fo, To):

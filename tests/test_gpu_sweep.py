@@ -4,9 +4,9 @@ Bars: the FP64 sweep within 1e-12 relative of orc_sweep per cell, direction and
 group (every operation is the oracle's in the oracle's order; only exp comes
 from CUDA's libm instead of glibc); the FP32 sweep within 1e-5.  The plain
 coupled step (FP64 sweep, FP64 scattering, reference con2prim guess) within
-1e-12 of the oracle's composition of the same step; the chosen form (FP32 sweep,
-tensor-core scattering, learned con2prim guess) keeps the hydro state within
-1e-10 of the plain form.
+1e-12 of the oracle's composition of the same step, per cell; the chosen form
+(mixed-precision sweep, tensor-core scattering, learned con2prim guess) keeps the
+scattering integral within 1e-6 and the hydro state within 1e-10 of the plain form.
 """
 import ctypes as C
 
@@ -74,6 +74,52 @@ def test_sweep_fp32_and_boundary_value():
     err = np.max(np.abs(Ig - Io) / np.abs(Io))
     print(f"\nfp32 sweep: max rel err {err:.2e}")
     assert err <= 1e-5
+
+
+def test_sweep_mixed_matches_oracle():
+    """Mixed precision: double arithmetic and face values, S read and I written in
+    float.  Against the oracle fed the same (float-rounded) S, the intensity differs
+    by its one rounding to float (2^-24 relative) plus the FP64 sweep's 1e-12."""
+    m = kuhn_box(7, 6, 5, lo=(-1, -1, -1), hi=(1, 1, 1), seed=23)
+    d = fibonacci_directions(32)
+    G = 4
+    alpha, betta, Q, S = _inputs(m, d.size, G, 29)
+    S = S.astype(np.float32).astype(np.float64)
+    Io, missing = oracle.port_sweep(m, d.dirs, alpha, betta, Q, S)
+    assert missing == 0
+    grid = rhllc.Grid(m, gamma=GAMMA_43)
+    dg = illum.DirectionGrid(d)
+    sw = illum.TransportSweep(grid, dg, groups=G, precision="mixed")
+    t64 = [torch.tensor(a, dtype=torch.float64, device="cuda").contiguous() for a in (alpha, betta, Q)]
+    I = illum.CalculateIllum(sw, *t64, torch.tensor(S, dtype=torch.float32, device="cuda"))
+    grid.sync()
+    Ig = I.double().cpu().numpy()
+    err = np.max(np.abs(Ig - Io) / np.abs(Io))
+    print(f"\nmixed sweep: max rel err {err:.2e}")
+    assert err <= 2.0 ** -24 * (1 + 1e-6) + 1e-12
+    grid.close()
+
+
+@pytest.mark.parametrize("dirs_per_batch", [8, 32])
+def test_plan_levels_are_the_reference_fronts(dirs_per_batch):
+    """The device plan sweeps every (cell, direction) in the level that the reference's
+    graph::RunGraphModule (graph/src/graph_by_direction.cpp, compiled from its sources)
+    gives as the cell's front for that direction.  Within a level the order does not
+    change any value: each out-face value reads only upwind faces of earlier levels."""
+    from oracle import loader as OL
+    if OL.ref_trace() is None:
+        pytest.skip("reference trace build not present (make -C oracle ref)")
+    from test_oracle_trace import _neighbour_faces, _outward_normals
+    m = kuhn_box(6, 5, 4, lo=(-1, -1, -1), hi=(1, 1, 1), seed=33, with_vertices=True)
+    d = fibonacci_directions(32)
+    lv_ref, bad = OL.ref_graph_levels(_neighbour_faces(m), _outward_normals(m), d.dirs)
+    assert bad == 0
+    grid = rhllc.Grid(m, gamma=GAMMA_43)
+    dg = illum.DirectionGrid(d)
+    sw = illum.TransportSweep(grid, dg, groups=1, precision="fp64", dirs_per_batch=dirs_per_batch)
+    lv = sw.plan_levels()
+    grid.close()
+    assert np.array_equal(lv, lv_ref)
 
 
 def test_sweep_independent_of_cell_numbering():
@@ -146,7 +192,38 @@ def _oracle_coupled(m, U, W, tau, d, G, S, mom, a=1.0, b=0.5):
     S = oracle.port_scatter(I, d.dirs, d.areas, d.full_area)
     Er, Fr, Tr = oracle.port_moments(I, d.dirs, d.areas, d.full_area)
     mom = (_sum_groups(Er, G), _sum_groups(Fr, G), _sum_groups(Tr, G))
-    return U, W, I, S, mom, G4
+    rows = np.concatenate([Er[:, None], Fr, Tr[:, [0, 0, 0, 1, 1, 2], [0, 1, 2, 1, 2, 2]]], 1)
+    return U, W, I, S, mom, G4, rows
+
+
+def _state_err(Ug, Wg, Uo, Wo):
+    """Largest error of a hydro state, per cell and relative to that cell's own
+    scale: D, E, rho and p relative to themselves; the momentum S relative to the
+    cell's E (|S| < E); the velocity in units of c."""
+    E = np.abs(Uo[:, 4])[:, None]
+    eU = max(np.max(np.abs(Ug[:, [0, 4]] - Uo[:, [0, 4]]) / np.abs(Uo[:, [0, 4]])),
+             np.max(np.abs(Ug[:, 1:4] - Uo[:, 1:4]) / E))
+    eW = max(np.max(np.abs(Wg[:, [0, 4]] - Wo[:, [0, 4]]) / np.abs(Wo[:, [0, 4]])),
+             np.max(np.abs(Wg[:, 1:4] - Wo[:, 1:4])))
+    return eU, eW
+
+
+def _moment_err(mg, mo):
+    """Per row: E relative to itself, F and T relative to the row's E."""
+    E = np.abs(mo[:, :1])
+    return max(np.max(np.abs(mg[:, 0] - mo[:, 0]) / E[:, 0]), np.max(np.abs(mg[:, 1:] - mo[:, 1:]) / E))
+
+
+def _g4_scale(W, mom, G, em, a=1.0, b=0.5):
+    """Per-cell magnitude of the terms of the 4-force (rad_rhd::GetRadSource):
+    rho gamma (alpha + sigma)(E + |F|) + |q| gamma, q = -alpha rho B / k."""
+    rho, v = W[:, 0], W[:, 1:4]
+    gamma = 1.0 / np.sqrt(1.0 - np.sum(v * v, 1))
+    m = mom.reshape(-1, G, 10).sum(1)
+    T = em[0] * W[:, 4] / rho
+    B = T ** 4 * em[1] / em[2]
+    q = a * rho * rho * B / em[3]
+    return rho * gamma * (a + b) * rho * (np.abs(m[:, 0]) + np.linalg.norm(m[:, 1:4], axis=1)) + q * gamma
 
 
 def _coupled_grid(m, W, U, d, G, precision):
@@ -159,6 +236,10 @@ def _coupled_grid(m, W, U, d, G, precision):
 
 
 def test_coupled_plain_matches_oracle():
+    """Three coupled steps of the plain form against the oracle's composition, every
+    quantity per cell: I and S per (cell, group, direction) relative to themselves, the
+    moments per row, the 4-force per cell against the size of its terms, and the
+    hydro state per cell (_state_err), all within 1e-12."""
     m, W = jet(6)
     W, U = oracle.port_p2c(W, 1, GAMMA_43)
     d = fibonacci_directions(64)
@@ -169,21 +250,25 @@ def test_coupled_plain_matches_oracle():
     S = np.zeros((m.n_cells * G, d.size))
     mom = (np.zeros(m.n_cells), np.zeros((m.n_cells, 3)), np.zeros((m.n_cells, 3, 3)))
     Uo, Wo = U, W
+    rows = np.zeros((m.n_cells * G, 10))
     for k in range(3):
         hs, ss = step(tau, stats=True)
-        Uo, Wo, Io, S, mom, G4o = _oracle_coupled(m, Uo, Wo, tau, d, G, S, mom)
+        used = rows  # the 4-force of a step reads the moments of the step before
+        Uo, Wo, Io, S, mom, G4o, rows = _oracle_coupled(m, Uo, Wo, tau, d, G, S, mom)
         assert ss.n_failed == 0
     Wg, Ug = g.get_state()
-    Ig, Sg, G4g = step.get("I"), step.get("S"), step.get("G4")
+    Ig, Sg, G4g, Mg = step.get("I"), step.get("S"), step.get("G4"), step.get("MOM")
     assert np.abs(G4o).max() > 0
-    rel = lambda a, b: np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300))
-    print(f"\nI {rel(Ig, Io):.2e} S {rel(Sg, S):.2e} G4 {np.max(np.abs(G4g - G4o)) / np.abs(G4o).max():.2e} "
-          f"U {np.max(np.abs(Ug - Uo) / np.abs(Uo).max(0)):.2e}")
+    rel = lambda a, b: np.max(np.abs(a - b) / np.abs(b))
+    eU, eW = _state_err(Ug, Wg, Uo, Wo)
+    eG4 = np.max(np.abs(G4g - G4o) / _g4_scale(Wo, used, G, EM)[:, None])
+    print(f"\nper cell: I {rel(Ig, Io):.2e} S {rel(Sg, S):.2e} moments {_moment_err(Mg, rows):.2e} "
+          f"G4 {eG4:.2e} U {eU:.2e} W {eW:.2e}")
     assert rel(Ig, Io) <= 1e-12
     assert rel(Sg, S) <= 1e-12
-    assert np.max(np.abs(G4g - G4o)) <= 1e-12 * np.abs(G4o).max()
-    assert np.all(np.abs(Ug - Uo) <= 1e-12 * np.abs(Uo).max(0))
-    assert np.all(np.abs(Wg - Wo) <= 1e-12 * np.abs(Wo).max(0))
+    assert _moment_err(Mg, rows) <= 1e-12
+    assert eG4 <= 1e-12
+    assert eU <= 1e-12 and eW <= 1e-12
     g.close()
 
 
@@ -197,6 +282,14 @@ def _trained_guess():
 
 
 def test_coupled_chosen_form_tracks_plain():
+    """Three coupled steps of the chosen form (mixed-precision sweep, tensor-core F16X3
+    scattering, learned con2prim guess) against the plain FP64 form, per cell: the
+    scattering integral S per (cell, group, direction) within 1e-6 relative, the
+    moments per row within 1e-6 (F and T relative to E), the 4-force within 1e-6 of the
+    size of its terms, the hydro state within 1e-10 (_state_err), the intensity within
+    1e-6.  (With the all-float sweep the intensity error accumulates along each
+    characteristic, 3.5e-6 here, and S reaches 1.15e-6: that form is kept for speed
+    comparisons only.)"""
     m, W = jet(8)
     W, U = oracle.port_p2c(W, 1, GAMMA_43)
     d = fibonacci_directions(64)
@@ -205,27 +298,34 @@ def test_coupled_chosen_form_tracks_plain():
     net = _trained_guess()
     out = {}
     for form in ("plain", "chosen"):
-        g, dg, sw = _coupled_grid(m, W, U, d, G, "fp64" if form == "plain" else "fp32")
+        g, dg, sw = _coupled_grid(m, W, U, d, G, "fp64" if form == "plain" else "mixed")
         step = rad_rhd.RadRHDStep(sw, em=rad_rhd.emission(*EM_JET), scatter="fp64" if form == "plain" else "f16x3",
                                   guess=None if form == "plain" else net)
         stats = [step(tau, stats=True) for _ in range(3)]
         Wg, Ug = g.get_state()
-        out[form] = (Ug, Wg, step.get("I"), stats)
+        out[form] = (Ug, Wg, step.get("I"), step.get("S"), step.get("MOM"), step.get("G4"), stats)
         g.close()
-    Up, Wp, Ip, sp = out["plain"]
-    Uc, Wc, Ic, sc = out["chosen"]
+    Up, Wp, Ip, Sp, Mp, Gp, sp = out["plain"]
+    Uc, Wc, Ic, Sc, Mc, Gc, sc = out["chosen"]
     it_p = sum(s[1].newton_iters for s in sp)
     it_c = sum(s[1].newton_iters for s in sc)
-    du = np.max(np.abs(Uc - Up) / np.abs(Up).max(0))
-    dI = np.max(np.abs(Ic - Ip) / np.abs(Ip).max())
-    print(f"\nchosen vs plain: U {du:.2e}, I {dI:.2e}; source con2prim Newton iterations {it_c} vs {it_p}")
-    assert np.all(np.abs(Uc - Up) <= 1e-10 * np.abs(Up).max(0))
-    assert np.all(np.abs(Wc - Wp) <= 1e-10 * np.abs(Wp).max(0))
-    assert dI <= 1e-4
+    eU, eW = _state_err(Uc, Wc, Up, Wp)
+    eI = np.max(np.abs(Ic - Ip) / np.abs(Ip))
+    eS = np.max(np.abs(Sc - Sp) / np.abs(Sp))
+    eM = _moment_err(Mc, Mp)
+    eG4 = np.max(np.abs(Gc - Gp) / _g4_scale(Wp, Mp, G, EM_JET)[:, None])
+    print(f"\nchosen vs plain, per cell: S {eS:.2e} moments {eM:.2e} G4 {eG4:.2e} I {eI:.2e} U {eU:.2e} "
+          f"W {eW:.2e}; source con2prim Newton iterations {it_c} vs {it_p}")
+    assert eS <= 1e-6
+    assert eM <= 1e-6
+    assert eG4 <= 1e-6
+    assert eU <= 1e-10 and eW <= 1e-10
+    assert eI <= 1e-6
     assert all(s[1].n_failed == 0 for s in sc)
 
 
-def test_coupled_chosen_row_scales_from_cell_pass():
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_coupled_chosen_row_scales_from_cell_pass(precision):
     """With one batch of 256 directions the sweep's cell pass hands the FP16 scattering
     its row scales; the step is bit-identical to two batches of 128, where the
     scattering computes them itself."""
@@ -238,7 +338,7 @@ def test_coupled_chosen_row_scales_from_cell_pass():
         g.set_boundary(-3, rhllc.BC_FIXED, JET_INFLOW)
         g.set_state(W, U)
         dg = illum.DirectionGrid(d)
-        sw = illum.TransportSweep(g, dg, groups=4, precision="fp32", dirs_per_batch=db)
+        sw = illum.TransportSweep(g, dg, groups=4, precision=precision, dirs_per_batch=db)
         step = rad_rhd.RadRHDStep(sw, em=rad_rhd.emission(*EM_JET), scatter="f16x3")
         for _ in range(2):
             step(0.3 * m.h_min)

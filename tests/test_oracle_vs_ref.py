@@ -122,7 +122,9 @@ def test_scatter_reference_direction_file():
     """The reference's own 26-direction test sphere (full_area 9.99, not 4 pi):
     normalisation by the file's full_area."""
     import os
-    path = "/root/reference/tests/data/surface_26_dir.txt"
+
+    from conftest import REFERENCE
+    path = os.path.join(REFERENCE, "tests", "data", "surface_26_dir.txt")
     if not os.path.exists(path):
         pytest.skip("reference tree not present")
     need("illum")

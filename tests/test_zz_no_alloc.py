@@ -75,3 +75,38 @@ def test_noalloc_rejects_oversized_batch():
           torch.cuda.current_stream().cuda_stream)
     assert r == L.RRHD_ERR_LIMIT
     assert b"fixed maximum" in L.lib.rrhd_last_error()
+
+
+def test_noalloc_empty_batch_gives_zero_totals():
+    """n = 0 launches only the reduction, which writes a zero total into the first record."""
+    f = _noalloc()
+    d = torch.zeros(5, dtype=torch.float64, device="cuda")
+    for fn in (f, L.lib.rrhd_con2prim_batch_stats):
+        st = L.C2pStats()
+        st.n_ok = st.n_fallback = st.n_failed = st.newton_iters = st.max_iters = 7
+        L.check(fn(1, GAMMA_43, d.data_ptr(), d.data_ptr(), None, 0, 1, ctypes.byref(st),
+                   torch.cuda.current_stream().cuda_stream))
+        assert (st.n_ok, st.n_fallback, st.n_failed, st.newton_iters, st.max_iters) == (0, 0, 0, 0, 0)
+
+
+def test_noalloc_at_the_fixed_maximum():
+    """A batch of exactly the maximum uses the last per-CTA record of the array and the
+    total right after it; a cheap uniform state, compared with the regular entry point."""
+    f = _noalloc()
+    U1, W1 = _batch(2, 41)
+    s = torch.cuda.current_stream().cuda_stream
+    out = []
+    for fn in (L.lib.rrhd_con2prim_batch_stats, f):
+        Ud = torch.tensor(U1[:1], device="cuda").expand(MAX_STATES, 5).contiguous()
+        Wd = torch.zeros_like(Ud)
+        sd = torch.zeros(MAX_STATES, dtype=torch.uint8, device="cuda")
+        st = L.C2pStats()
+        L.check(fn(1, GAMMA_43, Ud.data_ptr(), Wd.data_ptr(), sd.data_ptr(), MAX_STATES, 1, ctypes.byref(st), s))
+        torch.cuda.synchronize()
+        out.append((Ud, Wd, sd, st))
+        del Ud, Wd, sd
+    (Ua, Wa, sa, ta), (Ub, Wb, sb, tb) = out
+    assert torch.equal(Ua, Ub) and torch.equal(Wa, Wb) and torch.equal(sa, sb)
+    for k in ("n_ok", "n_fallback", "n_failed", "newton_iters", "max_iters"):
+        assert getattr(ta, k) == getattr(tb, k), k
+    assert ta.n_ok + ta.n_fallback == MAX_STATES
