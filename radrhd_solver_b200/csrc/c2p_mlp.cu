@@ -224,51 +224,57 @@ __device__ __forceinline__ float mlp_warp(const float *xs, const float *sW1, con
     for (int q = 0; q < 2; q++)
 #pragma unroll
       for (int a = 0; a < 3; a++) f[q][a] = __shfl_sync(0xffffffffu, xs[a], 16 * mt + g + 8 * q);
-    float acc[8][4];
-#pragma unroll
-    for (int nt = 0; nt < 8; nt++)
-#pragma unroll
-      for (int e = 0; e < 4; e++) acc[nt][e] = 0.f;
-#pragma unroll
-    for (int ks = 0; ks < 4; ks++) {
-      const int k0 = 16 * ks + 2 * c;
-      const int kk[4] = {k0, k0 + 1, k0 + 8, k0 + 9};
-      float hv[2][4];
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const int k = kk[j];
-        const float w0 = sW1[3 * k], w1 = sW1[3 * k + 1], w2 = sW1[3 * k + 2], bb = sb1[k];
-#pragma unroll
-        for (int q = 0; q < 2; q++)
-          hv[q][j] = fmaxf(fmaf(w2, f[q][2], fmaf(w1, f[q][1], fmaf(w0, f[q][0], bb))), 0.f);
-      }
-      const uint32_t a0 = pack_bf16(hv[0][0], hv[0][1]);
-      const uint32_t a1 = pack_bf16(hv[1][0], hv[1][1]);
-      const uint32_t a2 = pack_bf16(hv[0][2], hv[0][3]);
-      const uint32_t a3 = pack_bf16(hv[1][2], hv[1][3]);
-#pragma unroll
-      for (int nt = 0; nt < 8; nt++) {
-        const uint2 b = *reinterpret_cast<const uint2 *>(sfrag + 2 * ((nt * 4 + ks) * 32 + lane));
-        asm volatile(
-            "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-            "{%0,%1,%2,%3};\n"
-            : "+f"(acc[nt][0]), "+f"(acc[nt][1]), "+f"(acc[nt][2]), "+f"(acc[nt][3])
-            : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b.x), "r"(b.y));
-      }
-    }
-    // output layer: partial sums of rows g and g + 8 over this lane's 16 columns
+    // the 64 output columns in two halves of 4 n-tiles (16 accumulators live, not 32);
+    // the first layer is recomputed for the second half
     float p0 = 0.f, p1 = 0.f;
+#pragma unroll 1
+    for (int half = 0; half < 2; half++) {
+      float acc[4][4];
 #pragma unroll
-    for (int nt = 0; nt < 8; nt++)
+      for (int nt = 0; nt < 4; nt++)
 #pragma unroll
-      for (int e = 0; e < 4; e++) {
-        const int n = 8 * nt + 2 * c + (e & 1);
-        const float v = fmaxf(acc[nt][e] + sb2[n], 0.f) * sW3[n];
-        if (e < 2)
-          p0 += v;
-        else
-          p1 += v;
+        for (int e = 0; e < 4; e++) acc[nt][e] = 0.f;
+#pragma unroll
+      for (int ks = 0; ks < 4; ks++) {
+        const int k0 = 16 * ks + 2 * c;
+        const int kk[4] = {k0, k0 + 1, k0 + 8, k0 + 9};
+        float hv[2][4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int k = kk[j];
+          const float w0 = sW1[3 * k], w1 = sW1[3 * k + 1], w2 = sW1[3 * k + 2], bb = sb1[k];
+#pragma unroll
+          for (int q = 0; q < 2; q++)
+            hv[q][j] = fmaxf(fmaf(w2, f[q][2], fmaf(w1, f[q][1], fmaf(w0, f[q][0], bb))), 0.f);
+        }
+        const uint32_t a0 = pack_bf16(hv[0][0], hv[0][1]);
+        const uint32_t a1 = pack_bf16(hv[1][0], hv[1][1]);
+        const uint32_t a2 = pack_bf16(hv[0][2], hv[0][3]);
+        const uint32_t a3 = pack_bf16(hv[1][2], hv[1][3]);
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+          const int nt = 4 * half + t;
+          const uint2 b = *reinterpret_cast<const uint2 *>(sfrag + 2 * ((nt * 4 + ks) * 32 + lane));
+          asm volatile(
+              "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+              "{%0,%1,%2,%3};\n"
+              : "+f"(acc[t][0]), "+f"(acc[t][1]), "+f"(acc[t][2]), "+f"(acc[t][3])
+              : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b.x), "r"(b.y));
+        }
       }
+      // output layer: partial sums of rows g and g + 8 over this lane's columns of the half
+#pragma unroll
+      for (int t = 0; t < 4; t++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int n = 8 * (4 * half + t) + 2 * c + (e & 1);
+          const float v = fmaxf(acc[t][e] + sb2[n], 0.f) * sW3[n];
+          if (e < 2)
+            p0 += v;
+          else
+            p1 += v;
+        }
+    }
     p0 += __shfl_xor_sync(0xffffffffu, p0, 1);
     p0 += __shfl_xor_sync(0xffffffffu, p0, 2);
     p1 += __shfl_xor_sync(0xffffffffu, p1, 1);
@@ -286,11 +292,15 @@ __device__ __forceinline__ float mlp_warp(const float *xs, const float *sW1, con
   return y + b3;
 }
 
+// PhysPressureFix out of line: the rare fallback does not add to the registers of the
+// kernel's main path.
+__device__ __noinline__ int pressure_fix_call(Eos eos, double *U, double *W) { return pressure_fix(eos, U, W); }
+
 // States i live at U + stride*i and W + stride*i (stride 5 for separate arrays,
 // 10 for a solver state [n][10] = U, W).  With G4 != NULL the radiation source
 // is added first, U.E += tau G0 and U.S += tau G[1..3] (radRHD_main.cpp:117-126).
 #ifndef RRHD_MLP_MIN_BLOCKS
-#define RRHD_MLP_MIN_BLOCKS 1  // CTAs per SM the register budget of k_c2p_mlp is sized for
+#define RRHD_MLP_MIN_BLOCKS 5  // CTAs per SM the register budget of k_c2p_mlp is sized for
 #endif
 __global__ void __launch_bounds__(IT, RRHD_MLP_MIN_BLOCKS) k_c2p_mlp(Eos eos, double *U, double *W, int64_t stride, const double *G4,
                                                 double tau_src, uint8_t *status, int64_t n, int fallback,
@@ -309,53 +319,61 @@ __global__ void __launch_bounds__(IT, RRHD_MLP_MIN_BLOCKS) k_c2p_mlp(Eos eos, do
   for (int q = threadIdx.x; q < 2 * 8 * 4 * 32; q += IT) sfrag[q] = frag[q];
   const float b3 = theta[OFF_B3];
   __syncthreads();
-  unsigned long long ok = 0, gfb = 0, fb = 0, failed = 0, iters = 0, mx = 0;
+  unsigned ok = 0, gfb = 0, fb = 0, failed = 0, iters = 0, mx = 0;  // per thread (u32: a thread sees few states)
   const int lane = threadIdx.x & 31;
   const int64_t nwarps_total = (int64_t)gridDim.x * (IT / 32);
   for (int64_t w = (int64_t)blockIdx.x * (IT / 32) + (threadIdx.x >> 5); w * 32 < n; w += nwarps_total) {
     const int64_t i = w * 32 + lane;
     const bool live = i < n;
-    double u[5] = {0, 0, 0, 0, 0}, wv[5] = {0, 0, 0, 0, 0};
-    if (live) {
-      for (int q = 0; q < 5; q++) {
-        u[q] = U[stride * i + q];
-        wv[q] = W[stride * i + q];
-      }
+    // the state (with the radiation source added) is read twice: for the features, and
+    // again after the network, so that it is not held in registers across the network
+    auto load_u = [&](double *u) {
+      for (int q = 0; q < 5; q++) u[q] = U[stride * i + q];
       if (G4) {
         u[4] += tau_src * G4[4 * i];
         u[1] += tau_src * G4[4 * i + 1];
         u[2] += tau_src * G4[4 * i + 2];
         u[3] += tau_src * G4[4 * i + 3];
       }
-    }
+    };
     float f[3] = {0.f, 0.f, 0.f};
     double tau = 0.0;
-    const bool feat = live && features(u, f, tau);
+    bool feat = false;
+    if (live) {
+      double u0[5];
+      load_u(u0);
+      feat = features(u0, f, tau);
+    }
     float xs[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) xs[a] = feat ? (f[a] - nm.mu[a]) / nm.sig[a] : 0.f;
     const float y = mlp_warp(xs, sW1, sb1, sb2, sW3, b3, sfrag);
+    double u[5] = {0, 0, 0, 0, 0}, wv[5] = {0, 0, 0, 0, 0};
+    if (live) {
+      load_u(u);
+      for (int q = 0; q < 5; q++) wv[q] = W[stride * i + q];
+    }
     if (!live) continue;
-    int it1 = 0, it2 = 0, code = 1;
     bool u_dirty = G4 != nullptr;
-    if (feat) {
-      const double p0 = tau * (double)__expf(y * nm.sig_t + nm.mu_t);
-      if (guess_out) guess_out[i] = p0;
-      code = c2p_from(eos, u, wv, p0, true, &it1, k_stall);
+    const double p0 = feat ? tau * (double)__expf(y * nm.sig_t + nm.mu_t) : 0.0;
+    if (feat && guess_out) guess_out[i] = p0;
+    // attempt 0: Newton from the learned guess for at most k_stall iterations; attempt 1
+    // (a stalled or unusable guess): the reference solve from its own guess
+    int code = 1, itn = 0;
+    if (!feat) gfb++;
+    for (int attempt = feat ? 0 : 1; attempt < 2; attempt++) {
+      int it = 0;
+      code = c2p_from(eos, u, wv, p0, attempt == 0, &it, attempt == 0 ? k_stall : RRHD_MAX_ITER);
+      itn += it;
+      if (code == 0) break;
+      if (attempt == 0) gfb++;
     }
-    if (code) {  // stalled or unusable guess: the reference solve from its own guess
-      gfb++;
-      code = c2p_from(eos, u, wv, 0.0, false, &it2);
-      if (code == 0) ok++;
-    } else {
-      ok++;
-    }
-    const unsigned long long itn = (unsigned long long)(it1 + it2);
-    iters += itn;
-    mx = itn > mx ? itn : mx;
+    if (code == 0) ok++;
+    iters += (unsigned)itn;
+    mx = (unsigned)itn > mx ? (unsigned)itn : mx;
     if (code) {
       if (fallback) {
-        const int fix = pressure_fix(eos, u, wv);
+        const int fix = pressure_fix_call(eos, u, wv);
         code = code | 0x10 | (fix ? 0x20 : 0);
         fb++;
         failed += fix ? 1 : 0;
@@ -369,24 +387,25 @@ __global__ void __launch_bounds__(IT, RRHD_MLP_MIN_BLOCKS) k_c2p_mlp(Eos eos, do
     for (int q = 0; q < 5; q++) W[stride * i + q] = wv[q];
     if (status) status[i] = (uint8_t)code;
   }
+  unsigned long long okl = ok, gfbl = gfb, fbl = fb, failedl = failed, itl = iters, mxl = mx;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    ok += __shfl_xor_sync(0xffffffffu, ok, o);
-    gfb += __shfl_xor_sync(0xffffffffu, gfb, o);
-    fb += __shfl_xor_sync(0xffffffffu, fb, o);
-    failed += __shfl_xor_sync(0xffffffffu, failed, o);
-    iters += __shfl_xor_sync(0xffffffffu, iters, o);
-    const unsigned long long m2 = __shfl_xor_sync(0xffffffffu, mx, o);
-    mx = m2 > mx ? m2 : mx;
+    okl += __shfl_xor_sync(0xffffffffu, okl, o);
+    gfbl += __shfl_xor_sync(0xffffffffu, gfbl, o);
+    fbl += __shfl_xor_sync(0xffffffffu, fbl, o);
+    failedl += __shfl_xor_sync(0xffffffffu, failedl, o);
+    itl += __shfl_xor_sync(0xffffffffu, itl, o);
+    const unsigned long long m2 = __shfl_xor_sync(0xffffffffu, mxl, o);
+    mxl = m2 > mxl ? m2 : mxl;
   }
   const int wid = threadIdx.x >> 5;
   if (lane == 0) {
-    red[0][wid] = ok;
-    red[1][wid] = gfb;
-    red[2][wid] = fb;
-    red[3][wid] = failed;
-    red[4][wid] = iters;
-    red[5][wid] = mx;
+    red[0][wid] = okl;
+    red[1][wid] = gfbl;
+    red[2][wid] = fbl;
+    red[3][wid] = failedl;
+    red[4][wid] = itl;
+    red[5][wid] = mxl;
   }
   __syncthreads();
   if (threadIdx.x == 0) {

@@ -287,7 +287,9 @@ struct FaceSide {
   double p;           // W.p
 };
 
-__device__ __forceinline__ FaceSide face_side(const Eos &e, const Rot &R, const double *U, const double *W) {
+// cs2 = sound_speed2(e, W[0], W[4]): a function of the cell's state alone, so the step
+// computes it once per staged cell rather than once per face and side.
+__device__ __forceinline__ FaceSide face_side(const Rot &R, const double *U, const double *W, double cs2) {
   double vel[3];
   matvec(R, W + 1, vel);
   FaceSide s;
@@ -296,7 +298,6 @@ __device__ __forceinline__ FaceSide face_side(const Eos &e, const Rot &R, const 
   s.vn = vel[0];
   s.p = W[4];
   const double VV = dot3(vel[0], vel[1], vel[2], vel[0], vel[1], vel[2]);
-  const double cs2 = sound_speed2(e, W[0], W[4]);
   signal_speed(cs2, vel[0], VV, s.cmin, s.cmax);
   return s;
 }

@@ -43,19 +43,23 @@ namespace {
 constexpr int kSweepThreads = 128;
 
 // Per-cell record (RW words): 0-11 outward normals n_j, 12-15 heights H_j, then the
-// face-value slots and the neighbours as int32 (4 + 4: 4 doubles or 8 floats), then the
-// source record {k, betta/k, alpha Q_g/k} of the step.  RW makes a record a whole number
-// of 128-byte lines (G = 4: 256 B in double, 128 B in float), so one item touches one or
-// two lines for everything it needs of its cell.
+// face-value slots as int32 (4: 2 doubles or 4 floats; bit 31 set where the face has no
+// neighbour), then the source record {k, betta/k, alpha Q_g/k} of the step, and in the
+// last 16 bytes the neighbours (int32, -1 on the boundary), which only the plan reads.
+// RW makes a record a whole number of 128-byte lines (G = 4: 256 B in double, 128 B in
+// float); what one level item reads of its cell is 6 sectors (double) or 4 (float).
 template <class T>
 struct Rec {
-  static constexpr int IDS = 16;                       // word offset of the ids
-  static constexpr int DYN = sizeof(T) == 8 ? 20 : 24;  // word offset of the source record
-  static constexpr int LINE = 128 / (int)sizeof(T);      // words per 128-byte line
+  static constexpr int IDS = 16;                       // word offset of the face-value slots
+  static constexpr int DYN = sizeof(T) == 8 ? 18 : 20;  // word offset of the source record
+  static constexpr int NBRW = 16 / (int)sizeof(T);      // words of the neighbours, at the record's end
+  static constexpr int LINE = 128 / (int)sizeof(T);     // words per 128-byte line
 };
+constexpr int32_t kNoNeighbour = INT32_MIN;  // bit 31 of a face-value slot id
 
+// normals, heights and face-value slot ids (negative: a face without a neighbour)
 template <class T>
-__device__ __forceinline__ void load_rec(const T *r, T *g, int *fid, int *nbr) {
+__device__ __forceinline__ void load_rec(const T *r, T *g, int *fid) {
 #pragma unroll
   for (int q = 0; q < 16; q += 16 / (int)sizeof(T)) {
     if constexpr (sizeof(T) == 8) {
@@ -70,19 +74,18 @@ __device__ __forceinline__ void load_rec(const T *r, T *g, int *fid, int *nbr) {
       g[q + 3] = v.w;
     }
   }
-  const int4 *r4 = reinterpret_cast<const int4 *>(r + Rec<T>::IDS);
-  const int4 f = __ldg(r4), n = __ldg(r4 + 1);
+  const int4 f = __ldg(reinterpret_cast<const int4 *>(r + Rec<T>::IDS));
   fid[0] = f.x, fid[1] = f.y, fid[2] = f.z, fid[3] = f.w;
-  nbr[0] = n.x, nbr[1] = n.y, nbr[2] = n.z, nbr[3] = n.w;
 }
-// normals and neighbours only (the plan kernels)
+// normals and neighbours only (the plan kernels); RW: record words
 template <class T>
-__device__ __forceinline__ void load_normals(const T *r, T *g, int *nbr) {
+__device__ __forceinline__ void load_normals(const T *r, int RW, T *g, int *nbr) {
 #pragma unroll
   for (int q = 0; q < 12; q++) g[q] = __ldg(r + q);
-  const int4 n = __ldg(reinterpret_cast<const int4 *>(r + Rec<T>::IDS) + 1);
+  const int4 n = __ldg(reinterpret_cast<const int4 *>(r + RW - Rec<T>::NBRW));
   nbr[0] = n.x, nbr[1] = n.y, nbr[2] = n.z, nbr[3] = n.w;
 }
+__device__ __forceinline__ int64_t slot_of(int fid) { return (int64_t)(fid & 0x7fffffff); }
 
 template <class T>
 struct SweepArgs {
@@ -168,9 +171,9 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
   const int dl = (int)(it & (uint32_t)(a.DB - 1));
   const int d = a.d0 + dl;
   T g[16];
-  int fid[4], nbr[4];
+  int fid[4];
   const T *rc = a.rec + (int64_t)a.RW * c;
-  load_rec<T>(rc, g, fid, nbr);
+  load_rec<T>(rc, g, fid);
   const T *dy = rc + Rec<T>::DYN;
   const T k = dy[0], bk = dy[1];
   const SweepIO io = *a.io;
@@ -258,7 +261,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
     for (int q = 0; q < GT; q++) rhs[q] = dy[2 + q] + bk * (T)sv[q];
     asm volatile("griddepcontrol.wait;" ::: "memory");
     auto in_face = [&](int j, T (&fj)[GT]) {
-      if (cosf[j] < 0 && nbr[j] >= 0) {
+      if (cosf[j] < 0 && fid[j] >= 0) {
         ld_groups<T, GT>(a.fv + ((int64_t)fid[j] * a.DB + dl) * a.GS, fj);
       } else {
 #pragma unroll
@@ -271,7 +274,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
     in_face(3, f3);
     const T E1_0 = E1[0], E1_1 = E1[1], E1_2 = E1[2], E1_3 = E1[3];
     const T E4_0 = E4[0], E4_1 = E4[1], E4_2 = E4[2], E4_3 = E4[3];
-    const int fid0 = fid[0], fid1 = fid[1], fid2 = fid[2], fid3 = fid[3];
+    const int64_t fid0 = slot_of(fid[0]), fid1 = slot_of(fid[1]), fid2 = slot_of(fid[2]), fid3 = slot_of(fid[3]);
     // the (at most three) out-faces, one slot after another
     for (int o = 0; o < nout; o++) {
       const int j = (jo >> (2 * o)) & 3;
@@ -299,8 +302,8 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
         Icur += (e[2] * (I0[2] - rhs[q]) + rhs[q]);
         out[q] = Icur * (T)0.3333333333333333;
       }
-      const int fj = j == 0 ? fid0 : j == 1 ? fid1 : j == 2 ? fid2 : fid3;
-      st_slot<T, GT>(a.fv + ((int64_t)fj * a.DB + dl) * a.GS, out);
+      const int64_t fj = j == 0 ? fid0 : j == 1 ? fid1 : j == 2 ? fid2 : fid3;
+      st_slot<T, GT>(a.fv + (fj * a.DB + dl) * a.GS, out);
     }
   } else {
     asm volatile("griddepcontrol.wait;" ::: "memory");
@@ -309,7 +312,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
       T fvals[4];
 #pragma unroll
       for (int j = 0; j < 4; j++)
-        fvals[j] = (cosf[j] < 0 && nbr[j] >= 0) ? a.fv[((int64_t)fid[j] * a.DB + dl) * a.GS + gg] : a.bc;
+        fvals[j] = (cosf[j] < 0 && fid[j] >= 0) ? a.fv[((int64_t)fid[j] * a.DB + dl) * a.GS + gg] : a.bc;
       for (int o = 0; o < nout; o++) {
         const int j = (jo >> (2 * o)) & 3;
         T I0[3], e[3];
@@ -329,7 +332,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
         T Icur = e[0] * (I0[0] - rhs) + rhs;
         Icur += (e[1] * (I0[1] - rhs) + rhs);
         Icur += (e[2] * (I0[2] - rhs) + rhs);
-        a.fv[((int64_t)fid[j] * a.DB + dl) * a.GS + gg] = Icur * (T)0.3333333333333333;
+        a.fv[(slot_of(fid[j]) * a.DB + dl) * a.GS + gg] = Icur * (T)0.3333333333333333;
       }
     }
   }
@@ -349,8 +352,8 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
   const int dl = (int)(t - c * a.nbd);
   const int d = a.d0 + dl;
   T g[16];
-  int fid[4], nbr[4];
-  load_rec<T>(a.rec + (int64_t)a.RW * c, g, fid, nbr);
+  int fid[4];
+  load_rec<T>(a.rec + (int64_t)a.RW * c, g, fid);
   T cosf[4];
   face_cos(g, a.w[3 * d], a.w[3 * d + 1], a.w[3 * d + 2], cosf);
   T A[4];
@@ -369,7 +372,7 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
   const bool last = c == a.last;
   bool have[4];
 #pragma unroll
-  for (int j = 0; j < 4; j++) have[j] = cosf[j] > 0 || (cosf[j] < 0 && nbr[j] >= 0);
+  for (int j = 0; j < 4; j++) have[j] = cosf[j] > 0 || (cosf[j] < 0 && fid[j] >= 0);
   auto cell_value = [&](const T *fv) {
     T curI = 0;
     if (!last) {
@@ -392,7 +395,7 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
     T f0[GT], f1[GT], f2[GT], f3[GT];
     auto slot = [&](int j, T (&fj)[GT]) {
       if (have[j]) {
-        ld_groups<T, GT>(a.fv + ((int64_t)fid[j] * a.DB + dl) * a.GS, fj);
+        ld_groups<T, GT>(a.fv + (slot_of(fid[j]) * a.DB + dl) * a.GS, fj);
       } else {
 #pragma unroll
         for (int q = 0; q < GT; q++) fj[q] = a.bc;
@@ -450,7 +453,7 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
     for (int gg = 0; gg < a.G; gg++) {
       T fv[4];
 #pragma unroll
-      for (int j = 0; j < 4; j++) fv[j] = have[j] ? a.fv[((int64_t)fid[j] * a.DB + dl) * a.GS + gg] : a.bc;
+      for (int j = 0; j < 4; j++) fv[j] = have[j] ? a.fv[(slot_of(fid[j]) * a.DB + dl) * a.GS + gg] : a.bc;
       I[base + gg * gs] = (TI)cell_value(fv);
     }
   }
@@ -467,7 +470,7 @@ __global__ void k_plan_init(int64_t N, int nbd, int shift, int d0, const T *w, c
   const int d = d0 + dl;
   T g[12];
   int nbr[4];
-  load_normals<T>(rec + (int64_t)RW * c, g, nbr);
+  load_normals<T>(rec + (int64_t)RW * c, RW, g, nbr);
   T cosf[4];
   face_cos(g, w[3 * d], w[3 * d + 1], w[3 * d + 2], cosf);
   uint32_t cnt = 0;
@@ -488,7 +491,7 @@ __global__ void k_plan_expand(const uint32_t *cur, int64_t n, int nbd, int shift
   const int d = d0 + dl;
   T g[12];
   int nbr[4];
-  load_normals<T>(rec + (int64_t)RW * c, g, nbr);
+  load_normals<T>(rec + (int64_t)RW * c, RW, g, nbr);
   T cosf[4];
   face_cos(g, w[3 * d], w[3 * d + 1], w[3 * d + 2], cosf);
 #pragma unroll
@@ -813,7 +816,7 @@ template <class T, class TI>
 static rrhd_status rad_setup_t(rrhd_ctx *c) {
   RadState &R = c->rad;
   const int64_t N = c->N;
-  const int W = ((Rec<T>::DYN + 2 + R.G + Rec<T>::LINE - 1) / Rec<T>::LINE) * Rec<T>::LINE;
+  const int W = ((Rec<T>::DYN + 2 + R.G + Rec<T>::NBRW + Rec<T>::LINE - 1) / Rec<T>::LINE) * Rec<T>::LINE;
   R.RW = W;
   std::vector<T> rec((size_t)W * N, (T)0), area(4 * (size_t)N), w(3 * R.M);
   std::vector<int32_t> iperm(N);
@@ -842,10 +845,11 @@ static rrhd_status rad_setup_t(rrhd_ctx *c) {
       area[4 * cn + j] = (T)c->h_face_area[fc];
       const int32_t l = c->h_face_l[fc], rr = c->h_face_r[fc];
       const int32_t o = (l == p) ? rr : l;
-      ids[j] = fslot[fc];
+      ids[j] = o < 0 ? (fslot[fc] | kNoNeighbour) : fslot[fc];
       ids[4 + j] = o < 0 ? -1 : iperm[o];
     }
-    std::memcpy(r + Rec<T>::IDS, ids, sizeof ids);
+    std::memcpy(r + Rec<T>::IDS, ids, 4 * sizeof(int32_t));
+    std::memcpy(r + W - Rec<T>::NBRW, ids + 4, 4 * sizeof(int32_t));
   }
   for (int q = 0; q < 3 * R.M; q++) w[q] = (T)R.dirs->h_w[q];
   R.last_cell = iperm[N - 1];
