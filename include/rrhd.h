@@ -472,11 +472,15 @@ rrhd_status rrhd_rad_source(const rrhd_emission *em, const double *W, const doub
  * all launches of a sweep are one CUDA graph. */
 #define RRHD_RAD_FP64 0  /* sweep arithmetic and storage in double */
 #define RRHD_RAD_FP32 1  /* in float (input of the tensor-core scattering) */
-#define RRHD_RAD_MIXED 2 /* arithmetic, face values and opacities in double; the scattering
-                            integral S read and the intensity I written in float (the
-                            tensor-core scattering's input and output): the intensity is
-                            the double sweep's rounded once, where the float sweep's
-                            rounding accumulates along each characteristic */
+#define RRHD_RAD_MIXED 2 /* geometry, opacities and sources in float (the float form's
+                            records); the face values and the transport update
+                            e^{-k s} (I_in - rhs) + rhs in double; the scattering integral
+                            S read and the intensity I written in float (the tensor-core
+                            scattering's input and output).  Storing the face values in
+                            float is what lets the float form's rounding accumulate along
+                            each characteristic; the float geometry and sources only
+                            perturb each cell's attenuation and source term, errors that do
+                            not add up along a characteristic */
 typedef struct {
   int32_t groups;         /* frequency groups G >= 1 (grey copies, rows cell * G + g)           */
   int32_t precision;      /* RRHD_RAD_FP64, RRHD_RAD_FP32 or RRHD_RAD_MIXED                     */
@@ -497,8 +501,8 @@ rrhd_status rrhd_rad_plan_info(const rrhd_ctx *ctx, int64_t *levels, int64_t *ma
  * RunGraphModule puts c in (graph/src/graph_by_direction.cpp).  Synchronises. */
 rrhd_status rrhd_rad_plan_levels(const rrhd_ctx *ctx, int32_t *levels);
 /* One sweep of all directions and groups on ctx's stream.  Device pointers of the
- * setup's precision (double or float; RRHD_RAD_MIXED: alpha, betta, Q double, S and
- * I float), caller cell numbering: alpha, betta [N] absorption and scattering
+ * setup's precision (double for RRHD_RAD_FP64, float otherwise), caller cell
+ * numbering: alpha, betta [N] absorption and scattering
  * coefficients, Q [N][G] emission B / kRadiation per group, S [N*G][M] scattering
  * integral in, I [N*G][M] intensity out. */
 rrhd_status rrhd_sweep(rrhd_ctx *ctx, const void *alpha, const void *betta, const void *Q, const void *S, void *I);

@@ -220,7 +220,8 @@ __global__ void __launch_bounds__(kStepThreads, RRHD_STEP_MIN_BLOCKS) k_hydro_st
   const int e0 = P.off[b], e1 = P.off[b + 1];                 // this CTA's face records
   const int x0 = P.xoff[b], x1 = P.xoff[b + 1];               // the cross faces its cells touch
   const int ni = e1 - e0;                                     // even; cross fluxes go after the records
-  CellRec *scell = reinterpret_cast<CellRec *>(sface + 5 * (ni + x1 - x0));  // [cpb]
+  // the cell records start on a 16-byte boundary: after an even number of 40-byte slots
+  CellRec *scell = reinterpret_cast<CellRec *>(sface + 5 * ((ni + x1 - x0 + 1) & ~1));  // [cpb]
   double *scs2 = reinterpret_cast<double *>(scell + P.cpb);                  // [cpb] sound speeds^2
   __shared__ double s_red[kStepThreads / 32];
   __shared__ unsigned long long s_cnt[2];
@@ -698,7 +699,7 @@ extern "C" rrhd_status rrhd_create(const rrhd_mesh_desc *m, const rrhd_opts *opt
       ni++;
     }
     for (int32_t f : ex_f) xids.push_back(xidx[f]);
-    const int ne = ni + (int)ex_f.size();
+    const int ne = (ni + (int)ex_f.size() + 1) & ~1;  // slots, rounded to keep the cell records 16-byte aligned
     if (ne > 32767) return fail(rrhd_fail(RRHD_ERR_LIMIT, "CTA face list too long"));
     for (int64_t cn = c0; cn < c1; cn++) {
       const int32_t co = perm[cn];

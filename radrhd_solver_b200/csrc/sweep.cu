@@ -87,7 +87,9 @@ __device__ __forceinline__ void load_normals(const T *r, int RW, T *g, int *nbr)
 }
 __device__ __forceinline__ int64_t slot_of(int fid) { return (int64_t)(fid & 0x7fffffff); }
 
-template <class T>
+// T: geometry and source records (directions, per-cell records, face areas); TV: face
+// values and the transport arithmetic.
+template <class T, class TV>
 struct SweepArgs {
   const SweepIO *io;
   const uint32_t *items;
@@ -96,9 +98,9 @@ struct SweepArgs {
   const T *w;     // [M][3]
   const T *rec;   // [N][RW]
   const T *area;  // [N][4] face areas (cell values)
-  T *fv;         // [F][DB][GS] face values (GS >= G, full 32-byte sectors)
+  TV *fv;         // [F][DB][GS] face values (GS >= G, full 32-byte sectors)
   float *scale_out;  // cell pass: per-(cell, group) power-of-two scales for the FP16 scattering, or NULL
-  T bc;
+  TV bc;
   int64_t last;
 };
 
@@ -156,8 +158,8 @@ __device__ __forceinline__ void st_slot(T *p, const T (&v)[G]) {
 // node's own vertex, 1/6 otherwise), compared exactly as in the restatement.
 // The attenuations need only one exponential per in-face: E1_f = exp(-k r_f / 6)
 // and exp(-k 2 r_f / 3) = E1_f^4 (equal to a few ulp).
-template <class T, class TI, int GT>
-__global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
+template <class T, class TV, class TI, int GT>
+__global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T, TV> a) {
   // Levels after the first of a batch are launched with programmatic stream
   // serialisation: the next level may start while this one drains, and everything up to
   // the first face-value read (item, cell record, source record, S, geometry,
@@ -190,17 +192,18 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
   const T wx = a.w[3 * d], wy = a.w[3 * d + 1], wz = a.w[3 * d + 2];
   T cosf[4];
   face_cos(g, wx, wy, wz, cosf);
-  T t1[4], t4[4], E1[4], E4[4];
+  T t1[4], t4[4];
+  TV E1[4], E4[4];
 #pragma unroll
   for (int f = 0; f < 4; f++) {
     t1[f] = t4[f] = (T)0;
-    E1[f] = E4[f] = (T)1;
+    E1[f] = E4[f] = (TV)1;
     if (cosf[f] < 0) {
       const T r = dv(g[12 + f], -cosf[f]);
       t1[f] = (T)(1.0 / 6.0) * r;
       t4[f] = (T)(2.0 / 3.0) * r;
-      E1[f] = ex(-k * t1[f]);
-      const T e2 = E1[f] * E1[f];
+      E1[f] = ex((TV)(-k * t1[f]));
+      const TV e2 = E1[f] * E1[f];
       E4[f] = e2 * e2;
     }
   }
@@ -249,7 +252,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
   if constexpr (GT > 0) {
     // separate per-face arrays (not one [4][GT] array), selected by comparisons, so that
     // no selection turns into an indexed local-memory access
-    T rhs[GT], f0[GT], f1[GT], f2[GT], f3[GT];
+    TV rhs[GT], f0[GT], f1[GT], f2[GT], f3[GT];
     TI sv[GT];
     if (io.layout) {
       ld_groups<TI, GT>(Sv + base, sv);
@@ -258,11 +261,11 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
       for (int q = 0; q < GT; q++) sv[q] = Sv[base + q * gs];
     }
 #pragma unroll
-    for (int q = 0; q < GT; q++) rhs[q] = dy[2 + q] + bk * (T)sv[q];
+    for (int q = 0; q < GT; q++) rhs[q] = (TV)dy[2 + q] + (TV)bk * (TV)sv[q];
     asm volatile("griddepcontrol.wait;" ::: "memory");
-    auto in_face = [&](int j, T (&fj)[GT]) {
+    auto in_face = [&](int j, TV (&fj)[GT]) {
       if (cosf[j] < 0 && fid[j] >= 0) {
-        ld_groups<T, GT>(a.fv + ((int64_t)fid[j] * a.DB + dl) * a.GS, fj);
+        ld_groups<TV, GT>(a.fv + ((int64_t)fid[j] * a.DB + dl) * a.GS, fj);
       } else {
 #pragma unroll
         for (int q = 0; q < GT; q++) fj[q] = a.bc;
@@ -272,13 +275,13 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
     in_face(1, f1);
     in_face(2, f2);
     in_face(3, f3);
-    const T E1_0 = E1[0], E1_1 = E1[1], E1_2 = E1[2], E1_3 = E1[3];
-    const T E4_0 = E4[0], E4_1 = E4[1], E4_2 = E4[2], E4_3 = E4[3];
+    const TV E1_0 = E1[0], E1_1 = E1[1], E1_2 = E1[2], E1_3 = E1[3];
+    const TV E4_0 = E4[0], E4_1 = E4[1], E4_2 = E4[2], E4_3 = E4[3];
     const int64_t fid0 = slot_of(fid[0]), fid1 = slot_of(fid[1]), fid2 = slot_of(fid[2]), fid3 = slot_of(fid[3]);
     // the (at most three) out-faces, one slot after another
     for (int o = 0; o < nout; o++) {
       const int j = (jo >> (2 * o)) & 3;
-      T e[3];
+      TV e[3];
       int h[3];
 #pragma unroll
       for (int n = 0; n < 3; n++) {
@@ -288,40 +291,40 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
         e[n] = h[n] == 0 ? (four ? E4_0 : E1_0)
              : h[n] == 1 ? (four ? E4_1 : E1_1)
              : h[n] == 2 ? (four ? E4_2 : E1_2)
-             : h[n] == 3 ? (four ? E4_3 : E1_3) : (T)1;
+             : h[n] == 3 ? (four ? E4_3 : E1_3) : (TV)1;
       }
-      T out[GT];
+      TV out[GT];
 #pragma unroll
       for (int q = 0; q < GT; q++) {
-        T I0[3];
+        TV I0[3];
 #pragma unroll
         for (int n = 0; n < 3; n++)
           I0[n] = h[n] == 0 ? f0[q] : h[n] == 1 ? f1[q] : h[n] == 2 ? f2[q] : h[n] == 3 ? f3[q] : a.bc;
-        T Icur = e[0] * (I0[0] - rhs[q]) + rhs[q];
+        TV Icur = e[0] * (I0[0] - rhs[q]) + rhs[q];
         Icur += (e[1] * (I0[1] - rhs[q]) + rhs[q]);
         Icur += (e[2] * (I0[2] - rhs[q]) + rhs[q]);
-        out[q] = Icur * (T)0.3333333333333333;
+        out[q] = Icur * (TV)0.3333333333333333;
       }
       const int64_t fj = j == 0 ? fid0 : j == 1 ? fid1 : j == 2 ? fid2 : fid3;
-      st_slot<T, GT>(a.fv + (fj * a.DB + dl) * a.GS, out);
+      st_slot<TV, GT>(a.fv + (fj * a.DB + dl) * a.GS, out);
     }
   } else {
     asm volatile("griddepcontrol.wait;" ::: "memory");
     for (int gg = 0; gg < a.G; gg++) {
-      const T rhs = dy[2 + gg] + bk * (T)Sv[base + gg * gs];
-      T fvals[4];
+      const TV rhs = (TV)dy[2 + gg] + (TV)bk * (TV)Sv[base + gg * gs];
+      TV fvals[4];
 #pragma unroll
       for (int j = 0; j < 4; j++)
         fvals[j] = (cosf[j] < 0 && fid[j] >= 0) ? a.fv[((int64_t)fid[j] * a.DB + dl) * a.GS + gg] : a.bc;
       for (int o = 0; o < nout; o++) {
         const int j = (jo >> (2 * o)) & 3;
-        T I0[3], e[3];
+        TV I0[3], e[3];
 #pragma unroll
         for (int n = 0; n < 3; n++) {
           const uint32_t code = (uint32_t)(sel >> (12 * o + 4 * n)) & 15u;
           const int h = code & 8u ? -1 : (int)(code & 3u);
           I0[n] = a.bc;
-          e[n] = (T)1;
+          e[n] = (TV)1;
 #pragma unroll
           for (int f = 0; f < 4; f++)
             if (h == f) {
@@ -329,10 +332,10 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
               e[n] = code & 4u ? E4[f] : E1[f];
             }
         }
-        T Icur = e[0] * (I0[0] - rhs) + rhs;
+        TV Icur = e[0] * (I0[0] - rhs) + rhs;
         Icur += (e[1] * (I0[1] - rhs) + rhs);
         Icur += (e[2] * (I0[2] - rhs) + rhs);
-        a.fv[(slot_of(fid[j]) * a.DB + dl) * a.GS + gg] = Icur * (T)0.3333333333333333;
+        a.fv[(slot_of(fid[j]) * a.DB + dl) * a.GS + gg] = Icur * (TV)0.3333333333333333;
       }
     }
   }
@@ -344,8 +347,8 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T> a) {
 // parallel to it) hold the boundary value.  One thread per (cell, direction);
 // consecutive threads take consecutive directions of a cell, so face-value reads
 // and intensity writes are contiguous.
-template <class T, class TI, int GT>
-__global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
+template <class T, class TV, class TI, int GT>
+__global__ void __launch_bounds__(256) k_recalc(SweepArgs<T, TV> a, int64_t N) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= N * a.nbd) return;
   const int64_t c = t / a.nbd;
@@ -356,9 +359,9 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
   load_rec<T>(a.rec + (int64_t)a.RW * c, g, fid);
   T cosf[4];
   face_cos(g, a.w[3 * d], a.w[3 * d + 1], a.w[3 * d + 2], cosf);
-  T A[4];
+  TV A[4];
 #pragma unroll
-  for (int j = 0; j < 4; j++) A[j] = __ldg(a.area + 4 * c + j);
+  for (int j = 0; j < 4; j++) A[j] = (TV)__ldg(a.area + 4 * c + j);
   const SweepIO io = *a.io;
   TI *I = (TI *)io.I;
   int64_t base, gs;
@@ -373,10 +376,10 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
   bool have[4];
 #pragma unroll
   for (int j = 0; j < 4; j++) have[j] = cosf[j] > 0 || (cosf[j] < 0 && fid[j] >= 0);
-  auto cell_value = [&](const T *fv) {
-    T curI = 0;
+  auto cell_value = [&](const TV *fv) {
+    TV curI = 0;
     if (!last) {
-      T Ssum = 0;
+      TV Ssum = 0;
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         curI += fv[j] * A[j];
@@ -386,16 +389,16 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
     } else {
 #pragma unroll
       for (int j = 0; j < 4; j++) curI += fv[j];
-      curI /= (T)4;
+      curI /= (TV)4;
     }
     return curI;
   };
   if constexpr (GT > 0) {
     // all four face slots in flight at once, vector loads and a vector store
-    T f0[GT], f1[GT], f2[GT], f3[GT];
-    auto slot = [&](int j, T (&fj)[GT]) {
+    TV f0[GT], f1[GT], f2[GT], f3[GT];
+    auto slot = [&](int j, TV (&fj)[GT]) {
       if (have[j]) {
-        ld_groups<T, GT>(a.fv + (slot_of(fid[j]) * a.DB + dl) * a.GS, fj);
+        ld_groups<TV, GT>(a.fv + (slot_of(fid[j]) * a.DB + dl) * a.GS, fj);
       } else {
 #pragma unroll
         for (int q = 0; q < GT; q++) fj[q] = a.bc;
@@ -408,7 +411,7 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
     TI out[GT];  // the cell values as stored (rounded to float in the mixed form)
 #pragma unroll
     for (int q = 0; q < GT; q++) {
-      const T fv[4] = {f0[q], f1[q], f2[q], f3[q]};
+      const TV fv[4] = {f0[q], f1[q], f2[q], f3[q]};
       out[q] = (TI)cell_value(fv);
     }
     if (io.layout) {
@@ -451,7 +454,7 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T> a, int64_t N) {
     }
   } else {
     for (int gg = 0; gg < a.G; gg++) {
-      T fv[4];
+      TV fv[4];
 #pragma unroll
       for (int j = 0; j < 4; j++) fv[j] = have[j] ? a.fv[(slot_of(fid[j]) * a.DB + dl) * a.GS + gg] : a.bc;
       I[base + gg * gs] = (TI)cell_value(fv);
@@ -717,8 +720,8 @@ rrhd_status build_plan(rrhd_ctx *c) {
   return RRHD_OK;
 }
 
-template <class T, class TI, int GT>
-cudaError_t launch_level(const SweepArgs<T> &a, unsigned nb, cudaStream_t st, bool pdl) {
+template <class T, class TV, class TI, int GT>
+cudaError_t launch_level(const SweepArgs<T, TV> &a, unsigned nb, cudaStream_t st, bool pdl) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nb);
   cfg.blockDim = dim3(kSweepThreads);
@@ -729,10 +732,10 @@ cudaError_t launch_level(const SweepArgs<T> &a, unsigned nb, cudaStream_t st, bo
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = pdl ? 1 : 0;
-  return cudaLaunchKernelEx(&cfg, k_sweep_level<T, TI, GT>, a);
+  return cudaLaunchKernelEx(&cfg, k_sweep_level<T, TV, TI, GT>, a);
 }
 
-template <class T, class TI>
+template <class T, class TV, class TI>
 rrhd_status capture_sweep(rrhd_ctx *c) {
   RadState &R = c->rad;
   cudaStream_t cs = nullptr;
@@ -741,7 +744,7 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
   cudaError_t launch_err = cudaSuccess;
   cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    SweepArgs<T> a;
+    SweepArgs<T, TV> a;
     a.io = R.d_io;
     a.shift = R.shift;
     a.DB = R.DB;
@@ -751,9 +754,9 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
     a.w = (const T *)R.d_w;
     a.rec = (const T *)R.d_rec;
     a.area = (const T *)R.d_area;
-    a.fv = (T *)R.d_fv;
+    a.fv = (TV *)R.d_fv;
     a.scale_out = R.d_scale;
-    a.bc = (T)R.bc;
+    a.bc = (TV)R.bc;
     a.last = R.last_cell;
     a.GS = R.GS;
     int64_t base = 0;
@@ -769,19 +772,19 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
         const bool pdl = L > 0;  // the first level of a batch follows a full dependency
         cudaError_t le;
         switch (R.G) {
-          case 1: le = launch_level<T, TI, 1>(a, nb, cs, pdl); break;
-          case 2: le = launch_level<T, TI, 2>(a, nb, cs, pdl); break;
-          case 4: le = launch_level<T, TI, 4>(a, nb, cs, pdl); break;
-          default: le = launch_level<T, TI, 0>(a, nb, cs, pdl); break;
+          case 1: le = launch_level<T, TV, TI, 1>(a, nb, cs, pdl); break;
+          case 2: le = launch_level<T, TV, TI, 2>(a, nb, cs, pdl); break;
+          case 4: le = launch_level<T, TV, TI, 4>(a, nb, cs, pdl); break;
+          default: le = launch_level<T, TV, TI, 0>(a, nb, cs, pdl); break;
         }
         if (le != cudaSuccess && launch_err == cudaSuccess) launch_err = le;
       }
       const unsigned nr = grid_for(c->N * nbd, 256);
       switch (R.G) {
-        case 1: k_recalc<T, TI, 1><<<nr, 256, 0, cs>>>(a, c->N); break;
-        case 2: k_recalc<T, TI, 2><<<nr, 256, 0, cs>>>(a, c->N); break;
-        case 4: k_recalc<T, TI, 4><<<nr, 256, 0, cs>>>(a, c->N); break;
-        default: k_recalc<T, TI, 0><<<nr, 256, 0, cs>>>(a, c->N); break;
+        case 1: k_recalc<T, TV, TI, 1><<<nr, 256, 0, cs>>>(a, c->N); break;
+        case 2: k_recalc<T, TV, TI, 2><<<nr, 256, 0, cs>>>(a, c->N); break;
+        case 4: k_recalc<T, TV, TI, 4><<<nr, 256, 0, cs>>>(a, c->N); break;
+        default: k_recalc<T, TV, TI, 0><<<nr, 256, 0, cs>>>(a, c->N); break;
       }
       base += c->N * nbd;
     }
@@ -810,9 +813,10 @@ void rrhd_rad_release(rrhd_ctx *c) {
   R = RadState();
 }
 
-// T: arithmetic and storage of the records and face values; TI: the intensity and
-// scattering-integral arrays the sweep reads and writes.
-template <class T, class TI>
+// T: the records (geometry, opacities and sources) and directions; TV: the face values
+// and the transport arithmetic; TI: the intensity and scattering-integral arrays the
+// sweep reads and writes.
+template <class T, class TV, class TI>
 static rrhd_status rad_setup_t(rrhd_ctx *c) {
   RadState &R = c->rad;
   const int64_t N = c->N;
@@ -853,7 +857,7 @@ static rrhd_status rad_setup_t(rrhd_ctx *c) {
   }
   for (int q = 0; q < 3 * R.M; q++) w[q] = (T)R.dirs->h_w[q];
   R.last_cell = iperm[N - 1];
-  R.GS = sizeof(T) == 8 ? ((R.G + 3) & ~3) : ((R.G + 7) & ~7);
+  R.GS = sizeof(TV) == 8 ? ((R.G + 3) & ~3) : ((R.G + 7) & ~7);
   // the cell pass can hand the FP16 scattering its row scales when one CTA covers
   // every direction of a cell: one batch of 256 directions, float, G in {1, 2, 4}
   if (sizeof(TI) == 4 && R.nbatch == 1 && R.M == 256 && (R.G == 1 || R.G == 2 || R.G == 4) &&
@@ -869,10 +873,10 @@ static rrhd_status rad_setup_t(rrhd_ctx *c) {
       (s = up(&R.d_area, area.data(), sizeof(T) * area.size())))
     return s;
   if (cudaMalloc(&R.d_io, sizeof(SweepIO)) != cudaSuccess ||
-      cudaMalloc(&R.d_fv, sizeof(T) * (size_t)c->F * R.DB * R.GS) != cudaSuccess)
+      cudaMalloc(&R.d_fv, sizeof(TV) * (size_t)c->F * R.DB * R.GS) != cudaSuccess)
     return rrhd_fail(RRHD_ERR_OOM, "sweep allocation failed");
   if ((s = build_plan<T>(c))) return s;
-  return capture_sweep<T, TI>(c);
+  return capture_sweep<T, TV, TI>(c);
 }
 
 extern "C" rrhd_status rrhd_rad_setup(rrhd_ctx *c, const rrhd_dirs *dirs, const rrhd_rad_opts *o) {
@@ -902,9 +906,9 @@ extern "C" rrhd_status rrhd_rad_setup(rrhd_ctx *c, const rrhd_dirs *dirs, const 
   R.nbatch = (R.M + DB - 1) / DB;
   R.prec = o->precision;
   R.bc = o->boundary_value;
-  const rrhd_status s = R.prec == RRHD_RAD_FP64   ? rad_setup_t<double, double>(c)
-                        : R.prec == RRHD_RAD_MIXED ? rad_setup_t<double, float>(c)
-                                                   : rad_setup_t<float, float>(c);
+  const rrhd_status s = R.prec == RRHD_RAD_FP64   ? rad_setup_t<double, double, double>(c)
+                        : R.prec == RRHD_RAD_MIXED ? rad_setup_t<float, double, float>(c)
+                                                   : rad_setup_t<float, float, float>(c);
   if (s) {
     rrhd_rad_release(c);
     return s;
@@ -968,7 +972,7 @@ extern "C" rrhd_status rrhd_sweep(rrhd_ctx *c, const void *alpha, const void *be
   if (!R.ready) return rrhd_fail(RRHD_ERR_STATE, "rrhd_rad_setup has not run");
   RRHD_CUDA(cudaSetDevice(c->device));
   const int64_t N = c->N;
-  if (R.prec != RRHD_RAD_FP32)
+  if (R.prec == RRHD_RAD_FP64)
     k_dyn_from_arrays<double><<<grid_for(N, 256), 256, 0, c->stream>>>(
         N, R.G, R.RW, c->d_perm, (const double *)alpha, (const double *)betta, (const double *)Q, (double *)R.d_rec);
   else
@@ -1060,7 +1064,7 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
   RadState &R = c->rad;
   if (!R.ready) return rrhd_fail(RRHD_ERR_STATE, "rrhd_rad_setup has not run");
   const bool fp64 = R.prec == RRHD_RAD_FP64;         // intensity and scattering integral in double
-  const bool rec64 = R.prec != RRHD_RAD_FP32;        // sweep arithmetic and records in double
+  const bool rec64 = R.prec == RRHD_RAD_FP64;        // records (opacities, sources) in double
   const bool lowrank = o->scatter == RRHD_SCATTER_LOWRANK;
   RRHD_CHECK_ARG(lowrank || (fp64 ? o->scatter == RRHD_SCATTER_FP64
                                   : (o->scatter >= RRHD_TC_BF16X3 && o->scatter <= RRHD_TC_BF16)),

@@ -199,7 +199,7 @@ class TransportSweep:
     upwind order the reference reads from its offline graph/ and make_trace/
     outputs (sorted_graph, vec_x0), built on the GPU as levels.  precision:
     "fp64" or "fp32" (storage and arithmetic of alpha, betta, Q, S, I), or "mixed"
-    (double arithmetic and face values, alpha, betta, Q double, S and I float)."""
+    (float arrays as "fp32", face values and the transport update in double)."""
 
     def __init__(self, grid, dg: DirectionGrid, groups: int = 1, precision: str = "fp64", dirs_per_batch: int = 0,
                  boundary_value: float = 0.0):
@@ -225,15 +225,13 @@ class TransportSweep:
 def CalculateIllum(sw: TransportSweep, alpha, betta, Q, S, I=None):
     """One sweep of all directions and groups (the direction loop of
     solvers/illum/src/mpi/multi_gpu/illum_multi_gpu_face_calc.cpp:91-190) on the
-    grid's stream.  CUDA tensors in the sweep precision (mixed: alpha, betta, Q
-    double, S and I float), caller cell numbering: alpha, betta [N], Q [N, G],
-    S [N*G, M]; returns I [N*G, M]."""
+    grid's stream.  CUDA tensors, double for "fp64" and float otherwise, caller cell
+    numbering: alpha, betta [N], Q [N, G], S [N*G, M]; returns I [N*G, M]."""
     import torch
     if I is None:
         I = torch.empty_like(S)
-    f64 = torch.float64 if sw.precision in ("fp64", "mixed") else torch.float32
-    io = torch.float64 if sw.precision == "fp64" else torch.float32
-    for t, dt in ((alpha, f64), (betta, f64), (Q, f64), (S, io), (I, io)):
+    dt = torch.float64 if sw.precision == "fp64" else torch.float32
+    for t in (alpha, betta, Q, S, I):
         assert t.is_contiguous() and t.dtype == dt
     L.check(L.lib.rrhd_sweep(sw.grid.handle, L.ptr(alpha), L.ptr(betta), L.ptr(Q), L.ptr(S), L.ptr(I)),
             "CalculateIllum")

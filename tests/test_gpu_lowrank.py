@@ -126,7 +126,7 @@ def test_coupled_lowrank_matches_oracle():
     Uo, Wo = U, W
     for _ in range(3):
         hs, ss = step(tau, stats=True)
-        Uo, Wo, Io, S, mom, G4o = _oracle_coupled(m, Uo, Wo, tau, d, G, S, mom)
+        Uo, Wo, Io, S, mom, G4o, _ = _oracle_coupled(m, Uo, Wo, tau, d, G, S, mom)
         assert ss.n_failed == 0
     Wg, Ug = g.get_state()
     Ig, Sg, G4g = step.get("I"), step.get("S"), step.get("G4")
