@@ -233,12 +233,12 @@ def _p2c_fast(W):
     return np.repeat(Wu, len(W), 0), np.repeat(Uu, len(W), 0)
 
 
-def profile_traffic(name):
-    """dram bytes per launch recorded from an ncu capture in profiles/<name>."""
+def profile_figure(name, key="traffic_bytes_per_launch"):
+    """A figure recorded from an ncu capture in profiles/<name> as a line "key: value"."""
     p = os.path.join(ROOT, "profiles", name)
     try:
         for ln in open(p):
-            if ln.strip().startswith("traffic_bytes_per_launch:"):
+            if ln.strip().startswith(key + ":"):
                 return float(ln.split(":", 1)[1].split()[0])
     except Exception:
         pass
@@ -501,6 +501,11 @@ def coupled_component(dev, m, W, steps=100, warm=1, M=256, G=4, train_epochs=2, 
         ms = e0.elapsed_time(e1) / steps
         ph = step.phase_ms()
         levels, biggest = sw.plan_info()
+        # the reduced-precision scattering of the last step against FP64 from the same intensity
+        scat_err = None
+        if not fp64:
+            emax, erms, emom = step.scatter_error(65536)
+            scat_err = {"sample_cells": 65536, "max_rel": emax, "rms_rel": erms, "moments_max": emom}
         Wg, Ug = g.get_state()
         states[form] = Ug
         if form == "plain":
@@ -510,6 +515,7 @@ def coupled_component(dev, m, W, steps=100, warm=1, M=256, G=4, train_epochs=2, 
         out[form] = {"dirs_per_batch": batch[0] if fp64 else batch[1], "ms_per_step": ms, "steps_per_s": 1e3 / ms, "cell_updates_per_s": m.n_cells / (ms / 1e3),
                      "cell_dir_group_per_s": m.n_cells * M * G / (ms / 1e3), "phase_ms_last_step": ph,
                      "sweep_levels": levels, "largest_level": biggest, "plan_build_s": t_plan,
+                     "scatter_op_error": scat_err,
                      "sweep_alg_gbs": sweep_alg / (ph["sweep"] / 1e3) / 1e9,
                      "source_c2p": {"newton_iters_per_state_last_step": ss.newton_iters / m.n_cells,
                                     "failed_all_steps": fails[2]},
@@ -754,7 +760,8 @@ def run_ours(args):
     achieved = alg_bytes / (per_step / 1e3) / 1e9
     pk = peaks()
     peak = pk["hbm_gbs"] if pk else 6650.0
-    traffic = profile_traffic("hydro_step_jet96.md") if NHEX == 96 else None
+    traffic = profile_figure("hydro_step_jet96.md") if NHEX == 96 else None
+    fp64_pipe = profile_figure("hydro_step_jet96.md", "fp64_pipe_active_pct")
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_step, "higher_is_better": True, "scaling": "weak",
@@ -763,7 +770,9 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": "measured" if pk else "fallback",
-                         "algorithmic_bytes_per_cell_update": alg_bytes / m.n_cells},
+                         "algorithmic_bytes_per_cell_update": alg_bytes / m.n_cells,
+                         # the bound that binds: FP64 dependency chains (ncu, 64^3 capture of the same kernel)
+                         "fp64_pipe_active_pct": fp64_pipe},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
             "e2e_resident": e2e_res,
             "gpu_launches": args.steps,

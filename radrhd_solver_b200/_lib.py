@@ -155,6 +155,7 @@ _SIGS = {
     "rrhd_coupled_step": (I32, [P, D, P, P, P]),
     "rrhd_rad_get": (I32, [P, I32, P]),
     "rrhd_rad_set": (I32, [P, I32, P]),
+    "rrhd_coupled_scatter_error": (I32, [P, I64, P, P, P]),
     "rrhd_coupled_phase_ms": (I32, [P, P]),
     "rrhd_scatter_fp64_cdg": (I32, [P, P, P, I64, I32, I32, P]),
     "rrhd_moments_fp64_cdg": (I32, [P, P, P, P, P, I64, I32, P]),

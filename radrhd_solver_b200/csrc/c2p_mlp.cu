@@ -18,13 +18,12 @@
 // partial gradient with fixed-order loops; a second kernel sums the partials
 // over CTAs in order; Adam updates the parameters.
 //
-// Inference: each warp evaluates 32 states at once; the 64x64 layer runs on the
-// tensor cores as warp-level mma.sync m16n8k16 (bf16 operands, FP32
-// accumulation; the guess only seeds Newton, so bf16 is enough), the 3->64 and
-// 64->1 layers on the FP32 pipe.  Newton then starts from the guess; if it has
+// Inference: each warp evaluates 32 states at once, all three layers on the
+// tensor cores as warp-level mma.sync (f16 operands, FP32 accumulation; the
+// guess only seeds Newton, so f16 is enough).  Newton then starts from the guess; if it has
 // not converged after `k_stall` iterations the state is solved again from the
 // reference guess, so the result is always a converged reference Newton solve.
-#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -182,25 +181,40 @@ __global__ void k_adam(float *theta, float *m, float *v, const float *g, float l
   theta[p] -= lr * (mm / c1) / (sqrtf(vv / c2) + eps);
 }
 
-// bf16 B fragments of W2^T for mma.sync m16n8k16: [n-tile 8][k-step 4][lane 32] x 2 words
-__global__ void k_pack_w2(const float *theta, uint32_t *frag) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= 8 * 4 * 32) return;
-  const int lane = i & 31, ks = (i >> 5) & 3, nt = i >> 7;
-  const int g = lane >> 2, c = lane & 3;
-  const int n = 8 * nt + g, k0 = 16 * ks + 2 * c;
-  const float *W2 = theta + OFF_W2;
-  auto pk = [](float a, float b) {
-    return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a)) |
-           ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(b)) << 16);
-  };
-  frag[2 * i] = pk(W2[n * H + k0], W2[n * H + k0 + 1]);
-  frag[2 * i + 1] = pk(W2[n * H + k0 + 8], W2[n * H + k0 + 9]);
+// B fragments of the three layers for mma.sync (f16 operands, FP32 accumulation), in
+// uint32 words, each holding two f16 (the lower k index in the low half):
+//   FR_W2 [n-tile 8][k-step 4][lane 32][2]  W2^T for m16n8k16 (k = hidden input, n = output)
+//   FR_W1 [n-tile 8][lane 32]               [W1 | b1]^T for m16n8k8: k 0-2 the features,
+//                                           k 3 the bias (its A column is 1), k 4-7 zero
+//   FR_W3 [k-step 4][lane 32][2]            W3 as column 0 of an m16n8k16 B tile, the
+//                                           other 7 columns zero
+// Lane l of a B fragment holds column n = l / 4 and rows k = 2 (l % 4) + {0, 1} (+8 for
+// the second word of a k16 fragment).
+constexpr int FR_W2 = 0, FR_W1 = FR_W2 + 8 * 4 * 32 * 2, FR_W3 = FR_W1 + 8 * 32, NFRAG = FR_W3 + 4 * 32 * 2;  // 2560
+
+__device__ __forceinline__ uint32_t pack_f16(float lo, float hi) {
+  return (uint32_t)__half_as_ushort(__float2half_rn(lo)) | ((uint32_t)__half_as_ushort(__float2half_rn(hi)) << 16);
 }
 
-__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
-  return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a)) |
-         ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(b)) << 16);
+__global__ void k_pack_frags(const float *theta, uint32_t *frag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const float *W1 = theta + OFF_W1, *b1 = theta + OFF_B1, *W2 = theta + OFF_W2, *W3 = theta + OFF_W3;
+  if (i < 8 * 4 * 32) {
+    const int lane = i & 31, ks = (i >> 5) & 3, nt = i >> 7;
+    const int n = 8 * nt + (lane >> 2), k0 = 16 * ks + 2 * (lane & 3);
+    frag[FR_W2 + 2 * i] = pack_f16(W2[n * H + k0], W2[n * H + k0 + 1]);
+    frag[FR_W2 + 2 * i + 1] = pack_f16(W2[n * H + k0 + 8], W2[n * H + k0 + 9]);
+  } else if (i < 8 * 4 * 32 + 8 * 32) {
+    const int j = i - 8 * 4 * 32, lane = j & 31, nt = j >> 5;
+    const int n = 8 * nt + (lane >> 2), c = lane & 3;
+    frag[FR_W1 + j] = c == 0 ? pack_f16(W1[3 * n], W1[3 * n + 1]) : c == 1 ? pack_f16(W1[3 * n + 2], b1[n]) : 0u;
+  } else if (i < 8 * 4 * 32 + 8 * 32 + 4 * 32) {
+    const int j = i - 8 * 4 * 32 - 8 * 32, lane = j & 31, ks = j >> 5;
+    const int k0 = 16 * ks + 2 * (lane & 3);
+    const bool col0 = (lane >> 2) == 0;
+    frag[FR_W3 + 2 * j] = col0 ? pack_f16(W3[k0], W3[k0 + 1]) : 0u;
+    frag[FR_W3 + 2 * j + 1] = col0 ? pack_f16(W3[k0 + 8], W3[k0 + 9]) : 0u;
+  }
 }
 
 struct MlpPartial {
@@ -209,114 +223,107 @@ struct MlpPartial {
 
 constexpr int IT = 128;  // inference threads per CTA
 
-// Warp-cooperative guess for the 32 states of a warp; returns this lane's y.
-// The two m16 tiles (states 0-15, 16-31) are done one after the other so that
-// only one tile's 16x64 accumulator is live.
-__device__ __forceinline__ float mlp_warp(const float *xs, const float *sW1, const float *sb1, const float *sb2,
-                                          const float *sW3, float b3, const uint32_t *sfrag) {
+// ReLU of two FP32 accumulators packed as f16x2 (lo in the low half) in one conversion
+__device__ __forceinline__ uint32_t relu_f16x2(float lo, float hi) {
+  uint32_t d;
+  asm("cvt.rn.relu.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+  return d;
+}
+
+__device__ __forceinline__ void mma_k16(float *d, const uint32_t *a, uint2 b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b.x), "r"(b.y));
+}
+
+// Warp-cooperative guess for the 32 states of a warp (lane = state); returns this lane's
+// y.  All three layers run on the tensor cores, one m16 tile (16 states) at a time:
+// layer 1 as m16n8k8 over the features and a constant 1 (the bias), whose FP32 output
+// fragments are, after ReLU and packing to f16, the A fragments of layer 2 as they are
+// (the accumulator of n-tiles 2k, 2k+1 is the A operand of k-step k); the same for
+// layer 3, whose B tile holds W3 in column 0.
+__device__ __forceinline__ float mlp_warp(const float *xs, const float *sb2, float b3, const uint32_t *sfrag) {
   const int lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
-  float part[4];
+  // A columns of layer 1 held by a lane: c = 0 features 0, 1; c = 1 feature 2 and the 1
+  const uint32_t p01 = pack_f16(xs[0], xs[1]), p2 = pack_f16(xs[2], 1.f);
+  float y = 0.f;
 #pragma unroll 1
   for (int mt = 0; mt < 2; mt++) {
-    // features of the two states whose rows this lane holds in this tile: g, g + 8
-    float f[2][3];
+    const int r0 = 16 * mt + g;  // the states of rows g and g + 8 of this tile
+    const uint32_t x0a = __shfl_sync(0xffffffffu, p01, r0), x0b = __shfl_sync(0xffffffffu, p2, r0);
+    const uint32_t x1a = __shfl_sync(0xffffffffu, p01, r0 + 8), x1b = __shfl_sync(0xffffffffu, p2, r0 + 8);
+    const uint32_t a10 = c == 0 ? x0a : c == 1 ? x0b : 0u, a11 = c == 0 ? x1a : c == 1 ? x1b : 0u;
+    uint32_t a2[4][4];
 #pragma unroll
-    for (int q = 0; q < 2; q++)
-#pragma unroll
-      for (int a = 0; a < 3; a++) f[q][a] = __shfl_sync(0xffffffffu, xs[a], 16 * mt + g + 8 * q);
-    // the 64 output columns in two halves of 4 n-tiles (16 accumulators live, not 32);
-    // the first layer is recomputed for the second half
-    float p0 = 0.f, p1 = 0.f;
-#pragma unroll 1
-    for (int half = 0; half < 2; half++) {
-      float acc[4][4];
-#pragma unroll
-      for (int nt = 0; nt < 4; nt++)
-#pragma unroll
-        for (int e = 0; e < 4; e++) acc[nt][e] = 0.f;
-#pragma unroll
-      for (int ks = 0; ks < 4; ks++) {
-        const int k0 = 16 * ks + 2 * c;
-        const int kk[4] = {k0, k0 + 1, k0 + 8, k0 + 9};
-        float hv[2][4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          const int k = kk[j];
-          const float w0 = sW1[3 * k], w1 = sW1[3 * k + 1], w2 = sW1[3 * k + 2], bb = sb1[k];
-#pragma unroll
-          for (int q = 0; q < 2; q++)
-            hv[q][j] = fmaxf(fmaf(w2, f[q][2], fmaf(w1, f[q][1], fmaf(w0, f[q][0], bb))), 0.f);
-        }
-        const uint32_t a0 = pack_bf16(hv[0][0], hv[0][1]);
-        const uint32_t a1 = pack_bf16(hv[1][0], hv[1][1]);
-        const uint32_t a2 = pack_bf16(hv[0][2], hv[0][3]);
-        const uint32_t a3 = pack_bf16(hv[1][2], hv[1][3]);
-#pragma unroll
-        for (int t = 0; t < 4; t++) {
-          const int nt = 4 * half + t;
-          const uint2 b = *reinterpret_cast<const uint2 *>(sfrag + 2 * ((nt * 4 + ks) * 32 + lane));
-          asm volatile(
-              "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-              "{%0,%1,%2,%3};\n"
-              : "+f"(acc[t][0]), "+f"(acc[t][1]), "+f"(acc[t][2]), "+f"(acc[t][3])
-              : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b.x), "r"(b.y));
-        }
-      }
-      // output layer: partial sums of rows g and g + 8 over this lane's columns of the half
-#pragma unroll
-      for (int t = 0; t < 4; t++)
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-          const int n = 8 * (4 * half + t) + 2 * c + (e & 1);
-          const float v = fmaxf(acc[t][e] + sb2[n], 0.f) * sW3[n];
-          if (e < 2)
-            p0 += v;
-          else
-            p1 += v;
-        }
+    for (int nt = 0; nt < 8; nt++) {
+      float h[4] = {0.f, 0.f, 0.f, 0.f};
+      asm volatile(
+          "mma.sync.aligned.m16n8k8.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+          : "+f"(h[0]), "+f"(h[1]), "+f"(h[2]), "+f"(h[3])
+          : "r"(a10), "r"(a11), "r"(sfrag[FR_W1 + 32 * nt + lane]));
+      a2[nt >> 1][2 * (nt & 1)] = relu_f16x2(h[0], h[1]);
+      a2[nt >> 1][2 * (nt & 1) + 1] = relu_f16x2(h[2], h[3]);
     }
-    p0 += __shfl_xor_sync(0xffffffffu, p0, 1);
-    p0 += __shfl_xor_sync(0xffffffffu, p0, 2);
-    p1 += __shfl_xor_sync(0xffffffffu, p1, 1);
-    p1 += __shfl_xor_sync(0xffffffffu, p1, 2);
-    part[2 * mt] = p0;
-    part[2 * mt + 1] = p1;
-  }
-  // state s sits in row slot s / 8 of lanes 4 (s % 8) .. +3
-  float y = 0.f;
+    float acc[8][4];
 #pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const float v = __shfl_sync(0xffffffffu, part[q], 4 * (lane & 7));
-    if ((lane >> 3) == q) y = v;
+    for (int nt = 0; nt < 8; nt++) {
+      const float2 bb = *reinterpret_cast<const float2 *>(sb2 + 8 * nt + 2 * c);
+      acc[nt][0] = bb.x;
+      acc[nt][1] = bb.y;
+      acc[nt][2] = bb.x;
+      acc[nt][3] = bb.y;
+    }
+#pragma unroll
+    for (int ks = 0; ks < 4; ks++)
+#pragma unroll
+      for (int nt = 0; nt < 8; nt++)
+        mma_k16(acc[nt], a2[ks], *reinterpret_cast<const uint2 *>(sfrag + FR_W2 + 2 * ((nt * 4 + ks) * 32 + lane)));
+    float o[4] = {b3, 0.f, b3, 0.f};
+#pragma unroll
+    for (int ks = 0; ks < 4; ks++) {
+      const uint32_t a3[4] = {relu_f16x2(acc[2 * ks][0], acc[2 * ks][1]), relu_f16x2(acc[2 * ks][2], acc[2 * ks][3]),
+                              relu_f16x2(acc[2 * ks + 1][0], acc[2 * ks + 1][1]),
+                              relu_f16x2(acc[2 * ks + 1][2], acc[2 * ks + 1][3])};
+      mma_k16(o, a3, *reinterpret_cast<const uint2 *>(sfrag + FR_W3 + 2 * (ks * 32 + lane)));
+    }
+    // column 0: row g in o[0], row g + 8 in o[2] of lane 4 g
+    const float v0 = __shfl_sync(0xffffffffu, o[0], 4 * (lane & 7));
+    const float v1 = __shfl_sync(0xffffffffu, o[2], 4 * (lane & 7));
+    if ((lane >> 4) == mt) y = (lane & 8) ? v1 : v0;
   }
-  return y + b3;
+  return y;
 }
 
 // PhysPressureFix out of line: the rare fallback does not add to the registers of the
 // kernel's main path.
-__device__ __noinline__ int pressure_fix_call(Eos eos, double *U, double *W) { return pressure_fix(eos, U, W); }
+// The state goes in and out by value: a pointer to the kernel's own arrays would put them in
+// local memory for the whole loop, not only for this call.
+struct FixState {
+  double u[5], w[5];
+  int code;
+};
+__device__ __noinline__ FixState pressure_fix_call(Eos eos, FixState s) {
+  s.code = pressure_fix(eos, s.u, s.w);
+  return s;
+}
 
 // States i live at U + stride*i and W + stride*i (stride 5 for separate arrays,
 // 10 for a solver state [n][10] = U, W).  With G4 != NULL the radiation source
 // is added first, U.E += tau G0 and U.S += tau G[1..3] (radRHD_main.cpp:117-126).
 #ifndef RRHD_MLP_MIN_BLOCKS
-#define RRHD_MLP_MIN_BLOCKS 5  // CTAs per SM the register budget of k_c2p_mlp is sized for
+#define RRHD_MLP_MIN_BLOCKS 4  // CTAs per SM the register budget of k_c2p_mlp is sized for
 #endif
 __global__ void __launch_bounds__(IT, RRHD_MLP_MIN_BLOCKS) k_c2p_mlp(Eos eos, double *U, double *W, int64_t stride, const double *G4,
                                                 double tau_src, uint8_t *status, int64_t n, int fallback,
                                                 int k_stall, const float *__restrict__ theta,
                                                 const uint32_t *__restrict__ frag, Norm nm, MlpPartial *scratch,
                                                 double *guess_out) {
-  __shared__ float sW1[H * 3], sb1[H], sb2[H], sW3[H];
-  __shared__ uint32_t sfrag[2 * 8 * 4 * 32];
+  __shared__ __align__(16) float sb2[H];
+  __shared__ __align__(16) uint32_t sfrag[NFRAG];
   __shared__ unsigned long long red[6][IT / 32];
-  for (int q = threadIdx.x; q < H * 3; q += IT) sW1[q] = theta[OFF_W1 + q];
-  for (int q = threadIdx.x; q < H; q += IT) {
-    sb1[q] = theta[OFF_B1 + q];
-    sb2[q] = theta[OFF_B2 + q];
-    sW3[q] = theta[OFF_W3 + q];
-  }
-  for (int q = threadIdx.x; q < 2 * 8 * 4 * 32; q += IT) sfrag[q] = frag[q];
+  for (int q = threadIdx.x; q < H; q += IT) sb2[q] = theta[OFF_B2 + q];
+  for (int q = threadIdx.x; q < NFRAG; q += IT) sfrag[q] = frag[q];
   const float b3 = theta[OFF_B3];
   __syncthreads();
   unsigned ok = 0, gfb = 0, fb = 0, failed = 0, iters = 0, mx = 0;  // per thread (u32: a thread sees few states)
@@ -347,7 +354,7 @@ __global__ void __launch_bounds__(IT, RRHD_MLP_MIN_BLOCKS) k_c2p_mlp(Eos eos, do
     float xs[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) xs[a] = feat ? (f[a] - nm.mu[a]) / nm.sig[a] : 0.f;
-    const float y = mlp_warp(xs, sW1, sb1, sb2, sW3, b3, sfrag);
+    const float y = mlp_warp(xs, sb2, b3, sfrag);
     double u[5] = {0, 0, 0, 0, 0}, wv[5] = {0, 0, 0, 0, 0};
     if (live) {
       load_u(u);
@@ -355,6 +362,7 @@ __global__ void __launch_bounds__(IT, RRHD_MLP_MIN_BLOCKS) k_c2p_mlp(Eos eos, do
     }
     if (!live) continue;
     bool u_dirty = G4 != nullptr;
+    feat = feat && isfinite(y);  // an f16 overflow inside the network: the reference guess
     const double p0 = feat ? tau * (double)__expf(y * nm.sig_t + nm.mu_t) : 0.0;
     if (feat && guess_out) guess_out[i] = p0;
     // attempt 0: Newton from the learned guess for at most k_stall iterations; attempt 1
@@ -373,7 +381,19 @@ __global__ void __launch_bounds__(IT, RRHD_MLP_MIN_BLOCKS) k_c2p_mlp(Eos eos, do
     mx = (unsigned)itn > mx ? (unsigned)itn : mx;
     if (code) {
       if (fallback) {
-        const int fix = pressure_fix_call(eos, u, wv);
+        FixState fs;
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+          fs.u[q] = u[q];
+          fs.w[q] = wv[q];
+        }
+        fs = pressure_fix_call(eos, fs);
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+          u[q] = fs.u[q];
+          wv[q] = fs.w[q];
+        }
+        const int fix = fs.code;
         code = code | 0x10 | (fix ? 0x20 : 0);
         fb++;
         failed += fix ? 1 : 0;
@@ -459,7 +479,7 @@ struct rrhd_mlp {
 };
 
 static rrhd_status mlp_refresh(rrhd_mlp *m, cudaStream_t st) {
-  k_pack_w2<<<4, 256, 0, st>>>(m->d_theta, m->d_frag);
+  k_pack_frags<<<6, 256, 0, st>>>(m->d_theta, m->d_frag);
   RRHD_CUDA(cudaGetLastError());
   return RRHD_OK;
 }
@@ -481,7 +501,7 @@ extern "C" rrhd_status rrhd_mlp_create(int32_t device, uint64_t seed, rrhd_mlp *
   for (int q = 0; q < H * H; q++) th[OFF_W2 + q] = (float)(normal(1000 + q) * std::sqrt(2.0 / H));
   for (int q = 0; q < H; q++) th[OFF_W3 + q] = (float)(normal(9000 + q) * std::sqrt(1.0 / H));
   if (cudaMalloc(&m->d_theta, NPARAM * 4) || cudaMalloc(&m->d_m, NPARAM * 4) || cudaMalloc(&m->d_v, NPARAM * 4) ||
-      cudaMalloc(&m->d_grad, NPARAM * 4) || cudaMalloc(&m->d_frag, 2 * 8 * 4 * 32 * 4)) {
+      cudaMalloc(&m->d_grad, NPARAM * 4) || cudaMalloc(&m->d_frag, NFRAG * 4)) {
     rrhd_mlp_destroy(m);
     return rrhd_fail(RRHD_ERR_OOM, "network allocation failed");
   }

@@ -22,11 +22,8 @@ rrhd_status scatter_fp64_cdg(const rrhd_dirs *d, const double *I, double *S, int
                              cudaStream_t st);
 rrhd_status moments_fp64_cdg(const rrhd_dirs *d, const double *I, double *E, double *F, double *T, int64_t cells,
                              int G, cudaStream_t st);
-// row_scales (may be NULL): the per-row power-of-two scales of the FP16 forms,
-// 2^(14 - floor(log2 max_d |I|)), when the caller has them already (the sweep's cell pass).
 rrhd_status scatter_tc_cdg(const rrhd_scatter_tc *t, const float *I, float *S, float *mom, int64_t cells, int G,
-                           cudaStream_t st, const float *row_scales = nullptr);
-bool scatter_tc_scaled(const rrhd_scatter_tc *t);
+                           cudaStream_t st);
 // Low-rank (Thomson) scattering and moments, cell-direction-group layout, G = 1, 2, 4:
 // FP64 with the moments as E [rows], F [rows][3], T [rows][3][3] (any may be NULL
 // together), FP32 with the moments as [rows][16] (mom may be NULL).

@@ -75,7 +75,6 @@ struct RadState {
   // context numbering or -1), then the step's source record {k, betta/k, alpha Q_g/k}
   void *d_rec = nullptr;
   void *d_area = nullptr;  // [N][4] face areas
-  float *d_scale = nullptr;  // [N][G] row scales of the FP16 scattering, written by the cell pass
   uint32_t *d_plan = nullptr;               // all batches: items (cell << shift | d) in level order
   std::vector<std::vector<int64_t>> lvl;    // per batch: level offsets into d_plan
   int64_t levels = 0, max_level = 0;
@@ -107,7 +106,8 @@ struct rrhd_ctx {
   int64_t N = 0, F = 0;
   int cpb = 256;      // cells per CTA
   int nblocks = 0;
-  int max_entries = 0;  // largest per-CTA face list (records and staged cross-face fluxes)
+  int max_entries = 0;  // largest per-CTA face list
+  int max_halo = 0;     // largest per-CTA list of neighbour cells owned by other CTAs
   int64_t n_entries = 0;
   size_t step_smem = 0; // dynamic shared memory of the step kernel
 
@@ -115,21 +115,12 @@ struct rrhd_ctx {
   int32_t *d_perm = nullptr, *d_iperm = nullptr;
   std::vector<int32_t> h_perm;
 
-  // per-CTA face lists: the faces whose cells are all in the CTA (records), then the
-  // faces shared with another CTA ("cross" faces, whose fluxes k_cross_flux computes once)
-  int32_t *d_bface_off = nullptr;  // [nblocks+1] into d_bface_rec
+  // per-CTA face lists
+  int32_t *d_bface_off = nullptr;  // [nblocks+1]
   rrhd::FaceRec *d_bface_rec = nullptr;  // [E] face records, every CTA's list padded to an even count
-  int32_t *d_bface_gid = nullptr;  // [E] caller face id (-1 for the padding record)
-  int32_t *d_xoff = nullptr;       // [nblocks+1] into d_xids
-  int32_t *d_xids = nullptr;       // cross faces each CTA's cells touch, in the order they meet them
-  // the cross faces: records with context cell indices, numbered by the block of their
-  // left cell; their fluxes of the current step; the ones this context computes
-  int64_t n_cross = 0;
-  rrhd::FaceRec *d_cross_rec = nullptr;  // [n_cross]
-  int32_t *d_cross_gid = nullptr;        // [n_cross] caller face id
-  double *d_cross_flux = nullptr;        // [n_cross][5]
-  int64_t n_cross_list = 0;
-  int32_t *d_cross_list = nullptr;       // NULL: all; under a split: those the rank's blocks touch
+  int32_t *d_halo_off = nullptr;   // [nblocks+1]
+  int32_t *d_halo_ids = nullptr;   // neighbour cells (new numbering) staged after the CTA's own
+  int32_t *d_bface_gid = nullptr;  // [E] caller face id on the owner CTA, else -1
 
   // per cell (new numbering)
   rrhd::CellRec *d_cell_rec = nullptr;

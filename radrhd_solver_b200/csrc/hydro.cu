@@ -5,28 +5,26 @@
 //   state  [N][10] doubles = U(5) | W(5) per cell, 80 B, loaded as 5 x double2;
 //          two buffers (read one, write the other) so that no CTA overwrites a
 //          neighbour state another CTA still reads.
-//   cells are grouped into CTA blocks of cells_per_block consecutive cells.  A face
-//   whose cells lie in two blocks is a "cross" face: its flux is computed once per
-//   step by k_cross_flux (both states from global memory) into a flux array.  Per
-//   block, the faces whose cells are all in the block (a boundary face has one) as
-//   40-byte records {n0, n1, n2, area, l, r} (l, r block-local cells, r < 0 a
-//   boundary code), padded to an even count so that every block's list starts on a
-//   16-byte boundary, and the indices of the cross faces its cells touch.  Per cell a
-//   16-byte record {4 local face slots with the cell's sign bit in bit 15, volume}.
-// Per step: k_cross_flux, then one kernel does the rest:
-//   phase 0  cp.async stages the block's own states (one contiguous range), its face
-//            records, the fluxes of its cross faces and its cell records into shared
+//   per CTA (cells_per_block consecutive cells) a list of every face touching
+//   one of its cells as 40-byte records {n0, n1, n2, area, l, r} (l, r the
+//   CTA-local state slots, r < 0 a boundary code), padded to an even count so
+//   that every CTA's list starts on a 16-byte boundary; and a halo list of the
+//   neighbour cells owned by other CTAs.  A face between two CTAs sits in both
+//   lists and is computed by both, bit-identically.  Per cell a 16-byte record
+//   {4 local face slots with the cell's sign bit in bit 15, volume}.
+// One kernel does the whole step:
+//   phase 0  cp.async stages the CTA's own states (one contiguous range), its
+//            halo states, its face records and its cell records into shared
 //            memory, all requests in flight at once;
-//   then     the squared sound speed of every own cell (a function of its rho and p
-//            alone), once per cell rather than once per face side;
-//   phase 1  face fluxes of the block's own faces from the staged states; each
-//            thread overwrites the face record it has read with that face's flux;
+//   then     the squared sound speed of every staged cell (a function of its rho
+//            and p alone), once per cell rather than once per face side;
+//   phase 1  face fluxes from the staged states; each thread overwrites the
+//            face record it has read with that face's flux;
 //   phase 2  each cell sums its 4 faces in the reference's order (id_faces
 //            j = 0..3 with sign_n), updates U, runs con2prim with the
 //            PhysPressureFix fallback and writes U, W and a status byte.
-// Every face is computed once, bit-identically to the reference.  No atomics touch
-// the state; the max signal speed and the fallback counts are reduced per CTA (per
-// warp in k_cross_flux) and combined with atomics.
+// No atomics touch the state; the max signal speed and the fallback counts are
+// reduced per CTA and combined with one atomic per CTA.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -51,9 +49,9 @@ struct StepParams {
   int cpb;
   int b0;  // first CTA block of this launch (the rank's range under a split)
   const int32_t *__restrict__ off;
-  const int32_t *__restrict__ xoff;
-  const int32_t *__restrict__ xids;
-  const double *__restrict__ xflux;
+  const int32_t *__restrict__ halo_off;
+  const int32_t *__restrict__ halo_ids;
+  int max_halo;
   const FaceRec *__restrict__ face;
   const int32_t *__restrict__ gid;
   const CellRec *__restrict__ cell;
@@ -119,10 +117,6 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
@@ -142,70 +136,6 @@ __device__ __forceinline__ void load_state_smem(const double *s, int slot, doubl
   W[4] = f.y;
 }
 
-// A cell's U and W from the global state array (two 16-byte-aligned 80-byte rows per cell).
-__device__ __forceinline__ void load_state_global(const double *s, int64_t c, double *U, double *W) {
-  const double2 *p = reinterpret_cast<const double2 *>(s + 10 * c);
-  const double2 a = __ldg(p), b = __ldg(p + 1), d = __ldg(p + 2), e = __ldg(p + 3), f = __ldg(p + 4);
-  U[0] = a.x;
-  U[1] = a.y;
-  U[2] = b.x;
-  U[3] = b.y;
-  U[4] = d.x;
-  W[0] = d.y;
-  W[1] = e.x;
-  W[2] = e.y;
-  W[3] = f.x;
-  W[4] = f.y;
-}
-
-struct CrossParams {
-  Eos eos;
-  int64_t n;                             // faces to compute
-  const int32_t *__restrict__ list;      // their indices (NULL: 0 .. n-1)
-  const FaceRec *__restrict__ rec;       // {n, area, l, r} with context cell indices
-  const int32_t *__restrict__ gid;
-  const double *__restrict__ sin;
-  double *__restrict__ flux;             // [n_cross][5]
-  double *__restrict__ face_flux;        // caller numbering (kFaceFlux)
-  StepScalars *out;
-};
-
-// The fluxes of the faces between two CTA blocks, once each, before the step kernel
-// stages them: GetFluxStab (rhllc_flux_stab.cpp:240-431) from both cells' states in
-// global memory.  Their signal speeds join the step's max (one atomic per warp).
-template <bool kFaceFlux>
-__global__ void __launch_bounds__(256) k_cross_flux(const CrossParams X) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  double vmax = 0.0;
-  if (i < X.n) {
-    const int64_t k = X.list ? X.list[i] : i;
-    const FaceRec r = X.rec[k];
-    Rot R;
-    rotation(r.n0, r.n1, r.n2, R);
-    double U[5], W[5], Fl[5];
-    load_state_global(X.sin, r.l, U, W);
-    const FaceSide sl = face_side(R, U, W, sound_speed2(X.eos, W[0], W[4]));
-    load_state_global(X.sin, r.r, U, W);
-    const FaceSide sr = face_side(R, U, W, sound_speed2(X.eos, W[0], W[4]));
-    const FaceStar fs = face_star(sl, sr);
-    vmax = fs.vmax;
-    load_state_global(X.sin, fs.right ? r.r : r.l, U, W);
-    face_flux(R, U, fs.right ? sr : sl, fs, r.area, Fl);
-#pragma unroll
-    for (int q = 0; q < 5; q++) X.flux[5 * k + q] = Fl[q];
-    if (kFaceFlux) {
-#pragma unroll
-      for (int q = 0; q < 5; q++) X.face_flux[5 * (size_t)X.gid[k] + q] = Fl[q];
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) vmax = smax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-  // non-negative doubles order like their bit patterns
-  if ((threadIdx.x & 31) == 0 && vmax > 0.0)
-    atomicMax(reinterpret_cast<unsigned long long *>(&X.out->max_speed),
-              (unsigned long long)__double_as_longlong(vmax));
-}
-
 #ifndef RRHD_STEP_MIN_BLOCKS
 #define RRHD_STEP_MIN_BLOCKS 3  // CTAs per SM the register budget is sized for
 #endif
@@ -214,42 +144,39 @@ __global__ void __launch_bounds__(256) k_cross_flux(const CrossParams X) {
 template <bool kFaceFlux>
 __global__ void __launch_bounds__(kStepThreads, RRHD_STEP_MIN_BLOCKS) k_hydro_step(const StepParams P) {
   extern __shared__ double2 smem_raw[];
-  double *sstate = reinterpret_cast<double *>(smem_raw);      // [cpb][10]
-  double *sface = sstate + 10 * P.cpb;                        // [entries][5]: record, then flux
+  double *sstate = reinterpret_cast<double *>(smem_raw);      // [cpb + max_halo][10]
+  double *sface = sstate + 10 * (P.cpb + P.max_halo);         // [entries][5]: record, then flux
   const int b = P.b0 + blockIdx.x;
-  const int e0 = P.off[b], e1 = P.off[b + 1];                 // this CTA's face records
-  const int x0 = P.xoff[b], x1 = P.xoff[b + 1];               // the cross faces its cells touch
-  const int ni = e1 - e0;                                     // even; cross fluxes go after the records
-  // the cell records start on a 16-byte boundary: after an even number of 40-byte slots
-  CellRec *scell = reinterpret_cast<CellRec *>(sface + 5 * ((ni + x1 - x0 + 1) & ~1));  // [cpb]
-  double *scs2 = reinterpret_cast<double *>(scell + P.cpb);                  // [cpb] sound speeds^2
+  const int e0 = P.off[b], e1 = P.off[b + 1];
+  CellRec *scell = reinterpret_cast<CellRec *>(sface + 5 * (e1 - e0));  // [cpb]
+  double *scs2 = reinterpret_cast<double *>(scell + P.cpb);              // [cpb + max_halo] sound speeds^2
   __shared__ double s_red[kStepThreads / 32];
   __shared__ unsigned long long s_cnt[2];
   __shared__ unsigned short s_fail[kMaxCellsPerBlock];
   __shared__ int s_nfail;
   const int c0 = b * P.cpb;
   const int nc = min(P.cpb, P.N - c0);
+  const int h0 = P.halo_off[b], h1 = P.halo_off[b + 1];
   double tau = P.tau;
   if (P.device_tau) tau = P.cfl_hmin / P.prev->max_speed;
   if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0;
   if (threadIdx.x == 0) s_nfail = 0;
 
-  // phase 0: stage the own (contiguous) states, the face records, the fluxes of the
-  // cross faces (computed by k_cross_flux before this kernel) and the cell records.
-  // Each CTA's record list starts on a 16-byte boundary and holds an even number of
-  // 40-byte records; a cross flux (40 bytes) is copied as five 8-byte requests.
+  // phase 0: stage own (contiguous) and halo states, the face records and the
+  // cell records, 16 bytes per request.  Each CTA's face list starts on a
+  // 16-byte boundary and holds an even number of 40-byte records.
   {
     const char *g = reinterpret_cast<const char *>(P.sin);
     char *sm = reinterpret_cast<char *>(sstate);
     for (int q = threadIdx.x; q < nc * 5; q += kStepThreads)
       cp_async16(sm + 16 * q, g + 80 * (size_t)c0 + 16 * q);
+    for (int q = threadIdx.x; q < (h1 - h0) * 5; q += kStepThreads) {
+      const int h = q / 5, k = q - 5 * h;
+      cp_async16(sm + 80 * (P.cpb + h) + 16 * k, g + 80 * (size_t)P.halo_ids[h0 + h] + 16 * k);
+    }
     const char *gf = reinterpret_cast<const char *>(P.face + e0);
     char *sf = reinterpret_cast<char *>(sface);
-    for (int q = threadIdx.x; q < ni * 40 / 16; q += kStepThreads) cp_async16(sf + 16 * q, gf + 16 * q);
-    for (int q = threadIdx.x; q < (x1 - x0) * 5; q += kStepThreads) {
-      const int x = q / 5, i = q - 5 * x;
-      cp_async8(sface + 5 * (ni + x) + i, P.xflux + 5 * (size_t)P.xids[x0 + x] + i);
-    }
+    for (int q = threadIdx.x; q < (e1 - e0) * 40 / 16; q += kStepThreads) cp_async16(sf + 16 * q, gf + 16 * q);
     const char *gc = reinterpret_cast<const char *>(P.cell + c0);
     char *sc = reinterpret_cast<char *>(scell);
     for (int q = threadIdx.x; q < nc; q += kStepThreads) cp_async16(sc + 16 * q, gc + 16 * q);
@@ -258,15 +185,16 @@ __global__ void __launch_bounds__(kStepThreads, RRHD_STEP_MIN_BLOCKS) k_hydro_st
   __syncthreads();
   // the squared sound speed of every staged cell (GetFluxStab's cs^2, rhllc_flux_stab.cpp:276-291,
   // depends on the cell's rho and p alone): once per cell instead of once per face side
-  for (int q = threadIdx.x; q < nc; q += kStepThreads) {
-    const double *st = sstate + 10 * q;
-    scs2[q] = sound_speed2(P.eos, st[5], st[9]);
+  for (int q = threadIdx.x; q < nc + (h1 - h0); q += kStepThreads) {
+    const int slot = q < nc ? q : P.cpb + (q - nc);
+    const double *st = sstate + 10 * slot;
+    scs2[slot] = sound_speed2(P.eos, st[5], st[9]);
   }
   __syncthreads();
 
-  // phase 1: the faces whose cells are all in this CTA; the flux replaces the record
+  // phase 1: every face touching this CTA's cells; the flux replaces the record
   double vmax = 0.0;
-  for (int e = threadIdx.x; e < ni; e += kStepThreads) {
+  for (int e = threadIdx.x; e < e1 - e0; e += kStepThreads) {
     double *rec = sface + 5 * e;
     const double n0 = rec[0], n1 = rec[1], n2 = rec[2], area = rec[3];
     const int2 lr = *reinterpret_cast<const int2 *>(rec + 4);
@@ -587,8 +515,7 @@ void free_ctx(rrhd_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
   rrhd_rad_release(c);
-  void *ptrs[] = {c->d_perm, c->d_iperm, c->d_bface_off, c->d_bface_rec, c->d_xoff, c->d_xids, c->d_cross_rec,
-                  c->d_cross_gid, c->d_cross_flux, c->d_cross_list,
+  void *ptrs[] = {c->d_perm, c->d_iperm, c->d_bface_off, c->d_bface_rec, c->d_halo_off, c->d_halo_ids,
                   c->d_bface_gid, c->d_cell_rec, c->d_state[0],
                   c->d_state[1], c->d_status, c->d_scal, c->d_face_flux, c->d_scratch_io,
                   c->d_send_ids, c->d_recv_ids};
@@ -647,76 +574,65 @@ extern "C" rrhd_status rrhd_create(const rrhd_mesh_desc *m, const rrhd_opts *opt
   c->nblocks = nb;
   c->part_b1 = nb;
   c->part_c1 = N;
-  // cross faces (a cell in each of two blocks): numbered in the order their left cells
-  // meet them, so that the faces of one block are contiguous
-  std::vector<int32_t> xidx(F, -1), xgid;
-  std::vector<FaceRec> xrec;
-  for (int64_t cn = 0; cn < N; cn++) {
-    const int32_t co = perm[cn];
-    for (int j = 0; j < 4; j++) {
-      const int32_t f = m->cell_faces[4 * co + j];
-      if (xidx[f] >= 0 || m->face_id_r[f] < 0 || m->face_id_l[f] != co) continue;
-      const int32_t l = (int32_t)cn, r = iperm[m->face_id_r[f]];
-      if (l / cpb == r / cpb) continue;
-      xidx[f] = (int32_t)xrec.size();
-      xrec.push_back(FaceRec{m->face_n[3 * f], m->face_n[3 * f + 1], m->face_n[3 * f + 2], m->face_area[f], l, r});
-      xgid.push_back(f);
-    }
-  }
-  std::vector<int32_t> off(nb + 1, 0), xoff(nb + 1, 0), xids;
+  std::vector<int32_t> off(nb + 1, 0);
   std::vector<FaceRec> frec;
   std::vector<int32_t> gid;
-  frec.reserve((size_t)(F * 1.05));
-  gid.reserve((size_t)(F * 1.05));
-  xids.reserve(2 * xrec.size());
+  frec.reserve((size_t)(F * 1.3));
+  gid.reserve((size_t)(F * 1.3));
   std::vector<CellRec> crec(N);
-  std::vector<int32_t> stamp(F, -1), local(F, 0), in_f, ex_f;
-  int max_e = 0;
+  std::vector<int32_t> stamp(F, -1), local(F, 0);
+  std::vector<int32_t> hstamp(N, -1), hlocal(N, 0);
+  std::vector<int32_t> hoff(nb + 1, 0), hids;
+  hids.reserve((size_t)(N / 2));
+  int max_e = 0, max_h = 0;
   for (int b = 0; b < nb; b++) {
+    int ne = 0, nh = 0;
     const int64_t c0 = (int64_t)b * cpb, c1 = std::min<int64_t>(N, c0 + cpb);
-    in_f.clear();
-    ex_f.clear();
-    for (int64_t cn = c0; cn < c1; cn++)
-      for (int j = 0; j < 4; j++) {
-        const int32_t f = m->cell_faces[4 * perm[cn] + j];
-        if (stamp[f] == b) continue;
-        stamp[f] = b;
-        std::vector<int32_t> &lst = xidx[f] >= 0 ? ex_f : in_f;
-        local[f] = (int32_t)lst.size();
-        lst.push_back(f);
+    // CTA-local state slot of a cell: own cells first, then the halo
+    auto slot_of = [&](int32_t x) -> int32_t {
+      if (x >= c0 && x < c1) return (int32_t)(x - c0);
+      if (hstamp[x] != b) {
+        hstamp[x] = b;
+        hlocal[x] = nh++;
+        hids.push_back(x);
       }
-    // records of the faces whose cells are all in this block (a boundary face has one)
-    for (int32_t f : in_f) {
-      const int32_t ls = iperm[m->face_id_l[f]] - (int32_t)c0;
-      const int32_t rs = m->face_id_r[f] >= 0 ? iperm[m->face_id_r[f]] - (int32_t)c0 : m->face_id_r[f];
-      frec.push_back(FaceRec{m->face_n[3 * f], m->face_n[3 * f + 1], m->face_n[3 * f + 2], m->face_area[f], ls, rs});
-      gid.push_back(f);
-    }
-    int ni = (int)in_f.size();
-    if (ni & 1) {  // pad to an even count: every CTA's list then starts on a 16-byte boundary
-      frec.push_back(FaceRec{0.0, 0.0, 0.0, 0.0, 0, kFacePad});
-      gid.push_back(-1);
-      ni++;
-    }
-    for (int32_t f : ex_f) xids.push_back(xidx[f]);
-    const int ne = (ni + (int)ex_f.size() + 1) & ~1;  // slots, rounded to keep the cell records 16-byte aligned
-    if (ne > 32767) return fail(rrhd_fail(RRHD_ERR_LIMIT, "CTA face list too long"));
+      return cpb + hlocal[x];
+    };
     for (int64_t cn = c0; cn < c1; cn++) {
       const int32_t co = perm[cn];
-      CellRec &cr = crec[cn];
+      unsigned short s4[4];
       for (int j = 0; j < 4; j++) {
         const int32_t f = m->cell_faces[4 * co + j];
-        const int32_t sl = xidx[f] >= 0 ? ni + local[f] : local[f];
-        cr.s[j] = (uint16_t)(sl | (((m->cell_sign[co] >> j) & 1u) << 15));
+        if (stamp[f] != b) {
+          stamp[f] = b;
+          local[f] = ne++;
+          const int32_t l = iperm[m->face_id_l[f]];
+          const int32_t r = m->face_id_r[f] >= 0 ? iperm[m->face_id_r[f]] : m->face_id_r[f];
+          const int32_t ls = slot_of(l);
+          const int32_t rs = r >= 0 ? slot_of(r) : r;
+          frec.push_back(FaceRec{m->face_n[3 * f], m->face_n[3 * f + 1], m->face_n[3 * f + 2], m->face_area[f],
+                                 ls, rs});
+          gid.push_back((l / cpb == b) ? f : -1);
+        }
+        s4[j] = (unsigned short)local[f];
       }
+      CellRec &cr = crec[cn];
+      for (int j = 0; j < 4; j++)
+        cr.s[j] = (uint16_t)(s4[j] | (((m->cell_sign[co] >> j) & 1u) << 15));
       cr.V = m->cell_volume[co];
     }
+    if (ne & 1) {  // pad to an even count: every CTA's list then starts on a 16-byte boundary
+      frec.push_back(FaceRec{0.0, 0.0, 0.0, 0.0, 0, kFacePad});
+      gid.push_back(-1);
+      ne++;
+    }
+    if (ne > 32767) return fail(rrhd_fail(RRHD_ERR_LIMIT, "CTA face list too long"));
     max_e = std::max(max_e, ne);
-    off[b + 1] = off[b] + ni;
-    xoff[b + 1] = xoff[b] + (int32_t)ex_f.size();
+    max_h = std::max(max_h, nh);
+    off[b + 1] = off[b] + ne;
+    hoff[b + 1] = hoff[b] + nh;
   }
-  c->n_cross = (int64_t)xrec.size();
-  c->n_cross_list = c->n_cross;
+  c->max_halo = max_h;
   c->h_cell_faces.assign(m->cell_faces, m->cell_faces + 4 * N);
   c->h_cell_sign.assign(m->cell_sign, m->cell_sign + N);
   c->h_face_l.assign(m->face_id_l, m->face_id_l + F);
@@ -729,11 +645,9 @@ extern "C" rrhd_status rrhd_create(const rrhd_mesh_desc *m, const rrhd_opts *opt
   c->h_perm = perm;
   if ((st = upload(&c->d_perm, perm)) || (st = upload(&c->d_iperm, iperm)) ||
       (st = upload(&c->d_bface_off, off)) || (st = upload(&c->d_bface_rec, frec)) ||
-      (st = upload(&c->d_bface_gid, gid)) || (st = upload(&c->d_cell_rec, crec)) || (st = upload(&c->d_xoff, xoff)) ||
-      (st = upload(&c->d_xids, xids)) || (st = upload(&c->d_cross_rec, xrec)) || (st = upload(&c->d_cross_gid, xgid)))
+      (st = upload(&c->d_bface_gid, gid)) || (st = upload(&c->d_cell_rec, crec)) || (st = upload(&c->d_halo_off, hoff)) ||
+      (st = upload(&c->d_halo_ids, hids)))
     return fail(st);
-  if (cudaMalloc(&c->d_cross_flux, sizeof(double) * 5 * std::max<int64_t>(c->n_cross, 1)) != cudaSuccess)
-    return fail(rrhd_fail(RRHD_ERR_OOM, "device allocation of the cross-face fluxes failed"));
   const size_t ssz = sizeof(double) * 10 * N;
   if (cudaMalloc(&c->d_state[0], ssz) != cudaSuccess || cudaMalloc(&c->d_state[1], ssz) != cudaSuccess ||
       cudaMalloc(&c->d_status, N) != cudaSuccess || cudaMalloc(&c->d_scal, 2 * sizeof(StepScalars)) != cudaSuccess ||
@@ -746,8 +660,9 @@ extern "C" rrhd_status rrhd_create(const rrhd_mesh_desc *m, const rrhd_opts *opt
   cudaMemcpy(c->d_scal, init, sizeof init, cudaMemcpyHostToDevice);
   c->scal_cur = 0;
   for (int k = 0; k < 8; k++) c->bc.kind[k] = RRHD_BC_TRANSMISSIVE;
-  // staged own states, the CTA's face records (then fluxes) and cross fluxes, cell records, sound speeds
-  const size_t smem = sizeof(double) * (10 * (size_t)cpb + 5 * (size_t)max_e + (size_t)cpb) + sizeof(CellRec) * cpb;
+  // staged states (own + halo), the CTA's face records (then fluxes) and cell records
+  const size_t smem =
+      sizeof(double) * (10 * (size_t)(cpb + max_h) + 5 * (size_t)max_e + (size_t)(cpb + max_h)) + sizeof(CellRec) * cpb;
   c->step_smem = smem;
   if (smem > 227 * 1024)
     return fail(rrhd_fail(RRHD_ERR_LIMIT, "step needs %zu B of shared memory per CTA; lower cells_per_block", smem));
@@ -883,9 +798,9 @@ extern "C" rrhd_status rrhd_hydro_step(rrhd_ctx *c, double tau, rrhd_step_stats 
   P.cpb = c->cpb;
   P.b0 = c->part_b0;
   P.off = c->d_bface_off;
-  P.xoff = c->d_xoff;
-  P.xids = c->d_xids;
-  P.xflux = c->d_cross_flux;
+  P.halo_off = c->d_halo_off;
+  P.halo_ids = c->d_halo_ids;
+  P.max_halo = c->max_halo;
   P.face = c->d_bface_rec;
   P.gid = c->d_bface_gid;
   P.cell = c->d_cell_rec;
@@ -900,24 +815,6 @@ extern "C" rrhd_status rrhd_hydro_step(rrhd_ctx *c, double tau, rrhd_step_stats 
   P.cfl_hmin = c->cfl * c->h_min;
   P.bc = c->bc;
   RRHD_CUDA(cudaMemsetAsync(P.out, 0, sizeof(StepScalars), c->stream));
-  if (c->n_cross_list > 0) {
-    CrossParams X;
-    X.eos = P.eos;
-    X.n = c->n_cross_list;
-    X.list = c->d_cross_list;
-    X.rec = c->d_cross_rec;
-    X.gid = c->d_cross_gid;
-    X.sin = P.sin;
-    X.flux = c->d_cross_flux;
-    X.face_flux = P.face_flux;
-    X.out = P.out;
-    const unsigned nbx = (unsigned)((X.n + 255) / 256);
-    if (P.face_flux)
-      k_cross_flux<true><<<nbx, 256, 0, c->stream>>>(X);
-    else
-      k_cross_flux<false><<<nbx, 256, 0, c->stream>>>(X);
-    RRHD_CUDA(cudaGetLastError());
-  }
   if (P.face_flux)
     k_hydro_step<true><<<c->part_b1 - c->part_b0, kStepThreads, c->step_smem, c->stream>>>(P);
   else
@@ -994,37 +891,14 @@ extern "C" rrhd_status rrhd_hydro_set_part(rrhd_ctx *c, int32_t world, int32_t r
     if (d_rid) cudaFree(d_rid);
     return st;
   }
-  // the cross faces this rank's blocks touch (their fluxes are computed here)
-  const int b0 = (int)(c->nblocks * (int64_t)rank / world), b1 = (int)(c->nblocks * (int64_t)(rank + 1) / world);
-  int32_t *d_xl = nullptr;
-  int64_t nxl = c->n_cross;
-  if (world > 1) {
-    std::vector<int32_t> xoff(c->nblocks + 1), xl;
-    RRHD_CUDA(cudaMemcpy(xoff.data(), c->d_xoff, sizeof(int32_t) * (c->nblocks + 1), cudaMemcpyDeviceToHost));
-    std::vector<int32_t> ids(std::max(xoff[b1] - xoff[b0], 0));
-    if (!ids.empty())
-      RRHD_CUDA(cudaMemcpy(ids.data(), c->d_xids + xoff[b0], sizeof(int32_t) * ids.size(), cudaMemcpyDeviceToHost));
-    std::sort(ids.begin(), ids.end());
-    ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
-    nxl = (int64_t)ids.size();
-    if ((st = upload(&d_xl, ids))) {
-      cudaFree(d_sid);
-      cudaFree(d_rid);
-      if (d_xl) cudaFree(d_xl);
-      return st;
-    }
-  }
   if (c->d_send_ids) cudaFree(c->d_send_ids);
   if (c->d_recv_ids) cudaFree(c->d_recv_ids);
-  if (c->d_cross_list) cudaFree(c->d_cross_list);
   c->d_send_ids = d_sid;
   c->d_recv_ids = d_rid;
-  c->d_cross_list = d_xl;
-  c->n_cross_list = nxl;
   c->part_world = world;
   c->part_rank = rank;
-  c->part_b0 = b0;
-  c->part_b1 = b1;
+  c->part_b0 = (int)(c->nblocks * (int64_t)rank / world);
+  c->part_b1 = (int)(c->nblocks * (int64_t)(rank + 1) / world);
   c->part_c0 = range[0];
   c->part_c1 = range[1];
   c->n_send = ns;

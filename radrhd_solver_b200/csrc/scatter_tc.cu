@@ -14,6 +14,11 @@
 //            the same three products in fp16; B pre-scaled by 2^8
 //   F16    : per-row scaled fp16, one product
 //   BF16   : bf16, one product
+// The scaled forms (F16X3, F16) split the kernel 3 (1 + mu^2) / 4 into its isotropic
+// 3/4 and 3 mu^2 / 4: B carries only the second, and the drain adds 3/4 E_r with
+// E_r = sum_d (a_d / A) I[r][d] summed in FP64 by the row pre-pass, which also forms
+// the ten moments in FP64 (the scaled forms carry no moment columns).  The tensor
+// cores' rounding then scales with the anisotropic part, a quarter to a half of S.
 //
 // The tensor core's FP32 accumulation truncates, so an accumulator that takes
 // every MMA of a long K loop drifts by about one ulp per MMA.  Each chunk of
@@ -28,7 +33,7 @@
 // FP32 intensity tile (brought in by TMA, two chunks ahead) into hi/lo 16-bit
 // tiles written in the UMMA K-major 128B-swizzled layout, warps 10-17 drain
 // the chunk accumulators (tcgen05.ld), sum, unscale and store.  Two smem stages
-// of K = 64 directions.  The row scales of the FP16 forms come from k_row_scale.
+// of K = 64 directions.  The row scales of the FP16 forms come from k_row_prepass.
 // Every mbarrier wait is bounded: on a timeout the kernel records an error
 // word, skips the remaining work, frees its TMEM and returns.
 #include <cuda.h>
@@ -51,6 +56,11 @@ namespace {
 
 constexpr int kForms = 4;
 enum { FORM_BF16X3 = 0, FORM_F16X3 = 1, FORM_F16 = 2, FORM_BF16 = 3 };
+// The Thomson kernel 3 (1 + mu^2) / 4 splits into an isotropic 3/4 and 3 mu^2 / 4.  The
+// scaled forms put only the second part on the tensor cores and add 3/4 E_r (FP64 row
+// integral from the row pre-pass) in the drain: the tensor cores' accumulation error then
+// applies to the smaller part of S only.
+constexpr double kIsoWeight = 0.75;
 
 constexpr int BM = 128;      // rows per CTA (UMMA M)
 constexpr int BK = 64;       // directions per stage (one 128-byte swizzle row of 16-bit values)
@@ -174,6 +184,7 @@ struct TcParams {
   float *S;
   float *mom;          // [rows][16] or null
   const float *scale;  // [rows] power-of-two row scales (scaled forms)
+  const double *erow;  // [rows] FP64 isotropic integrals E_r (scaled forms)
   int64_t rows;
   int M;
   float b_unscale;
@@ -181,55 +192,93 @@ struct TcParams {
   int b_copies;  // copies of the kernel matrix in global memory (resident kernel)
 };
 
-// Row scale for the scaled FP16 forms: 2^(14 - floor(log2(max_d |I[r][d]|))),
-// so that max |s_r I| lies in [2^14, 2^15).  One warp per row, streaming.
-__global__ void k_row_scale(const float *__restrict__ I, int64_t rows, int M, float *__restrict__ scale) {
-  const int64_t r = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (r >= rows) return;
-  const float4 *row = reinterpret_cast<const float4 *>(I + r * M);
-  float m = 0.f;
-  for (int c = lane; c < M / 4; c += 32) {
-    const float4 v = __ldg(row + c);
-    m = fmaxf(m, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+// Per-row pre-pass of the scaled FP16 forms over a cell-direction-group array [cells][M][NG]
+// (NG = 1 is the rows layout [rows][M]); one warp per cell, lane l taking directions
+// l, l + 32, ... with all NG groups of each:
+//   scale  2^(14 - floor(log2(max_d |I[r][d]|))), so that max |s_r I| lies in [2^14, 2^15);
+//   erow   E_r = sum_d (a_d / A) I[r][d] in FP64, the isotropic part of the Thomson
+//          kernel's integral, which the scaled forms add outside the tensor cores;
+//   mom    (MOM) the ten moments in FP64, stored as FP32 [rows][16] (columns 10-15 zero):
+//          the scaled forms take them from here, not from the tensor cores.
+// mw [M][10] holds (a_d / A) {1, wx, wy, wz, wx^2, wx wy, wx wz, wy^2, wy wz, wz^2}
+// (cuda_illum_sep_param.cu:9-69), so each term is one fused multiply-add.  The sums run in
+// one fixed order: per lane in direction order, then lanes l, l ^ 16, l ^ 8, l ^ 24 by
+// shuffles, then the eight lane groups in order through shared memory.
+constexpr int kPrepassWarps = 8;
+template <int NG, bool MOM>
+__global__ void __launch_bounds__(32 * kPrepassWarps) k_row_prepass(const float *__restrict__ I, int64_t cells, int M,
+                                                                  const double *__restrict__ mw,
+                                                                  float *__restrict__ scale, double *__restrict__ erow,
+                                                                  float *__restrict__ mom) {
+  constexpr int NM = MOM ? 10 : 1;
+  __shared__ double red[kPrepassWarps][NG * NM][8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t c = blockIdx.x * (int64_t)kPrepassWarps + warp;
+  if (c >= cells) return;  // whole warps
+  const float *blk = I + c * (int64_t)M * NG;
+  float mx[NG];
+  double m[NG][NM];
+#pragma unroll
+  for (int g = 0; g < NG; g++) {
+    mx[g] = 0.f;
+#pragma unroll
+    for (int k = 0; k < NM; k++) m[g][k] = 0.0;
+  }
+  for (int d = lane; d < M; d += 32) {
+    float v[4];
+    if constexpr (NG == 4) {
+      const float4 x = __ldcs(reinterpret_cast<const float4 *>(blk) + d);
+      v[0] = x.x, v[1] = x.y, v[2] = x.z, v[3] = x.w;
+    } else if constexpr (NG == 2) {
+      const float2 x = __ldcs(reinterpret_cast<const float2 *>(blk) + d);
+      v[0] = x.x, v[1] = x.y;
+    } else {
+      v[0] = __ldcs(blk + d);
+    }
+    double w[NM];
+#pragma unroll
+    for (int k = 0; k < NM; k++) w[k] = __ldg(mw + 10 * d + k);
+#pragma unroll
+    for (int g = 0; g < NG; g++) {
+      mx[g] = fmaxf(mx[g], fabsf(v[g]));
+#pragma unroll
+      for (int k = 0; k < NM; k++) m[g][k] = __fma_rn((double)v[g], w[k], m[g][k]);
+    }
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if (lane == 0) scale[r] = (m > 0.f && isfinite(m)) ? ldexpf(1.f, 14 - ilogbf(m)) : 1.f;
+  for (int g = 0; g < NG; g++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx[g] = fmaxf(mx[g], __shfl_xor_sync(0xffffffffu, mx[g], o));
+#pragma unroll
+    for (int k = 0; k < NM; k++) {
+      m[g][k] += __shfl_xor_sync(0xffffffffu, m[g][k], 16);
+      m[g][k] += __shfl_xor_sync(0xffffffffu, m[g][k], 8);
+      if (lane < 8) red[warp][g * NM + k][lane] = m[g][k];
+    }
+  }
+  __syncwarp();
+  for (int t = lane; t < NG * NM; t += 32) {
+    double r = red[warp][t][0];
+#pragma unroll
+    for (int j = 1; j < 8; j++) r += red[warp][t][j];
+    const int g = t / NM, k = t - g * NM;
+    const int64_t row = c * NG + g;
+    if (k == 0) erow[row] = r;
+    if (MOM) mom[16 * row + k] = (float)r;
+  }
+  if (lane < NG) {
+    float mg = mx[0];
+#pragma unroll
+    for (int g = 1; g < NG; g++)
+      if (lane == g) mg = mx[g];
+    scale[c * NG + lane] = (mg > 0.f && isfinite(mg)) ? ldexpf(1.f, 14 - ilogbf(mg)) : 1.f;
+  }
+  if (MOM && lane >= 32 - 6 * NG) {  // moment columns 10-15 of the cell's rows
+    const int q = lane - (32 - 6 * NG);
+    mom[16 * (c * NG + q / 6) + 10 + q % 6] = 0.f;
+  }
 }
 
-// The same for a cell-direction-group array [cells][M][ng]: one warp per cell,
-// scale[cell * ng + g] from the maximum over the cell's group-g values.
-__global__ void k_row_scale_cdg(const float *__restrict__ I, int64_t cells, int M, int ng,
-                                float *__restrict__ scale) {
-  const int64_t c = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (c >= cells) return;
-  const float4 *blk = reinterpret_cast<const float4 *>(I + c * (int64_t)M * ng);
-  float m[4] = {0.f, 0.f, 0.f, 0.f};  // per float4 component; component q holds group q % ng
-  for (int i = lane; i < M * ng / 4; i += 32) {
-    const float4 v = __ldg(blk + i);
-    m[0] = fmaxf(m[0], fabsf(v.x));
-    m[1] = fmaxf(m[1], fabsf(v.y));
-    m[2] = fmaxf(m[2], fabsf(v.z));
-    m[3] = fmaxf(m[3], fabsf(v.w));
-  }
-#pragma unroll
-  for (int q = 0; q < 4; q++)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m[q] = fmaxf(m[q], __shfl_xor_sync(0xffffffffu, m[q], o));
-  if (lane < ng) {
-    float mg = 0.f;
-    for (int q = lane; q < 4; q += ng) mg = fmaxf(mg, m[q]);
-    scale[c * ng + lane] = (mg > 0.f && isfinite(mg)) ? ldexpf(1.f, 14 - ilogbf(mg)) : 1.f;
-  }
-}
-
-// Persistent: CTA b takes tiles b, b + gridDim.x, ...; tile t covers rows
-// 128 (t / n_nt) .. +127 and output directions 128 (t % n_nt) .. +127.  The
-// chunk counter g runs on across tiles, so smem stages and TMEM accumulators
-// keep cycling and the accumulator warps store one tile while the next is
-// being multiplied.
 template <int FORM, int NG>
 __global__ void __launch_bounds__(THREADS, 1)
     k_scatter_tc(const __grid_constant__ CUtensorMap tm_bh, const __grid_constant__ CUtensorMap tm_bl,
@@ -516,12 +565,19 @@ __global__ void __launch_bounds__(THREADS, 1)
       }
       if (ok && gr < P.rows) {
         const float inv = (SCALED ? 1.f / __ldg(P.scale + gr) : 1.f) * P.b_unscale;
+        const double eiso = SCALED ? __ldg(P.erow + gr) : 0.0;  // the isotropic part, added in FP64
 #pragma unroll
         for (int j = 0; j < MAX_HALF / 4; j++) {
           const int col = c0 + 4 * j;
           if (4 * j < half) {
-            const float4 v = make_float4(run[4 * j] * inv, run[4 * j + 1] * inv, run[4 * j + 2] * inv,
-                                         run[4 * j + 3] * inv);
+            float4 v = make_float4(run[4 * j] * inv, run[4 * j + 1] * inv, run[4 * j + 2] * inv,
+                                   run[4 * j + 3] * inv);
+            if (SCALED && col < nS) {
+              v.x = (float)((double)v.x + kIsoWeight * eiso);
+              v.y = (float)((double)v.y + kIsoWeight * eiso);
+              v.z = (float)((double)v.z + kIsoWeight * eiso);
+              v.w = (float)((double)v.w + kIsoWeight * eiso);
+            }
             if (col < nS) {
               if constexpr (NG > 1) {
                 float *o = P.S + ((gr / NG) * P.M + nt * NT + col) * NG + gr % NG;
@@ -923,6 +979,7 @@ __global__ void __launch_bounds__(R_THREADS, 1)
       const int64_t cell = gr / NG;  // the quad (pair) of lanes holding one cell's groups
       // the row's unscale factor, loaded before the sums arrive
       const float inv = (SCALED ? 1.f / (gr < P.rows ? __ldg(P.scale + gr) : 1.f) : 1.f) * P.b_unscale;
+      const double eiso = (SCALED && gr < P.rows) ? __ldg(P.erow + gr) : 0.0;  // the isotropic part, in FP64
       for (int h = 0; h < n_h && ok; h++) {
         const bool with_mom = (h == 0) && mom;
         const int half = (nS + (with_mom ? NMOM : 0)) >> 1;  // multiple of 8
@@ -978,6 +1035,10 @@ __global__ void __launch_bounds__(R_THREADS, 1)
           const int col = c0 + 4 * j;
           if (4 * j < half) {
             float v[4] = {run[4 * j] * inv, run[4 * j + 1] * inv, run[4 * j + 2] * inv, run[4 * j + 3] * inv};
+            if (SCALED && col < nS) {
+#pragma unroll
+              for (int i = 0; i < 4; i++) v[i] = (float)((double)v[i] + kIsoWeight * eiso);
+            }
             if (col < nS) {
               if constexpr (NG == 4) {
                 // lane (cell, g) holds group g of directions n..n+3 -> lane (cell, p): direction n+p, groups 0..3
@@ -1035,7 +1096,9 @@ struct rrhd_scatter_tc {
   float b_unscale = 1.f;
   int *d_err = nullptr;
   float *d_scale = nullptr;  // row scales of the FP16 forms (grown on demand)
+  double *d_erow = nullptr;  // their FP64 isotropic row integrals (grown with d_scale)
   int64_t scale_cap = 0;
+  double *d_mw = nullptr;    // [M][10] (a_d / A) times the moment weights (pre-pass)
   int num_sms = 148;
 };
 
@@ -1065,7 +1128,8 @@ extern "C" rrhd_status rrhd_scatter_tc_create(const rrhd_dirs *d, int32_t form, 
       if (n < M) {
         const double *wn = &d->h_w[3 * n];
         const double mu = (w[0] * wn[0] + w[1] * wn[1]) + w[2] * wn[2];
-        v = (3. * (1. + mu * mu)) / 4. * d->h_a[dd] / A;
+        // the scaled forms take the anisotropic part only (kIsoWeight E_r is added in FP64)
+        v = (f16 ? 3. * (mu * mu) : 3. * (1. + mu * mu)) / 4. * d->h_a[dd] / A;
       } else {
         const double f[10] = {1.0, w[0], w[1], w[2], w[0] * w[0], w[0] * w[1], w[0] * w[2], w[1] * w[1], w[1] * w[2], w[2] * w[2]};
         const int j = n - M;
@@ -1095,9 +1159,10 @@ extern "C" rrhd_status rrhd_scatter_tc_create(const rrhd_dirs *d, int32_t form, 
   t->copies = (M == 128 || M == 256) ? R_COPIES : 1;
   const size_t bytes = sizeof(uint16_t) * bh.size();
   if (cudaMalloc(&t->d_bh, bytes * t->copies) != cudaSuccess || cudaMalloc(&t->d_bl, bytes * t->copies) != cudaSuccess ||
-      cudaMalloc(&t->d_err, sizeof(int)) != cudaSuccess) {
+      cudaMalloc(&t->d_err, sizeof(int)) != cudaSuccess || cudaMalloc(&t->d_mw, sizeof(double) * 10 * M) != cudaSuccess) {
     cudaFree(t->d_bh);
     cudaFree(t->d_bl);
+    cudaFree(t->d_mw);
     cudaFree(t->d_err);
     delete t;
     return rrhd_fail(RRHD_ERR_OOM, "tensor-core operand allocation failed");
@@ -1107,6 +1172,15 @@ extern "C" rrhd_status rrhd_scatter_tc_create(const rrhd_dirs *d, int32_t form, 
     cudaMemcpy(t->d_bl + (size_t)c * bl.size(), bl.data(), bytes, cudaMemcpyHostToDevice);
   }
   cudaMemset(t->d_err, 0, sizeof(int));
+  {
+    std::vector<double> mw(10 * (size_t)M);
+    for (int dd = 0; dd < M; dd++) {
+      const double aw = d->h_a[dd] / A, x = d->h_w[3 * dd], y = d->h_w[3 * dd + 1], z = d->h_w[3 * dd + 2];
+      const double f[10] = {1.0, x, y, z, x * x, x * y, x * z, y * y, y * z, z * z};
+      for (int k = 0; k < 10; k++) mw[10 * (size_t)dd + k] = aw * f[k];
+    }
+    cudaMemcpy(t->d_mw, mw.data(), sizeof(double) * mw.size(), cudaMemcpyHostToDevice);
+  }
   const CUtensorMapDataType dt = f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
   auto make = [&](CUtensorMap *m, uint16_t *base, int rows_total, int box_rows, int row0) -> bool {
     cuuint64_t dims[2] = {(cuuint64_t)M, (cuuint64_t)rows_total};
@@ -1126,6 +1200,7 @@ extern "C" rrhd_status rrhd_scatter_tc_create(const rrhd_dirs *d, int32_t form, 
     cudaFree(t->d_bl);
     cudaFree(t->d_err);
     delete t;
+    cudaFree(t->d_mw);
     return rrhd_fail(RRHD_ERR_CUDA, "tensor map encoding failed");
   }
   *out = t;
@@ -1139,6 +1214,8 @@ extern "C" rrhd_status rrhd_scatter_tc_destroy(rrhd_scatter_tc *t) {
   cudaFree(t->d_bl);
   cudaFree(t->d_err);
   cudaFree(t->d_scale);
+  cudaFree(t->d_erow);
+  cudaFree(t->d_mw);
   delete t;
   return RRHD_OK;
 }
@@ -1146,7 +1223,7 @@ extern "C" rrhd_status rrhd_scatter_tc_destroy(rrhd_scatter_tc *t) {
 // NG = 1: I, S are [rows][M]; NG = 2, 4: [rows / NG][M][NG] (row = cell * NG + group)
 template <int FORM, int NG>
 static rrhd_status launch_tc(const rrhd_scatter_tc *t, const float *I, float *S, float *mom, int64_t rows,
-                             const float *scales, cudaStream_t st) {
+                             cudaStream_t st) {
   constexpr int ng = NG;
   static bool attr = false;
   if (!attr) {
@@ -1154,14 +1231,18 @@ static rrhd_status launch_tc(const rrhd_scatter_tc *t, const float *I, float *S,
     attr = true;
   }
   constexpr bool SCALED = (FORM == FORM_F16X3 || FORM == FORM_F16);
-  if (SCALED && !scales) {
-    if (ng > 1)
-      k_row_scale_cdg<<<(unsigned)((rows / ng + 7) / 8), 256, 0, st>>>(I, rows / ng, t->M, ng, t->d_scale);
+  if (SCALED) {
+    const int64_t cells = ng > 1 ? rows / ng : rows;  // the rows layout is the one-group case
+    const unsigned nb = (unsigned)((cells + kPrepassWarps - 1) / kPrepassWarps);
+    if (mom)
+      k_row_prepass<NG, true><<<nb, 32 * kPrepassWarps, 0, st>>>(I, cells, t->M, t->d_mw, t->d_scale, t->d_erow, mom);
     else
-      k_row_scale<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(I, rows, t->M, t->d_scale);
+      k_row_prepass<NG, false><<<nb, 32 * kPrepassWarps, 0, st>>>(I, cells, t->M, t->d_mw, t->d_scale, t->d_erow,
+                                                                  nullptr);
     RRHD_CUDA(cudaGetLastError());
   }
-  TcParams P{I, S, mom, scales ? scales : t->d_scale, rows, t->M, t->b_unscale, t->d_err, t->copies};
+  // the scaled forms' moments come from the pre-pass, in FP64
+  TcParams P{I, S, SCALED ? nullptr : mom, t->d_scale, t->d_erow, rows, t->M, t->b_unscale, t->d_err, t->copies};
   // M = 128 or 256: one CTA per 128-row tile and all output columns, converted
   // intensity resident.  Its warpgroups move registers between them (setmaxnreg);
   // the kernel is used only if the registers it is launched with cover the split.
@@ -1203,23 +1284,27 @@ static rrhd_status launch_tc(const rrhd_scatter_tc *t, const float *I, float *S,
 }
 
 static rrhd_status run_tc(const rrhd_scatter_tc *t, const float *I, float *S, float *mom, int64_t rows, int ng,
-                          const float *scales, cudaStream_t st) {
-  if ((t->form == FORM_F16X3 || t->form == FORM_F16) && !scales && t->scale_cap < rows) {
+                          cudaStream_t st) {
+  const bool scaled = t->form == FORM_F16X3 || t->form == FORM_F16;
+  if (scaled && t->scale_cap < rows) {
     rrhd_scatter_tc *tm = const_cast<rrhd_scatter_tc *>(t);
     RRHD_CUDA(cudaStreamSynchronize(st));
     cudaFree(tm->d_scale);
+    cudaFree(tm->d_erow);
     tm->d_scale = nullptr;
+    tm->d_erow = nullptr;
     tm->scale_cap = 0;
     RRHD_CUDA(cudaMalloc(&tm->d_scale, sizeof(float) * rows));
+    RRHD_CUDA(cudaMalloc(&tm->d_erow, sizeof(double) * rows));
     tm->scale_cap = rows;
   }
   RRHD_CHECK_ARG(((uintptr_t)I & 15) == 0 && ((uintptr_t)S & 15) == 0 && ((uintptr_t)mom & 15) == 0,
                  "I, S and moments must be 16-byte aligned");
   switch (t->form * 3 + (ng == 4 ? 2 : ng == 2 ? 1 : 0)) {
 #define RRHD_TC_CASE(F)                                                        \
-  case 3 * F + 0: return launch_tc<F, 1>(t, I, S, mom, rows, scales, st);   \
-  case 3 * F + 1: return launch_tc<F, 2>(t, I, S, mom, rows, scales, st);   \
-  case 3 * F + 2: return launch_tc<F, 4>(t, I, S, mom, rows, scales, st);
+  case 3 * F + 0: return launch_tc<F, 1>(t, I, S, mom, rows, st);   \
+  case 3 * F + 1: return launch_tc<F, 2>(t, I, S, mom, rows, st);   \
+  case 3 * F + 2: return launch_tc<F, 4>(t, I, S, mom, rows, st);
     RRHD_TC_CASE(FORM_BF16X3)
     RRHD_TC_CASE(FORM_F16X3)
     RRHD_TC_CASE(FORM_F16)
@@ -1230,21 +1315,20 @@ static rrhd_status run_tc(const rrhd_scatter_tc *t, const float *I, float *S, fl
 }
 
 rrhd_status rrhd::scatter_tc_cdg(const rrhd_scatter_tc *t, const float *I, float *S, float *mom, int64_t cells,
-                                 int ng, cudaStream_t st, const float *row_scales) {
+                                 int ng, cudaStream_t st) {
   RRHD_CHECK_ARG(t && cells >= 0 && (ng == 1 || ng == 2 || ng == 4), "bad arguments");
   if (cells == 0) return RRHD_OK;
   RRHD_CHECK_ARG(I && S, "null I or S");
-  return run_tc(t, I, S, mom, cells * ng, ng, row_scales, st);
+  return run_tc(t, I, S, mom, cells * ng, ng, st);
 }
 
-bool rrhd::scatter_tc_scaled(const rrhd_scatter_tc *t) { return t->form == FORM_F16X3 || t->form == FORM_F16; }
 
 extern "C" rrhd_status rrhd_scatter_tc_run(const rrhd_scatter_tc *t, const float *I, float *S, float *mom,
                                            int64_t rows, void *stream) {
   RRHD_CHECK_ARG(t && rows >= 0, "bad arguments");
   if (rows == 0) return RRHD_OK;
   RRHD_CHECK_ARG(I && S, "null I or S");
-  return run_tc(t, I, S, mom, rows, 0, nullptr, (cudaStream_t)stream);
+  return run_tc(t, I, S, mom, rows, 0, (cudaStream_t)stream);
 }
 
 extern "C" rrhd_status rrhd_scatter_tc_run_cdg(const rrhd_scatter_tc *t, const float *I, float *S, float *mom,

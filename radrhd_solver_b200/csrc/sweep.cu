@@ -99,7 +99,6 @@ struct SweepArgs {
   const T *rec;   // [N][RW]
   const T *area;  // [N][4] face areas (cell values)
   TV *fv;         // [F][DB][GS] face values (GS >= G, full 32-byte sectors)
-  float *scale_out;  // cell pass: per-(cell, group) power-of-two scales for the FP16 scattering, or NULL
   TV bc;
   int64_t last;
 };
@@ -428,30 +427,6 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T, TV> a, int64_t N) {
 #pragma unroll
       for (int q = 0; q < GT; q++) I[base + q * gs] = out[q];
     }
-    if constexpr (sizeof(TI) == 4) {
-      if (a.scale_out) {
-        // one CTA is one cell (all its directions): the row scales of the FP16
-        // scattering, 2^(14 - floor(log2 max_d |I|)) per group, as the scattering's own
-        // pre-pass would compute them from the same values
-        __shared__ float s_max[256 / 32][GT];
-        float m[GT];
-#pragma unroll
-        for (int q = 0; q < GT; q++) {
-          m[q] = fabsf(out[q]);
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) m[q] = fmaxf(m[q], __shfl_xor_sync(0xffffffffu, m[q], o));
-        }
-        if ((threadIdx.x & 31) == 0)
-#pragma unroll
-          for (int q = 0; q < GT; q++) s_max[threadIdx.x >> 5][q] = m[q];
-        __syncthreads();
-        if (threadIdx.x < GT) {
-          float mg = 0.f;
-          for (int w = 0; w < (int)(blockDim.x >> 5); w++) mg = fmaxf(mg, s_max[w][threadIdx.x]);
-          a.scale_out[c * GT + threadIdx.x] = (mg > 0.f && isfinite(mg)) ? ldexpf(1.f, 14 - ilogbf(mg)) : 1.f;
-        }
-      }
-    }
   } else {
     for (int gg = 0; gg < a.G; gg++) {
       TV fv[4];
@@ -508,18 +483,18 @@ __global__ void k_plan_expand(const uint32_t *cur, int64_t n, int nbd, int shift
 // Source record {k = alpha + betta, betta / k, alpha Q_g / k} of each context cell
 // (rhs_g = alpha Q_g / k + (betta / k) S_g, GetRhsOpt with the division by k
 // distributed) from caller arrays (caller numbering) ...
-template <class T>
-__global__ void k_dyn_from_arrays(int64_t N, int G, int RW, const int32_t *perm, const T *alpha, const T *betta,
-                                  const T *Q, T *rec) {
+template <class T, class TA>
+__global__ void k_dyn_from_arrays(int64_t N, int G, int RW, const int32_t *perm, const TA *alpha, const TA *betta,
+                                  const TA *Q, T *rec) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= N) return;
   const int64_t p = perm[c];
-  const T al = alpha[p], be = betta[p];
+  const T al = (T)alpha[p], be = (T)betta[p];
   T *o = rec + (int64_t)RW * c + Rec<T>::DYN;
   const T k = al + be;
   o[0] = k;
   o[1] = be / k;
-  for (int g = 0; g < G; g++) o[2 + g] = (al * Q[p * G + g]) / k;
+  for (int g = 0; g < G; g++) o[2 + g] = (al * (T)Q[p * G + g]) / k;
 }
 
 // ... or from the solver state: alpha = a rho, betta = b rho, Q_g = B(T) / kRadiation / G.
@@ -755,7 +730,6 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
     a.rec = (const T *)R.d_rec;
     a.area = (const T *)R.d_area;
     a.fv = (TV *)R.d_fv;
-    a.scale_out = R.d_scale;
     a.bc = (TV)R.bc;
     a.last = R.last_cell;
     a.GS = R.GS;
@@ -803,7 +777,7 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
 void rrhd_rad_release(rrhd_ctx *c) {
   RadState &R = c->rad;
   if (R.graph) cudaGraphExecDestroy(R.graph);
-  void *ptrs[] = {R.d_w, R.d_rec, R.d_area, R.d_scale, R.d_plan, R.d_io, R.d_fv, R.d_I, R.d_S, R.d_G4, R.d_mE, R.d_mF, R.d_mT,
+  void *ptrs[] = {R.d_w, R.d_rec, R.d_area, R.d_plan, R.d_io, R.d_fv, R.d_I, R.d_S, R.d_G4, R.d_mE, R.d_mF, R.d_mT,
                   R.d_mom, R.d_cnt};
   for (void *p : ptrs) cudaFree(p);
   for (cudaEvent_t e : R.ev)
@@ -858,11 +832,6 @@ static rrhd_status rad_setup_t(rrhd_ctx *c) {
   for (int q = 0; q < 3 * R.M; q++) w[q] = (T)R.dirs->h_w[q];
   R.last_cell = iperm[N - 1];
   R.GS = sizeof(TV) == 8 ? ((R.G + 3) & ~3) : ((R.G + 7) & ~7);
-  // the cell pass can hand the FP16 scattering its row scales when one CTA covers
-  // every direction of a cell: one batch of 256 directions, float, G in {1, 2, 4}
-  if (sizeof(TI) == 4 && R.nbatch == 1 && R.M == 256 && (R.G == 1 || R.G == 2 || R.G == 4) &&
-      cudaMalloc(&R.d_scale, sizeof(float) * (size_t)N * R.G) != cudaSuccess)
-    return rrhd_fail(RRHD_ERR_OOM, "sweep allocation failed");
   auto up = [&](void **dst, const void *src, size_t bytes) -> rrhd_status {
     if (cudaMalloc(dst, bytes) != cudaSuccess) return rrhd_fail(RRHD_ERR_OOM, "sweep allocation failed");
     RRHD_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
@@ -907,7 +876,7 @@ extern "C" rrhd_status rrhd_rad_setup(rrhd_ctx *c, const rrhd_dirs *dirs, const 
   R.prec = o->precision;
   R.bc = o->boundary_value;
   const rrhd_status s = R.prec == RRHD_RAD_FP64   ? rad_setup_t<double, double, double>(c)
-                        : R.prec == RRHD_RAD_MIXED ? rad_setup_t<float, double, float>(c)
+                        : R.prec == RRHD_RAD_MIXED ? rad_setup_t<double, double, float>(c)
                                                    : rad_setup_t<float, float, float>(c);
   if (s) {
     rrhd_rad_release(c);
@@ -973,10 +942,13 @@ extern "C" rrhd_status rrhd_sweep(rrhd_ctx *c, const void *alpha, const void *be
   RRHD_CUDA(cudaSetDevice(c->device));
   const int64_t N = c->N;
   if (R.prec == RRHD_RAD_FP64)
-    k_dyn_from_arrays<double><<<grid_for(N, 256), 256, 0, c->stream>>>(
+    k_dyn_from_arrays<double, double><<<grid_for(N, 256), 256, 0, c->stream>>>(
         N, R.G, R.RW, c->d_perm, (const double *)alpha, (const double *)betta, (const double *)Q, (double *)R.d_rec);
+  else if (R.prec == RRHD_RAD_MIXED)  // float arrays, double records
+    k_dyn_from_arrays<double, float><<<grid_for(N, 256), 256, 0, c->stream>>>(
+        N, R.G, R.RW, c->d_perm, (const float *)alpha, (const float *)betta, (const float *)Q, (double *)R.d_rec);
   else
-    k_dyn_from_arrays<float><<<grid_for(N, 256), 256, 0, c->stream>>>(
+    k_dyn_from_arrays<float, float><<<grid_for(N, 256), 256, 0, c->stream>>>(
         N, R.G, R.RW, c->d_perm, (const float *)alpha, (const float *)betta, (const float *)Q, (float *)R.d_rec);
   RRHD_CUDA(cudaGetLastError());
   SweepIO io{S, I, c->d_perm, 0};
@@ -1064,7 +1036,7 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
   RadState &R = c->rad;
   if (!R.ready) return rrhd_fail(RRHD_ERR_STATE, "rrhd_rad_setup has not run");
   const bool fp64 = R.prec == RRHD_RAD_FP64;         // intensity and scattering integral in double
-  const bool rec64 = R.prec == RRHD_RAD_FP64;        // records (opacities, sources) in double
+  const bool rec64 = R.prec != RRHD_RAD_FP32;        // records (geometry, opacities, sources) in double
   const bool lowrank = o->scatter == RRHD_SCATTER_LOWRANK;
   RRHD_CHECK_ARG(lowrank || (fp64 ? o->scatter == RRHD_SCATTER_FP64
                                   : (o->scatter >= RRHD_TC_BF16X3 && o->scatter <= RRHD_TC_BF16)),
@@ -1153,8 +1125,7 @@ extern "C" rrhd_status rrhd_coupled_step(rrhd_ctx *c, double tau, const rrhd_cou
     if ((s = scatter_fp64_cdg(R.dirs, (const double *)R.d_I, (double *)R.d_S, N, R.G, false, st))) return s;
     if ((s = moments_fp64_cdg(R.dirs, (const double *)R.d_I, R.d_mE, R.d_mF, R.d_mT, N, R.G, st))) return s;
   } else {
-    const float *scales = (R.d_scale && scatter_tc_scaled(R.tc)) ? R.d_scale : nullptr;
-    if ((s = scatter_tc_cdg(R.tc, (const float *)R.d_I, (float *)R.d_S, R.d_mom, N, R.G, st, scales))) return s;
+    if ((s = scatter_tc_cdg(R.tc, (const float *)R.d_I, (float *)R.d_S, R.d_mom, N, R.G, st))) return s;
   }
   RRHD_CUDA(cudaEventRecord(R.ev[6], st));
   return hstat;
@@ -1171,6 +1142,82 @@ extern "C" rrhd_status rrhd_coupled_phase_ms(rrhd_ctx *c, float *ms) {
   RRHD_CUDA(cudaEventElapsedTime(ms + 1, R.ev[3], R.ev[2]));
   RRHD_CUDA(cudaEventElapsedTime(ms + 2, R.ev[3], R.ev[4]));
   RRHD_CUDA(cudaEventElapsedTime(ms + 3, R.ev[5], R.ev[6]));
+  return RRHD_OK;
+}
+
+namespace {
+// The scattering integral and moments the last coupled step left (FP32, cell-direction-group
+// layout, moments [rows][16]) against their FP64 values from the same FP32 intensity, on
+// every stride-th cell: one thread per (sampled cell, group) loops over the output
+// directions (S relative to itself) and forms the ten moments (F and T relative to E).
+// err: {max S, sum of squared S errors, count, max moments} as doubles, the maxima as the
+// bit patterns of non-negative doubles.
+__global__ void k_coupled_scatter_error(int64_t ncell, int64_t stride, int M, int G, const double *__restrict__ K,
+                                        const double *__restrict__ w, const double *__restrict__ a, double area,
+                                        const float *__restrict__ I, const float *__restrict__ S,
+                                        const float *__restrict__ mom, double *err) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= ncell * G) return;
+  const int64_t c = (t / G) * stride;
+  const int g = (int)(t % G);
+  const float *Ic = I + c * (int64_t)M * G + g;
+  double emax = 0.0, esq = 0.0;
+  for (int o = 0; o < M; o++) {
+    double ref = 0.0;
+    for (int d = 0; d < M; d++) ref += K[(int64_t)d * M + o] * (double)Ic[(int64_t)d * G];  // K[d][o] = Gamma a_d / A
+    const double e = fabs((double)S[(c * M + o) * G + g] - ref) / fabs(ref);
+    if (ref != 0.0) {
+      emax = fmax(emax, e);
+      esq += e * e;
+    }
+  }
+  double m[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int d = 0; d < M; d++) {
+    const double wi = a[d] / area * (double)Ic[(int64_t)d * G];
+    const double x = w[3 * d], y = w[3 * d + 1], z = w[3 * d + 2];
+    const double f[10] = {1.0, x, y, z, x * x, x * y, x * z, y * y, y * z, z * z};
+    for (int k = 0; k < 10; k++) m[k] += f[k] * wi;
+  }
+  double mmax = 0.0;
+  if (mom && m[0] != 0.0) {
+    const float *mr = mom + 16 * (c * G + g);
+    mmax = fabs((double)mr[0] - m[0]) / fabs(m[0]);
+    for (int k = 1; k < 10; k++) mmax = fmax(mmax, fabs((double)mr[k] - m[k]) / fabs(m[0]));
+  }
+  atomicMax(reinterpret_cast<unsigned long long *>(err), (unsigned long long)__double_as_longlong(emax));
+  atomicAdd(err + 1, esq);
+  atomicAdd(err + 2, (double)M);
+  atomicMax(reinterpret_cast<unsigned long long *>(err + 3), (unsigned long long)__double_as_longlong(mmax));
+}
+}  // namespace
+
+extern "C" rrhd_status rrhd_coupled_scatter_error(rrhd_ctx *c, int64_t sample_cells, double *max_rel, double *rms_rel,
+                                                  double *moments_max) {
+  RRHD_CHECK_ARG(c && sample_cells > 0, "bad argument");
+  RadState &R = c->rad;
+  if (!R.ready || !R.d_I) return rrhd_fail(RRHD_ERR_STATE, "no coupled step has run");
+  if (R.prec == RRHD_RAD_FP64) return rrhd_fail(RRHD_ERR_STATE, "the FP64 form has no reduced-precision scattering");
+  RRHD_CUDA(cudaSetDevice(c->device));
+  const int64_t N = c->N;
+  const int64_t stride = std::max<int64_t>(1, N / sample_cells);
+  const int64_t ncell = (N + stride - 1) / stride;
+  double *d_err = nullptr;
+  RRHD_CUDA(cudaMalloc(&d_err, 4 * sizeof(double)));
+  double h[4] = {0, 0, 0, 0};
+  cudaError_t e = cudaMemsetAsync(d_err, 0, 4 * sizeof(double), c->stream);
+  if (e == cudaSuccess) {
+    k_coupled_scatter_error<<<grid_for(ncell * R.G, 128), 128, 0, c->stream>>>(
+        ncell, stride, R.M, R.G, R.dirs->d_K, R.dirs->d_w, R.dirs->d_a, R.dirs->full_area, (const float *)R.d_I,
+        (const float *)R.d_S, R.d_mom, d_err);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h, d_err, sizeof h, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d_err);
+  RRHD_CUDA(e);
+  if (max_rel) *max_rel = h[0];
+  if (rms_rel) *rms_rel = h[2] > 0 ? std::sqrt(h[1] / h[2]) : 0.0;
+  if (moments_max) *moments_max = h[3];
   return RRHD_OK;
 }
 

@@ -97,6 +97,15 @@ class RadRHDStep:
         L.check(L.lib.rrhd_rad_get(self.grid.handle, self._KEYS[what], L.ptr(out)), "rrhd_rad_get")
         return out
 
+    def scatter_error(self, sample_cells: int = 65536):
+        """Accuracy of this step's reduced-precision scattering (rrhd_coupled_scatter_error):
+        (max, rms) relative error of S against FP64 from the same FP32 intensity, and the
+        largest moment error (F, T relative to E), on a sample of cells."""
+        mx, rms, mm = C.c_double(), C.c_double(), C.c_double()
+        L.check(L.lib.rrhd_coupled_scatter_error(self.grid.handle, sample_cells, C.byref(mx), C.byref(rms),
+                                                 C.byref(mm)), "rrhd_coupled_scatter_error")
+        return mx.value, rms.value, mm.value
+
     def set(self, what: str, values):
         """Writes "I" or "S" [N*G, M] (caller numbering)."""
         assert what in ("I", "S")
