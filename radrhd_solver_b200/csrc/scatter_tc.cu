@@ -193,89 +193,84 @@ struct TcParams {
 };
 
 // Per-row pre-pass of the scaled FP16 forms over a cell-direction-group array [cells][M][NG]
-// (NG = 1 is the rows layout [rows][M]); one warp per cell, lane l taking directions
-// l, l + 32, ... with all NG groups of each:
+// (NG = 1 is the rows layout [rows][M]); one thread per row (cell * NG + g), which walks the
+// row's M values in direction order (the loads of a warp's rows share L1 lines, each line
+// serving eight or more steps):
 //   scale  2^(14 - floor(log2(max_d |I[r][d]|))), so that max |s_r I| lies in [2^14, 2^15);
 //   erow   E_r = sum_d (a_d / A) I[r][d] in FP64, the isotropic part of the Thomson
 //          kernel's integral, which the scaled forms add outside the tensor cores;
 //   mom    (MOM) the ten moments in FP64, stored as FP32 [rows][16] (columns 10-15 zero):
 //          the scaled forms take them from here, not from the tensor cores.
-// mw [M][10] holds (a_d / A) {1, wx, wy, wz, wx^2, wx wy, wx wz, wy^2, wy wz, wz^2}
-// (cuda_illum_sep_param.cu:9-69), so each term is one fused multiply-add.  The sums run in
-// one fixed order: per lane in direction order, then lanes l, l ^ 16, l ^ 8, l ^ 24 by
-// shuffles, then the eight lane groups in order through shared memory.
-constexpr int kPrepassWarps = 8;
+// mw [10][M] holds (a_d / A) {1, wx, wy, wz, wx^2, wx wy, wx wz, wy^2, wy wz, wz^2}
+// (cuda_illum_sep_param.cu:9-69), staged in shared memory direction-major; each term is one
+// fused multiply-add, summed in direction order.
 template <int NG, bool MOM>
-__global__ void __launch_bounds__(32 * kPrepassWarps) k_row_prepass(const float *__restrict__ I, int64_t cells, int M,
-                                                                  const double *__restrict__ mw,
-                                                                  float *__restrict__ scale, double *__restrict__ erow,
-                                                                  float *__restrict__ mom) {
+__global__ void __launch_bounds__(256) k_row_prepass(const float *__restrict__ I, int64_t rows, int M,
+                                                     const double *__restrict__ mw, float *__restrict__ scale,
+                                                     double *__restrict__ erow, float *__restrict__ mom) {
   constexpr int NM = MOM ? 10 : 1;
-  __shared__ double red[kPrepassWarps][NG * NM][8];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t c = blockIdx.x * (int64_t)kPrepassWarps + warp;
-  if (c >= cells) return;  // whole warps
-  const float *blk = I + c * (int64_t)M * NG;
-  float mx[NG];
-  double m[NG][NM];
-#pragma unroll
-  for (int g = 0; g < NG; g++) {
-    mx[g] = 0.f;
-#pragma unroll
-    for (int k = 0; k < NM; k++) m[g][k] = 0.0;
+  extern __shared__ double2 smw2[];  // [M][NM] (direction-major here: one direction's weights
+  double *smw = reinterpret_cast<double *>(smw2);  // are read as NM / 2 16-byte loads)
+  for (int q = threadIdx.x; q < NM * M; q += blockDim.x) {
+    const int k = q / M, d = q - k * M;
+    smw[d * NM + k] = __ldg(mw + q);
   }
-  for (int d = lane; d < M; d += 32) {
-    float v[4];
-    if constexpr (NG == 4) {
-      const float4 x = __ldcs(reinterpret_cast<const float4 *>(blk) + d);
-      v[0] = x.x, v[1] = x.y, v[2] = x.z, v[3] = x.w;
-    } else if constexpr (NG == 2) {
-      const float2 x = __ldcs(reinterpret_cast<const float2 *>(blk) + d);
-      v[0] = x.x, v[1] = x.y;
+  __syncthreads();
+  auto weights = [&](int d, double (&w)[NM]) {
+    if constexpr (MOM) {
+#pragma unroll
+      for (int j = 0; j < NM / 2; j++) {
+        const double2 x = smw2[d * (NM / 2) + j];
+        w[2 * j] = x.x;
+        w[2 * j + 1] = x.y;
+      }
     } else {
-      v[0] = __ldcs(blk + d);
+      w[0] = smw[d];
     }
-    double w[NM];
+  };
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t cell = r / NG;
+    const int g = (int)(r - cell * NG);
+    float mx = 0.f;
+    double m[NM];
 #pragma unroll
-    for (int k = 0; k < NM; k++) w[k] = __ldg(mw + 10 * d + k);
+    for (int k = 0; k < NM; k++) m[k] = 0.0;
+    if constexpr (NG == 1) {
+      const float4 *row = reinterpret_cast<const float4 *>(I + r * M);
+#pragma unroll 2
+      for (int d4 = 0; d4 < M / 4; d4++) {
+        const float4 x = __ldg(row + d4);
+        const float v[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
-    for (int g = 0; g < NG; g++) {
-      mx[g] = fmaxf(mx[g], fabsf(v[g]));
+        for (int q = 0; q < 4; q++) {
+          double w[NM];
+          weights(4 * d4 + q, w);
+          mx = fmaxf(mx, fabsf(v[q]));
 #pragma unroll
-      for (int k = 0; k < NM; k++) m[g][k] = __fma_rn((double)v[g], w[k], m[g][k]);
+          for (int k = 0; k < NM; k++) m[k] = __fma_rn((double)v[q], w[k], m[k]);
+        }
+      }
+    } else {
+      const float *row = I + cell * (int64_t)M * NG + g;
+#pragma unroll 4
+      for (int d = 0; d < M; d++) {
+        const float v = __ldg(row + (int64_t)d * NG);
+        double w[NM];
+        weights(d, w);
+        mx = fmaxf(mx, fabsf(v));
+#pragma unroll
+        for (int k = 0; k < NM; k++) m[k] = __fma_rn((double)v, w[k], m[k]);
+      }
     }
-  }
-#pragma unroll
-  for (int g = 0; g < NG; g++) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx[g] = fmaxf(mx[g], __shfl_xor_sync(0xffffffffu, mx[g], o));
-#pragma unroll
-    for (int k = 0; k < NM; k++) {
-      m[g][k] += __shfl_xor_sync(0xffffffffu, m[g][k], 16);
-      m[g][k] += __shfl_xor_sync(0xffffffffu, m[g][k], 8);
-      if (lane < 8) red[warp][g * NM + k][lane] = m[g][k];
+    scale[r] = (mx > 0.f && isfinite(mx)) ? ldexpf(1.f, 14 - ilogbf(mx)) : 1.f;
+    erow[r] = m[0];
+    if (MOM) {
+      float4 *o = reinterpret_cast<float4 *>(mom + 16 * r);
+      o[0] = make_float4((float)m[0], (float)m[1], (float)m[2], (float)m[3]);
+      o[1] = make_float4((float)m[4], (float)m[5], (float)m[6], (float)m[7]);
+      o[2] = make_float4((float)m[8], (float)m[9], 0.f, 0.f);
+      o[3] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
-  }
-  __syncwarp();
-  for (int t = lane; t < NG * NM; t += 32) {
-    double r = red[warp][t][0];
-#pragma unroll
-    for (int j = 1; j < 8; j++) r += red[warp][t][j];
-    const int g = t / NM, k = t - g * NM;
-    const int64_t row = c * NG + g;
-    if (k == 0) erow[row] = r;
-    if (MOM) mom[16 * row + k] = (float)r;
-  }
-  if (lane < NG) {
-    float mg = mx[0];
-#pragma unroll
-    for (int g = 1; g < NG; g++)
-      if (lane == g) mg = mx[g];
-    scale[c * NG + lane] = (mg > 0.f && isfinite(mg)) ? ldexpf(1.f, 14 - ilogbf(mg)) : 1.f;
-  }
-  if (MOM && lane >= 32 - 6 * NG) {  // moment columns 10-15 of the cell's rows
-    const int q = lane - (32 - 6 * NG);
-    mom[16 * (c * NG + q / 6) + 10 + q % 6] = 0.f;
   }
 }
 
@@ -1098,7 +1093,7 @@ struct rrhd_scatter_tc {
   float *d_scale = nullptr;  // row scales of the FP16 forms (grown on demand)
   double *d_erow = nullptr;  // their FP64 isotropic row integrals (grown with d_scale)
   int64_t scale_cap = 0;
-  double *d_mw = nullptr;    // [M][10] (a_d / A) times the moment weights (pre-pass)
+  double *d_mw = nullptr;    // [10][M] (a_d / A) times the moment weights (pre-pass)
   int num_sms = 148;
 };
 
@@ -1177,7 +1172,7 @@ extern "C" rrhd_status rrhd_scatter_tc_create(const rrhd_dirs *d, int32_t form, 
     for (int dd = 0; dd < M; dd++) {
       const double aw = d->h_a[dd] / A, x = d->h_w[3 * dd], y = d->h_w[3 * dd + 1], z = d->h_w[3 * dd + 2];
       const double f[10] = {1.0, x, y, z, x * x, x * y, x * z, y * y, y * z, z * z};
-      for (int k = 0; k < 10; k++) mw[10 * (size_t)dd + k] = aw * f[k];
+      for (int k = 0; k < 10; k++) mw[(size_t)k * M + dd] = aw * f[k];
     }
     cudaMemcpy(t->d_mw, mw.data(), sizeof(double) * mw.size(), cudaMemcpyHostToDevice);
   }
@@ -1232,13 +1227,19 @@ static rrhd_status launch_tc(const rrhd_scatter_tc *t, const float *I, float *S,
   }
   constexpr bool SCALED = (FORM == FORM_F16X3 || FORM == FORM_F16);
   if (SCALED) {
-    const int64_t cells = ng > 1 ? rows / ng : rows;  // the rows layout is the one-group case
-    const unsigned nb = (unsigned)((cells + kPrepassWarps - 1) / kPrepassWarps);
-    if (mom)
-      k_row_prepass<NG, true><<<nb, 32 * kPrepassWarps, 0, st>>>(I, cells, t->M, t->d_mw, t->d_scale, t->d_erow, mom);
-    else
-      k_row_prepass<NG, false><<<nb, 32 * kPrepassWarps, 0, st>>>(I, cells, t->M, t->d_mw, t->d_scale, t->d_erow,
-                                                                  nullptr);
+    const unsigned nb = (unsigned)std::min<int64_t>((rows + 255) / 256, 8 * t->num_sms);
+    const size_t wbytes = sizeof(double) * (mom ? 10 : 1) * t->M;  // <= 80 KiB (M <= 1024)
+    if (mom) {
+      static bool attr = false;
+      if (!attr) {
+        RRHD_CUDA(cudaFuncSetAttribute(k_row_prepass<NG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(sizeof(double) * 10 * 1024)));
+        attr = true;
+      }
+      k_row_prepass<NG, true><<<nb, 256, wbytes, st>>>(I, rows, t->M, t->d_mw, t->d_scale, t->d_erow, mom);
+    } else {
+      k_row_prepass<NG, false><<<nb, 256, wbytes, st>>>(I, rows, t->M, t->d_mw, t->d_scale, t->d_erow, nullptr);
+    }
     RRHD_CUDA(cudaGetLastError());
   }
   // the scaled forms' moments come from the pre-pass, in FP64
