@@ -556,6 +556,28 @@ rrhd_status rrhd_coupled_phase_ms(rrhd_ctx *ctx, float *ms4);
 #define RRHD_RAD_G4 2
 #define RRHD_RAD_MOM 3
 rrhd_status rrhd_rad_get(rrhd_ctx *ctx, int32_t what, double *out);
+/* Pieces of the coupled step on caller arrays, for a step composed over ranks
+ * (rad_rhd::RunRadRHDMpiModule, solvers/RadRHD/src/radRHD_mpi_main.cpp:107-122), where each
+ * rank runs them on its share of cells or rows.  Device pointers; W, U [n][stride] with the
+ * five primitives / conservatives first.
+ *   rrhd_rad_opacities       alpha = absorption rho, betta = scattering rho, Q [n][groups]
+ *                            = B(T) / rad_unit / groups (the coupled step's rule)
+ *   rrhd_rad_source_rows     the 4-force G4 [n][4] of each cell from the FP64 moments of its
+ *                            groups' rows (E [n groups], F [n groups][3], T [n groups][9], as
+ *                            rrhd_moments_fp64 writes them), summed over the groups
+ *   rrhd_rad_source_con2prim U.E += tau G0, U.S += tau G[1..3], then GetPhysValueStab from its
+ *                            own guess without fallback (the coupled step's source update);
+ *                            stats (may be NULL) synchronise the stream. */
+rrhd_status rrhd_rad_opacities(const rrhd_emission *em, const double *W, int64_t stride, int64_t n,
+                               double absorption, double scattering, int32_t groups, double *alpha,
+                               double *betta, double *Q, void *stream);
+rrhd_status rrhd_rad_source_rows(const rrhd_emission *em, const double *W, int64_t stride, int64_t n,
+                                 double absorption, double scattering, int32_t groups, const double *E,
+                                 const double *F, const double *T, double *G4, void *stream);
+rrhd_status rrhd_rad_source_con2prim(int32_t eos, double gamma, double *U, double *W, int64_t stride,
+                                     const double *G4, double tau, int64_t n, rrhd_c2p_stats *stats,
+                                     void *stream);
+
 /* Accuracy of the reduced-precision scattering of the last coupled step (FP32 or
  * mixed sweep precision; not FP64): on every (N / sample_cells)-th cell, the FP32
  * scattering integral against its FP64 value from the same FP32 intensity (per

@@ -156,6 +156,9 @@ _SIGS = {
     "rrhd_rad_get": (I32, [P, I32, P]),
     "rrhd_rad_set": (I32, [P, I32, P]),
     "rrhd_coupled_scatter_error": (I32, [P, I64, P, P, P]),
+    "rrhd_rad_opacities": (I32, [P, P, I64, I64, D, D, I32, P, P, P, P]),
+    "rrhd_rad_source_rows": (I32, [P, P, I64, I64, D, D, I32, P, P, P, P, P]),
+    "rrhd_rad_source_con2prim": (I32, [I32, D, P, P, I64, P, D, I64, P, P]),
     "rrhd_coupled_phase_ms": (I32, [P, P]),
     "rrhd_scatter_fp64_cdg": (I32, [P, P, P, I64, I32, I32, P]),
     "rrhd_moments_fp64_cdg": (I32, [P, P, P, P, P, I64, I32, P]),

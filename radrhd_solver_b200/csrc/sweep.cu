@@ -1221,6 +1221,151 @@ extern "C" rrhd_status rrhd_coupled_scatter_error(rrhd_ctx *c, int64_t sample_ce
   return RRHD_OK;
 }
 
+// ---------------------------------------------------------------- caller-array pieces of the coupled step
+// (for a step composed over ranks, where each piece runs on a rank's share of cells or rows)
+namespace {
+// alpha = a rho, betta = b rho, Q_g = B(T) / kRadiation / G from primitives W [n][stride]
+// (the opacity and emission rule of the coupled step, as k_dyn_from_state forms them).
+__global__ void k_rad_opacities(int64_t n, int64_t stride, int G, const double *W, double a_coef, double b_coef,
+                                Emission em, double *alpha, double *betta, double *Q) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const double rho = W[stride * c], prs = W[stride * c + 4];
+  alpha[c] = a_coef * rho;
+  betta[c] = b_coef * rho;
+  const double q = planck_B(em, rho, prs) / em.rad_unit / (double)G;
+  for (int g = 0; g < G; g++) Q[c * G + g] = q;
+}
+
+// 4-force per cell from the FP64 moments of its G rows (E [n G], F [n G][3], T [n G][9]),
+// summed over the groups in order as k_source does.
+__global__ void k_rad_source_rows(int64_t n, int64_t stride, int G, const double *W, double a_coef, double b_coef,
+                                  Emission em, const double *mE, const double *mF, const double *mT, double *G4) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  double E = 0, F[3] = {0, 0, 0}, Tm[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int g = 0; g < G; g++) {
+    const int64_t r = c * G + g;
+    E += mE[r];
+#pragma unroll
+    for (int q = 0; q < 3; q++) F[q] += mF[3 * r + q];
+#pragma unroll
+    for (int q = 0; q < 9; q++) Tm[q] += mT[9 * r + q];
+  }
+  double w[5];
+#pragma unroll
+  for (int q = 0; q < 5; q++) w[q] = W[stride * c + q];
+  double out[4];
+  rad_source_cell(em, w, a_coef * w[0], b_coef * w[0], E, F, Tm, out);
+#pragma unroll
+  for (int q = 0; q < 4; q++) G4[4 * c + q] = out[q];
+}
+
+// U.E += tau G0, U.S += tau G (radRHD_main.cpp:117-126), then GetPhysValueStab from its own
+// guess without fallback, on caller arrays; cnt as in k_source_c2p.
+__global__ void k_rad_source_c2p(int64_t n, int64_t stride, Eos eos, double *U, double *W, const double *G4,
+                                 double tau, unsigned long long *cnt) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  unsigned long long ok = 0, failed = 0, iters = 0;
+  if (c < n) {
+    double u[5], w[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+      u[q] = U[stride * c + q];
+      w[q] = W[stride * c + q];
+    }
+    u[4] += tau * G4[4 * c];
+    u[1] += tau * G4[4 * c + 1];
+    u[2] += tau * G4[4 * c + 2];
+    u[3] += tau * G4[4 * c + 3];
+    int it = 0;
+    const int code = c2p_from(eos, u, w, 0.0, false, &it);
+    ok = code == 0;
+    failed = code != 0;
+    iters = (unsigned long long)it;
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+      U[stride * c + q] = u[q];
+      W[stride * c + q] = w[q];
+    }
+  }
+  unsigned long long mx = iters;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ok += __shfl_xor_sync(0xffffffffu, ok, o);
+    failed += __shfl_xor_sync(0xffffffffu, failed, o);
+    iters += __shfl_xor_sync(0xffffffffu, iters, o);
+    const unsigned long long m2 = __shfl_xor_sync(0xffffffffu, mx, o);
+    mx = m2 > mx ? m2 : mx;
+  }
+  if ((threadIdx.x & 31) == 0 && (ok | failed)) {
+    atomicAdd(cnt + 0, ok);
+    atomicAdd(cnt + 1, failed);
+    atomicAdd(cnt + 2, iters);
+    atomicMax(cnt + 3, mx);
+  }
+}
+}  // namespace
+
+extern "C" rrhd_status rrhd_rad_opacities(const rrhd_emission *em, const double *W, int64_t stride, int64_t n,
+                                          double absorption, double scattering, int32_t groups, double *alpha,
+                                          double *betta, double *Q, void *stream) {
+  RRHD_CHECK_ARG(em && W && alpha && betta && Q && n >= 0 && stride >= 5 && groups >= 1, "bad arguments");
+  if (n == 0) return RRHD_OK;
+  const Emission e{em->temp_coef, em->sigma_sb, em->pi, em->rad_unit};
+  k_rad_opacities<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(n, stride, groups, W, absorption, scattering, e,
+                                                                      alpha, betta, Q);
+  RRHD_CUDA(cudaGetLastError());
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_rad_source_rows(const rrhd_emission *em, const double *W, int64_t stride, int64_t n,
+                                            double absorption, double scattering, int32_t groups, const double *E,
+                                            const double *F, const double *T, double *G4, void *stream) {
+  RRHD_CHECK_ARG(em && W && E && F && T && G4 && n >= 0 && stride >= 5 && groups >= 1, "bad arguments");
+  if (n == 0) return RRHD_OK;
+  const Emission e{em->temp_coef, em->sigma_sb, em->pi, em->rad_unit};
+  k_rad_source_rows<<<grid_for(n, 128), 128, 0, (cudaStream_t)stream>>>(n, stride, groups, W, absorption, scattering,
+                                                                        e, E, F, T, G4);
+  RRHD_CUDA(cudaGetLastError());
+  return RRHD_OK;
+}
+
+extern "C" rrhd_status rrhd_rad_source_con2prim(int32_t eos, double gamma, double *U, double *W, int64_t stride,
+                                                const double *G4, double tau, int64_t n, rrhd_c2p_stats *stats,
+                                                void *stream) {
+  RRHD_CHECK_ARG(U && W && G4 && n >= 0 && stride >= 5 && (eos == 1 || eos == 2), "bad arguments");
+  if (n == 0) {
+    if (stats) *stats = rrhd_c2p_stats{0, 0, 0, 0, 0};
+    return RRHD_OK;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  Eos e;
+  e.eos = eos;
+  e.g1 = gamma;
+  e.gg = gamma / (gamma - 1.0);
+  unsigned long long *cnt = nullptr;
+  RRHD_CUDA(cudaMallocAsync(&cnt, 4 * sizeof(unsigned long long), st));
+  cudaError_t err = cudaMemsetAsync(cnt, 0, 4 * sizeof(unsigned long long), st);
+  if (err == cudaSuccess) {
+    k_rad_source_c2p<<<grid_for(n, 256), 256, 0, st>>>(n, stride, e, U, W, G4, tau, cnt);
+    err = cudaGetLastError();
+  }
+  unsigned long long h[4] = {0, 0, 0, 0};
+  if (err == cudaSuccess && stats) err = cudaMemcpyAsync(h, cnt, sizeof h, cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(cnt, st);
+  if (err == cudaSuccess && stats) err = cudaStreamSynchronize(st);
+  RRHD_CUDA(err);
+  if (stats) {
+    stats->n_ok = (int64_t)h[0];
+    stats->n_fallback = 0;
+    stats->n_failed = (int64_t)h[1];
+    stats->newton_iters = (int64_t)h[2];
+    stats->max_iters = (int32_t)h[3];
+  }
+  return RRHD_OK;
+}
+
 extern "C" rrhd_status rrhd_rad_get(rrhd_ctx *c, int32_t what, double *out) {
   RRHD_CHECK_ARG(c && out, "null argument");
   RadState &R = c->rad;

@@ -44,15 +44,20 @@ class DirectionShard:
     """Direction split of M directions and row split of `rows` rows (cell * G + g) over the
     ranks of `group`; the two transposes between them."""
 
-    def __init__(self, rows: int, M: int, group=None):
+    def __init__(self, rows: int, M: int, group=None, unit: int = 1):
+        """unit: rows are split in whole blocks of `unit` (the G group rows of one cell, so
+        that a rank's rows are whole cells)."""
         self.group = group
         self.world = dist.get_world_size(group)
         self.rank = dist.get_rank(group)
-        if self.world > M or self.world > rows:
+        if rows % unit:
+            raise ValueError(f"{rows} rows are not whole blocks of {unit}")
+        if self.world > M or self.world > rows // unit:
             raise ValueError(f"{self.world} ranks for {M} directions and {rows} rows")
-        self.rows, self.M = rows, M
+        self.rows, self.M, self.unit = rows, M, unit
         self.dir_counts, self.dir_disp = GetSend(self.world, M), GetDisp(self.world, M)
-        self.row_counts, self.row_disp = GetSend(self.world, rows), GetDisp(self.world, rows)
+        self.row_counts = [c * unit for c in GetSend(self.world, rows // unit)]
+        self.row_disp = [c * unit for c in GetDisp(self.world, rows // unit)]
 
     @property
     def my_dirs(self):
