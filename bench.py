@@ -441,15 +441,16 @@ EM_JET = (1.0, 10.0, float(np.pi), 1.0)  # temp_coef, a_R, pi, kRadiation in cod
 
 
 def coupled_component(dev, m, W, steps=100, warm=1, M=256, G=4, train_epochs=2, forms=("plain", "chosen"),
-                      batch=(128, 256)):
+                      batch=(128, 256), item_geometry=True):
     """Config-4 coupled radiation-hydro jet step (radRHD_main.cpp:96-139) on the
     benchmark mesh: hydro step, opacities alpha = rho, betta = 0.5 rho, emission
     Q = a_R T^4 / pi / G per grey group, sweep of M directions x G groups,
     4-force + source con2prim, scattering integral + moments.  Plain form: FP64
     sweep, FP64 scattering (one FMA per term), reference con2prim guess.  Chosen
     form: mixed-precision sweep (FP64 arithmetic and face values, FP32 intensity
-    and scattering integral), tensor-core F16X3 scattering, learned con2prim guess
-    trained on the plain run's own states.  "plain_lowrank" / "chosen_lowrank": the
+    and scattering integral; with item_geometry, each (cell, direction) item's
+    geometry precomputed at setup and streamed), tensor-core F16X3 scattering,
+    learned con2prim guess trained on the plain run's own states.  "plain_lowrank" / "chosen_lowrank": the
     same with the scattering through the rank-7 Thomson identity (FP64 arithmetic).
     All forms start from the same state; the intensity arrays (N*G*M = 5.4e9
     values) are far larger than L2."""
@@ -472,8 +473,9 @@ def coupled_component(dev, m, W, steps=100, warm=1, M=256, G=4, train_epochs=2, 
         g.set_state_prim(W)
         dg = illum.DirectionGrid(d, dev)
         t0 = time.perf_counter()
+        geo = item_geometry and not fp64
         sw = illum.TransportSweep(g, dg, groups=G, precision="fp64" if fp64 else "mixed",
-                                  dirs_per_batch=batch[0] if fp64 else batch[1])
+                                  dirs_per_batch=batch[0] if fp64 else batch[1], item_geometry=geo)
         t_plan = time.perf_counter() - t0
         if not fp64 and net is None and "plain_dump" in states:
             Wp, Up = states["plain_dump"]
@@ -512,7 +514,9 @@ def coupled_component(dev, m, W, steps=100, warm=1, M=256, G=4, train_epochs=2, 
             states["plain_dump"] = (Wg, Ug)
         bio = 8 if fp64 else 4  # bytes per intensity / scattering value; face values are double
         sweep_alg = (2.0 * m.n_cells * bio + 2.0 * m.n_faces * 8) * M * G + m.n_cells * (20 * 8 + 32.0)
-        out[form] = {"dirs_per_batch": batch[0] if fp64 else batch[1], "ms_per_step": ms, "steps_per_s": 1e3 / ms, "cell_updates_per_s": m.n_cells / (ms / 1e3),
+        if geo:
+            sweep_alg += 16.0 * m.n_cells * M  # the item-geometry stream
+        out[form] = {"dirs_per_batch": batch[0] if fp64 else batch[1], "item_geometry": geo, "ms_per_step": ms, "steps_per_s": 1e3 / ms, "cell_updates_per_s": m.n_cells / (ms / 1e3),
                      "cell_dir_group_per_s": m.n_cells * M * G / (ms / 1e3), "phase_ms_last_step": ph,
                      "sweep_levels": levels, "largest_level": biggest, "plan_build_s": t_plan,
                      "scatter_op_error": scat_err,
@@ -781,7 +785,8 @@ def run_ours(args):
     g.close()
     if rank == 0 and not args.no_coupled:
         line["coupled"] = coupled_component(dev, m, W, steps=args.coupled_steps,
-                                            batch=tuple(int(x) for x in args.coupled_batch.split(",")))
+                                            batch=tuple(int(x) for x in args.coupled_batch.split(",")),
+                                            item_geometry=bool(args.coupled_item_geometry))
     if rank == 0 and not args.no_cpu:
         import oracle
         threads = cpu_threads()
@@ -835,6 +840,8 @@ def main():
                     help="only time the coupled step on an NHEX^3 x 6 jet mesh (profiling runs)")
     ap.add_argument("--coupled-forms", default="plain,chosen", help="forms of --coupled-only")
     ap.add_argument("--coupled-batch", default="128,256", help="directions per sweep batch (plain,chosen)")
+    ap.add_argument("--coupled-item-geometry", type=int, default=1,
+                    help="chosen forms: stream the precomputed per-item sweep geometry (1) or not (0)")
     ap.add_argument("--c2p-only", type=int, default=0, metavar="STATES",
                     help="only time the con2prim component on STATES states (profiling runs)")
     ap.add_argument("--no-compton", action="store_true", help="skip the full-spectrum Compton component")
@@ -879,7 +886,8 @@ def main():
         m, W = make_jet(args.coupled_only)
         print(json.dumps(coupled_component(0, m, W, steps=args.coupled_steps,
                                            forms=tuple(args.coupled_forms.split(",")),
-                                           batch=tuple(int(x) for x in args.coupled_batch.split(",")))), flush=True)
+                                           batch=tuple(int(x) for x in args.coupled_batch.split(",")),
+                                           item_geometry=bool(args.coupled_item_geometry))), flush=True)
         return
     if args.sweep_only:
         import torch

@@ -493,6 +493,14 @@ typedef struct {
                              kept for them): power of two <= 256; 0 = min(64, M)                */
   double boundary_value;  /* intensity entering through boundary faces (illum::BoundaryConditions
                              returns 0 for free, lock and outer boundaries, illum_utils.cpp:52-65) */
+  int32_t item_geometry;  /* 1: precompute at setup, per (cell, direction) item in sweep order, which
+                             faces are in- and out-faces, the in-face each interpolation node is
+                             traced to and the in-face distances H_f / -cos_f (16 bytes per item,
+                             cells x directions x 16 bytes of device memory); the sweep then reads
+                             that stream in order instead of each item's cell normals and heights.
+                             RRHD_RAD_FP32 and RRHD_RAD_MIXED only: the distances are stored as
+                             float (FP32: the same values; MIXED: the double distance rounded
+                             once, every choice made in double).  0: off                         */
 } rrhd_rad_opts;
 /* Builds the sweep geometry and plan for ctx's mesh and the direction set (which
  * must outlive the context's radiation use).  RRHD_ERR_STATE if the mesh has a

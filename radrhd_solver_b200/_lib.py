@@ -84,7 +84,8 @@ RRHD_RAD_MOM = 3
 
 
 class RadOpts(C.Structure):
-    _fields_ = [("groups", I32), ("precision", I32), ("dirs_per_batch", I32), ("boundary_value", D)]
+    _fields_ = [("groups", I32), ("precision", I32), ("dirs_per_batch", I32), ("boundary_value", D),
+                ("item_geometry", I32)]
 
 
 class CoupledOpts(C.Structure):

@@ -76,6 +76,8 @@ struct RadState {
   void *d_rec = nullptr;
   void *d_area = nullptr;  // [N][4] face areas
   uint32_t *d_plan = nullptr;               // all batches: items (cell << shift | d) in level order
+  bool item_geometry = false;
+  uint4 *d_geo = nullptr;                   // item_geometry: per plan item {code, in-face distances}
   std::vector<std::vector<int64_t>> lvl;    // per batch: level offsets into d_plan
   int64_t levels = 0, max_level = 0;
   cudaGraphExec_t graph = nullptr;          // every level launch of one sweep

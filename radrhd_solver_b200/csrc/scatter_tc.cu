@@ -193,9 +193,9 @@ struct TcParams {
 };
 
 // Per-row pre-pass of the scaled FP16 forms over a cell-direction-group array [cells][M][NG]
-// (NG = 1 is the rows layout [rows][M]); one thread per row (cell * NG + g), which walks the
-// row's M values in direction order (the loads of a warp's rows share L1 lines, each line
-// serving eight or more steps):
+// (NG = 1 is the rows layout [rows][M]); one thread per cell, which walks the cell's M
+// directions in order with its NG group values as one vector load (the loads of a warp's
+// cells share L1 lines, each line serving two or more steps):
 //   scale  2^(14 - floor(log2(max_d |I[r][d]|))), so that max |s_r I| lies in [2^14, 2^15);
 //   erow   E_r = sum_d (a_d / A) I[r][d] in FP64, the isotropic part of the Thomson
 //          kernel's integral, which the scaled forms add outside the tensor cores;
@@ -228,15 +228,18 @@ __global__ void __launch_bounds__(256) k_row_prepass(const float *__restrict__ I
       w[0] = smw[d];
     }
   };
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t cell = r / NG;
-    const int g = (int)(r - cell * NG);
-    float mx = 0.f;
-    double m[NM];
+  const int64_t cells = rows / NG;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < cells; c += (int64_t)gridDim.x * blockDim.x) {
+    float mx[NG];
+    double m[NG][NM];
 #pragma unroll
-    for (int k = 0; k < NM; k++) m[k] = 0.0;
+    for (int g = 0; g < NG; g++) {
+      mx[g] = 0.f;
+#pragma unroll
+      for (int k = 0; k < NM; k++) m[g][k] = 0.0;
+    }
     if constexpr (NG == 1) {
-      const float4 *row = reinterpret_cast<const float4 *>(I + r * M);
+      const float4 *row = reinterpret_cast<const float4 *>(I + c * M);
 #pragma unroll 2
       for (int d4 = 0; d4 < M / 4; d4++) {
         const float4 x = __ldg(row + d4);
@@ -245,31 +248,46 @@ __global__ void __launch_bounds__(256) k_row_prepass(const float *__restrict__ I
         for (int q = 0; q < 4; q++) {
           double w[NM];
           weights(4 * d4 + q, w);
-          mx = fmaxf(mx, fabsf(v[q]));
+          mx[0] = fmaxf(mx[0], fabsf(v[q]));
 #pragma unroll
-          for (int k = 0; k < NM; k++) m[k] = __fma_rn((double)v[q], w[k], m[k]);
+          for (int k = 0; k < NM; k++) m[0][k] = __fma_rn((double)v[q], w[k], m[0][k]);
         }
       }
     } else {
-      const float *row = I + cell * (int64_t)M * NG + g;
-#pragma unroll 4
+      // the cell's NG groups of one direction are contiguous: one vector load, one set of weights
+      const float *blk = I + c * (int64_t)M * NG;
+#pragma unroll 2
       for (int d = 0; d < M; d++) {
-        const float v = __ldg(row + (int64_t)d * NG);
+        float v[4];
+        if constexpr (NG == 4) {
+          const float4 x = __ldg(reinterpret_cast<const float4 *>(blk) + d);
+          v[0] = x.x, v[1] = x.y, v[2] = x.z, v[3] = x.w;
+        } else {
+          const float2 x = __ldg(reinterpret_cast<const float2 *>(blk) + d);
+          v[0] = x.x, v[1] = x.y;
+        }
         double w[NM];
         weights(d, w);
-        mx = fmaxf(mx, fabsf(v));
 #pragma unroll
-        for (int k = 0; k < NM; k++) m[k] = __fma_rn((double)v, w[k], m[k]);
+        for (int g = 0; g < NG; g++) {
+          mx[g] = fmaxf(mx[g], fabsf(v[g]));
+#pragma unroll
+          for (int k = 0; k < NM; k++) m[g][k] = __fma_rn((double)v[g], w[k], m[g][k]);
+        }
       }
     }
-    scale[r] = (mx > 0.f && isfinite(mx)) ? ldexpf(1.f, 14 - ilogbf(mx)) : 1.f;
-    erow[r] = m[0];
-    if (MOM) {
-      float4 *o = reinterpret_cast<float4 *>(mom + 16 * r);
-      o[0] = make_float4((float)m[0], (float)m[1], (float)m[2], (float)m[3]);
-      o[1] = make_float4((float)m[4], (float)m[5], (float)m[6], (float)m[7]);
-      o[2] = make_float4((float)m[8], (float)m[9], 0.f, 0.f);
-      o[3] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int g = 0; g < NG; g++) {
+      const int64_t r = c * NG + g;
+      scale[r] = (mx[g] > 0.f && isfinite(mx[g])) ? ldexpf(1.f, 14 - ilogbf(mx[g])) : 1.f;
+      erow[r] = m[g][0];
+      if (MOM) {
+        float4 *o = reinterpret_cast<float4 *>(mom + 16 * r);
+        o[0] = make_float4((float)m[g][0], (float)m[g][1], (float)m[g][2], (float)m[g][3]);
+        o[1] = make_float4((float)m[g][4], (float)m[g][5], (float)m[g][6], (float)m[g][7]);
+        o[2] = make_float4((float)m[g][8], (float)m[g][9], 0.f, 0.f);
+        o[3] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
     }
   }
 }
@@ -1227,7 +1245,7 @@ static rrhd_status launch_tc(const rrhd_scatter_tc *t, const float *I, float *S,
   }
   constexpr bool SCALED = (FORM == FORM_F16X3 || FORM == FORM_F16);
   if (SCALED) {
-    const unsigned nb = (unsigned)std::min<int64_t>((rows + 255) / 256, 8 * t->num_sms);
+    const unsigned nb = (unsigned)std::min<int64_t>((rows / ng + 255) / 256, 8 * t->num_sms);  // a thread per cell
     const size_t wbytes = sizeof(double) * (mom ? 10 : 1) * t->M;  // <= 80 KiB (M <= 1024)
     if (mom) {
       static bool attr = false;

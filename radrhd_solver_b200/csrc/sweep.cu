@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <cub/device/device_radix_sort.cuh>
@@ -99,6 +100,7 @@ struct SweepArgs {
   const T *rec;   // [N][RW]
   const T *area;  // [N][4] face areas (cell values)
   TV *fv;         // [F][DB][GS] face values (GS >= G, full 32-byte sectors)
+  const uint4 *geo;  // per item of the level (items[i] <-> geo[i]): its geometry, or null
   TV bc;
   int64_t last;
 };
@@ -112,6 +114,63 @@ template <class T>
 __device__ __forceinline__ void face_cos(const T *g, T wx, T wy, T wz, T *cosf) {
 #pragma unroll
   for (int j = 0; j < 4; j++) cosf[j] = (g[3 * j] * wx + g[3 * j + 1] * wy) + g[3 * j + 2] * wz;
+}
+
+// Geometry of one (cell, direction) item from the cell's normals and heights g[16]:
+// r[f] = H_f / -cos_f for the in-faces (cos_f < 0), 0 for the others, and the code word
+//   bits 0-3   in-faces (cos_f < 0)
+//   bits 4-7   out-faces (cos_f > 0)
+//   bits 8-23  per vertex v (4 bits at 8 + 4v) the in-face its node is traced to: face
+//              index, bit 2 lam = 2/3 (the face opposite v), bit 3 no in-face.
+// Node selection: the restatement takes, for each node, the in-face with the smallest
+// (t, face index); t = t4 = 2r/3 for the face opposite the node's own vertex, t1 = r/6 for
+// the others.  So only the two smallest in-faces by (t1, index) are needed: the node's
+// candidate among the other faces is the best unless that is its own opposite face.  The
+// choice depends on the node's vertex only, not on the out-face the node belongs to.
+template <class T>
+__device__ __forceinline__ uint32_t item_geometry(const T *g, T wx, T wy, T wz, T (&r)[4]) {
+  T cosf[4], t1[4], t4[4];
+  face_cos(g, wx, wy, wz, cosf);
+  uint32_t code = 0;
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    r[f] = t1[f] = t4[f] = (T)0;
+    if (cosf[f] < 0) {
+      r[f] = dv(g[12 + f], -cosf[f]);
+      t1[f] = (T)(1.0 / 6.0) * r[f];
+      t4[f] = (T)(2.0 / 3.0) * r[f];
+      code |= 1u << f;
+    } else if (cosf[f] > 0) {
+      code |= 16u << f;
+    }
+  }
+  int b1 = -1, b2 = -1;
+  T tb1 = 0, tb2 = 0;
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    if (!(cosf[f] < 0)) continue;
+    if (b1 < 0 || t1[f] < tb1) {
+      b2 = b1;
+      tb2 = tb1;
+      b1 = f;
+      tb1 = t1[f];
+    } else if (b2 < 0 || t1[f] < tb2) {
+      b2 = f;
+      tb2 = t1[f];
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < 4; v++) {
+    const int B = b1 != v ? b1 : b2;
+    const T tB = b1 != v ? tb1 : tb2;
+    uint32_t cv;
+    if (cosf[v] < 0 && (B < 0 || t4[v] < tB || (t4[v] == tB && v < B)))
+      cv = (uint32_t)v | 4u;
+    else
+      cv = B < 0 ? 8u : (uint32_t)B;
+    code |= cv << (8 + 4 * v);
+  }
+  return code;
 }
 
 
@@ -157,7 +216,7 @@ __device__ __forceinline__ void st_slot(T *p, const T (&v)[G]) {
 // node's own vertex, 1/6 otherwise), compared exactly as in the restatement.
 // The attenuations need only one exponential per in-face: E1_f = exp(-k r_f / 6)
 // and exp(-k 2 r_f / 3) = E1_f^4 (equal to a few ulp).
-template <class T, class TV, class TI, int GT>
+template <class T, class TV, class TI, int GT, bool PRE>
 __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T, TV> a) {
   // Levels after the first of a batch are launched with programmatic stream
   // serialisation: the next level may start while this one drains, and everything up to
@@ -168,13 +227,49 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T, TV> 
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= a.n) return;
   const uint32_t it = a.items[i];
+  uint4 gq = make_uint4(0u, 0u, 0u, 0u);
+  if constexpr (PRE) gq = __ldcs(a.geo + i);  // read once per sweep, in item order
   const int64_t c = it >> a.shift;
   const int dl = (int)(it & (uint32_t)(a.DB - 1));
   const int d = a.d0 + dl;
-  T g[16];
   int fid[4];
+  T r[4];
+  uint32_t code;
   const T *rc = a.rec + (int64_t)a.RW * c;
-  load_rec<T>(rc, g, fid);
+  if constexpr (PRE) {
+    // the item's geometry from the stream (item_geometry at setup, the in-face distances
+    // in face order, k_plan_geometry's format); of the cell record only the face-value
+    // slots and the source record are read
+    const int4 f = __ldg(reinterpret_cast<const int4 *>(rc + Rec<T>::IDS));
+    fid[0] = f.x, fid[1] = f.y, fid[2] = f.z, fid[3] = f.w;
+    code = gq.x;
+    int m = 0;
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+      for (int f = 0; f < 4; f++) {
+        r[f] = (T)0;
+        if ((code >> f) & 1u) {
+          r[f] = __uint_as_float(m == 0 ? gq.y : m == 1 ? gq.z : gq.w);
+          m++;
+        }
+      }
+    } else {
+      // 2^(e-32), exact: e in [-127, 127]
+      const double down = __hiloint2double((int)((code >> 24) - 128u - 32u + 1023u) << 20, 0);
+#pragma unroll
+      for (int f = 0; f < 4; f++) {
+        r[f] = (T)0;
+        if ((code >> f) & 1u) {
+          r[f] = (T)((double)(m == 0 ? gq.y : m == 1 ? gq.z : gq.w) * down);
+          m++;
+        }
+      }
+    }
+  } else {
+    T g[16];
+    load_rec<T>(rc, g, fid);
+    code = item_geometry<T>(g, a.w[3 * d], a.w[3 * d + 1], a.w[3 * d + 2], r);
+  }
   const T *dy = rc + Rec<T>::DYN;
   const T k = dy[0], bk = dy[1];
   const SweepIO io = *a.io;
@@ -188,62 +283,29 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T, TV> 
     base = (int64_t)io.row_of[c] * a.G * a.M + d;
     gs = a.M;
   }
-  const T wx = a.w[3 * d], wy = a.w[3 * d + 1], wz = a.w[3 * d + 2];
-  T cosf[4];
-  face_cos(g, wx, wy, wz, cosf);
-  T t1[4], t4[4];
   TV E1[4], E4[4];
 #pragma unroll
   for (int f = 0; f < 4; f++) {
-    t1[f] = t4[f] = (T)0;
     E1[f] = E4[f] = (TV)1;
-    if (cosf[f] < 0) {
-      const T r = dv(g[12 + f], -cosf[f]);
-      t1[f] = (T)(1.0 / 6.0) * r;
-      t4[f] = (T)(2.0 / 3.0) * r;
-      E1[f] = ex((TV)(-k * t1[f]));
+    if ((code >> f) & 1u) {
+      const T t1 = (T)(1.0 / 6.0) * r[f];
+      E1[f] = ex((TV)(-k * t1));
       const TV e2 = E1[f] * E1[f];
       E4[f] = e2 * e2;
     }
   }
-  // node selection.  The restatement takes, for each node, the in-face with the smallest
-  // (t, face index); t = t4 for the face opposite the node's own vertex, t1 for the others.
-  // So only the two smallest in-faces by (t1, index) are needed: the node's candidate
-  // among the other faces is the best unless that is its own opposite face.
-  int b1 = -1, b2 = -1;
-  T tb1 = 0, tb2 = 0;
-#pragma unroll
-  for (int f = 0; f < 4; f++) {
-    if (!(cosf[f] < 0)) continue;
-    if (b1 < 0 || t1[f] < tb1) {
-      b2 = b1;
-      tb2 = tb1;
-      b1 = f;
-      tb1 = t1[f];
-    } else if (b2 < 0 || t1[f] < tb2) {
-      b2 = f;
-      tb2 = t1[f];
-    }
-  }
-  // 4 bits per (out-face, node): face index, bit 2 lam = 2/3, bit 3 no in-face; out-faces
-  // compacted into slots (2 bits each in jo)
+  // 4 bits per (out-face, node) from the node's vertex code; out-faces compacted into
+  // slots (2 bits each in jo)
   uint64_t sel = 0;
   uint32_t jo = 0;
   int nout = 0;
 #pragma unroll
   for (int j = 0; j < 4; j++) {
-    if (!(cosf[j] > 0)) continue;
+    if (!((code >> (4 + j)) & 1u)) continue;
 #pragma unroll
     for (int q = 0; q < 3; q++) {
       const int vq = (j + 1 + q) & 3;
-      const int B = b1 != vq ? b1 : b2;
-      const T tB = b1 != vq ? tb1 : tb2;
-      uint32_t code;
-      if (cosf[vq] < 0 && (B < 0 || t4[vq] < tB || (t4[vq] == tB && vq < B)))
-        code = (uint32_t)vq | 4u;
-      else
-        code = B < 0 ? 8u : (uint32_t)B;
-      sel |= (uint64_t)code << (12 * nout + 4 * q);
+      sel |= (uint64_t)((code >> (8 + 4 * vq)) & 15u) << (12 * nout + 4 * q);
     }
     jo |= (uint32_t)j << (2 * nout);
     nout++;
@@ -263,7 +325,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T, TV> 
     for (int q = 0; q < GT; q++) rhs[q] = (TV)dy[2 + q] + (TV)bk * (TV)sv[q];
     asm volatile("griddepcontrol.wait;" ::: "memory");
     auto in_face = [&](int j, TV (&fj)[GT]) {
-      if (cosf[j] < 0 && fid[j] >= 0) {
+      if (((code >> j) & 1u) && fid[j] >= 0) {
         ld_groups<TV, GT>(a.fv + ((int64_t)fid[j] * a.DB + dl) * a.GS, fj);
       } else {
 #pragma unroll
@@ -314,7 +376,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T, TV> 
       TV fvals[4];
 #pragma unroll
       for (int j = 0; j < 4; j++)
-        fvals[j] = (cosf[j] < 0 && fid[j] >= 0) ? a.fv[((int64_t)fid[j] * a.DB + dl) * a.GS + gg] : a.bc;
+        fvals[j] = (((code >> j) & 1u) && fid[j] >= 0) ? a.fv[((int64_t)fid[j] * a.DB + dl) * a.GS + gg] : a.bc;
       for (int o = 0; o < nout; o++) {
         const int j = (jo >> (2 * o)) & 3;
         TV I0[3], e[3];
@@ -478,6 +540,74 @@ __global__ void k_plan_expand(const uint32_t *cur, int64_t n, int nbd, int shift
     const int64_t q = (int64_t)nbr[j] * nbd + dl;
     if (atomicSub(indeg + q, 1u) == 1u) plan[atomicAdd(tail, 1ull)] = ((uint32_t)nbr[j] << shift) | (uint32_t)dl;
   }
+}
+
+// The geometry stream: per plan item (in plan order) item_geometry's code word and the
+// distances r_f of the in-faces, in face order (at most three in-faces: the four outward
+// normals weighted by the face areas sum to zero).
+//   T = float: the distances as float, the values the sweep computes anyway.
+//   T = double: block floating point.  Only in-faces that some node of an out-face is traced
+//   to matter (the others are never read), and for those t = lam r_f is the distance from
+//   the node back to where its characteristic enters the cell, so r_f is at most six cell
+//   diameters.  With 2^(e-1) <= max r_f < 2^e over those faces, each is stored as
+//   round(r_f 2^(32-e)) in 32 bits and e in bits 24-31 of the code word (biased by 128):
+//   the error of every used distance is at most max r_f 2^-33, so an attenuation
+//   exp(-k t) moves by at most k (6 diameters) 2^-33 relative.
+template <class T>
+__global__ void k_plan_geometry(const uint32_t *items, int64_t n, int shift, int DB, int d0, const T *w,
+                                const T *rec, int RW, uint4 *geo) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t it = items[i];
+  const int64_t c = it >> shift;
+  const int d = d0 + (int)(it & (uint32_t)(DB - 1));
+  T g[16];
+  int fid[4];
+  load_rec<T>(rec + (int64_t)RW * c, g, fid);
+  T r[4];
+  uint32_t code = item_geometry<T>(g, w[3 * d], w[3 * d + 1], w[3 * d + 2], r);
+  uint32_t q[3] = {0u, 0u, 0u};
+  if constexpr (sizeof(T) == 4) {
+    int m = 0;
+#pragma unroll
+    for (int f = 0; f < 4; f++)
+      if ((code >> f) & 1u) {
+        const uint32_t v = __float_as_uint(r[f]);
+        if (m == 0) q[0] = v;
+        else if (m == 1) q[1] = v;
+        else q[2] = v;
+        m++;
+      }
+  } else {
+    uint32_t used = 0;  // in-faces some node of an out-face is traced to
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      if (!((code >> (4 + j)) & 1u)) continue;
+#pragma unroll
+      for (int qq = 0; qq < 3; qq++) {
+        const uint32_t cv = (code >> (8 + 4 * (((j + 1 + qq) & 3)))) & 15u;
+        if (!(cv & 8u)) used |= 1u << (cv & 3u);
+      }
+    }
+    double rmax = 0.0;
+#pragma unroll
+    for (int f = 0; f < 4; f++)
+      if ((used >> f) & 1u) rmax = fmax(rmax, (double)r[f]);
+    const int e = rmax > 0.0 ? max(-127, min(127, ilogb(rmax) + 1)) : 0;
+    const double up = ldexp(1.0, 32 - e);
+    int m = 0;
+#pragma unroll
+    for (int f = 0; f < 4; f++)
+      if ((code >> f) & 1u) {
+        const uint32_t v = ((used >> f) & 1u) ? (uint32_t)fmin(rint((double)r[f] * up), 4294967295.0) : 0u;
+        if (m == 0) q[0] = v;
+        else if (m == 1) q[1] = v;
+        else q[2] = v;
+        m++;
+      }
+    code |= (uint32_t)(e + 128) << 24;
+  }
+  geo[i] = make_uint4(code, q[0], q[1], q[2]);
 }
 
 // Source record {k = alpha + betta, betta / k, alpha Q_g / k} of each context cell
@@ -695,7 +825,7 @@ rrhd_status build_plan(rrhd_ctx *c) {
   return RRHD_OK;
 }
 
-template <class T, class TV, class TI, int GT>
+template <class T, class TV, class TI, int GT, bool PRE>
 cudaError_t launch_level(const SweepArgs<T, TV> &a, unsigned nb, cudaStream_t st, bool pdl) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nb);
@@ -707,7 +837,16 @@ cudaError_t launch_level(const SweepArgs<T, TV> &a, unsigned nb, cudaStream_t st
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
   cfg.numAttrs = pdl ? 1 : 0;
-  return cudaLaunchKernelEx(&cfg, k_sweep_level<T, TV, TI, GT>, a);
+  return cudaLaunchKernelEx(&cfg, k_sweep_level<T, TV, TI, GT, PRE>, a);
+}
+
+// the geometry stream exists for the float-intensity forms only (its distances are float)
+template <class T, class TV, class TI, int GT>
+cudaError_t launch_level_any(const SweepArgs<T, TV> &a, unsigned nb, cudaStream_t st, bool pdl) {
+  if constexpr (sizeof(TI) == 4) {
+    if (a.geo) return launch_level<T, TV, TI, GT, true>(a, nb, st, pdl);
+  }
+  return launch_level<T, TV, TI, GT, false>(a, nb, st, pdl);
 }
 
 template <class T, class TV, class TI>
@@ -730,6 +869,7 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
     a.rec = (const T *)R.d_rec;
     a.area = (const T *)R.d_area;
     a.fv = (TV *)R.d_fv;
+    a.geo = nullptr;
     a.bc = (TV)R.bc;
     a.last = R.last_cell;
     a.GS = R.GS;
@@ -745,11 +885,12 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
         const unsigned nb = grid_for(a.n, kSweepThreads);
         const bool pdl = L > 0;  // the first level of a batch follows a full dependency
         cudaError_t le;
+        a.geo = R.d_geo ? R.d_geo + base + off[L] : nullptr;
         switch (R.G) {
-          case 1: le = launch_level<T, TV, TI, 1>(a, nb, cs, pdl); break;
-          case 2: le = launch_level<T, TV, TI, 2>(a, nb, cs, pdl); break;
-          case 4: le = launch_level<T, TV, TI, 4>(a, nb, cs, pdl); break;
-          default: le = launch_level<T, TV, TI, 0>(a, nb, cs, pdl); break;
+          case 1: le = launch_level_any<T, TV, TI, 1>(a, nb, cs, pdl); break;
+          case 2: le = launch_level_any<T, TV, TI, 2>(a, nb, cs, pdl); break;
+          case 4: le = launch_level_any<T, TV, TI, 4>(a, nb, cs, pdl); break;
+          default: le = launch_level_any<T, TV, TI, 0>(a, nb, cs, pdl); break;
         }
         if (le != cudaSuccess && launch_err == cudaSuccess) launch_err = le;
       }
@@ -777,8 +918,8 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
 void rrhd_rad_release(rrhd_ctx *c) {
   RadState &R = c->rad;
   if (R.graph) cudaGraphExecDestroy(R.graph);
-  void *ptrs[] = {R.d_w, R.d_rec, R.d_area, R.d_plan, R.d_io, R.d_fv, R.d_I, R.d_S, R.d_G4, R.d_mE, R.d_mF, R.d_mT,
-                  R.d_mom, R.d_cnt};
+  void *ptrs[] = {R.d_w, R.d_rec, R.d_area, R.d_plan, R.d_geo, R.d_io, R.d_fv, R.d_I, R.d_S, R.d_G4, R.d_mE, R.d_mF,
+                  R.d_mT, R.d_mom, R.d_cnt};
   for (void *p : ptrs) cudaFree(p);
   for (cudaEvent_t e : R.ev)
     if (e) cudaEventDestroy(e);
@@ -845,6 +986,25 @@ static rrhd_status rad_setup_t(rrhd_ctx *c) {
       cudaMalloc(&R.d_fv, sizeof(TV) * (size_t)c->F * R.DB * R.GS) != cudaSuccess)
     return rrhd_fail(RRHD_ERR_OOM, "sweep allocation failed");
   if ((s = build_plan<T>(c))) return s;
+  if (R.item_geometry) {
+    const int64_t total = N * (int64_t)R.M;
+    if (cudaMalloc(&R.d_geo, sizeof(uint4) * total) != cudaSuccess) {
+      R.d_geo = nullptr;
+      return rrhd_fail(RRHD_ERR_OOM, "sweep geometry stream allocation failed (%lld bytes)",
+                       (long long)(sizeof(uint4) * total));
+    }
+    int64_t base = 0;
+    for (int b = 0; b < R.nbatch; b++) {
+      const int d0 = b * R.DB;
+      const int64_t n = N * std::min(R.DB, R.M - d0);
+      k_plan_geometry<T><<<grid_for(n, 256), 256, 0, c->stream>>>(R.d_plan + base, n, R.shift, R.DB, d0,
+                                                                  (const T *)R.d_w, (const T *)R.d_rec, R.RW,
+                                                                  R.d_geo + base);
+      RRHD_CUDA(cudaGetLastError());
+      base += n;
+    }
+    RRHD_CUDA(cudaStreamSynchronize(c->stream));
+  }
   return capture_sweep<T, TV, TI>(c);
 }
 
@@ -854,6 +1014,9 @@ extern "C" rrhd_status rrhd_rad_setup(rrhd_ctx *c, const rrhd_dirs *dirs, const 
   RRHD_CHECK_ARG(o->precision == RRHD_RAD_FP64 || o->precision == RRHD_RAD_FP32 || o->precision == RRHD_RAD_MIXED,
                  "bad precision");
   RRHD_CHECK_ARG(dirs->device == c->device, "direction set lives on another device");
+  RRHD_CHECK_ARG(o->item_geometry == 0 || o->item_geometry == 1, "item_geometry: 0 or 1");
+  RRHD_CHECK_ARG(o->item_geometry == 0 || o->precision != RRHD_RAD_FP64,
+                 "item_geometry needs RRHD_RAD_FP32 or RRHD_RAD_MIXED (its distances are float)");
   int DB = o->dirs_per_batch;
   RRHD_CHECK_ARG(DB == 0 || (DB > 0 && DB <= 256 && (DB & (DB - 1)) == 0), "dirs_per_batch: power of two <= 256");
   RRHD_CUDA(cudaSetDevice(c->device));
@@ -875,6 +1038,7 @@ extern "C" rrhd_status rrhd_rad_setup(rrhd_ctx *c, const rrhd_dirs *dirs, const 
   R.nbatch = (R.M + DB - 1) / DB;
   R.prec = o->precision;
   R.bc = o->boundary_value;
+  R.item_geometry = o->item_geometry != 0;
   const rrhd_status s = R.prec == RRHD_RAD_FP64   ? rad_setup_t<double, double, double>(c)
                         : R.prec == RRHD_RAD_MIXED ? rad_setup_t<double, double, float>(c)
                                                    : rad_setup_t<float, float, float>(c);

@@ -199,14 +199,19 @@ class TransportSweep:
     upwind order the reference reads from its offline graph/ and make_trace/
     outputs (sorted_graph, vec_x0), built on the GPU as levels.  precision:
     "fp64" or "fp32" (storage and arithmetic of alpha, betta, Q, S, I), or "mixed"
-    (float arrays as "fp32", face values and the transport update in double)."""
+    (float arrays as "fp32", face values and the transport update in double).
+    item_geometry ("fp32" and "mixed"): precompute every (cell, direction) item's
+    in/out faces, node choices and in-face distances (float) at setup, 16 bytes per
+    item, and stream them in sweep order instead of reading each cell's geometry per
+    item."""
 
     def __init__(self, grid, dg: DirectionGrid, groups: int = 1, precision: str = "fp64", dirs_per_batch: int = 0,
-                 boundary_value: float = 0.0):
+                 boundary_value: float = 0.0, item_geometry: bool = False):
         prec = {"fp64": L.RRHD_RAD_FP64, "fp32": L.RRHD_RAD_FP32, "mixed": L.RRHD_RAD_MIXED}[precision]
-        o = L.RadOpts(groups, prec, dirs_per_batch, boundary_value)
+        o = L.RadOpts(groups, prec, dirs_per_batch, boundary_value, int(item_geometry))
         L.check(L.lib.rrhd_rad_setup(grid.handle, dg.handle, C.byref(o)), "rrhd_rad_setup")
         self.grid, self.dg, self.groups, self.precision = grid, dg, groups, precision
+        self.item_geometry = bool(item_geometry)
 
     def plan_levels(self):
         """[M, N] (caller numbering): the level in which each (cell, direction) is swept,

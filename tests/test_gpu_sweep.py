@@ -93,18 +93,25 @@ def test_sweep_mixed_matches_oracle(n):
     alpha = alpha.astype(np.float32).astype(np.float64)
     Io, missing = oracle.port_sweep(m, d.dirs, alpha, betta, Q, S)
     assert missing == 0
-    errs = {}
-    for prec in ("mixed", "fp32"):
+    errs, outs = {}, {}
+    for prec, geo in (("mixed", False), ("mixed", True), ("fp32", False), ("fp32", True)):
         grid = rhllc.Grid(m, gamma=GAMMA_43)
         dg = illum.DirectionGrid(d)
-        sw = illum.TransportSweep(grid, dg, groups=G, precision=prec)
+        sw = illum.TransportSweep(grid, dg, groups=G, precision=prec, item_geometry=geo)
         t32 = [torch.tensor(a, dtype=torch.float32, device="cuda").contiguous() for a in (alpha, betta, Q, S)]
         I = illum.CalculateIllum(sw, *t32)
         grid.sync()
-        errs[prec] = float(np.max(np.abs(I.double().cpu().numpy() - Io) / np.abs(Io)))
+        outs[prec, geo] = I.cpu().numpy()
+        errs[prec, geo] = float(np.max(np.abs(outs[prec, geo].astype(np.float64) - Io) / np.abs(Io)))
         grid.close()
-    print(f"\n{m.n_cells} cells: sweep max rel err mixed {errs['mixed']:.2e}, fp32 {errs['fp32']:.2e}")
-    assert errs["mixed"] <= 1e-7  # one float rounding of the output: 2^-24 = 6e-8
+    print(f"\n{m.n_cells} cells: sweep max rel err mixed {errs['mixed', False]:.2e} (item geometry "
+          f"{errs['mixed', True]:.2e}), fp32 {errs['fp32', False]:.2e}")
+    assert errs["mixed", False] <= 1e-7  # one float rounding of the output: 2^-24 = 6e-8
+    # the item-geometry stream holds the in-face distances rounded to float once (every
+    # choice made in double): the attenuation moves by k r 2^-24, below the output rounding
+    assert errs["mixed", True] <= 1e-7
+    # in the all-float sweep the streamed distances are the values it computes anyway
+    assert np.array_equal(outs["fp32", True], outs["fp32", False])
 
 
 @pytest.mark.parametrize("dirs_per_batch", [8, 32])
@@ -148,6 +155,8 @@ def test_sweep_errors():
     assert st == L.RRHD_ERR_STATE
     dg = illum.DirectionGrid(fibonacci_directions(8))
     o = L.RadOpts(1, L.RRHD_RAD_FP64, 3, 0.0)  # not a power of two
+    assert L.lib.rrhd_rad_setup(grid.handle, dg.handle, C.byref(o)) == L.RRHD_ERR_INVALID
+    o = L.RadOpts(1, L.RRHD_RAD_FP64, 0, 0.0, 1)  # the geometry stream holds float distances
     assert L.lib.rrhd_rad_setup(grid.handle, dg.handle, C.byref(o)) == L.RRHD_ERR_INVALID
     sw = illum.TransportSweep(grid, dg, groups=1, precision="fp64")
     step = rad_rhd.RadRHDStep(sw, scatter="f16x3")  # tensor-core scattering needs the fp32 sweep
@@ -233,12 +242,12 @@ def _g4_scale(W, mom, G, em, a=1.0, b=0.5):
     return rho * gamma * (a + b) * rho * (np.abs(m[:, 0]) + np.linalg.norm(m[:, 1:4], axis=1)) + q * gamma
 
 
-def _coupled_grid(m, W, U, d, G, precision):
+def _coupled_grid(m, W, U, d, G, precision, item_geometry=False):
     g = rhllc.Grid(m, gamma=GAMMA_43)
     g.set_boundary(-3, rhllc.BC_FIXED, JET_INFLOW)
     g.set_state(W, U)
     dg = illum.DirectionGrid(d)
-    sw = illum.TransportSweep(g, dg, groups=G, precision=precision)
+    sw = illum.TransportSweep(g, dg, groups=G, precision=precision, item_geometry=item_geometry)
     return g, dg, sw
 
 
@@ -290,8 +299,9 @@ def _trained_guess():
 
 @pytest.mark.parametrize("M", [64, 256])
 def test_coupled_chosen_form_tracks_plain(M):
-    """Three coupled steps of the chosen form (mixed-precision sweep, tensor-core F16X3
-    scattering, learned con2prim guess) against the FP64 oracle and the plain form.
+    """Three coupled steps of the chosen form (mixed-precision sweep with the item-geometry
+    stream, tensor-core F16X3 scattering, learned con2prim guess) against the FP64 oracle
+    and the plain form.
 
     The scattering integral as an operation: the chosen form's S and moments against the
     FP64 oracle's scattering integral and moments of the chosen form's own intensity,
@@ -310,7 +320,7 @@ def test_coupled_chosen_form_tracks_plain(M):
     out = {}
     lib_err = None
     for form in ("plain", "chosen"):
-        g, dg, sw = _coupled_grid(m, W, U, d, G, "fp64" if form == "plain" else "mixed")
+        g, dg, sw = _coupled_grid(m, W, U, d, G, "fp64" if form == "plain" else "mixed", item_geometry=form != "plain")
         step = rad_rhd.RadRHDStep(sw, em=rad_rhd.emission(*EM_JET), scatter="fp64" if form == "plain" else "f16x3",
                                   guess=None if form == "plain" else net)
         stats = [step(tau, stats=True) for _ in range(3)]
@@ -348,11 +358,11 @@ def test_coupled_chosen_form_tracks_plain(M):
     assert all(s[1].n_failed == 0 for s in sc)
 
 
-@pytest.mark.parametrize("precision", ["fp32", "mixed"])
-def test_coupled_chosen_independent_of_batching(precision):
+@pytest.mark.parametrize("precision,item_geometry", [("fp32", False), ("mixed", False), ("mixed", True)])
+def test_coupled_chosen_independent_of_batching(precision, item_geometry):
     """The chosen coupled step with one batch of 256 directions is bit-identical to the
     same step with two batches of 128: the batches change which level launch a
-    (cell, direction) item runs in, never its arithmetic."""
+    (cell, direction) item runs in, never its arithmetic (nor its streamed geometry)."""
     m, W = jet(5)
     W, U = oracle.port_p2c(W, 1, GAMMA_43)
     d = fibonacci_directions(256)
@@ -362,7 +372,8 @@ def test_coupled_chosen_independent_of_batching(precision):
         g.set_boundary(-3, rhllc.BC_FIXED, JET_INFLOW)
         g.set_state(W, U)
         dg = illum.DirectionGrid(d)
-        sw = illum.TransportSweep(g, dg, groups=4, precision=precision, dirs_per_batch=db)
+        sw = illum.TransportSweep(g, dg, groups=4, precision=precision, dirs_per_batch=db,
+                                  item_geometry=item_geometry)
         step = rad_rhd.RadRHDStep(sw, em=rad_rhd.emission(*EM_JET), scatter="f16x3")
         for _ in range(2):
             step(0.3 * m.h_min)
