@@ -193,100 +193,137 @@ struct TcParams {
 };
 
 // Per-row pre-pass of the scaled FP16 forms over a cell-direction-group array [cells][M][NG]
-// (NG = 1 is the rows layout [rows][M]); one thread per cell, which walks the cell's M
-// directions in order with its NG group values as one vector load (the loads of a warp's
-// cells share L1 lines, each line serving two or more steps):
+// (NG = 1 is the rows layout [rows][M]):
 //   scale  2^(14 - floor(log2(max_d |I[r][d]|))), so that max |s_r I| lies in [2^14, 2^15);
 //   erow   E_r = sum_d (a_d / A) I[r][d] in FP64, the isotropic part of the Thomson
 //          kernel's integral, which the scaled forms add outside the tensor cores;
 //   mom    (MOM) the ten moments in FP64, stored as FP32 [rows][16] (columns 10-15 zero):
 //          the scaled forms take them from here, not from the tensor cores.
 // mw [10][M] holds (a_d / A) {1, wx, wy, wz, wx^2, wx wy, wx wz, wy^2, wy wz, wz^2}
-// (cuda_illum_sep_param.cu:9-69), staged in shared memory direction-major; each term is one
-// fused multiply-add, summed in direction order.
+// (cuda_illum_sep_param.cu:9-69).  A warp takes four cells, eight lanes per cell: a cell's
+// values are NV = M NG / 4 float4 vectors (P = 4 / NG directions of NG groups each), lane q
+// takes vectors q, q + 8, q + 16, ..., so each load instruction reads a whole 128-byte line
+// of each of the four cells.  Each term is one fused multiply-add in FP64; the eight lanes'
+// partial sums are combined by a fixed butterfly (reduce-scatter over lane bits 4, 2, 1), the
+// same order for every cell.  The weight table sits in shared memory by (sub-direction,
+// vector), so the eight lanes of a cell read eight consecutive records (no bank conflicts).
+constexpr int kPrepassThreads = 256;
 template <int NG, bool MOM>
-__global__ void __launch_bounds__(256) k_row_prepass(const float *__restrict__ I, int64_t rows, int M,
-                                                     const double *__restrict__ mw, float *__restrict__ scale,
-                                                     double *__restrict__ erow, float *__restrict__ mom) {
+__global__ void __launch_bounds__(kPrepassThreads, 2) k_row_prepass(const float *__restrict__ I, int64_t rows, int M,
+                                                                 const double *__restrict__ mw,
+                                                                 float *__restrict__ scale, double *__restrict__ erow,
+                                                                 float *__restrict__ mom) {
   constexpr int NM = MOM ? 10 : 1;
-  extern __shared__ double2 smw2[];  // [M][NM] (direction-major here: one direction's weights
-  double *smw = reinterpret_cast<double *>(smw2);  // are read as NM / 2 16-byte loads)
-  for (int q = threadIdx.x; q < NM * M; q += blockDim.x) {
-    const int k = q / M, d = q - k * M;
-    smw[d * NM + k] = __ldg(mw + q);
+  constexpr int P = 4 / NG;                 // directions per float4
+  constexpr int V = NG * NM;                // sums per cell
+  constexpr int VP = (V + 7) / 8 * 8;       // padded to the reduce-scatter's eight lanes
+  extern __shared__ double2 smw2[];         // [P][M / P][NM]
+  double *smw = reinterpret_cast<double *>(smw2);
+  const int MP = M / P;
+  for (int x = threadIdx.x; x < NM * M; x += blockDim.x) {
+    const int k = x / M, d = x - k * M;
+    smw[((d % P) * MP + d / P) * NM + k] = __ldg(mw + x);
   }
   __syncthreads();
-  auto weights = [&](int d, double (&w)[NM]) {
-    if constexpr (MOM) {
-#pragma unroll
-      for (int j = 0; j < NM / 2; j++) {
-        const double2 x = smw2[d * (NM / 2) + j];
-        w[2 * j] = x.x;
-        w[2 * j + 1] = x.y;
-      }
-    } else {
-      w[0] = smw[d];
+  const int lane = threadIdx.x & 31, q = lane & 7;
+  const int NV = M * NG / 4;  // float4 per cell, a multiple of 8
+  const int64_t cells = rows / NG;
+  const int64_t quads = (cells + 3) / 4;
+  const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const float4 *I4 = reinterpret_cast<const float4 *>(I);
+  // the four cells of a group are contiguous (16 NV bytes each): one lane asks L2 for the
+  // warp's next group while the warp works on this one, so that the lanes' loads find it there
+  auto prefetch = [&](int64_t g4) {
+    if (lane == 0 && g4 < quads) {
+      const int64_t n = min((int64_t)4, cells - 4 * g4) * NV * 16;  // bytes, a multiple of 16
+      const float4 *src = I4 + 4 * g4 * NV;
+      for (int64_t o = 0; o < n; o += 65536)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(reinterpret_cast<const char *>(src) + o),
+                     "r"((uint32_t)min((int64_t)65536, n - o))
+                     : "memory");
     }
   };
-  const int64_t cells = rows / NG;
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < cells; c += (int64_t)gridDim.x * blockDim.x) {
+  prefetch(wid);
+  for (int64_t c4 = wid; c4 < quads; c4 += nw) {  // warp-uniform
+    prefetch(c4 + nw);
+    const int64_t c = c4 * 4 + (lane >> 3);
+    const bool valid = c < cells;
+    double acc[VP];
+#pragma unroll
+    for (int k = 0; k < VP; k++) acc[k] = 0.0;
     float mx[NG];
-    double m[NG][NM];
 #pragma unroll
-    for (int g = 0; g < NG; g++) {
-      mx[g] = 0.f;
-#pragma unroll
-      for (int k = 0; k < NM; k++) m[g][k] = 0.0;
-    }
-    if constexpr (NG == 1) {
-      const float4 *row = reinterpret_cast<const float4 *>(I + c * M);
+    for (int g = 0; g < NG; g++) mx[g] = 0.f;
+    if (valid) {
+      const float4 *row = I4 + c * NV;
 #pragma unroll 2
-      for (int d4 = 0; d4 < M / 4; d4++) {
-        const float4 x = __ldg(row + d4);
-        const float v[4] = {x.x, x.y, x.z, x.w};
+      for (int v = q; v < NV; v += 8) {
+        const float4 x = __ldcs(row + v);
+        const float e[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
+        for (int s = 0; s < P; s++) {
           double w[NM];
-          weights(4 * d4 + q, w);
-          mx[0] = fmaxf(mx[0], fabsf(v[q]));
+          const double2 *wr = smw2 + ((s * MP + v) * NM) / 2;
+          if constexpr (MOM) {
 #pragma unroll
-          for (int k = 0; k < NM; k++) m[0][k] = __fma_rn((double)v[q], w[k], m[0][k]);
-        }
-      }
-    } else {
-      // the cell's NG groups of one direction are contiguous: one vector load, one set of weights
-      const float *blk = I + c * (int64_t)M * NG;
-#pragma unroll 2
-      for (int d = 0; d < M; d++) {
-        float v[4];
-        if constexpr (NG == 4) {
-          const float4 x = __ldg(reinterpret_cast<const float4 *>(blk) + d);
-          v[0] = x.x, v[1] = x.y, v[2] = x.z, v[3] = x.w;
-        } else {
-          const float2 x = __ldg(reinterpret_cast<const float2 *>(blk) + d);
-          v[0] = x.x, v[1] = x.y;
-        }
-        double w[NM];
-        weights(d, w);
+            for (int j = 0; j < NM / 2; j++) {
+              const double2 t = wr[j];
+              w[2 * j] = t.x;
+              w[2 * j + 1] = t.y;
+            }
+          } else {
+            w[0] = smw[s * MP + v];
+          }
 #pragma unroll
-        for (int g = 0; g < NG; g++) {
-          mx[g] = fmaxf(mx[g], fabsf(v[g]));
+          for (int g = 0; g < NG; g++) {
+            const float val = e[s * NG + g];
+            mx[g] = fmaxf(mx[g], fabsf(val));
 #pragma unroll
-          for (int k = 0; k < NM; k++) m[g][k] = __fma_rn((double)v[g], w[k], m[g][k]);
+            for (int k = 0; k < NM; k++) acc[g * NM + k] = __fma_rn((double)val, w[k], acc[g * NM + k]);
+          }
         }
       }
     }
+    // the group maxima to every lane of the cell; the sums reduce-scattered
 #pragma unroll
-    for (int g = 0; g < NG; g++) {
-      const int64_t r = c * NG + g;
-      scale[r] = (mx[g] > 0.f && isfinite(mx[g])) ? ldexpf(1.f, 14 - ilogbf(mx[g])) : 1.f;
-      erow[r] = m[g][0];
-      if (MOM) {
-        float4 *o = reinterpret_cast<float4 *>(mom + 16 * r);
-        o[0] = make_float4((float)m[g][0], (float)m[g][1], (float)m[g][2], (float)m[g][3]);
-        o[1] = make_float4((float)m[g][4], (float)m[g][5], (float)m[g][6], (float)m[g][7]);
-        o[2] = make_float4((float)m[g][8], (float)m[g][9], 0.f, 0.f);
-        o[3] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int o = 4; o >= 1; o >>= 1)
+#pragma unroll
+      for (int g = 0; g < NG; g++) mx[g] = fmaxf(mx[g], __shfl_xor_sync(0xffffffffu, mx[g], o));
+#pragma unroll
+    for (int o = 4, h = VP / 2; o >= 1; o >>= 1, h >>= 1) {
+      const bool up = lane & o;
+#pragma unroll
+      for (int k = 0; k < VP / 2; k++) {
+        if (k < h) {
+          const double send = up ? acc[k] : acc[h + k];
+          const double keep = up ? acc[h + k] : acc[k];
+          acc[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+      }
+    }
+    // this lane now holds sums base .. base + VP/8 - 1 of its cell
+    const int base = ((lane >> 2) & 1) * (VP / 2) + ((lane >> 1) & 1) * (VP / 4) + (lane & 1) * (VP / 8);
+#pragma unroll
+    for (int k = 0; k < VP / 8; k++) {
+      const int f = base + k;
+      if (valid && f < V) {
+        const int g = f / NM, kk = f - g * NM;
+        const int64_t r = c * NG + g;
+        if (kk == 0) {
+          float m = mx[0];
+#pragma unroll
+          for (int gg = 1; gg < NG; gg++)
+            if (g == gg) m = mx[gg];
+          scale[r] = (m > 0.f && isfinite(m)) ? ldexpf(1.f, 14 - ilogbf(m)) : 1.f;
+          erow[r] = acc[k];
+        }
+        if (MOM) {
+          mom[16 * r + kk] = (float)acc[k];
+          if (kk == NM - 1)
+#pragma unroll
+            for (int z = NM; z < 16; z++) mom[16 * r + z] = 0.f;
+        }
       }
     }
   }
@@ -1245,7 +1282,9 @@ static rrhd_status launch_tc(const rrhd_scatter_tc *t, const float *I, float *S,
   }
   constexpr bool SCALED = (FORM == FORM_F16X3 || FORM == FORM_F16);
   if (SCALED) {
-    const unsigned nb = (unsigned)std::min<int64_t>((rows / ng + 255) / 256, 8 * t->num_sms);  // a thread per cell
+    // a warp per four cells
+    const unsigned nb = (unsigned)std::min<int64_t>((rows / ng + 4 * (kPrepassThreads / 32) - 1) /
+                                                        (4 * (kPrepassThreads / 32)), 8 * t->num_sms);
     const size_t wbytes = sizeof(double) * (mom ? 10 : 1) * t->M;  // <= 80 KiB (M <= 1024)
     if (mom) {
       static bool attr = false;
@@ -1254,9 +1293,9 @@ static rrhd_status launch_tc(const rrhd_scatter_tc *t, const float *I, float *S,
                                        (int)(sizeof(double) * 10 * 1024)));
         attr = true;
       }
-      k_row_prepass<NG, true><<<nb, 256, wbytes, st>>>(I, rows, t->M, t->d_mw, t->d_scale, t->d_erow, mom);
+      k_row_prepass<NG, true><<<nb, kPrepassThreads, wbytes, st>>>(I, rows, t->M, t->d_mw, t->d_scale, t->d_erow, mom);
     } else {
-      k_row_prepass<NG, false><<<nb, 256, wbytes, st>>>(I, rows, t->M, t->d_mw, t->d_scale, t->d_erow, nullptr);
+      k_row_prepass<NG, false><<<nb, kPrepassThreads, wbytes, st>>>(I, rows, t->M, t->d_mw, t->d_scale, t->d_erow, nullptr);
     }
     RRHD_CUDA(cudaGetLastError());
   }
