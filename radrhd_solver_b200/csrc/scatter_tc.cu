@@ -951,10 +951,24 @@ __global__ void __launch_bounds__(R_THREADS, 1)
     auto scale_of = [&](const uint32_t (&e)[2], int j) {
       return __uint_as_float(((e[j >> 2] >> (8 * (j & 3))) & 0xffu) << 23);
     };
+    // a tile's rows are contiguous: CPT cells x M x NG floats (128 rows of M); when a tile's
+    // first chunk is loaded, one thread asks L2 for the CTA's next tile, so that the
+    // converters' loads of it find it there
+    const int64_t tile_bytes = (int64_t)BM * P.M * 4;
+    auto prefetch_tile = [&](int64_t rt) {
+      if (t != 0 || rt >= n_rt) return;
+      const char *src = reinterpret_cast<const char *>(P.I) + rt * tile_bytes;
+      const int64_t n = std::min(tile_bytes, (int64_t)P.rows * P.M * 4 - rt * tile_bytes);
+      for (int64_t o = 0; o < n; o += 65536)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(src + o),
+                     "r"((uint32_t)std::min((int64_t)65536, n - o))
+                     : "memory");
+    };
     auto load = [&](int64_t gc, float4 (&buf)[8], bool with_scales) {
       const int64_t rt = blockIdx.x + (gc / nk) * gridDim.x;
       const int k = (int)(gc % nk);
       const int64_t cell0 = rt * CPT;
+      if (k == 0) prefetch_tile(rt + gridDim.x);
 #pragma unroll
       for (int j = 0; j < 8; j++) {
         const int64_t c = cell0 + cellrel(j);
@@ -1008,6 +1022,7 @@ __global__ void __launch_bounds__(R_THREADS, 1)
       if (lane == 0) mbar_arrive(&a_full[k]);
       return true;
     };
+    prefetch_tile(blockIdx.x);
     if (nchunks > 0) load(0, bufA, true);
     for (int64_t gc = 0; gc < nchunks; gc += 2) {
       if (gc + 1 < nchunks) load(gc + 1, bufB, false);
