@@ -18,11 +18,13 @@
 // partial gradient with fixed-order loops; a second kernel sums the partials
 // over CTAs in order; Adam updates the parameters.
 //
-// Inference: each warp evaluates 32 states at once, all three layers on the
-// tensor cores as warp-level mma.sync (f16 operands, FP32 accumulation; the
-// guess only seeds Newton, so f16 is enough).  Newton then starts from the guess; if it has
-// not converged after `k_stall` iterations the state is solved again from the
-// reference guess, so the result is always a converged reference Newton solve.
+// Inference, two kernels: k_mlp_guess evaluates the network for tiles of 128 states (the
+// 64 x 64 hidden layer as one tcgen05 MMA with f16 operands and an FP32 accumulator in
+// tensor memory, the first and last layers in FP32; the guess only seeds Newton, so f16
+// is enough) and writes the initial pressures; k_c2p_guess runs Newton from them with the
+// plain con2prim kernel's structure.  If Newton has not converged after `k_stall`
+// iterations the state is solved again from the reference guess, so the result is always a
+// converged reference Newton solve.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -34,6 +36,7 @@
 #include "rng.h"
 #include "coupled.h"
 #include "rrhd_internal.h"
+#include "umma.cuh"
 
 using namespace rrhd;
 
@@ -181,118 +184,201 @@ __global__ void k_adam(float *theta, float *m, float *v, const float *g, float l
   theta[p] -= lr * (mm / c1) / (sqrtf(vv / c2) + eps);
 }
 
-// B fragments of the three layers for mma.sync (f16 operands, FP32 accumulation), in
-// uint32 words, each holding two f16 (the lower k index in the low half):
-//   FR_W2 [n-tile 8][k-step 4][lane 32][2]  W2^T for m16n8k16 (k = hidden input, n = output)
-//   FR_W1 [n-tile 8][lane 32]               [W1 | b1]^T for m16n8k8: k 0-2 the features,
-//                                           k 3 the bias (its A column is 1), k 4-7 zero
-//   FR_W3 [k-step 4][lane 32][2]            W3 as column 0 of an m16n8k16 B tile, the
-//                                           other 7 columns zero
-// Lane l of a B fragment holds column n = l / 4 and rows k = 2 (l % 4) + {0, 1} (+8 for
-// the second word of a k16 fragment).
-constexpr int FR_W2 = 0, FR_W1 = FR_W2 + 8 * 4 * 32 * 2, FR_W3 = FR_W1 + 8 * 32, NFRAG = FR_W3 + 4 * 32 * 2;  // 2560
-
 __device__ __forceinline__ uint32_t pack_f16(float lo, float hi) {
   return (uint32_t)__half_as_ushort(__float2half_rn(lo)) | ((uint32_t)__half_as_ushort(__float2half_rn(hi)) << 16);
 }
 
-__global__ void k_pack_frags(const float *theta, uint32_t *frag) {
+// ---------------------------------------------------------------- inference
+// The guess kernel: one CTA of 128 threads per tile of 128 states (thread t = state t = row t
+// of both layer products = TMEM lane t), persistent over tiles.  Per tile:
+//   the features (FP32 from FP64 differences), normalised, and a constant 1 as row t of the
+//   f16 A tile (K = 16, columns 4-15 zero);
+//   layer 1 as one 128 x 64 x 16 tcgen05 MMA against [W1 | b1] (f16, FP32 accumulator in 64
+//   TMEM columns); the thread reads its row back and writes ReLU(h1) as f16 into row t of
+//   the same A tile (K = 64);
+//   layer 2 as four 128 x 64 x 16 MMAs against W2 into the same TMEM columns;
+//   b2, ReLU and layer 3 (64 -> 1) in FP32 from the thread's TMEM row, with b2, W3 and b3
+//   taken from the kernel's parameter (constant bank).
+// A and B tiles are K-major, 128-byte swizzled.  Output p0 = tau exp(y sigma_t + mu_t), or 0
+// where the state has no usable features or the network gives a non-finite y (the Newton
+// kernel then uses the reference guess).
+constexpr int GT = 128;
+constexpr int G_SMEM = 1024 /*alignment*/ + GT * 128 /*A*/ + 2 * H * 128 /*B1, B2*/ + 64 /*barrier, TMEM slot*/;
+
+// [W1 | b1] (k 0-2 the weights, k 3 the bias, k 4-63 zero) and W2 as the f16 B operands of
+// the two MMAs: K-major, 64 rows each, 128-byte swizzled, 8 KiB each.
+__global__ void k_pack_b(const float *theta, __half *b1t, __half *w2t) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const float *W1 = theta + OFF_W1, *b1 = theta + OFF_B1, *W2 = theta + OFF_W2, *W3 = theta + OFF_W3;
-  if (i < 8 * 4 * 32) {
-    const int lane = i & 31, ks = (i >> 5) & 3, nt = i >> 7;
-    const int n = 8 * nt + (lane >> 2), k0 = 16 * ks + 2 * (lane & 3);
-    frag[FR_W2 + 2 * i] = pack_f16(W2[n * H + k0], W2[n * H + k0 + 1]);
-    frag[FR_W2 + 2 * i + 1] = pack_f16(W2[n * H + k0 + 8], W2[n * H + k0 + 9]);
-  } else if (i < 8 * 4 * 32 + 8 * 32) {
-    const int j = i - 8 * 4 * 32, lane = j & 31, nt = j >> 5;
-    const int n = 8 * nt + (lane >> 2), c = lane & 3;
-    frag[FR_W1 + j] = c == 0 ? pack_f16(W1[3 * n], W1[3 * n + 1]) : c == 1 ? pack_f16(W1[3 * n + 2], b1[n]) : 0u;
-  } else if (i < 8 * 4 * 32 + 8 * 32 + 4 * 32) {
-    const int j = i - 8 * 4 * 32 - 8 * 32, lane = j & 31, ks = j >> 5;
-    const int k0 = 16 * ks + 2 * (lane & 3);
-    const bool col0 = (lane >> 2) == 0;
-    frag[FR_W3 + 2 * j] = col0 ? pack_f16(W3[k0], W3[k0 + 1]) : 0u;
-    frag[FR_W3 + 2 * j + 1] = col0 ? pack_f16(W3[k0 + 8], W3[k0 + 9]) : 0u;
-  }
+  if (i >= H * H) return;
+  const int nrow = i / H, k = i - nrow * H;
+  w2t[rrhd_umma::sw128_offset(nrow, k) / 2] = __float2half_rn(theta[OFF_W2 + i]);
+  const float v = k < 3 ? theta[OFF_W1 + 3 * nrow + k] : k == 3 ? theta[OFF_B1 + nrow] : 0.f;
+  b1t[rrhd_umma::sw128_offset(nrow, k) / 2] = __float2half_rn(v);
 }
 
 struct MlpPartial {
-  unsigned long long ok, guess_fallback, fallback, failed, iters, max_iters;
+  unsigned long long ok, guess_fallback, fallback, failed, iters, max_iters, err;
 };
 
-constexpr int IT = 128;  // inference threads per CTA
+// the last layer's parameters, passed by value: the kernel's FP32 multiply-adds take them
+// from the constant bank, with no load instructions
+struct MlpOuter {
+  float b2w3[H][2];  // b2[j], W3[j]
+  float b3;
+};
 
-// ReLU of two FP32 accumulators packed as f16x2 (lo in the low half) in one conversion
+// ReLU of two FP32 values packed as f16x2 (lo in the low half) in one conversion
 __device__ __forceinline__ uint32_t relu_f16x2(float lo, float hi) {
   uint32_t d;
   asm("cvt.rn.relu.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
   return d;
 }
 
-__device__ __forceinline__ void mma_k16(float *d, const uint32_t *a, uint2 b) {
+// 16 TMEM columns of the warp's 32 lanes (this thread's row) from column c0
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
   asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b.x), "r"(b.y));
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(addr));
 }
 
-// Warp-cooperative guess for the 32 states of a warp (lane = state); returns this lane's
-// y.  All three layers run on the tensor cores, one m16 tile (16 states) at a time:
-// layer 1 as m16n8k8 over the features and a constant 1 (the bias), whose FP32 output
-// fragments are, after ReLU and packing to f16, the A fragments of layer 2 as they are
-// (the accumulator of n-tiles 2k, 2k+1 is the A operand of k-step k); the same for
-// layer 3, whose B tile holds W3 in column 0.
-__device__ __forceinline__ float mlp_warp(const float *xs, const float *sb2, float b3, const uint32_t *sfrag) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
-  // A columns of layer 1 held by a lane: c = 0 features 0, 1; c = 1 feature 2 and the 1
-  const uint32_t p01 = pack_f16(xs[0], xs[1]), p2 = pack_f16(xs[2], 1.f);
-  float y = 0.f;
-#pragma unroll 1
-  for (int mt = 0; mt < 2; mt++) {
-    const int r0 = 16 * mt + g;  // the states of rows g and g + 8 of this tile
-    const uint32_t x0a = __shfl_sync(0xffffffffu, p01, r0), x0b = __shfl_sync(0xffffffffu, p2, r0);
-    const uint32_t x1a = __shfl_sync(0xffffffffu, p01, r0 + 8), x1b = __shfl_sync(0xffffffffu, p2, r0 + 8);
-    const uint32_t a10 = c == 0 ? x0a : c == 1 ? x0b : 0u, a11 = c == 0 ? x1a : c == 1 ? x1b : 0u;
-    uint32_t a2[4][4];
-#pragma unroll
-    for (int nt = 0; nt < 8; nt++) {
-      float h[4] = {0.f, 0.f, 0.f, 0.f};
-      asm volatile(
-          "mma.sync.aligned.m16n8k8.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
-          : "+f"(h[0]), "+f"(h[1]), "+f"(h[2]), "+f"(h[3])
-          : "r"(a10), "r"(a11), "r"(sfrag[FR_W1 + 32 * nt + lane]));
-      a2[nt >> 1][2 * (nt & 1)] = relu_f16x2(h[0], h[1]);
-      a2[nt >> 1][2 * (nt & 1) + 1] = relu_f16x2(h[2], h[3]);
-    }
-    float acc[8][4];
-#pragma unroll
-    for (int nt = 0; nt < 8; nt++) {
-      const float2 bb = *reinterpret_cast<const float2 *>(sb2 + 8 * nt + 2 * c);
-      acc[nt][0] = bb.x;
-      acc[nt][1] = bb.y;
-      acc[nt][2] = bb.x;
-      acc[nt][3] = bb.y;
-    }
-#pragma unroll
-    for (int ks = 0; ks < 4; ks++)
-#pragma unroll
-      for (int nt = 0; nt < 8; nt++)
-        mma_k16(acc[nt], a2[ks], *reinterpret_cast<const uint2 *>(sfrag + FR_W2 + 2 * ((nt * 4 + ks) * 32 + lane)));
-    float o[4] = {b3, 0.f, b3, 0.f};
-#pragma unroll
-    for (int ks = 0; ks < 4; ks++) {
-      const uint32_t a3[4] = {relu_f16x2(acc[2 * ks][0], acc[2 * ks][1]), relu_f16x2(acc[2 * ks][2], acc[2 * ks][3]),
-                              relu_f16x2(acc[2 * ks + 1][0], acc[2 * ks + 1][1]),
-                              relu_f16x2(acc[2 * ks + 1][2], acc[2 * ks + 1][3])};
-      mma_k16(o, a3, *reinterpret_cast<const uint2 *>(sfrag + FR_W3 + 2 * (ks * 32 + lane)));
-    }
-    // column 0: row g in o[0], row g + 8 in o[2] of lane 4 g
-    const float v0 = __shfl_sync(0xffffffffu, o[0], 4 * (lane & 7));
-    const float v1 = __shfl_sync(0xffffffffu, o[2], 4 * (lane & 7));
-    if ((lane >> 4) == mt) y = (lane & 8) ? v1 : v0;
+__global__ void __launch_bounds__(GT) k_mlp_guess(const double *__restrict__ U, int64_t stride,
+                                                  const double *__restrict__ G4, double tau_src, int64_t n,
+                                                  const __grid_constant__ MlpOuter pw, const uint4 *__restrict__ b1t,
+                                                  const uint4 *__restrict__ w2t, Norm nm, double *__restrict__ p0_out,
+                                                  int *err) {
+  using namespace rrhd_umma;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *sm = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t *sA = sm;               // [128 states][64] f16: the features, then h1
+  uint8_t *sB1 = sm + GT * 128;   // [64 hidden][64] f16: [W1 | b1 | 0]
+  uint8_t *sB2 = sB1 + H * 128;   // [64 out][64 in] f16: W2
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sB2 + H * 128);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+  const int t = threadIdx.x, warp = t >> 5;
+  for (int q = t; q < H * 128 / 16; q += GT) {
+    reinterpret_cast<uint4 *>(sB1)[q] = b1t[q];
+    reinterpret_cast<uint4 *>(sB2)[q] = w2t[q];
   }
-  return y;
+  if (t == 0) {
+    mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;\n" ::"r"(smem_u32(tslot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tslot;
+  const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's TMEM lanes
+  const uint64_t adesc = umma_desc(smem_u32(sA)), b1desc = umma_desc(smem_u32(sB1)), b2desc = umma_desc(smem_u32(sB2));
+  constexpr uint32_t idesc = umma_idesc(0, H, GT);
+  const float isig[3] = {1.f / nm.sig[0], 1.f / nm.sig[1], 1.f / nm.sig[2]};
+  const int64_t ntiles = (n + GT - 1) / GT;
+  uint32_t phase = 0;
+  bool ok = true;
+  // one MMA group and its completion (bounded waits; false after a timeout)
+  auto mma_sync = [&](uint64_t bdesc, int ksteps) -> bool {
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // A writes -> async proxy
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (t == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      for (int kk = 0; kk < ksteps; kk++) umma(tmem, adesc + 2 * kk, bdesc + 2 * kk, idesc, kk > 0 ? 1u : 0u);
+      umma_commit(bar);
+    }
+    bool got = mbar_wait(bar, phase);
+    if (!got) got = mbar_wait(bar, phase);  // a second bounded wait before giving up
+    phase ^= 1u;
+    if (__syncthreads_or(!got)) {
+      if (t == 0) atomicOr(err, 1);
+      return false;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    return true;
+  };
+  // the state of the thread's next tile is loaded one tile ahead (with the source added)
+  double un[5];
+  auto load_state = [&](int64_t rt) {
+    const int64_t i = rt * GT + t;
+    if (rt < ntiles && i < n) {
+#pragma unroll
+      for (int q = 0; q < 5; q++) un[q] = U[stride * i + q];
+      if (G4) {
+        un[4] += tau_src * G4[4 * i];
+        un[1] += tau_src * G4[4 * i + 1];
+        un[2] += tau_src * G4[4 * i + 2];
+        un[3] += tau_src * G4[4 * i + 3];
+      }
+    }
+  };
+  load_state(blockIdx.x);
+  for (int64_t rt = blockIdx.x; rt < ntiles && ok; rt += gridDim.x) {  // CTA-uniform
+    const int64_t i = rt * GT + t;
+    double u[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) u[q] = un[q];
+    load_state(rt + gridDim.x);
+    float x[3] = {0.f, 0.f, 0.f};
+    double tau = 0.0;
+    bool feat = false;
+    if (i < n) {
+      float f[3];
+      feat = features(u, f, tau);
+      if (feat)
+#pragma unroll
+        for (int a = 0; a < 3; a++) x[a] = (f[a] - nm.mu[a]) * isig[a];
+    }
+    // row t, k 0-15: the features, 1 (the bias), zeros
+    *reinterpret_cast<uint4 *>(sA + sw128_offset(t, 0)) =
+        make_uint4(pack_f16(x[0], x[1]), pack_f16(x[2], 1.f), 0u, 0u);
+    *reinterpret_cast<uint4 *>(sA + sw128_offset(t, 8)) = make_uint4(0u, 0u, 0u, 0u);
+    if (!mma_sync(b1desc, 1)) {
+      ok = false;
+      break;
+    }
+    // ReLU(h1) as f16 into row t (the MMA has read the features)
+#pragma unroll
+    for (int c0 = 0; c0 < H; c0 += 16) {
+      uint32_t r[16];
+      tmem_ld16(trow + (uint32_t)c0, r);
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+      for (int h = 0; h < 2; h++)
+        *reinterpret_cast<uint4 *>(sA + sw128_offset(t, c0 + 8 * h)) = make_uint4(
+            relu_f16x2(__uint_as_float(r[8 * h]), __uint_as_float(r[8 * h + 1])),
+            relu_f16x2(__uint_as_float(r[8 * h + 2]), __uint_as_float(r[8 * h + 3])),
+            relu_f16x2(__uint_as_float(r[8 * h + 4]), __uint_as_float(r[8 * h + 5])),
+            relu_f16x2(__uint_as_float(r[8 * h + 6]), __uint_as_float(r[8 * h + 7])));
+    }
+    if (!mma_sync(b2desc, H / 16)) {
+      ok = false;
+      break;
+    }
+    float ys[4] = {pw.b3, 0.f, 0.f, 0.f};  // four partial sums: short dependency chains
+#pragma unroll
+    for (int c0 = 0; c0 < H; c0 += 16) {
+      uint32_t r[16];
+      tmem_ld16(trow + (uint32_t)c0, r);
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+      for (int q = 0; q < 16; q++)
+        ys[q & 3] = fmaf(pw.b2w3[c0 + q][1], fmaxf(__uint_as_float(r[q]) + pw.b2w3[c0 + q][0], 0.f), ys[q & 3]);
+    }
+    const float y = (ys[0] + ys[1]) + (ys[2] + ys[3]);
+    if (i < n) p0_out[i] = (feat && isfinite(y)) ? tau * (double)__expf(y * nm.sig_t + nm.mu_t) : 0.0;
+    // this tile's TMEM reads and A reads are ordered before the next tile's writes and MMA
+    // by the next barrier
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;\n" ::"r"(tmem));
+  }
 }
 
 // PhysPressureFix out of line: the rare fallback does not add to the registers of the
@@ -308,103 +394,87 @@ __device__ __noinline__ FixState pressure_fix_call(Eos eos, FixState s) {
   return s;
 }
 
-// States i live at U + stride*i and W + stride*i (stride 5 for separate arrays,
-// 10 for a solver state [n][10] = U, W).  With G4 != NULL the radiation source
-// is added first, U.E += tau G0 and U.S += tau G[1..3] (radRHD_main.cpp:117-126).
+// The Newton kernel (the structure of the plain k_c2p_stats: 8 states per thread, the
+// states that fail set aside in shared memory for a second pass).  States i live at
+// U + stride*i and W + stride*i (stride 5 for separate arrays, 10 for a solver state
+// [n][10] = U, W).  With G4 != NULL the radiation source is added first, U.E += tau G0 and
+// U.S += tau G[1..3] (radRHD_main.cpp:117-126), and U is written back.  Per state: Newton
+// from the learned guess p0[i] for at most k_stall iterations; if that stalls, or p0[i] is
+// not a usable guess, the reference solve from its own guess; then (second pass)
+// PhysPressureFix when fallback != 0.
+constexpr int kGThreads = 256;
+constexpr int kGPerThread = 8;
+constexpr int kGPerBlock = kGThreads * kGPerThread;
 #ifndef RRHD_MLP_MIN_BLOCKS
-#define RRHD_MLP_MIN_BLOCKS 4  // CTAs per SM the register budget of k_c2p_mlp is sized for
+#define RRHD_MLP_MIN_BLOCKS 3  // CTAs per SM the register budget of k_c2p_guess is sized for
 #endif
-__global__ void __launch_bounds__(IT, RRHD_MLP_MIN_BLOCKS) k_c2p_mlp(Eos eos, double *U, double *W, int64_t stride, const double *G4,
-                                                double tau_src, uint8_t *status, int64_t n, int fallback,
-                                                int k_stall, const float *__restrict__ theta,
-                                                const uint32_t *__restrict__ frag, Norm nm, MlpPartial *scratch,
-                                                double *guess_out) {
-  __shared__ __align__(16) float sb2[H];
-  __shared__ __align__(16) uint32_t sfrag[NFRAG];
-  __shared__ unsigned long long red[6][IT / 32];
-  for (int q = threadIdx.x; q < H; q += IT) sb2[q] = theta[OFF_B2 + q];
-  for (int q = threadIdx.x; q < NFRAG; q += IT) sfrag[q] = frag[q];
-  const float b3 = theta[OFF_B3];
+__global__ void __launch_bounds__(kGThreads, RRHD_MLP_MIN_BLOCKS)
+    k_c2p_guess(Eos eos, double *U, double *W, int64_t stride, const double *G4, double tau_src,
+                const double *__restrict__ p0s, uint8_t *status, int64_t n, int fallback, int k_stall,
+                MlpPartial *scratch) {
+  __shared__ unsigned short s_fail[kGPerBlock];  // local index | code << 12
+  __shared__ int s_nfail;
+  __shared__ unsigned long long red[6][kGThreads / 32];
+  if (threadIdx.x == 0) s_nfail = 0;
   __syncthreads();
-  unsigned ok = 0, gfb = 0, fb = 0, failed = 0, iters = 0, mx = 0;  // per thread (u32: a thread sees few states)
-  const int lane = threadIdx.x & 31;
-  const int64_t nwarps_total = (int64_t)gridDim.x * (IT / 32);
-  for (int64_t w = (int64_t)blockIdx.x * (IT / 32) + (threadIdx.x >> 5); w * 32 < n; w += nwarps_total) {
-    const int64_t i = w * 32 + lane;
-    const bool live = i < n;
-    // the state (with the radiation source added) is read twice: for the features, and
-    // again after the network, so that it is not held in registers across the network
-    auto load_u = [&](double *u) {
-      for (int q = 0; q < 5; q++) u[q] = U[stride * i + q];
-      if (G4) {
-        u[4] += tau_src * G4[4 * i];
-        u[1] += tau_src * G4[4 * i + 1];
-        u[2] += tau_src * G4[4 * i + 2];
-        u[3] += tau_src * G4[4 * i + 3];
-      }
-    };
-    float f[3] = {0.f, 0.f, 0.f};
-    double tau = 0.0;
-    bool feat = false;
-    if (live) {
-      double u0[5];
-      load_u(u0);
-      feat = features(u0, f, tau);
+  unsigned ok = 0, gfb = 0, fb = 0, failed = 0, iters = 0, mx = 0;
+  const int64_t base = (int64_t)blockIdx.x * kGPerBlock;
+  for (int k = 0; k < kGPerThread; k++) {
+    const int loc = k * kGThreads + threadIdx.x;
+    const int64_t i = base + loc;
+    if (i >= n) break;
+    double u[5], w[5];
+    for (int q = 0; q < 5; q++) {
+      u[q] = U[stride * i + q];
+      w[q] = W[stride * i + q];
     }
-    float xs[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) xs[a] = feat ? (f[a] - nm.mu[a]) / nm.sig[a] : 0.f;
-    const float y = mlp_warp(xs, sb2, b3, sfrag);
-    double u[5] = {0, 0, 0, 0, 0}, wv[5] = {0, 0, 0, 0, 0};
-    if (live) {
-      load_u(u);
-      for (int q = 0; q < 5; q++) wv[q] = W[stride * i + q];
+    if (G4) {
+      u[4] += tau_src * G4[4 * i];
+      u[1] += tau_src * G4[4 * i + 1];
+      u[2] += tau_src * G4[4 * i + 2];
+      u[3] += tau_src * G4[4 * i + 3];
+      for (int q = 0; q < 5; q++) U[stride * i + q] = u[q];
     }
-    if (!live) continue;
-    bool u_dirty = G4 != nullptr;
-    feat = feat && isfinite(y);  // an f16 overflow inside the network: the reference guess
-    const double p0 = feat ? tau * (double)__expf(y * nm.sig_t + nm.mu_t) : 0.0;
-    if (feat && guess_out) guess_out[i] = p0;
-    // attempt 0: Newton from the learned guess for at most k_stall iterations; attempt 1
-    // (a stalled or unusable guess): the reference solve from its own guess
+    const double p0 = p0s[i];
+    const bool usable = p0 > 0.0;
     int code = 1, itn = 0;
-    if (!feat) gfb++;
-    for (int attempt = feat ? 0 : 1; attempt < 2; attempt++) {
+    if (!usable) gfb++;
+    for (int attempt = usable ? 0 : 1; attempt < 2; attempt++) {
       int it = 0;
-      code = c2p_from(eos, u, wv, p0, attempt == 0, &it, attempt == 0 ? k_stall : RRHD_MAX_ITER);
+      code = c2p_from(eos, u, w, p0, attempt == 0, &it, attempt == 0 ? k_stall : RRHD_MAX_ITER);
       itn += it;
       if (code == 0) break;
       if (attempt == 0) gfb++;
     }
-    if (code == 0) ok++;
     iters += (unsigned)itn;
     mx = (unsigned)itn > mx ? (unsigned)itn : mx;
-    if (code) {
-      if (fallback) {
-        FixState fs;
-#pragma unroll
-        for (int q = 0; q < 5; q++) {
-          fs.u[q] = u[q];
-          fs.w[q] = wv[q];
-        }
-        fs = pressure_fix_call(eos, fs);
-#pragma unroll
-        for (int q = 0; q < 5; q++) {
-          u[q] = fs.u[q];
-          wv[q] = fs.w[q];
-        }
-        const int fix = fs.code;
-        code = code | 0x10 | (fix ? 0x20 : 0);
-        fb++;
-        failed += fix ? 1 : 0;
-        u_dirty = true;
-      } else {
-        failed++;
-      }
+    if (code == 0) {
+      ok++;
+      for (int q = 0; q < 5; q++) W[stride * i + q] = w[q];
+      if (status) status[i] = 0;
+    } else {
+      s_fail[atomicAdd(&s_nfail, 1)] = (unsigned short)(loc | (code << 12));
     }
-    if (u_dirty)
-      for (int q = 0; q < 5; q++) U[stride * i + q] = u[q];
-    for (int q = 0; q < 5; q++) W[stride * i + q] = wv[q];
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < s_nfail; q += kGThreads) {
+    const int64_t i = base + (s_fail[q] & 0xfff);
+    int code = s_fail[q] >> 12;
+    FixState fs;
+    for (int r = 0; r < 5; r++) {
+      fs.u[r] = U[stride * i + r];
+      fs.w[r] = W[stride * i + r];
+    }
+    if (fallback) {
+      fs = pressure_fix_call(eos, fs);
+      code = code | 0x10 | (fs.code ? 0x20 : 0);
+      fb++;
+      failed += fs.code ? 1 : 0;
+      for (int r = 0; r < 5; r++) U[stride * i + r] = fs.u[r];
+    } else {
+      failed++;
+    }
+    for (int r = 0; r < 5; r++) W[stride * i + r] = fs.w[r];
     if (status) status[i] = (uint8_t)code;
   }
   unsigned long long okl = ok, gfbl = gfb, fbl = fb, failedl = failed, itl = iters, mxl = mx;
@@ -419,7 +489,7 @@ __global__ void __launch_bounds__(IT, RRHD_MLP_MIN_BLOCKS) k_c2p_mlp(Eos eos, do
     mxl = m2 > mxl ? m2 : mxl;
   }
   const int wid = threadIdx.x >> 5;
-  if (lane == 0) {
+  if ((threadIdx.x & 31) == 0) {
     red[0][wid] = okl;
     red[1][wid] = gfbl;
     red[2][wid] = fbl;
@@ -429,8 +499,8 @@ __global__ void __launch_bounds__(IT, RRHD_MLP_MIN_BLOCKS) k_c2p_mlp(Eos eos, do
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    MlpPartial p = {0, 0, 0, 0, 0, 0};
-    for (int q = 0; q < IT / 32; q++) {
+    MlpPartial p = {0, 0, 0, 0, 0, 0, 0};
+    for (int q = 0; q < kGThreads / 32; q++) {
       p.ok += red[0][q];
       p.guess_fallback += red[1][q];
       p.fallback += red[2][q];
@@ -442,10 +512,12 @@ __global__ void __launch_bounds__(IT, RRHD_MLP_MIN_BLOCKS) k_c2p_mlp(Eos eos, do
   }
 }
 
-__global__ void k_mlp_stats_reduce(MlpPartial *scratch, int nblocks) {
-  if (threadIdx.x != 0) return;
-  MlpPartial t = {0, 0, 0, 0, 0, 0};
-  for (int b = 0; b < nblocks; b++) {
+// Sums the per-CTA partials into scratch[nblocks] (integer counts: exact in any order) and
+// moves the guess kernel's error word into it (err reset for the next call).
+__global__ void __launch_bounds__(256) k_mlp_stats_reduce(MlpPartial *scratch, int nblocks, int *err) {
+  __shared__ MlpPartial red[256];
+  MlpPartial t = {0, 0, 0, 0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nblocks; b += 256) {
     const MlpPartial q = scratch[b];
     t.ok += q.ok;
     t.guess_fallback += q.guess_fallback;
@@ -454,7 +526,26 @@ __global__ void k_mlp_stats_reduce(MlpPartial *scratch, int nblocks) {
     t.iters += q.iters;
     t.max_iters = q.max_iters > t.max_iters ? q.max_iters : t.max_iters;
   }
-  scratch[nblocks] = t;
+  red[threadIdx.x] = t;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      MlpPartial &a = red[threadIdx.x];
+      const MlpPartial b = red[threadIdx.x + o];
+      a.ok += b.ok;
+      a.guess_fallback += b.guess_fallback;
+      a.fallback += b.fallback;
+      a.failed += b.failed;
+      a.iters += b.iters;
+      a.max_iters = b.max_iters > a.max_iters ? b.max_iters : a.max_iters;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    red[0].err = (unsigned long long)*err;
+    *err = 0;
+    scratch[nblocks] = red[0];
+  }
 }
 
 Eos make_eos(int eos, double gamma) {
@@ -470,17 +561,30 @@ Eos make_eos(int eos, double gamma) {
 struct rrhd_mlp {
   int device = 0;
   float *d_theta = nullptr, *d_m = nullptr, *d_v = nullptr, *d_grad = nullptr;
-  uint32_t *d_frag = nullptr;
+  __half *d_b1t = nullptr, *d_w2t = nullptr;  // [W1 | b1] and W2 as the f16 UMMA operands
+  MlpOuter outer{};         // b2, W3, b3 for the guess kernel's parameter
   MlpPartial *d_stats = nullptr;
   int stats_cap = 0;
+  double *d_guess = nullptr;  // initial pressures when the caller passes no array
+  int64_t guess_cap = 0;
+  int *d_err = nullptr;  // a wait of the guess kernel that timed out
   Norm norm{{0, 0, 0}, {1, 1, 1}, 0, 1};
   int adam_t = 0;
   int num_sms = 148;
 };
 
+// the inference copies of the parameters (after every change of d_theta)
 static rrhd_status mlp_refresh(rrhd_mlp *m, cudaStream_t st) {
-  k_pack_frags<<<6, 256, 0, st>>>(m->d_theta, m->d_frag);
+  k_pack_b<<<H * H / 256, 256, 0, st>>>(m->d_theta, m->d_b1t, m->d_w2t);
   RRHD_CUDA(cudaGetLastError());
+  std::vector<float> th(NPARAM);
+  RRHD_CUDA(cudaMemcpyAsync(th.data(), m->d_theta, NPARAM * sizeof(float), cudaMemcpyDeviceToHost, st));
+  RRHD_CUDA(cudaStreamSynchronize(st));
+  for (int j = 0; j < H; j++) {
+    m->outer.b2w3[j][0] = th[OFF_B2 + j];
+    m->outer.b2w3[j][1] = th[OFF_W3 + j];
+  }
+  m->outer.b3 = th[OFF_B3];
   return RRHD_OK;
 }
 
@@ -501,13 +605,15 @@ extern "C" rrhd_status rrhd_mlp_create(int32_t device, uint64_t seed, rrhd_mlp *
   for (int q = 0; q < H * H; q++) th[OFF_W2 + q] = (float)(normal(1000 + q) * std::sqrt(2.0 / H));
   for (int q = 0; q < H; q++) th[OFF_W3 + q] = (float)(normal(9000 + q) * std::sqrt(1.0 / H));
   if (cudaMalloc(&m->d_theta, NPARAM * 4) || cudaMalloc(&m->d_m, NPARAM * 4) || cudaMalloc(&m->d_v, NPARAM * 4) ||
-      cudaMalloc(&m->d_grad, NPARAM * 4) || cudaMalloc(&m->d_frag, NFRAG * 4)) {
+      cudaMalloc(&m->d_grad, NPARAM * 4) || cudaMalloc(&m->d_b1t, H * H * 2) || cudaMalloc(&m->d_w2t, H * H * 2) ||
+      cudaMalloc(&m->d_err, sizeof(int))) {
     rrhd_mlp_destroy(m);
     return rrhd_fail(RRHD_ERR_OOM, "network allocation failed");
   }
   cudaMemcpy(m->d_theta, th.data(), NPARAM * 4, cudaMemcpyHostToDevice);
   cudaMemset(m->d_m, 0, NPARAM * 4);
   cudaMemset(m->d_v, 0, NPARAM * 4);
+  cudaMemset(m->d_err, 0, sizeof(int));
   rrhd_status s = mlp_refresh(m, 0);
   if (s) {
     rrhd_mlp_destroy(m);
@@ -525,7 +631,10 @@ extern "C" rrhd_status rrhd_mlp_destroy(rrhd_mlp *m) {
   cudaFree(m->d_m);
   cudaFree(m->d_v);
   cudaFree(m->d_grad);
-  cudaFree(m->d_frag);
+  cudaFree(m->d_b1t);
+  cudaFree(m->d_w2t);
+  cudaFree(m->d_guess);
+  cudaFree(m->d_err);
   cudaFree(m->d_stats);
   delete m;
   return RRHD_OK;
@@ -751,19 +860,52 @@ rrhd_status rrhd::mlp_c2p(const rrhd_mlp *m, int eos, double gamma, double *U, d
                           const double *G4, double tau_src, uint8_t *status, int64_t n, int fallback, int k_stall,
                           rrhd_c2p_stats *stats, int64_t *n_guess_fallback, double *guess, cudaStream_t st) {
   rrhd_mlp *mm = const_cast<rrhd_mlp *>(m);
-  const int64_t warps = (n + 31) / 32;
-  const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>((warps + IT / 32 - 1) / (IT / 32), 8 * m->num_sms));
-  if (mm->stats_cap < nblk + 1) {
+  const int nblk = (int)std::max<int64_t>(1, (n + kGPerBlock - 1) / kGPerBlock);
+  if (mm->stats_cap < nblk + 1 || (!guess && mm->guess_cap < n)) {
     RRHD_CUDA(cudaStreamSynchronize(st));
-    cudaFree(mm->d_stats);
-    mm->d_stats = nullptr;
-    RRHD_CUDA(cudaMalloc(&mm->d_stats, sizeof(MlpPartial) * (nblk + 1)));
-    mm->stats_cap = nblk + 1;
+    if (mm->stats_cap < nblk + 1) {
+      cudaFree(mm->d_stats);
+      mm->d_stats = nullptr;
+      RRHD_CUDA(cudaMalloc(&mm->d_stats, sizeof(MlpPartial) * (nblk + 1)));
+      mm->stats_cap = nblk + 1;
+    }
+    if (!guess && mm->guess_cap < n) {
+      cudaFree(mm->d_guess);
+      mm->d_guess = nullptr;
+      RRHD_CUDA(cudaMalloc(&mm->d_guess, sizeof(double) * n));
+      mm->guess_cap = n;
+    }
   }
-  k_c2p_mlp<<<nblk, IT, 0, st>>>(make_eos(eos, gamma), U, W, stride, G4, tau_src, status, n, fallback, k_stall,
-                                 m->d_theta, m->d_frag, m->norm, mm->d_stats, guess);
-  RRHD_CUDA(cudaGetLastError());
-  k_mlp_stats_reduce<<<1, 32, 0, st>>>(mm->d_stats, nblk);
+  double *p0 = guess ? guess : mm->d_guess;
+  if (n > 0) {
+    // persistent CTAs: as many as are resident at once, from the kernel's registers and
+    // shared memory (the occupancy calculator counts one CTA per SM for a kernel that
+    // allocates tensor memory) and the 512 TMEM columns (64 per CTA)
+    static int per_sm = 0;
+    if (per_sm == 0) {
+      RRHD_CUDA(cudaFuncSetAttribute(k_mlp_guess, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
+      cudaFuncAttributes fa;
+      RRHD_CUDA(cudaFuncGetAttributes(&fa, k_mlp_guess));
+      int smem_sm = 0;
+      RRHD_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, m->device));
+      const int by_regs = 65536 / (((fa.numRegs + 7) & ~7) * GT);
+      const int by_smem = smem_sm / (G_SMEM + 1024);
+      per_sm = std::max(1, std::min(std::min(by_regs, by_smem), 512 / 64));
+    }
+    const int64_t tiles = (n + GT - 1) / GT;
+    const unsigned gblk = (unsigned)std::min<int64_t>(tiles, (int64_t)per_sm * m->num_sms);
+    k_mlp_guess<<<gblk, GT, G_SMEM, st>>>(U, stride, G4, tau_src, n, m->outer,
+                                          reinterpret_cast<const uint4 *>(m->d_b1t),
+                                          reinterpret_cast<const uint4 *>(m->d_w2t), m->norm, p0, mm->d_err);
+    RRHD_CUDA(cudaGetLastError());
+    k_c2p_guess<<<nblk, kGThreads, 0, st>>>(make_eos(eos, gamma), U, W, stride, G4, tau_src, p0, status, n, fallback,
+                                            k_stall, mm->d_stats);
+    RRHD_CUDA(cudaGetLastError());
+  } else {
+    RRHD_CUDA(cudaMemsetAsync(mm->d_stats, 0, sizeof(MlpPartial), st));
+  }
+  k_mlp_stats_reduce<<<1, 256, 0, st>>>(mm->d_stats, nblk, mm->d_err);
   RRHD_CUDA(cudaGetLastError());
   if (stats || n_guess_fallback) {
     MlpPartial t;
@@ -777,6 +919,7 @@ rrhd_status rrhd::mlp_c2p(const rrhd_mlp *m, int eos, double gamma, double *U, d
       stats->max_iters = (int32_t)t.max_iters;
     }
     if (n_guess_fallback) *n_guess_fallback = (int64_t)t.guess_fallback;
+    if (t.err) return rrhd_fail(RRHD_ERR_CUDA, "learned-guess kernel: a tensor-core completion wait timed out");
   }
   return RRHD_OK;
 }
@@ -784,7 +927,8 @@ rrhd_status rrhd::mlp_c2p(const rrhd_mlp *m, int eos, double gamma, double *U, d
 // con2prim batch seeded by the network: Newton from the learned guess for at
 // most k_stall iterations, then (if needed) the reference solve from its own
 // guess, then PhysPressureFix when fallback != 0.  stats (host, may be NULL).
-// guess (device [n], may be NULL) receives the learned initial pressures.
+// guess (device [n], may be NULL) receives the learned initial pressures (0 where the
+// network gives no usable guess).
 extern "C" rrhd_status rrhd_con2prim_batch_mlp(const rrhd_mlp *m, int32_t eos, double gamma, double *U, double *W,
                                                uint8_t *status, int64_t n, int32_t fallback, int32_t k_stall,
                                                rrhd_c2p_stats *stats, int64_t *n_guess_fallback, double *guess,

@@ -51,8 +51,10 @@
 #include "rrhd_internal.h"
 
 #include "dirs.h"
+#include "umma.cuh"
 
 namespace {
+using namespace rrhd_umma;
 
 constexpr int kForms = 4;
 enum { FORM_BF16X3 = 0, FORM_F16X3 = 1, FORM_F16 = 2, FORM_BF16 = 3 };
@@ -82,37 +84,6 @@ constexpr int MAX_HALF = (NT + NMOM) / 2;              // accumulator columns pe
 constexpr int A32_BYTES = BM * BK * 4;                  // 32 KiB FP32 intensity tile
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + A32_STAGES * A32_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 constexpr float kF16BScale = 256.0f;
-constexpr long long kSpinLimit = 1ll << 22;  // polls before a wait is declared timed out
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-  asm volatile("{\n.reg .b64 st;\nmbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("{\n.reg .b64 st;\nmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-// Bounded wait for the phase with the given parity; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  const uint32_t a = smem_u32(bar);
-  for (long long i = 0; i < kSpinLimit; i++) {
-    uint32_t done;
-    asm volatile(
-        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
 
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
   asm volatile(
@@ -122,34 +93,8 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 
-// UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t addr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((addr & 0x3FFFF) >> 4);
-  d |= (uint64_t)1 << 16;            // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;  // stride byte offset
-  d |= (uint64_t)1 << 46;            // descriptor version for sm_100
-  d |= (uint64_t)2 << 61;            // SWIZZLE_128B
-  return d;
-}
-
-// Instruction descriptor, kind::f16: D f32, A/B bf16 (fmt 1) or f16 (fmt 0), both K-major.
-__host__ __device__ constexpr uint32_t umma_idesc(int fmt, int n) {
-  return (1u << 4) | ((uint32_t)fmt << 7) | ((uint32_t)fmt << 10) | ((uint32_t)(n >> 3) << 17) |
-         ((uint32_t)(BM >> 4) << 24);
-}
-
-__device__ __forceinline__ void umma(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                     uint32_t accumulate) {
-  asm volatile(
-      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-__device__ __forceinline__ void umma_commit(uint64_t *bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
-               : "memory");
-}
+// instruction descriptor of the BM-row tiles
+__host__ __device__ constexpr uint32_t umma_idesc(int fmt, int n) { return rrhd_umma::umma_idesc(fmt, n, BM); }
 
 // Four values to packed hi (and lo) 16-bit parts: hi = round-to-nearest 16-bit value, lo =
 // the rounded remainder (the three-product forms), two values per conversion instruction.
