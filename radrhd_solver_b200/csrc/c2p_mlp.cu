@@ -423,11 +423,8 @@ __global__ void __launch_bounds__(kGThreads, RRHD_MLP_MIN_BLOCKS)
     const int loc = k * kGThreads + threadIdx.x;
     const int64_t i = base + loc;
     if (i >= n) break;
-    double u[5], w[5];
-    for (int q = 0; q < 5; q++) {
-      u[q] = U[stride * i + q];
-      w[q] = W[stride * i + q];
-    }
+    double u[5], w[5];  // w: the solve's output (the Newton solve reads no old W)
+    for (int q = 0; q < 5; q++) u[q] = U[stride * i + q];
     if (G4) {
       u[4] += tau_src * G4[4 * i];
       u[1] += tau_src * G4[4 * i + 1];

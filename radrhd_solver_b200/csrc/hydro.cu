@@ -384,11 +384,8 @@ __global__ void __launch_bounds__(kC2pThreads, RRHD_C2P_MIN_BLOCKS) k_c2p_stats(
     const int loc = k * kC2pThreads + threadIdx.x;
     const int64_t i = base + loc;
     if (i >= n) break;
-    double u[5], w[5];
-    for (int q = 0; q < 5; q++) {
-      u[q] = U[5 * i + q];
-      w[q] = W[5 * i + q];
-    }
+    double u[5], w[5];  // w: the solve's output (the Newton solve reads no old W)
+    for (int q = 0; q < 5; q++) u[q] = U[5 * i + q];
     int it = 0;
     const int code = c2p_from(eos, u, w, 0.0, false, &it);
     it_sum += (unsigned)it;
