@@ -273,7 +273,10 @@ rrhd_status rrhd_mlp_gradient(rrhd_mlp *m, const double *U, const double *p, int
 /* con2prim batch seeded by the network: Newton from the learned guess for at
  * most k_stall iterations, else the reference solve from its own guess, then
  * PhysPressureFix when fallback != 0.  stats / n_guess_fallback (host) and
- * guess (device [n], the learned initial pressures) may be NULL. */
+ * guess (device [n], the learned initial pressures, 0 where the network gives
+ * no usable guess) may be NULL.  The network object holds the call's scratch
+ * (per-CTA statistics, the guesses when guess is NULL): calls with one object
+ * must not overlap (one stream, or the caller serialises them). */
 rrhd_status rrhd_con2prim_batch_mlp(const rrhd_mlp *m, int32_t eos, double gamma, double *U, double *W,
                                     uint8_t *status, int64_t n, int32_t fallback, int32_t k_stall,
                                     rrhd_c2p_stats *stats, int64_t *n_guess_fallback, double *guess,
