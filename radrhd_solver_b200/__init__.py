@@ -12,7 +12,8 @@ which raises ImportError when librrhd.so is missing (there is no fallback).
 """
 import importlib
 
-__all__ = ["c2p_mlp", "files_sys", "illum", "illum_mpi", "mesh", "rad_rhd", "ray_tracing", "rhllc", "rhllc_mpi"]
+__all__ = ["c2p_mlp", "files_sys", "illum", "illum_mpi", "mesh", "rad_rhd", "rad_rhd_mpi", "ray_tracing", "rhllc",
+           "rhllc_mpi"]
 
 
 def __getattr__(name):
