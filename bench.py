@@ -703,6 +703,7 @@ def run_ours(args):
 
     m, W = make_jet()
     g = rhllc.Grid(m, eos=rhllc.EOS_IDEAL, gamma=GAMMA, device=dev, cells_per_block=args.cpb)
+    layout = g.layout_info()
     g.set_boundary(-3, rhllc.BC_FIXED, INFLOW)
     g.set_state_prim(W)
     tau = CFL * m.h_min
@@ -787,7 +788,10 @@ def run_ours(args):
                          "peak_source": "measured" if pk else "fallback",
                          "algorithmic_bytes_per_cell_update": alg_bytes / m.n_cells,
                          # the bound that binds: FP64 dependency chains (ncu, 64^3 capture of the same kernel)
-                         "fp64_pipe_active_pct": fp64_pipe},
+                         "fp64_pipe_active_pct": fp64_pipe,
+                         # faces between two CTA blocks are fluxed by both (lists padded to even lengths)
+                         "face_flux_evaluations_per_face": layout["face_entries"] / layout["faces"],
+                         "cells_per_block": layout["cells_per_block"]},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
             "e2e_resident": e2e_res,
             "gpu_launches": args.steps,

@@ -95,6 +95,12 @@ typedef struct {
  * (cuda/include/short_characteristics/separate_gpu/cuda_multi_interface.h:44)
  * and grid_t::InitMemory (lib/grids/src/solvers_struct.cpp:146-180). */
 rrhd_status rrhd_create(const rrhd_mesh_desc *mesh, const rrhd_opts *opts, rrhd_ctx **out);
+/* The step kernel's layout (no counterpart in the reference): cells per CTA, the number of
+ * CTA blocks, and face_entries, the length of all CTAs' face lists together (a face between
+ * two CTAs' blocks is fluxed by both; each list is padded to an even length), against the
+ * mesh's faces.  Any pointer may be NULL. */
+rrhd_status rrhd_hydro_layout_info(const rrhd_ctx *ctx, int32_t *cells_per_block, int32_t *blocks,
+                                   int64_t *face_entries, int64_t *faces);
 
 /* Frees everything.  Stands behind separate_device::ClearDevice / ClearHost
  * (cuda_multi_interface.h:50, :57). */

@@ -113,6 +113,7 @@ _SIGS = {
     "rrhd_part_plan": (I32, [P, P, I32, I32, I32, P, P, P, P, P]),
     "rrhd_hydro_set_part": (I32, [P, I32, I32]),
     "rrhd_hydro_part_info": (I32, [P, P, P, P, P]),
+    "rrhd_hydro_layout_info": (I32, [P, P, P, P, P]),
     "rrhd_hydro_pack_halo": (I32, [P, P]),
     "rrhd_hydro_unpack_halo": (I32, [P, P]),
     "rrhd_hydro_max_speed_ptr": (I32, [P, P]),

@@ -759,6 +759,16 @@ extern "C" rrhd_status rrhd_set_state(rrhd_ctx *c, const double *W, const double
   return state_transfer(c, const_cast<double *>(W), const_cast<double *>(U), stride, where, true);
 }
 
+extern "C" rrhd_status rrhd_hydro_layout_info(const rrhd_ctx *c, int32_t *cells_per_block, int32_t *blocks,
+                                              int64_t *face_entries, int64_t *faces) {
+  RRHD_CHECK_ARG(c, "null context");
+  if (cells_per_block) *cells_per_block = c->cpb;
+  if (blocks) *blocks = c->nblocks;
+  if (face_entries) *face_entries = c->n_entries;
+  if (faces) *faces = c->F;
+  return RRHD_OK;
+}
+
 extern "C" rrhd_status rrhd_get_state(rrhd_ctx *c, double *W, double *U, int64_t stride, int32_t where) {
   return state_transfer(c, W, U, stride, where, false);
 }

@@ -107,6 +107,14 @@ class Grid:
     def sync(self):
         L.check(L.lib.rrhd_sync(self._h), "sync")
 
+    def layout_info(self):
+        """The step kernel's layout: cells per CTA, CTA blocks, the length of all CTAs' face
+        lists together (faces between two blocks are fluxed by both) and the mesh's faces."""
+        cpb, nb, fe, f = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int64()
+        L.check(L.lib.rrhd_hydro_layout_info(self._h, C.byref(cpb), C.byref(nb), C.byref(fe), C.byref(f)),
+                "rrhd_hydro_layout_info")
+        return {"cells_per_block": cpb.value, "blocks": nb.value, "face_entries": fe.value, "faces": f.value}
+
 
 def _where(W, U):
     t = W if W is not None else U

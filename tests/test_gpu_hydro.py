@@ -296,3 +296,19 @@ def test_config0_shock_tube_200_steps_matches_reference():
     g.close()
     if use_ref:
         ref.close()
+
+
+@pytest.mark.parametrize("cpb", [128, 256])
+def test_layout_info_counts_the_cta_face_lists(cpb):
+    """rrhd_hydro_layout_info: the CTA blocks cover the cells, and the CTAs' face lists hold
+    every face at least once and at most twice (a face between two blocks is fluxed by both;
+    each list padded to an even length, at most one pad per block)."""
+    m, _ = shock_tube(12, 3, 3)
+    g = rhllc.Grid(m, gamma=GAMMA_53, cells_per_block=cpb)
+    info = g.layout_info()
+    g.close()
+    assert info["cells_per_block"] == cpb
+    assert info["blocks"] == -(-m.n_cells // cpb)
+    assert info["faces"] == m.n_faces
+    assert m.n_faces <= info["face_entries"] <= 2 * m.n_faces + info["blocks"]
+    print(f"\n{cpb} cells per CTA: {info['face_entries'] / m.n_faces:.3f} face flux evaluations per face")
