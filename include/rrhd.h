@@ -498,7 +498,7 @@ rrhd_status rrhd_rad_source(const rrhd_emission *em, const double *W, const doub
 typedef struct {
   int32_t groups;         /* frequency groups G >= 1 (grey copies, rows cell * G + g)           */
   int32_t precision;      /* RRHD_RAD_FP64, RRHD_RAD_FP32 or RRHD_RAD_MIXED                     */
-  int32_t dirs_per_batch; /* directions swept together (face values [F][dirs_per_batch][groups] are
+  int32_t dirs_per_batch; /* directions swept together (face values [dirs_per_batch][F][groups] are
                              kept for them): power of two <= 256; 0 = min(64, M)                */
   double boundary_value;  /* intensity entering through boundary faces (illum::BoundaryConditions
                              returns 0 for free, lock and outer boundaries, illum_utils.cpp:52-65) */

@@ -75,7 +75,7 @@ struct RadState {
   // context numbering or -1), then the step's source record {k, betta/k, alpha Q_g/k}
   void *d_rec = nullptr;
   void *d_area = nullptr;  // [N][4] face areas
-  uint32_t *d_plan = nullptr;               // all batches: items (cell << shift | d) in level order
+  uint32_t *d_plan = nullptr;               // all batches: items (d << shift | cell) in level order
   bool item_geometry = false;
   uint4 *d_geo = nullptr;                   // item_geometry: per plan item {code, in-face distances}
   std::vector<std::vector<int64_t>> lvl;    // per batch: level offsets into d_plan
@@ -88,7 +88,7 @@ struct RadState {
   // start and 4 source done (side stream), 5 join, 6 scattering done
   cudaEvent_t ev[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   cudaStream_t side = nullptr;  // the coupled step's source term runs here, beside the sweep
-  void *d_fv = nullptr;  // [F][DB][GS] face values
+  void *d_fv = nullptr;  // [DB][F][GS] face values, direction-major
   // coupled step (context numbering, [N][M][G])
   void *d_I = nullptr, *d_S = nullptr;
   double *d_G4 = nullptr;                                    // [N][4] radiation 4-force of the last step

@@ -9,7 +9,7 @@
 // pairs of a level are independent, so one level is one kernel launch with one
 // thread per pair, and a sweep is one CUDA graph of all level launches.  A batch
 // of DB directions is swept together, so the face values of one batch,
-// [F][DB][G], are the only scratch.
+// [DB][F][G] (direction-major), are the only scratch.
 //
 // Per pair the kernel classifies the four faces by the sign of n_j . w, traces
 // the three nodes of each out-face back to the in-face they came through (the
@@ -95,11 +95,12 @@ struct SweepArgs {
   const SweepIO *io;
   const uint32_t *items;
   int64_t n;  // items of this level
-  int shift, DB, d0, M, G, RW, GS, nbd;
+  int shift, DB, d0, M, G, RW, GS, nbd;  // item = direction << shift | cell
+  int64_t NF;                            // face-value slots
   const T *w;     // [M][3]
   const T *rec;   // [N][RW]
   const T *area;  // [N][4] face areas (cell values)
-  TV *fv;         // [F][DB][GS] face values (GS >= G, full 32-byte sectors)
+  TV *fv;         // [DB][NF][GS] face values, direction-major (GS >= G, full 32-byte sectors)
   const uint4 *geo;  // per item of the level (items[i] <-> geo[i]): its geometry, or null
   TV bc;
   int64_t last;
@@ -229,8 +230,8 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T, TV> 
   const uint32_t it = a.items[i];
   uint4 gq = make_uint4(0u, 0u, 0u, 0u);
   if constexpr (PRE) gq = __ldcs(a.geo + i);  // read once per sweep, in item order
-  const int64_t c = it >> a.shift;
-  const int dl = (int)(it & (uint32_t)(a.DB - 1));
+  const int64_t c = it & ((1u << a.shift) - 1u);
+  const int dl = (int)(it >> a.shift);
   const int d = a.d0 + dl;
   int fid[4];
   T r[4];
@@ -326,7 +327,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T, TV> 
     asm volatile("griddepcontrol.wait;" ::: "memory");
     auto in_face = [&](int j, TV (&fj)[GT]) {
       if (((code >> j) & 1u) && fid[j] >= 0) {
-        ld_groups<TV, GT>(a.fv + ((int64_t)fid[j] * a.DB + dl) * a.GS, fj);
+        ld_groups<TV, GT>(a.fv + ((int64_t)dl * a.NF + fid[j]) * a.GS, fj);
       } else {
 #pragma unroll
         for (int q = 0; q < GT; q++) fj[q] = a.bc;
@@ -367,7 +368,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T, TV> 
         out[q] = Icur * (TV)0.3333333333333333;
       }
       const int64_t fj = j == 0 ? fid0 : j == 1 ? fid1 : j == 2 ? fid2 : fid3;
-      st_slot<TV, GT>(a.fv + (fj * a.DB + dl) * a.GS, out);
+      st_slot<TV, GT>(a.fv + ((int64_t)dl * a.NF + fj) * a.GS, out);
     }
   } else {
     asm volatile("griddepcontrol.wait;" ::: "memory");
@@ -376,7 +377,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T, TV> 
       TV fvals[4];
 #pragma unroll
       for (int j = 0; j < 4; j++)
-        fvals[j] = (((code >> j) & 1u) && fid[j] >= 0) ? a.fv[((int64_t)fid[j] * a.DB + dl) * a.GS + gg] : a.bc;
+        fvals[j] = (((code >> j) & 1u) && fid[j] >= 0) ? a.fv[((int64_t)dl * a.NF + fid[j]) * a.GS + gg] : a.bc;
       for (int o = 0; o < nout; o++) {
         const int j = (jo >> (2 * o)) & 3;
         TV I0[3], e[3];
@@ -396,55 +397,58 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_level(SweepArgs<T, TV> 
         TV Icur = e[0] * (I0[0] - rhs) + rhs;
         Icur += (e[1] * (I0[1] - rhs) + rhs);
         Icur += (e[2] * (I0[2] - rhs) + rhs);
-        a.fv[(slot_of(fid[j]) * a.DB + dl) * a.GS + gg] = Icur * (TV)0.3333333333333333;
+        a.fv[((int64_t)dl * a.NF + slot_of(fid[j])) * a.GS + gg] = Icur * (TV)0.3333333333333333;
       }
     }
   }
 }
 
 // Cell values of one direction batch from its face values: ReCalcIllumOpt
-// (illum_utils.cpp:377-433), the area-weighted face mean, a plain mean for the
-// caller's last cell.  Faces nobody wrote for a direction (inflow boundary,
-// parallel to it) hold the boundary value.  One thread per (cell, direction);
-// consecutive threads take consecutive directions of a cell, so face-value reads
-// and intensity writes are contiguous.
+// (illum_utils.cpp:377-433), the area-weighted face mean, a plain mean for the caller's
+// last cell.  Faces nobody wrote for a direction (inflow boundary, parallel to it) hold
+// the boundary value.  A CTA takes 32 cells (lane = cell) x 32 directions of the batch (four
+// per warp): the face values of one direction are stored direction-major, so a warp's reads
+// of 32 neighbouring cells' face slots fall close together (a face shared by two of them is
+// read from L1 the second time), and each cell's record is read once per CTA.  The cell
+// values go through a shared-memory tile [direction][cell + 1 pad] and each warp writes four
+// cells' rows, lane = direction, so the stores of a cell's 32 directions are contiguous.
+constexpr int kRcCells = 32, kRcDirs = 32;
 template <class T, class TV, class TI, int GT>
 __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T, TV> a, int64_t N) {
-  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= N * a.nbd) return;
-  const int64_t c = t / a.nbd;
-  const int dl = (int)(t - c * a.nbd);
-  const int d = a.d0 + dl;
-  T g[16];
-  int fid[4];
-  load_rec<T>(a.rec + (int64_t)a.RW * c, g, fid);
-  T cosf[4];
-  face_cos(g, a.w[3 * d], a.w[3 * d + 1], a.w[3 * d + 2], cosf);
-  TV A[4];
+  constexpr int GQ = GT > 0 ? GT : 1;
+  __shared__ __align__(16) TI tile[kRcDirs][kRcCells + 1][GQ];
+  // the tile's cells: outward normals, face areas and face-value slots, read once per CTA
+  __shared__ T s_n[kRcCells][12];
+  __shared__ T s_area[kRcCells][4];
+  __shared__ int s_fid[kRcCells][4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t c = (int64_t)blockIdx.x * kRcCells + lane;
+  const int dl0 = (int)blockIdx.y * kRcDirs;
+  const bool cell_ok = c < N;
+  if (warp == 0 && cell_ok) {
+    T g[16];
+    int f[4];
+    load_rec<T>(a.rec + (int64_t)a.RW * c, g, f);
 #pragma unroll
-  for (int j = 0; j < 4; j++) A[j] = (TV)__ldg(a.area + 4 * c + j);
+    for (int q = 0; q < 12; q++) s_n[lane][q] = g[q];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      s_area[lane][j] = __ldg(a.area + 4 * c + j);
+      s_fid[lane][j] = f[j];
+    }
+  }
+  __syncthreads();
   const SweepIO io = *a.io;
   TI *I = (TI *)io.I;
-  int64_t base, gs;
-  if (io.layout) {
-    base = (c * a.M + d) * a.G;
-    gs = 1;
-  } else {
-    base = (int64_t)io.row_of[c] * a.G * a.M + d;
-    gs = a.M;
-  }
   const bool last = c == a.last;
-  bool have[4];
-#pragma unroll
-  for (int j = 0; j < 4; j++) have[j] = cosf[j] > 0 || (cosf[j] < 0 && fid[j] >= 0);
   auto cell_value = [&](const TV *fv) {
     TV curI = 0;
     if (!last) {
       TV Ssum = 0;
 #pragma unroll
       for (int j = 0; j < 4; j++) {
-        curI += fv[j] * A[j];
-        Ssum += A[j];
+        curI += fv[j] * (TV)s_area[lane][j];
+        Ssum += (TV)s_area[lane][j];
       }
       curI /= Ssum;
     } else {
@@ -454,47 +458,87 @@ __global__ void __launch_bounds__(256) k_recalc(SweepArgs<T, TV> a, int64_t N) {
     }
     return curI;
   };
-  if constexpr (GT > 0) {
-    // all four face slots in flight at once, vector loads and a vector store
-    TV f0[GT], f1[GT], f2[GT], f3[GT];
-    auto slot = [&](int j, TV (&fj)[GT]) {
-      if (have[j]) {
-        ld_groups<TV, GT>(a.fv + (slot_of(fid[j]) * a.DB + dl) * a.GS, fj);
-      } else {
+#pragma unroll 1
+  for (int k = 0; k < kRcDirs / 8; k++) {
+    const int dd = warp * (kRcDirs / 8) + k;  // direction within the tile
+    const int dl = dl0 + dd;
+    if (!cell_ok || dl >= a.nbd) continue;
+    const int d = a.d0 + dl;
+    T cosf[4];
+    face_cos(s_n[lane], a.w[3 * d], a.w[3 * d + 1], a.w[3 * d + 2], cosf);
+    int fid[4];
+    bool have[4];
 #pragma unroll
-        for (int q = 0; q < GT; q++) fj[q] = a.bc;
-      }
-    };
-    slot(0, f0);
-    slot(1, f1);
-    slot(2, f2);
-    slot(3, f3);
-    TI out[GT];  // the cell values as stored (rounded to float in the mixed form)
-#pragma unroll
-    for (int q = 0; q < GT; q++) {
-      const TV fv[4] = {f0[q], f1[q], f2[q], f3[q]};
-      out[q] = (TI)cell_value(fv);
+    for (int j = 0; j < 4; j++) {
+      fid[j] = s_fid[lane][j];
+      have[j] = cosf[j] > 0 || (cosf[j] < 0 && fid[j] >= 0);
     }
-    if (io.layout) {
-      if constexpr (sizeof(TI) == 8 && GT % 2 == 0) {
+    const TV *fvd = a.fv + (int64_t)dl * a.NF * a.GS;
+    if constexpr (GT > 0) {
+      // all four face slots in flight at once, vector loads
+      TV f0[GT], f1[GT], f2[GT], f3[GT];
+      auto slot = [&](int j, TV (&fj)[GT]) {
+        if (have[j]) {
+          ld_groups<TV, GT>(fvd + slot_of(fid[j]) * a.GS, fj);
+        } else {
 #pragma unroll
-        for (int q = 0; q < GT / 2; q++) reinterpret_cast<double2 *>(I + base)[q] = make_double2(out[2 * q], out[2 * q + 1]);
-      } else if constexpr (sizeof(TI) == 4 && GT == 4) {
-        *reinterpret_cast<float4 *>(I + base) = make_float4(out[0], out[1], out[2], out[3]);
-      } else {
+          for (int q = 0; q < GT; q++) fj[q] = a.bc;
+        }
+      };
+      slot(0, f0);
+      slot(1, f1);
+      slot(2, f2);
+      slot(3, f3);
 #pragma unroll
-        for (int q = 0; q < GT; q++) I[base + q] = out[q];
+      for (int q = 0; q < GT; q++) {
+        const TV fv[4] = {f0[q], f1[q], f2[q], f3[q]};
+        tile[dd][lane][q] = (TI)cell_value(fv);  // the cell values as stored (float in the mixed form)
       }
     } else {
+      int64_t base, gs;
+      if (io.layout) {
+        base = (c * a.M + d) * a.G;
+        gs = 1;
+      } else {
+        base = (int64_t)io.row_of[c] * a.G * a.M + d;
+        gs = a.M;
+      }
+      for (int gg = 0; gg < a.G; gg++) {
+        TV fv[4];
 #pragma unroll
-      for (int q = 0; q < GT; q++) I[base + q * gs] = out[q];
+        for (int j = 0; j < 4; j++) fv[j] = have[j] ? fvd[slot_of(fid[j]) * a.GS + gg] : a.bc;
+        I[base + gg * gs] = (TI)cell_value(fv);
+      }
     }
-  } else {
-    for (int gg = 0; gg < a.G; gg++) {
-      TV fv[4];
+  }
+  if constexpr (GT > 0) {
+    __syncthreads();
+    const int dl = dl0 + lane;
+    if (dl < a.nbd) {
+      const int d = a.d0 + dl;
+#pragma unroll 1
+      for (int k = 0; k < kRcCells / 8; k++) {
+        const int cl = warp * (kRcCells / 8) + k;
+        const int64_t cc = (int64_t)blockIdx.x * kRcCells + cl;
+        if (cc >= N) break;
+        const TI *v = tile[lane][cl];
+        if (io.layout) {
+          TI *o = I + (cc * a.M + d) * a.G;
+          if constexpr (sizeof(TI) == 8 && GT % 2 == 0) {
 #pragma unroll
-      for (int j = 0; j < 4; j++) fv[j] = have[j] ? a.fv[(slot_of(fid[j]) * a.DB + dl) * a.GS + gg] : a.bc;
-      I[base + gg * gs] = (TI)cell_value(fv);
+            for (int q = 0; q < GT / 2; q++) reinterpret_cast<double2 *>(o)[q] = make_double2(v[2 * q], v[2 * q + 1]);
+          } else if constexpr (sizeof(TI) == 4 && GT == 4) {
+            *reinterpret_cast<float4 *>(o) = make_float4(v[0], v[1], v[2], v[3]);
+          } else {
+#pragma unroll
+            for (int q = 0; q < GT; q++) o[q] = v[q];
+          }
+        } else {
+          const int64_t base = (int64_t)io.row_of[cc] * a.G * a.M + d;
+#pragma unroll
+          for (int q = 0; q < GT; q++) I[base + (int64_t)q * a.M] = v[q];
+        }
+      }
     }
   }
 }
@@ -517,7 +561,7 @@ __global__ void k_plan_init(int64_t N, int nbd, int shift, int d0, const T *w, c
 #pragma unroll
   for (int j = 0; j < 4; j++) cnt += (cosf[j] < 0 && nbr[j] >= 0) ? 1u : 0u;
   indeg[i] = cnt;
-  if (cnt == 0) plan[atomicAdd(tail, 1ull)] = ((uint32_t)c << shift) | (uint32_t)dl;
+  if (cnt == 0) plan[atomicAdd(tail, 1ull)] = ((uint32_t)dl << shift) | (uint32_t)c;
 }
 
 template <class T>
@@ -526,8 +570,8 @@ __global__ void k_plan_expand(const uint32_t *cur, int64_t n, int nbd, int shift
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t it = cur[i];
-  const int64_t c = it >> shift;
-  const int dl = (int)(it & ((1u << shift) - 1));
+  const int64_t c = it & ((1u << shift) - 1u);
+  const int dl = (int)(it >> shift);
   const int d = d0 + dl;
   T g[12];
   int nbr[4];
@@ -538,7 +582,7 @@ __global__ void k_plan_expand(const uint32_t *cur, int64_t n, int nbd, int shift
   for (int j = 0; j < 4; j++) {
     if (!(cosf[j] > 0) || nbr[j] < 0) continue;
     const int64_t q = (int64_t)nbr[j] * nbd + dl;
-    if (atomicSub(indeg + q, 1u) == 1u) plan[atomicAdd(tail, 1ull)] = ((uint32_t)nbr[j] << shift) | (uint32_t)dl;
+    if (atomicSub(indeg + q, 1u) == 1u) plan[atomicAdd(tail, 1ull)] = ((uint32_t)dl << shift) | (uint32_t)nbr[j];
   }
 }
 
@@ -559,8 +603,8 @@ __global__ void k_plan_geometry(const uint32_t *items, int64_t n, int shift, int
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t it = items[i];
-  const int64_t c = it >> shift;
-  const int d = d0 + (int)(it & (uint32_t)(DB - 1));
+  const int64_t c = it & ((1u << shift) - 1u);
+  const int d = d0 + (int)(it >> shift);
   T g[16];
   int fid[4];
   load_rec<T>(rec + (int64_t)RW * c, g, fid);
@@ -770,8 +814,9 @@ rrhd_status build_plan(rrhd_ctx *c) {
     cleanup();
     return rrhd_fail(RRHD_ERR_OOM, "sweep plan allocation failed");
   }
-  int end_bit = R.shift;
-  while ((int64_t(1) << (end_bit - R.shift)) < N) end_bit++;
+  int db_bits = 0;
+  while ((1 << db_bits) < R.DB) db_bits++;
+  const int end_bit = R.shift + db_bits;
   cub::DeviceRadixSort::SortKeys(nullptr, sort_bytes, (const uint32_t *)nullptr, (uint32_t *)nullptr, bmax, 0,
                                  end_bit, st);
   if (cudaMalloc(&sort_tmp, sort_bytes) != cudaSuccess) {
@@ -800,8 +845,9 @@ rrhd_status build_plan(rrhd_ctx *c) {
       RRHD_CUDA(cudaStreamSynchronize(st));
       const int64_t hi = (int64_t)hi_u;
       if (hi == lo) break;
-      // items of a level in ascending (cell, direction) order: deterministic
-      // launches and neighbouring cells' rows close together
+      // items of a level in ascending (direction, cell) order: deterministic launches,
+      // and the items of one direction in cell order, so that neighbouring cells' face
+      // slots (direction-major) and records are read close together
       cub::DeviceRadixSort::SortKeys(sort_tmp, sort_bytes, plan + lo, tmp, hi - lo, 0, end_bit, st);
       RRHD_CUDA(cudaMemcpyAsync(plan + lo, tmp, sizeof(uint32_t) * (hi - lo), cudaMemcpyDeviceToDevice, st));
       off.push_back(hi);
@@ -869,6 +915,7 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
     a.rec = (const T *)R.d_rec;
     a.area = (const T *)R.d_area;
     a.fv = (TV *)R.d_fv;
+    a.NF = c->F;
     a.geo = nullptr;
     a.bc = (TV)R.bc;
     a.last = R.last_cell;
@@ -894,7 +941,7 @@ rrhd_status capture_sweep(rrhd_ctx *c) {
         }
         if (le != cudaSuccess && launch_err == cudaSuccess) launch_err = le;
       }
-      const unsigned nr = grid_for(c->N * nbd, 256);
+      const dim3 nr((unsigned)((c->N + kRcCells - 1) / kRcCells), (unsigned)((nbd + kRcDirs - 1) / kRcDirs));
       switch (R.G) {
         case 1: k_recalc<T, TV, TI, 1><<<nr, 256, 0, cs>>>(a, c->N); break;
         case 2: k_recalc<T, TV, TI, 2><<<nr, 256, 0, cs>>>(a, c->N); break;
@@ -1031,10 +1078,11 @@ extern "C" rrhd_status rrhd_rad_setup(rrhd_ctx *c, const rrhd_dirs *dirs, const 
     while (DB < std::min(R.M, 64)) DB <<= 1;
   }
   R.DB = DB;
-  R.shift = 0;
-  while ((1 << R.shift) < DB) R.shift++;
-  if ((c->N << R.shift) > (int64_t)UINT32_MAX)
-    return rrhd_fail(RRHD_ERR_LIMIT, "sweep items are 32-bit: cells x dirs_per_batch must stay below 2^32");
+  R.shift = 0;  // item = direction << shift | cell
+  while ((int64_t(1) << R.shift) < c->N) R.shift++;
+  if (R.shift > 31 || ((int64_t)DB << R.shift) > (int64_t)UINT32_MAX + 1)
+    return rrhd_fail(RRHD_ERR_LIMIT, "sweep items are 32-bit: dirs_per_batch x 2^ceil(log2 cells) must stay "
+                                     "within 2^32");
   R.nbatch = (R.M + DB - 1) / DB;
   R.prec = o->precision;
   R.bc = o->boundary_value;
@@ -1076,8 +1124,8 @@ extern "C" rrhd_status rrhd_rad_plan_levels(const rrhd_ctx *c, int32_t *levels) 
     for (size_t L = 0; L + 1 < off.size(); L++)
       for (int64_t k = off[L]; k < off[L + 1]; k++) {
         const uint32_t it = plan[(size_t)(base + k)];
-        const int64_t cc = it >> R.shift;
-        const int d = d0 + (int)(it & (uint32_t)(R.DB - 1));
+        const int64_t cc = it & ((1u << R.shift) - 1u);
+        const int d = d0 + (int)(it >> R.shift);
         levels[(int64_t)d * N + c->h_perm[cc]] = (int32_t)L;
       }
     base += N * nbd;
